@@ -1,0 +1,314 @@
+"""Throughput benchmark of the B200 RNS-CKKS hot path.
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--workload ntt] [--impl reference]
+
+Workload "ntt": batched forward + inverse negacyclic NTT at N=2^16 over 32
+limbs of 50-bit primes q = 1 mod 2N (the reference's prime search), 64
+polynomials per launch, residues uniform in [0, q). One step = one forward and
+one inverse transform of the whole batch. Metric: limb-polynomial transforms
+per second (forward and inverse each count once).
+
+One JSON line on rank 0. Under torchrun each rank runs an independent replica
+(the path shards into independent polynomials/ciphertexts; no collective on
+the data path): value = units of all ranks / max-over-ranks time.
+`--impl reference` times the CPU restatement of the reference algorithm
+(oracle/, the reference itself is Rust and cannot be built here) on the host
+cores with every thread, on the same workload and metric.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "ccmm-rs_b200"))
+
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def peaks():
+    try:
+        with open(PEAKS_PATH) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ------------------------------------------------------------ clocks sampler
+class Clocks:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.QUERY,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# --------------------------------------------------------------- distributed
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, value):
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ------------------------------------------------------------------- NTT
+NTT_LOG_N, NTT_LIMBS, NTT_POLYS, NTT_BITS = 16, 32, 64, 50
+
+
+def ntt_primes():
+    # the reference's prime search: descending from 2^50-1 in steps of 2N
+    # (security/p6a/generate_candidates.py:53-73)
+    sys.path.insert(0, os.path.join(ROOT, "ccmm-rs_b200"))
+    import ckks_b200.params as params
+    return params.primes_below_bits(NTT_BITS, 1 << NTT_LOG_N, NTT_LIMBS)
+
+
+def ntt_config():
+    return {"workload": "batched NTT+iNTT, N=2^16, 32 x 50-bit limbs, 64 polys/launch",
+            "log_n": NTT_LOG_N, "limbs": NTT_LIMBS, "polys_per_launch": NTT_POLYS,
+            "l2": "inputs (1.07 GB) larger than L2", "parallelism": "replicas"}
+
+
+def bench_ntt_gpu(args, world, rank, local):
+    import torch
+    import ckks_b200 as cb
+    dev = torch.device("cuda", local)
+    n = 1 << NTT_LOG_N
+    primes = ntt_primes()
+    ctx = cb.Context(NTT_LOG_N, primes)
+    rng = np.random.default_rng(1234 + rank)
+    host = np.stack([rng.integers(0, q, (NTT_POLYS, n), dtype=np.uint64) for q in primes], axis=1)
+    data = cb.as_u64_tensor(host, dev)
+    tmp = torch.empty_like(data)
+    st = torch.cuda.current_stream()
+
+    def step():
+        ctx.ntt_forward(data, out=tmp)
+        ctx.ntt_inverse(tmp, out=data)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    # per-kernel timing of one forward transform (both passes) for the roofline
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    fwd_ms = []
+    for _ in range(3):
+        ev[0].record(st)
+        ctx.ntt_forward(data, out=tmp)
+        ev[1].record(st)
+        torch.cuda.synchronize()
+        fwd_ms.append(ev[0].elapsed_time(ev[1]))
+        ctx.ntt_inverse(tmp, out=data)
+    torch.cuda.synchronize()
+
+    clocks = Clocks(local)
+    clocks.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(st)
+    for _ in range(args.steps):
+        step()
+    t1.record(st)
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = t0.elapsed_time(t1)
+    clk = clocks.stop()
+    ms_max = max_over_ranks(world, ms)
+    units = 2 * NTT_POLYS * NTT_LIMBS * args.steps * world
+    value = units / (ms_max / 1000.0)
+
+    # roofline: forward NTT = 16 N bytes per limb-poly (read + write)
+    alg_bytes = 16 * n * NTT_POLYS * NTT_LIMBS
+    fwd = float(np.median(fwd_ms))
+    peak, kind = peaks()
+    achieved = alg_bytes / (fwd / 1000.0) / 1e9
+
+    # end to end through the C ABI host-buffer call (pinned host memory)
+    pinned_in = torch.from_numpy(host.view(np.int64)).pin_memory()
+    pinned_out = torch.empty_like(pinned_in).pin_memory()
+    hin = pinned_in.numpy().view(np.uint64)
+    hout = pinned_out.numpy().view(np.uint64)
+    import ctypes
+    lib = cb.lib()
+    e2e_steps = max(1, min(args.steps, 5))
+    ctx.ntt_forward_host(hin)  # warm
+    barrier(world)
+    t = time.perf_counter()
+    for _ in range(e2e_steps):
+        rc = lib.ckks_ntt_forward_host(ctx.handle, hin.ctypes.data_as(cb.u64p), hout.ctypes.data_as(cb.u64p),
+                                       NTT_POLYS, 0, NTT_LIMBS)
+        cb.check(rc)
+    e2e_s = max_over_ranks(world, (time.perf_counter() - t))
+    e2e_value = NTT_POLYS * NTT_LIMBS * e2e_steps * world / e2e_s
+
+    line = {
+        "metric": "limb-polynomial NTT transforms/s (N=2^16, 50-bit limbs)", "value": value,
+        "unit": "limb-NTT/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u64", "data": "synthetic (seeded uniform residues)", "config": ntt_config(),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_kind": kind,
+                     "kernel": "forward NTT (pass1+pass2), %d limb-polys/launch" % (NTT_POLYS * NTT_LIMBS),
+                     "kernel_ms": fwd},
+        "e2e": {"value": e2e_value, "unit": "limb-NTT/s", "h2d_bytes_per_step": int(host.nbytes),
+                "d2h_bytes_per_step": int(host.nbytes), "path": "ckks_ntt_forward_host"},
+        "gpu_launches": 4 * args.steps, "clocks": clk,
+    }
+    return line
+
+
+def ntt_cpu_sample(threads, seconds_target=10.0):
+    """Times the oracle NTT (restated reference radix-2 Shoup NTT) on host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import Oracle, P, arr
+    import concurrent.futures as cf
+    o = Oracle()
+    n = 1 << NTT_LOG_N
+    primes = ntt_primes()
+    rng = np.random.default_rng(99)
+    per_thread = np.stack([rng.integers(0, q, n, dtype=np.uint64) for q in primes])  # 32 limbs
+    moduli = arr(primes)
+    bufs = [per_thread.copy() for _ in range(threads)]
+
+    def work(b):
+        o.L.oracle_ntt_forward(P(moduli), NTT_LIMBS, n, P(b), 1)
+        o.L.oracle_ntt_inverse(P(moduli), NTT_LIMBS, n, P(b), 1)
+
+    work(bufs[0])
+    t = time.perf_counter()
+    rounds = 0
+    with cf.ThreadPoolExecutor(threads) as ex:
+        while time.perf_counter() - t < seconds_target:
+            list(ex.map(work, bufs))
+            rounds += 1
+    dt = time.perf_counter() - t
+    units = rounds * threads * 2 * NTT_LIMBS
+    return units / dt, "%d rounds x %d threads x 32 limbs x (fwd+inv) at N=2^16" % (rounds, threads)
+
+
+def reference_arm(args, world, rank):
+    if rank != 0:
+        return None
+    threads = os.cpu_count() or 1
+    per_step = []
+    sample = None
+    for i in range(args.warmup + args.steps):
+        v, sample = ntt_cpu_sample(threads, seconds_target=max(2.0, 20.0 / max(1, args.steps + args.warmup)))
+        if i >= args.warmup:
+            per_step.append(v)
+    value = float(np.median(per_step))
+    return {
+        "metric": "limb-polynomial NTT transforms/s (N=2^16, 50-bit limbs)", "value": value,
+        "unit": "limb-NTT/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * 2 * NTT_POLYS * NTT_LIMBS / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded uniform residues)",
+        "config": ntt_config(), "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "limb-NTT/s", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "limb-NTT/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="ntt", choices=["ntt"])
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    world, rank, local = dist_setup() if args.impl == "b200" else (
+        int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0)
+    if args.impl == "reference":
+        line = reference_arm(args, world, rank)
+        if line:
+            print(json.dumps(line), flush=True)
+        return
+    line = bench_ntt_gpu(args, world, rank, local)
+    if rank == 0:
+        threads = os.cpu_count() or 1
+        v, sample = ntt_cpu_sample(threads, seconds_target=10.0)
+        line["cpu_baseline"] = {"value": v, "unit": "limb-NTT/s", "cores": threads, "kind": "port",
+                                "sample": sample}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

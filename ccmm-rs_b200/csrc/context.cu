@@ -1,0 +1,278 @@
+// context.cu -- context creation (moduli validation, psi search, NTT table
+// construction and upload), scratch management and error reporting.
+#include <cstring>
+#include <thread>
+
+#include "context.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+typedef unsigned __int128 u128;
+
+u64 mulmod(u64 a, u64 b, u64 q) { return (u64)((u128)a * b % q); }
+u64 powmod(u64 b, u64 e, u64 q) {
+    u64 r = 1 % q;
+    b %= q;
+    while (e) {
+        if (e & 1) r = mulmod(r, b, q);
+        b = mulmod(b, b, q);
+        e >>= 1;
+    }
+    return r;
+}
+u64 invmod(u64 a, u64 q) { return powmod(a, q - 2, q); }
+
+// Deterministic Miller-Rabin for u64 (witness set of ring/ntt_prime.rs:28).
+bool is_prime(u64 n) {
+    static const u64 small[] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37};
+    static const u64 wit[] = {2, 325, 9375, 28178, 450775, 9780504, 1795265022};
+    if (n < 2) return false;
+    for (u64 p : small) {
+        if (n == p) return true;
+        if (n % p == 0) return false;
+    }
+    u64 d = n - 1;
+    int s = 0;
+    while (!(d & 1)) { d >>= 1; ++s; }
+    for (u64 a : wit) {
+        a %= n;
+        if (!a) continue;
+        u64 x = powmod(a, d, n);
+        if (x == 1 || x == n - 1) continue;
+        bool comp = true;
+        for (int i = 1; i < s; ++i) {
+            x = mulmod(x, x, n);
+            if (x == n - 1) { comp = false; break; }
+            if (x == 1) return false;
+        }
+        if (comp) return false;
+    }
+    return true;
+}
+
+// Smallest generator candidate g >= 2 with psi = g^((q-1)/2N), psi^N = -1
+// (the reference's find_negacyclic_root, ring/ntt_params.rs:16-50).
+u64 find_root(u64 q, u32 n) {
+    u64 e = (q - 1) / (2ull * n);
+    for (u64 g = 2; g < q; ++g) {
+        u64 psi = powmod(g, e, q);
+        if (powmod(psi, n, q) == q - 1) return psi;
+    }
+    return 0;
+}
+
+u32 brev(u32 x, int bits) {
+    u32 r = 0;
+    for (int i = 0; i < bits; ++i) { r = (r << 1) | (x & 1); x >>= 1; }
+    return r;
+}
+
+// Host tables of one modulus, in the order of the device layout.
+struct HostTables {
+    std::vector<u64> psi_rev, psi_inv_rev, w, w_inv, mid, imid;
+};
+
+void build_tables(u64 q, u64 psi, u32 log_n1, u32 log_n2, HostTables& t) {
+    const u32 N1 = 1u << log_n1, N2 = 1u << log_n2, N = N1 * N2;
+    u64 psi_inv = invmod(psi, q), n_inv = invmod(N % q, q);
+    u64 psi2 = powmod(psi, N1, q), psi2_inv = invmod(psi2, q);
+    u64 w1 = powmod(psi, 2ull * N2, q), w1_inv = invmod(w1, q);
+    t.psi_rev.resize(N2);
+    t.psi_inv_rev.resize(N2);
+    for (u32 i = 0; i < N2; ++i) {
+        t.psi_rev[i] = powmod(psi2, brev(i, log_n2), q);
+        t.psi_inv_rev[i] = powmod(psi2_inv, brev(i, log_n2), q);
+    }
+    t.w.resize(N1 / 2);
+    t.w_inv.resize(N1 / 2);
+    u64 a = 1, b = 1;
+    for (u32 i = 0; i < N1 / 2; ++i) {
+        t.w[i] = a;
+        t.w_inv[i] = b;
+        a = mulmod(a, w1, q);
+        b = mulmod(b, w1_inv, q);
+    }
+    t.mid.resize(N);
+    t.imid.resize(N);
+    for (u32 j1 = 0; j1 < N1; ++j1) {  // psi^((2k2+1) j1)
+        u64 v = powmod(psi, j1, q), step = mulmod(v, v, q);
+        for (u32 k2 = 0; k2 < N2; ++k2) {
+            t.mid[(size_t)j1 * N2 + k2] = v;
+            v = mulmod(v, step, q);
+        }
+    }
+    for (u32 k2 = 0; k2 < N2; ++k2) {  // N^-1 psi^-((2k2+1) j1)
+        u64 base = powmod(psi_inv, 2ull * k2 + 1, q), v = n_inv;
+        for (u32 j1 = 0; j1 < N1; ++j1) {
+            t.imid[(size_t)k2 * N1 + j1] = v;
+            v = mulmod(v, base, q);
+        }
+    }
+}
+
+}  // namespace
+
+void ckks_set_error(const std::string& msg) { g_last_error = msg; }
+
+void ntt_set_smem_limits();
+
+int32_t ctx_scratch(ckks_ctx* ctx, size_t words, u64** out) {
+    std::lock_guard<std::mutex> lock(ctx->scratch_mutex);
+    if (ctx->scratch_words < words) {
+        if (ctx->scratch) cudaFree(ctx->scratch);
+        ctx->scratch = nullptr;
+        ctx->scratch_words = 0;
+        if (cudaMalloc(&ctx->scratch, words * sizeof(u64)) != cudaSuccess) {
+            cudaGetLastError();
+            ckks_set_error("out of device memory for NTT scratch");
+            return CKKS_ERR_OOM;
+        }
+        ctx->scratch_words = words;
+    }
+    *out = ctx->scratch;
+    return CKKS_OK;
+}
+
+extern "C" {
+
+const char* ckks_last_error_string(void) { return g_last_error.c_str(); }
+const char* ckks_version(void) { return "ckks_b200 0.1 (sm_100a)"; }
+
+int32_t ckks_ctx_create(uint32_t log_n, const uint64_t* q, uint32_t L, const uint64_t* p, uint32_t K,
+                        ckks_ctx** out) {
+    CKKS_CHECK_ARG(out != nullptr, "ckks_ctx_create: out is null");
+    *out = nullptr;
+    CKKS_CHECK_ARG(log_n >= 2 && log_n <= 17, "ckks_ctx_create: log_n must be in [2, 17]");
+    CKKS_CHECK_ARG(L >= 1 && (q != nullptr), "ckks_ctx_create: need at least one Q limb");
+    CKKS_CHECK_ARG(K == 0 || p != nullptr, "ckks_ctx_create: p is null");
+    CKKS_CHECK_ARG(L + K <= 64, "ckks_ctx_create: at most 64 limbs");
+    const u32 n = 1u << log_n;
+    std::vector<u64> mod(q, q + L);
+    if (K) mod.insert(mod.end(), p, p + K);
+    for (size_t i = 0; i < mod.size(); ++i) {
+        u64 m = mod[i];
+        if (m >= (1ull << 62) || m < 3 || !(m & 1) || (m - 1) % (2ull * n) != 0 || !is_prime(m)) {
+            ckks_set_error("ckks_ctx_create: modulus " + std::to_string(m) +
+                           " must be an odd prime below 2^62 with q = 1 mod 2N");
+            return CKKS_ERR_BAD_ARG;
+        }
+        for (size_t j = 0; j < i; ++j)
+            if (mod[j] == m) {
+                ckks_set_error("ckks_ctx_create: moduli must be pairwise distinct");
+                return CKKS_ERR_BAD_ARG;
+            }
+    }
+    auto* ctx = new ckks_ctx();
+    ctx->log_n = log_n;
+    ctx->n = n;
+    ctx->log_n2 = log_n / 2;
+    ctx->log_n1 = log_n - ctx->log_n2;
+    ctx->L = L;
+    ctx->K = K;
+    ctx->moduli = mod;
+    cudaGetDevice(&ctx->device);
+    const size_t M = mod.size();
+    ctx->psi.resize(M);
+    std::vector<HostTables> ht(M);
+    {
+        std::vector<std::thread> th;
+        for (size_t i = 0; i < M; ++i)
+            th.emplace_back([&, i]() {
+                ctx->psi[i] = find_root(mod[i], n);
+                build_tables(mod[i], ctx->psi[i], ctx->log_n1, ctx->log_n2, ht[i]);
+            });
+        for (auto& t : th) t.join();
+    }
+    const u32 N1 = 1u << ctx->log_n1, N2 = 1u << ctx->log_n2;
+    // per modulus: 2*(N2 + N2 + N1/2 + N1/2 + N + N) words (value + Shoup)
+    const size_t per = 2 * (2 * (size_t)N2 + N1 + 2 * (size_t)n);
+    std::vector<u64> host(per * M);
+    ctx->h_tabs.resize(M);
+    if (cudaMalloc(&ctx->d_table_mem, host.size() * sizeof(u64)) != cudaSuccess ||
+        cudaMalloc(&ctx->d_tabs, M * sizeof(NttTab)) != cudaSuccess) {
+        cudaGetLastError();
+        ckks_ctx_destroy(ctx);
+        ckks_set_error("ckks_ctx_create: out of device memory for NTT tables");
+        return CKKS_ERR_OOM;
+    }
+    for (size_t i = 0; i < M; ++i) {
+        u64 m = mod[i];
+        size_t off = per * i;
+        NttTab& T = ctx->h_tabs[i];
+        T.q = m;
+        barrett_host(m, &T.mu_hi, &T.mu_lo);
+        auto put = [&](const std::vector<u64>& v, const u64** val, const u64** quo) {
+            for (size_t k = 0; k < v.size(); ++k) {
+                host[off + k] = v[k];
+                host[off + v.size() + k] = shoup_quotient_host(v[k], m);
+            }
+            *val = ctx->d_table_mem + off;
+            *quo = ctx->d_table_mem + off + v.size();
+            off += 2 * v.size();
+        };
+        put(ht[i].psi_rev, &T.psi_rev, &T.psi_rev_q);
+        put(ht[i].psi_inv_rev, &T.psi_inv_rev, &T.psi_inv_rev_q);
+        put(ht[i].w, &T.w, &T.w_q);
+        put(ht[i].w_inv, &T.w_inv, &T.w_inv_q);
+        put(ht[i].mid, &T.mid, &T.mid_q);
+        put(ht[i].imid, &T.imid, &T.imid_q);
+    }
+    if (cudaMemcpy(ctx->d_table_mem, host.data(), host.size() * sizeof(u64), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(ctx->d_tabs, ctx->h_tabs.data(), M * sizeof(NttTab), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        std::string e = cudaGetErrorString(cudaGetLastError());
+        ckks_ctx_destroy(ctx);
+        ckks_set_error("ckks_ctx_create: " + e);
+        return CKKS_ERR_CUDA;
+    }
+    ntt_set_smem_limits();
+    *out = ctx;
+    return CKKS_OK;
+}
+
+uint64_t ckks_find_negacyclic_root(uint64_t q, uint32_t degree) {
+    if (degree < 2 || (degree & (degree - 1)) || q < 3 || (q - 1) % (2ull * degree) != 0) return 0;
+    return find_root(q, degree);
+}
+
+int32_t ckks_is_prime(uint64_t value) { return is_prime(value) ? 1 : 0; }
+
+int32_t ckks_primes_below_bits(uint32_t bits, uint32_t degree, uint32_t count, uint64_t* out) {
+    CKKS_CHECK_ARG(out != nullptr, "ckks_primes_below_bits: out is null");
+    CKKS_CHECK_ARG(bits >= 2 && bits <= 62 && degree >= 2 && !(degree & (degree - 1)),
+                   "ckks_primes_below_bits: bits must be in [2, 62] and degree a power of two");
+    u64 two_n = 2ull * degree;
+    u64 cand = (1ull << bits) - 1;
+    cand -= (cand - 1) % two_n;
+    uint32_t found = 0;
+    while (cand > two_n + 1 && found < count) {
+        if (is_prime(cand)) out[found++] = cand;
+        cand -= two_n;
+    }
+    if (found != count) {
+        ckks_set_error("ckks_primes_below_bits: not enough NTT-friendly primes below 2^bits");
+        return CKKS_ERR_BAD_ARG;
+    }
+    return CKKS_OK;
+}
+
+int32_t ckks_ctx_destroy(ckks_ctx* ctx) {
+    if (!ctx) return CKKS_OK;
+    if (ctx->own_stream) cudaStreamSynchronize(ctx->own_stream);
+    if (ctx->scratch) cudaFree(ctx->scratch);
+    if (ctx->d_tabs) cudaFree(ctx->d_tabs);
+    if (ctx->d_table_mem) cudaFree(ctx->d_table_mem);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return CKKS_OK;
+}
+
+int32_t ckks_ctx_psi(const ckks_ctx* ctx, uint64_t* psi_host) {
+    CKKS_CHECK_ARG(ctx && psi_host, "ckks_ctx_psi: null argument");
+    std::memcpy(psi_host, ctx->psi.data(), ctx->psi.size() * sizeof(u64));
+    return CKKS_OK;
+}
+
+}  // extern "C"
