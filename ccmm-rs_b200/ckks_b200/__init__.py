@@ -21,6 +21,8 @@ HEADER = os.path.join(ROOT, "include", "ckks_b200.h")
 
 U32, U64, I32, VP = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int32, ctypes.c_void_p
 u64p = ctypes.POINTER(ctypes.c_uint64)
+u32p = ctypes.POINTER(ctypes.c_uint32)
+i8p = ctypes.POINTER(ctypes.c_int8)
 
 _SIGS = {
     "ckks_last_error_string": (ctypes.c_char_p, []),
@@ -35,6 +37,29 @@ _SIGS = {
     "ckks_ntt_inverse": (I32, [VP, VP, VP, U32, U32, U32, VP]),
     "ckks_ntt_forward_host": (I32, [VP, u64p, u64p, U32, U32, U32]),
     "ckks_ntt_inverse_host": (I32, [VP, u64p, u64p, U32, U32, U32]),
+    "ckks_automorphism_coef": (I32, [VP, VP, VP, U32, U32, U32, U64, VP]),
+    "ckks_automorphism_ntt": (I32, [VP, VP, VP, U32, U32, U32, U64, VP]),
+    "ckks_rotation_exponent_left": (U64, [U32, U64]),
+    "ckks_rotation_exponent_right": (U64, [U32, U64]),
+    "ckks_conjugation_exponent": (U64, [U32]),
+    "ckks_pointwise": (I32, [VP, VP, VP, VP, U32, U32, U32, I32, VP]),
+    "ckks_rescale": (I32, [VP, VP, VP, U32, U32, VP]),
+    "ckks_mod_down": (I32, [VP, VP, VP, U32, U32, VP]),
+    "ckks_bounded_digit_count": (I32, [VP, U32, U32, ctypes.POINTER(U32)]),
+    "ckks_bounded_decompose": (I32, [VP, VP, U32, U32, U32, VP, VP]),
+    "ckks_bounded_digits_automorphism": (I32, [VP, VP, VP, U32, U32, U32, U64, VP]),
+    "ckks_hybrid_key_generate": (I32, [VP, U32, U32, U64, i8p, U64, ctypes.c_double, ctypes.POINTER(VP)]),
+    "ckks_hybrid_key_upload": (I32, [VP, U32, U32, U64, u64p, ctypes.POINTER(VP)]),
+    "ckks_rnsblock_key_generate": (I32, [VP, U32, u32p, U32, U64, i8p, U64, ctypes.c_double, ctypes.POINTER(VP)]),
+    "ckks_rnsblock_key_upload": (I32, [VP, U32, u32p, U32, U64, u64p, ctypes.POINTER(VP)]),
+    "ckks_relin_key_generate": (I32, [VP, U32, U32, i8p, U64, ctypes.c_double, ctypes.POINTER(VP)]),
+    "ckks_relin_key_upload": (I32, [VP, U32, U32, u64p, ctypes.POINTER(VP)]),
+    "ckks_ksk_info": (I32, [VP, ctypes.POINTER(U32), ctypes.POINTER(U64)]),
+    "ckks_ksk_download": (I32, [VP, u64p]),
+    "ckks_ksk_destroy": (I32, [VP]),
+    "ckks_rotate": (I32, [VP, VP, VP, VP, U32, VP]),
+    "ckks_rotate_hoisted": (I32, [VP, ctypes.POINTER(VP), U32, VP, VP, U32, VP]),
+    "ckks_rotate_hoisted_host": (I32, [VP, ctypes.POINTER(VP), U32, u64p, u64p, U32]),
 }
 
 STATUS = {0: "OK", -1: "BAD_ARG", -2: "BASIS_MISMATCH", -3: "EXPONENT_MISMATCH", -4: "OOM", -5: "CUDA",
@@ -172,6 +197,202 @@ class Context:
         check(lib().ckks_ntt_inverse_host(self.handle, ap, out.ctypes.data_as(u64p), a.size // (limbs * self.n),
                                           limb_begin, limbs))
         return out
+
+
+    # ---------------------------------------------------------- ring ops
+    def automorphism_coef(self, data, exponent, limb_begin=0, out=None, stream=None):
+        """ckks/automorphism.rs:8-48 over [n_polys][limbs][N]."""
+        import torch
+        limbs = data.shape[-2]
+        out = torch.empty_like(data) if out is None else out
+        check(lib().ckks_automorphism_coef(self.handle, _dptr(data), _dptr(out), data.numel() // (limbs * self.n),
+                                           limb_begin, limbs, int(exponent), _stream(stream)))
+        return out
+
+    def automorphism_ntt(self, data, exponent, limb_begin=0, out=None, stream=None):
+        """ring/ntt_galois_permutation.rs:5-19 over NTT-domain [n_polys][limbs][N]."""
+        import torch
+        limbs = data.shape[-2]
+        out = torch.empty_like(data) if out is None else out
+        check(lib().ckks_automorphism_ntt(self.handle, _dptr(data), _dptr(out), data.numel() // (limbs * self.n),
+                                          limb_begin, limbs, int(exponent), _stream(stream)))
+        return out
+
+    def pointwise(self, a, b, op, limb_begin=0, out=None, stream=None):
+        import torch
+        limbs = a.shape[-2]
+        out = torch.empty_like(a) if out is None else out
+        check(lib().ckks_pointwise(self.handle, _dptr(a), _dptr(b), _dptr(out), a.numel() // (limbs * self.n),
+                                   limb_begin, limbs, {"mul": 0, "add": 1, "sub": 2}[op], _stream(stream)))
+        return out
+
+    def rescale(self, data, stream=None):
+        """ckks/rns_rescale.rs:107-167: [..., limbs, N] -> [..., limbs-1, N]."""
+        import torch
+        limbs = data.shape[-2]
+        out = torch.empty(data.shape[:-2] + (limbs - 1, self.n), dtype=torch.int64, device=data.device)
+        check(lib().ckks_rescale(self.handle, _dptr(data), _dptr(out), data.numel() // (limbs * self.n), limbs,
+                                 _stream(stream)))
+        return out
+
+    def mod_down(self, data, stream=None):
+        """ring/auxiliary_modulus.rs:89-171: [..., q_limbs+K, N] -> [..., q_limbs, N]."""
+        import torch
+        q_limbs = data.shape[-2] - len(self.p)
+        out = torch.empty(data.shape[:-2] + (q_limbs, self.n), dtype=torch.int64, device=data.device)
+        check(lib().ckks_mod_down(self.handle, _dptr(data), _dptr(out), data.numel() // ((q_limbs + len(self.p)) * self.n),
+                                  q_limbs, _stream(stream)))
+        return out
+
+    def digit_count(self, q_limbs, base_log):
+        d = U32()
+        check(lib().ckks_bounded_digit_count(self.handle, q_limbs, base_log, ctypes.byref(d)))
+        return d.value
+
+    def bounded_decompose(self, poly, base_log, stream=None):
+        """grafting/bounded_gadget.rs:59-118: [..., q_limbs, N] -> int64 digits [..., D, N]."""
+        import torch
+        q_limbs = poly.shape[-2]
+        npoly = poly.numel() // (q_limbs * self.n)
+        D = self.digit_count(q_limbs, base_log)
+        out = torch.empty(poly.shape[:-2] + (D, self.n), dtype=torch.int64, device=poly.device)
+        check(lib().ckks_bounded_decompose(self.handle, _dptr(poly), npoly, q_limbs, base_log, _dptr(out),
+                                           _stream(stream)))
+        return out
+
+    def bounded_digits_automorphism(self, digits, base_log, exponent, stream=None):
+        import torch
+        D = digits.shape[-2]
+        out = torch.empty_like(digits)
+        check(lib().ckks_bounded_digits_automorphism(self.handle, _dptr(digits), _dptr(out),
+                                                     digits.numel() // (D * self.n), D, base_log, int(exponent),
+                                                     _stream(stream)))
+        return out
+
+    def rotation_exponent_left(self, steps):
+        return int(lib().ckks_rotation_exponent_left(self.n, int(steps)))
+
+    def rotation_exponent_right(self, steps):
+        return int(lib().ckks_rotation_exponent_right(self.n, int(steps)))
+
+
+class KeySwitchKey:
+    """A key-switching key resident in HBM (ckks_ksk)."""
+
+    HYBRID_BOUNDED, HYBRID_RNS_BLOCK, RELIN_BOUNDED = 0, 1, 2
+
+    def __init__(self, ctx, handle, kind, q_limbs, exponent=1, base_log=0, blocks=()):
+        self.ctx, self.handle, self.kind = ctx, handle, kind
+        self.q_limbs, self.exponent, self.base_log, self.blocks = q_limbs, exponent, base_log, tuple(blocks)
+
+    @staticmethod
+    def _secret(secret):
+        s = np.ascontiguousarray(np.asarray(secret, dtype=np.int8))
+        return s, s.ctypes.data_as(i8p)
+
+    @classmethod
+    def hybrid_generate(cls, ctx, q_limbs, base_log, exponent, secret, seed, sigma=3.2):
+        """PreparedHybridRnsGaloisKey::generate_with_distribution_ntt_rng (hybrid_rns_galois_key.rs:61-170)."""
+        s, sp = cls._secret(secret)
+        h = ctypes.c_void_p()
+        check(lib().ckks_hybrid_key_generate(ctx.handle, q_limbs, base_log, int(exponent), sp, seed, sigma,
+                                             ctypes.byref(h)))
+        return cls(ctx, h, cls.HYBRID_BOUNDED, q_limbs, exponent, base_log)
+
+    @classmethod
+    def hybrid_upload(cls, ctx, q_limbs, base_log, exponent, entries):
+        e, ep = _u64(entries)
+        h = ctypes.c_void_p()
+        check(lib().ckks_hybrid_key_upload(ctx.handle, q_limbs, base_log, int(exponent), ep, ctypes.byref(h)))
+        return cls(ctx, h, cls.HYBRID_BOUNDED, q_limbs, exponent, base_log)
+
+    @classmethod
+    def rnsblock_generate(cls, ctx, q_limbs, blocks, exponent, secret, seed, sigma=3.2):
+        s, sp = cls._secret(secret)
+        b = np.ascontiguousarray(np.asarray(blocks, np.uint32))
+        h = ctypes.c_void_p()
+        check(lib().ckks_rnsblock_key_generate(ctx.handle, q_limbs, b.ctypes.data_as(u32p), len(b), int(exponent), sp,
+                                               seed, sigma, ctypes.byref(h)))
+        return cls(ctx, h, cls.HYBRID_RNS_BLOCK, q_limbs, exponent, 0, blocks)
+
+    @classmethod
+    def rnsblock_upload(cls, ctx, q_limbs, blocks, exponent, entries):
+        e, ep = _u64(entries)
+        b = np.ascontiguousarray(np.asarray(blocks, np.uint32))
+        h = ctypes.c_void_p()
+        check(lib().ckks_rnsblock_key_upload(ctx.handle, q_limbs, b.ctypes.data_as(u32p), len(b), int(exponent), ep,
+                                             ctypes.byref(h)))
+        return cls(ctx, h, cls.HYBRID_RNS_BLOCK, q_limbs, exponent, 0, blocks)
+
+    @classmethod
+    def relin_generate(cls, ctx, q_limbs, base_log, secret, seed, sigma=3.2):
+        """BoundedRnsMultiplicationKey::generate_with_distribution_ntt_rng (bounded_key_switch.rs:28-104)."""
+        s, sp = cls._secret(secret)
+        h = ctypes.c_void_p()
+        check(lib().ckks_relin_key_generate(ctx.handle, q_limbs, base_log, sp, seed, sigma, ctypes.byref(h)))
+        return cls(ctx, h, cls.RELIN_BOUNDED, q_limbs, 1, base_log)
+
+    @classmethod
+    def relin_upload(cls, ctx, q_limbs, base_log, entries):
+        e, ep = _u64(entries)
+        h = ctypes.c_void_p()
+        check(lib().ckks_relin_key_upload(ctx.handle, q_limbs, base_log, ep, ctypes.byref(h)))
+        return cls(ctx, h, cls.RELIN_BOUNDED, q_limbs, 1, base_log)
+
+    def info(self):
+        d, w = U32(), U64()
+        check(lib().ckks_ksk_info(self.handle, ctypes.byref(d), ctypes.byref(w)))
+        return d.value, w.value
+
+    def download(self):
+        D, words = self.info()
+        out = np.zeros(words, np.uint64)
+        check(lib().ckks_ksk_download(self.handle, out.ctypes.data_as(u64p)))
+        return out
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().ckks_ksk_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def rotate(ctx, key, ct, out=None, stream=None):
+    """Key-switched Galois automorphism of [n_ct][2][q_limbs][N] ciphertexts
+    (apply_hybrid_rns_galois_automorphism_with_prepared_ntt, hybrid_rns_galois_key.rs:293)."""
+    import torch
+    out = torch.empty_like(ct) if out is None else out
+    n_ct = ct.numel() // (2 * key.q_limbs * ctx.n)
+    check(lib().ckks_rotate(ctx.handle, key.handle, _dptr(ct), _dptr(out), n_ct, _stream(stream)))
+    return out
+
+
+def rotate_hoisted(ctx, keys, ct, out=None, stream=None):
+    """Hoisted rotations: out [n_ct][n_keys][2][q_limbs][N]."""
+    import torch
+    q_limbs = keys[0].q_limbs
+    n_ct = ct.numel() // (2 * q_limbs * ctx.n)
+    if out is None:
+        out = torch.empty((n_ct, len(keys), 2, q_limbs, ctx.n), dtype=torch.int64, device=ct.device)
+    arr = (VP * len(keys))(*[k.handle.value for k in keys])
+    check(lib().ckks_rotate_hoisted(ctx.handle, arr, len(keys), _dptr(ct), _dptr(out), n_ct, _stream(stream)))
+    return out
+
+
+def rotate_hoisted_host(ctx, keys, ct_host, out_host=None):
+    a, ap = _u64(ct_host)
+    q_limbs = keys[0].q_limbs
+    n_ct = a.size // (2 * q_limbs * ctx.n)
+    if out_host is None:
+        out_host = np.empty((n_ct, len(keys), 2, q_limbs, ctx.n), np.uint64)
+    arr = (VP * len(keys))(*[k.handle.value for k in keys])
+    check(lib().ckks_rotate_hoisted_host(ctx.handle, arr, len(keys), ap, out_host.ctypes.data_as(u64p), n_ct))
+    return out_host
 
 
 class PreparedRnsNttPlan:

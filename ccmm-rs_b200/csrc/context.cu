@@ -112,28 +112,128 @@ void build_tables(u64 q, u64 psi, u32 log_n1, u32 log_n2, HostTables& t) {
     }
 }
 
+// Rescale, ModDown, P-factor and Q-Garner constants (device copies).
+int32_t build_constants(ckks_ctx* ctx) {
+    const u32 L = ctx->L, K = ctx->K;
+    const std::vector<u64>& m = ctx->moduli;
+    // layout: rescale [L][2][L] | pmodq [2][L] | md.q [L] | pre, pre_q [L][kMaxAux] x2 | p_mod_q [L] |
+    //         pinv_mod_q [L] | pinv_mod_q_q [L] | gq, gq_q [L][L] x2 | ginv, ginv_q [L] x2
+    const size_t n_res = (size_t)L * 2 * L, n_pm = 2 * (size_t)L, n_md = (size_t)L * (4 + 2 * kMaxAux),
+                 n_g = 2 * (size_t)L * L + 2 * (size_t)L;
+    std::vector<u64> h(n_res + n_pm + n_md + n_g, 0);
+    u64* res = h.data();
+    for (u32 d = 1; d < L; ++d)
+        for (u32 i = 0; i < d; ++i) {
+            u64 inv = invmod(m[d] % m[i], m[i]);
+            res[(size_t)d * 2 * L + i] = inv;
+            res[(size_t)d * 2 * L + L + i] = shoup_quotient_host(inv, m[i]);
+        }
+    u64* pm = res + n_res;
+    for (u32 i = 0; i < L; ++i) {
+        u64 pf = 1 % m[i];
+        for (u32 k = 0; k < K; ++k) pf = mulmod(pf, m[L + k] % m[i], m[i]);
+        pm[i] = pf;
+        pm[L + i] = shoup_quotient_host(pf, m[i]);
+    }
+    u64* mdq = pm + n_pm;
+    u64* pre = mdq + L;
+    u64* pre_q = pre + (size_t)L * kMaxAux;
+    u64* pmq = pre_q + (size_t)L * kMaxAux;
+    u64* pinvq = pmq + L;
+    u64* pinvq_q = pinvq + L;
+    ModDownConst& md = ctx->mod_down;
+    md.K = (int)K;
+    for (u32 i = 0; i < K; ++i) {
+        u64 pi = m[L + i], pp = 1 % pi;
+        md.p[i] = pi;
+        for (u32 j = 0; j < K; ++j) {
+            md.pp[i][j] = pp;
+            md.pp_q[i][j] = shoup_quotient_host(pp, pi);
+            if (j < i) pp = mulmod(pp, m[L + j] % pi, pi);
+        }
+        md.pinv[i] = invmod(md.pp[i][i], pi);
+        md.pinv_q[i] = shoup_quotient_host(md.pinv[i], pi);
+    }
+    if (K) {  // mixed-radix digits of floor(P/2): P = prod p_i, P/2 via digits of (P-1)/2
+        // (P-1)/2 has mixed-radix digits ((p_i - 1)/2 ... ) only when computed exactly:
+        // do a long division of the words of P by 2 then repeated division by p_i.
+        std::vector<u64> P(K + 2, 0);
+        P[0] = 1;
+        for (u32 k = 0; k < K; ++k) {
+            unsigned __int128 c = 0;
+            for (auto& w : P) {
+                unsigned __int128 t = (unsigned __int128)w * m[L + k] + c;
+                w = (u64)t;
+                c = t >> 64;
+            }
+        }
+        std::vector<u64> half(P.size());
+        for (size_t i = 0; i < P.size(); ++i) half[i] = (P[i] >> 1) | (i + 1 < P.size() ? (P[i + 1] << 63) : 0);
+        for (u32 k = 0; k < K; ++k) {
+            unsigned __int128 r = 0;
+            for (size_t w = half.size(); w-- > 0;) {
+                unsigned __int128 cur = (r << 64) | half[w];
+                half[w] = (u64)(cur / m[L + k]);
+                r = cur % m[L + k];
+            }
+            md.half[k] = (u64)r;
+        }
+    }
+    for (u32 i = 0; i < L; ++i) {
+        mdq[i] = m[i];
+        u64 pp = 1 % m[i];
+        for (u32 j = 0; j < K; ++j) {
+            pre[(size_t)i * kMaxAux + j] = pp;
+            pre_q[(size_t)i * kMaxAux + j] = shoup_quotient_host(pp, m[i]);
+            pp = mulmod(pp, m[L + j] % m[i], m[i]);
+        }
+        pmq[i] = pp;  // P mod q_i
+        pinvq[i] = K ? invmod(pp, m[i]) : 1;
+        pinvq_q[i] = shoup_quotient_host(pinvq[i], m[i]);
+    }
+    u64* gq = pinvq_q + L;
+    u64* gq_q = gq + (size_t)L * L;
+    u64* ginv = gq_q + (size_t)L * L;
+    u64* ginv_q = ginv + L;
+    for (u32 i = 0; i < L; ++i) {
+        u64 pp = 1 % m[i];
+        for (u32 j = 0; j < L; ++j) {
+            gq[(size_t)i * L + j] = pp;
+            gq_q[(size_t)i * L + j] = shoup_quotient_host(pp, m[i]);
+            if (j < i) pp = mulmod(pp, m[j] % m[i], m[i]);
+        }
+        ginv[i] = invmod(gq[(size_t)i * L + i], m[i]);
+        ginv_q[i] = shoup_quotient_host(ginv[i], m[i]);
+    }
+    if (cudaMalloc(&ctx->d_const_mem, h.size() * sizeof(u64)) != cudaSuccess) {
+        cudaGetLastError();
+        return CKKS_ERR_OOM;
+    }
+    if (cudaMemcpy(ctx->d_const_mem, h.data(), h.size() * sizeof(u64), cudaMemcpyHostToDevice) != cudaSuccess)
+        return CKKS_ERR_CUDA;
+    u64* d = ctx->d_const_mem;
+    ctx->d_rescale_inv = d;
+    ctx->d_pmodq = d + n_res;
+    u64* dmd = d + n_res + n_pm;
+    md.q = dmd;
+    md.pre = dmd + L;
+    md.pre_q = md.pre + (size_t)L * kMaxAux;
+    md.p_mod_q = md.pre_q + (size_t)L * kMaxAux;
+    md.pinv_mod_q = md.p_mod_q + L;
+    md.pinv_mod_q_q = md.pinv_mod_q + L;
+    u64* dg = d + n_res + n_pm + n_md;
+    ctx->garner.gq = dg;
+    ctx->garner.gq_q = dg + (size_t)L * L;
+    ctx->garner.ginv = dg + 2 * (size_t)L * L;
+    ctx->garner.ginv_q = ctx->garner.ginv + L;
+    return CKKS_OK;
+}
+
 }  // namespace
 
 void ckks_set_error(const std::string& msg) { g_last_error = msg; }
 
 void ntt_set_smem_limits();
-
-int32_t ctx_scratch(ckks_ctx* ctx, size_t words, u64** out) {
-    std::lock_guard<std::mutex> lock(ctx->scratch_mutex);
-    if (ctx->scratch_words < words) {
-        if (ctx->scratch) cudaFree(ctx->scratch);
-        ctx->scratch = nullptr;
-        ctx->scratch_words = 0;
-        if (cudaMalloc(&ctx->scratch, words * sizeof(u64)) != cudaSuccess) {
-            cudaGetLastError();
-            ckks_set_error("out of device memory for NTT scratch");
-            return CKKS_ERR_OOM;
-        }
-        ctx->scratch_words = words;
-    }
-    *out = ctx->scratch;
-    return CKKS_OK;
-}
 
 extern "C" {
 
@@ -227,6 +327,23 @@ int32_t ckks_ctx_create(uint32_t log_n, const uint64_t* q, uint32_t L, const uin
         ckks_set_error("ckks_ctx_create: " + e);
         return CKKS_ERR_CUDA;
     }
+    if (K > (u32)kMaxAux) {
+        ckks_ctx_destroy(ctx);
+        ckks_set_error("ckks_ctx_create: at most 8 auxiliary limbs");
+        return CKKS_ERR_BAD_ARG;
+    }
+    if (int32_t rc = build_constants(ctx)) {
+        ckks_ctx_destroy(ctx);
+        ckks_set_error("ckks_ctx_create: cannot upload constants");
+        return rc;
+    }
+    {  // keep freed stream-ordered workspaces cached in the device pool
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess) {
+            uint64_t thr = ~0ull;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        }
+    }
     ntt_set_smem_limits();
     *out = ctx;
     return CKKS_OK;
@@ -261,9 +378,9 @@ int32_t ckks_primes_below_bits(uint32_t bits, uint32_t degree, uint32_t count, u
 int32_t ckks_ctx_destroy(ckks_ctx* ctx) {
     if (!ctx) return CKKS_OK;
     if (ctx->own_stream) cudaStreamSynchronize(ctx->own_stream);
-    if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->d_tabs) cudaFree(ctx->d_tabs);
     if (ctx->d_table_mem) cudaFree(ctx->d_table_mem);
+    if (ctx->d_const_mem) cudaFree(ctx->d_const_mem);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return CKKS_OK;

@@ -11,6 +11,7 @@
 #include "modarith.cuh"
 #include "../../include/ckks_b200.h"
 
+
 // Per-modulus NTT tables (device pointers). N = N1 * N2 with N2 = 2^floor(logN/2).
 // The forward transform is the two-pass decomposition
 //   A[k2 + N2 k1] = sum_j1 w1^(j1 k1) psi^((2k2+1) j1) sum_j2 a[j1 + N1 j2] psi2^((2k2+1) j2)
@@ -27,6 +28,28 @@ struct NttTab {
     const u64 *imid, *imid_q;               // [N2][N1] N^-1 psi^-((2k2+1) j1)
 };
 
+constexpr int kMaxAux = 8;  // auxiliary (P) limbs
+constexpr int kMaxQ = 64;   // Q limbs
+
+// Exact ModDown constants (ring/auxiliary_modulus.rs:89-171).
+struct ModDownConst {
+    int K;
+    u64 p[kMaxAux];
+    u64 pp[kMaxAux][kMaxAux], pp_q[kMaxAux][kMaxAux];  // (p_0..p_{j-1}) mod p_i
+    u64 pinv[kMaxAux], pinv_q[kMaxAux];                // ((p_0..p_{i-1}) mod p_i)^-1
+    u64 half[kMaxAux];                                 // mixed-radix digits of floor(P/2)
+    const u64* q;                                      // [L]
+    const u64 *pre, *pre_q;                            // [L][kMaxAux]: (p_0..p_{j-1}) mod q_i
+    const u64* p_mod_q;                                // [L]
+    const u64 *pinv_mod_q, *pinv_mod_q_q;              // [L]: (P mod q_i)^-1
+};
+
+// Garner constants of the Q basis prefix (shared by every prefix length).
+struct GarnerQ {
+    const u64 *gq, *gq_q;    // [L][L]: (q_0..q_{j-1}) mod q_i
+    const u64 *ginv, *ginv_q;  // [L]: ((q_0..q_{i-1}) mod q_i)^-1
+};
+
 struct ckks_ctx {
     int device = 0;
     u32 log_n = 0, n = 0, log_n1 = 0, log_n2 = 0;
@@ -37,10 +60,14 @@ struct ckks_ctx {
     NttTab* d_tabs = nullptr;  // [L+K]
     std::vector<NttTab> h_tabs;
     cudaStream_t own_stream = nullptr;
-    // scratch for in-place transforms, grown on demand
-    std::mutex scratch_mutex;
-    u64* scratch = nullptr;
-    size_t scratch_words = 0;
+    // (P mod q_l, Shoup) for l < L at [0, 2L)
+    u64* d_pmodq = nullptr;
+    // rescale: for drop index d, [2][L] = ((q_d mod q_i)^-1, Shoup) at d*2L
+    u64* d_rescale_inv = nullptr;
+    // exact ModDown and Q-prefix Garner constants (see kernels.cuh)
+    u64* d_const_mem = nullptr;
+    ModDownConst mod_down{};
+    GarnerQ garner{};
 };
 
 // ---------------------------------------------------------------- errors
@@ -63,9 +90,22 @@ void ckks_set_error(const std::string& msg);
         }                                  \
     } while (0)
 
-inline cudaStream_t ckks_stream(ckks_ctx* ctx, void* s) {
-    return s ? (cudaStream_t)s : ctx->own_stream;
+// NULL selects the CUDA default (legacy) stream, so calls order with the
+// caller's default-stream work; the context's own stream serves the
+// host-buffer entry points only.
+inline cudaStream_t ckks_stream(ckks_ctx*, void* s) {
+    return (cudaStream_t)s;
 }
+
+// Local limb index -> table index: limbs [0, split) map to b0 + limb, the rest
+// to b1 + (limb - split). Covers a contiguous range and "Q prefix + P".
+struct LimbMap {
+    int b0, split, b1;
+    CKKS_HD int operator()(int limb) const { return limb < split ? b0 + limb : b1 + (limb - split); }
+    static LimbMap range(u32 begin, u32 count) { return LimbMap{(int)begin, (int)count, 0}; }
+    // Q limbs 0..q_limbs-1 followed by the context's K auxiliary limbs
+    static LimbMap qp(const ckks_ctx* c, u32 q_limbs);
+};
 
 // ------------------------------------------------------------- launchers
 // data layout [n_polys][limb_count][N]; table index = limb_begin + limb.
@@ -73,5 +113,27 @@ int32_t ntt_forward_launch(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, 
                            u32 limb_count, cudaStream_t st);
 int32_t ntt_inverse_launch(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, u32 limb_begin,
                            u32 limb_count, cudaStream_t st);
-// Scratch of at least `words` u64 (grown on demand; serialises growth).
-int32_t ctx_scratch(ckks_ctx* ctx, size_t words, u64** out);
+int32_t ntt_forward_launch_map(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, LimbMap lm, u32 limb_count,
+                               cudaStream_t st);
+int32_t ntt_inverse_launch_map(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, LimbMap lm, u32 limb_count,
+                               cudaStream_t st);
+inline LimbMap LimbMap::qp(const ckks_ctx* c, u32 q_limbs) { return LimbMap{0, (int)q_limbs, (int)c->L}; }
+// Stream-ordered workspace (cudaMallocAsync / cudaFreeAsync on `st`).
+template <typename T>
+struct Workspace {
+    T* p = nullptr;
+    cudaStream_t st = nullptr;
+    int32_t alloc(size_t count, cudaStream_t s) {
+        st = s;
+        if (cudaMallocAsync((void**)&p, count * sizeof(T) + 16, s) != cudaSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+            ckks_set_error("out of device memory for a workspace");
+            return CKKS_ERR_OOM;
+        }
+        return CKKS_OK;
+    }
+    ~Workspace() {
+        if (p) cudaFreeAsync(p, st);
+    }
+};

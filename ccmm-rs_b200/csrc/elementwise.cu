@@ -1,0 +1,162 @@
+// elementwise.cu -- limb-parallel kernels: Galois automorphisms (coefficient
+// and NTT domain), NTT-domain products and sums, rescale, and the exact
+// QP -> Q ModDown. One thread per (limb, coefficient); grids are
+// (N / 256, limbs, polys), coalesced on the contiguous coefficient axis.
+#include "context.cuh"
+#include "kernels.cuh"
+
+namespace {
+
+constexpr int kT = 256;
+
+// ckks/automorphism.rs:8-48, output-driven: out[t] = +-in[s], s = t * k^-1 mod 2N
+__global__ void k_automorphism_coef(const u64* __restrict__ in, u64* __restrict__ out, const NttTab* __restrict__ tabs,
+                                    LimbMap lm, int limbs, int log_n, u64 k_inv) {
+    const u32 n = 1u << log_n;
+    const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int limb = blockIdx.y;
+    const size_t base = ((size_t)blockIdx.z * limbs + limb) << log_n;
+    const u64 s = ((u64)t * k_inv) & (2ull * n - 1);
+    const u64 q = tabs[lm(limb)].q;
+    u64 v = in[base + (s & (n - 1))];
+    out[base + t] = s >= n ? neg_mod(v, q) : v;
+}
+
+// ring/ntt_galois_permutation.rs:5-19: out[i] = in[((k (2i+1)) mod 2N - 1) / 2]
+__global__ void k_automorphism_ntt(const u64* __restrict__ in, u64* __restrict__ out, int limbs, int log_n, u64 k) {
+    const u32 n = 1u << log_n;
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const size_t base = ((size_t)blockIdx.z * limbs + blockIdx.y) << log_n;
+    out[base + i] = in[base + (galois_src(i, k, log_n))];
+}
+
+// op: 0 mul, 1 add, 2 sub (ring/ntt_polynomial.rs:186-236, ring/polynomial.rs add/sub)
+__global__ void k_pointwise(const u64* __restrict__ a, const u64* __restrict__ b, u64* __restrict__ out,
+                            const NttTab* __restrict__ tabs, LimbMap lm, int limbs, int log_n, int op) {
+    const u32 n = 1u << log_n;
+    const u32 c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const int limb = blockIdx.y;
+    const size_t i = (((size_t)blockIdx.z * limbs + limb) << log_n) + c;
+    const NttTab& T = tabs[lm(limb)];
+    Barrett m{T.q, T.mu_hi, T.mu_lo};
+    u64 x = a[i], y = b[i];
+    out[i] = op == 0 ? mul_barrett(x, y, m) : op == 1 ? add_mod(x, y, T.q) : sub_mod(x, y, T.q);
+}
+
+// ckks/rns_rescale.rs:107-167: ((x - centered(x mod q_d)) * q_d^-1) mod q_i
+__global__ void k_rescale(const u64* __restrict__ in, u64* __restrict__ out, const NttTab* __restrict__ tabs,
+                          const u64* __restrict__ inv, const u64* __restrict__ inv_q, int limbs_in, int log_n) {
+    const u32 n = 1u << log_n;
+    const u32 c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const int i = blockIdx.y, drop = limbs_in - 1;
+    const u64 qd = tabs[drop].q, qi = tabs[i].q;
+    const size_t src = (size_t)blockIdx.z * limbs_in << log_n;
+    const size_t dst = (size_t)blockIdx.z * (limbs_in - 1) << log_n;
+    u64 r = in[src + ((size_t)drop << log_n) + c];
+    u64 rq;
+    if (r > qd / 2) {
+        u64 mag = qd - r;
+        mag = mag >= qi ? mag % qi : mag;
+        rq = neg_mod(mag, qi);
+    } else {
+        rq = r >= qi ? r % qi : r;
+    }
+    u64 d = sub_mod(in[src + ((size_t)i << log_n) + c], rq, qi);
+    out[dst + ((size_t)i << log_n) + c] = mul_shoup(d, inv[i], inv_q[i], qi);
+}
+
+// ring/auxiliary_modulus.rs:89-171: centered CRT over P from the K auxiliary
+// residues (mixed-radix Garner, exact), then (x_i - r) * P^-1 mod q_i.
+__global__ void k_mod_down(const u64* __restrict__ in, u64* __restrict__ out, ModDownConst md, int q_limbs,
+                           int log_n) {
+    const u32 n = 1u << log_n;
+    const u32 c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const int K = md.K;
+    const size_t src = (size_t)blockIdx.z * (q_limbs + K) << log_n;
+    const size_t dst = (size_t)blockIdx.z * q_limbs << log_n;
+    u64 v[kMaxAux];
+    // Garner: v_i = (x_i - sum_{j<i} v_j * (p_0..p_{j-1} mod p_i)) * (p_0..p_{i-1})^-1 mod p_i
+    for (int i = 0; i < K; ++i) {
+        const u64 p = md.p[i];
+        u64 x = in[src + ((size_t)(q_limbs + i) << log_n) + c];
+        u64 acc = 0;
+        for (int j = 0; j < i; ++j) acc = add_mod(acc, mul_shoup(v[j], md.pp[i][j], md.pp_q[i][j], p), p);
+        v[i] = mul_shoup(sub_mod(x, acc, p), md.pinv[i], md.pinv_q[i], p);
+    }
+    // centered: value > floor(P/2) -> negative (lexicographic mixed-radix compare)
+    bool neg = false;
+    for (int i = K - 1; i >= 0; --i) {
+        if (v[i] != md.half[i]) { neg = v[i] > md.half[i]; break; }
+    }
+    const int i = blockIdx.y;
+    const u64 qi = md.q[i];
+    u64 r = 0;
+    for (int j = 0; j < K; ++j)
+        r = add_mod(r, mul_shoup(v[j], md.pre[i * kMaxAux + j], md.pre_q[i * kMaxAux + j], qi), qi);
+    if (neg) r = sub_mod(r, md.p_mod_q[i], qi);
+    u64 d = sub_mod(in[src + ((size_t)i << log_n) + c], r, qi);
+    out[dst + ((size_t)i << log_n) + c] = mul_shoup(d, md.pinv_mod_q[i], md.pinv_mod_q_q[i], qi);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ launchers
+int32_t automorphism_coef_launch(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, LimbMap lm, u32 limbs, u64 k,
+                                 cudaStream_t st) {
+    if (!n_polys || !limbs) return CKKS_OK;
+    const u64 two_n = 2ull * ctx->n;
+    k %= two_n;
+    u64 k_inv = 1;  // inverse of k modulo 2N (odd k): k^(N/2 * 2 - 1) via repeated squaring in Z/2N
+    {
+        u64 e = ctx->n - 1, b = k;  // group (Z/2NZ)^* has exponent N/2; k^(N-1) = k^-1
+        while (e) {
+            if (e & 1) k_inv = (k_inv * b) % two_n;
+            b = (b * b) % two_n;
+            e >>= 1;
+        }
+    }
+    dim3 g((ctx->n + kT - 1) / kT, limbs, n_polys);
+    k_automorphism_coef<<<g, kT, 0, st>>>(in, out, ctx->d_tabs, lm, limbs, ctx->log_n, k_inv);
+    CKKS_CUDA_TRY(cudaGetLastError());
+    return CKKS_OK;
+}
+
+int32_t automorphism_ntt_launch(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, u32 limbs, u64 k,
+                                cudaStream_t st) {
+    if (!n_polys || !limbs) return CKKS_OK;
+    dim3 g((ctx->n + kT - 1) / kT, limbs, n_polys);
+    k_automorphism_ntt<<<g, kT, 0, st>>>(in, out, limbs, ctx->log_n, k % (2ull * ctx->n));
+    CKKS_CUDA_TRY(cudaGetLastError());
+    return CKKS_OK;
+}
+
+int32_t pointwise_launch(ckks_ctx* ctx, const u64* a, const u64* b, u64* out, u32 n_polys, LimbMap lm, u32 limbs,
+                         int op, cudaStream_t st) {
+    if (!n_polys || !limbs) return CKKS_OK;
+    dim3 g((ctx->n + kT - 1) / kT, limbs, n_polys);
+    k_pointwise<<<g, kT, 0, st>>>(a, b, out, ctx->d_tabs, lm, limbs, ctx->log_n, op);
+    CKKS_CUDA_TRY(cudaGetLastError());
+    return CKKS_OK;
+}
+
+int32_t rescale_launch(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, u32 limbs_in, cudaStream_t st) {
+    if (!n_polys) return CKKS_OK;
+    const u64* inv = ctx->d_rescale_inv + (size_t)(limbs_in - 1) * 2 * ctx->L;
+    dim3 g((ctx->n + kT - 1) / kT, limbs_in - 1, n_polys);
+    k_rescale<<<g, kT, 0, st>>>(in, out, ctx->d_tabs, inv, inv + ctx->L, limbs_in, ctx->log_n);
+    CKKS_CUDA_TRY(cudaGetLastError());
+    return CKKS_OK;
+}
+
+int32_t mod_down_launch(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, u32 q_limbs, cudaStream_t st) {
+    if (!n_polys) return CKKS_OK;
+    dim3 g((ctx->n + kT - 1) / kT, q_limbs, n_polys);
+    k_mod_down<<<g, kT, 0, st>>>(in, out, ctx->mod_down, q_limbs, ctx->log_n);
+    CKKS_CUDA_TRY(cudaGetLastError());
+    return CKKS_OK;
+}

@@ -1,0 +1,30 @@
+// kernels.cuh -- shared device helpers, constant blocks and launcher
+// declarations of the elementwise, gadget and key-switching kernels.
+#pragma once
+#include "context.cuh"
+
+// ring/ntt_galois_permutation.rs:5-19 source index of output i under X -> X^k
+CKKS_HD u32 galois_src(u32 i, u64 k, int log_n) {
+    u64 mask = (2ull << log_n) - 1;
+    u64 rot = (k * (2ull * i + 1)) & mask;
+    return (u32)((rot - 1) >> 1);
+}
+
+int32_t automorphism_coef_launch(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, LimbMap lm, u32 limbs, u64 k,
+                                 cudaStream_t st);
+int32_t automorphism_ntt_launch(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, u32 limbs, u64 k,
+                                cudaStream_t st);
+int32_t pointwise_launch(ckks_ctx* ctx, const u64* a, const u64* b, u64* out, u32 n_polys, LimbMap lm, u32 limbs,
+                         int op, cudaStream_t st);
+int32_t rescale_launch(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, u32 limbs_in, cudaStream_t st);
+int32_t mod_down_launch(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, u32 q_limbs, cudaStream_t st);
+
+// Bounded (balanced base-2^base_log) gadget, grafting/bounded_gadget.rs.
+int32_t bounded_digit_count(ckks_ctx* ctx, u32 q_limbs, u32 base_log, u32* out);
+int32_t bounded_decompose_launch(ckks_ctx* ctx, const u64* poly, u32 n_polys, u32 q_limbs, u32 base_log, i64* digits,
+                                 u32* flags, cudaStream_t st);
+int32_t digits_automorphism_launch(ckks_ctx* ctx, const i64* in, i64* out, u32 n_polys, u32 D, u32 base_log, u64 k,
+                                   cudaStream_t st);
+// Forward NTT of signed digits lifted to every limb of `lm` ([D][limbs][N] out).
+int32_t ntt_forward_digits_launch(ckks_ctx* ctx, const i64* digits, u64* out, u32 D, LimbMap lm, u32 limbs,
+                                  cudaStream_t st);

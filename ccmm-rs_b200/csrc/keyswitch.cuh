@@ -1,0 +1,46 @@
+// keyswitch.cuh -- key-switching key objects and pipeline entry points.
+#pragma once
+#include <vector>
+
+#include "kernels.cuh"
+
+// A key-switching key resident in HBM.
+//   HYBRID_BOUNDED : entries [D][q_limbs+K][2][N], NTT domain, encrypting
+//                    P * B^j * sigma(s) over QP (hybrid_rns_galois_key.rs:61-170)
+//   HYBRID_RNS_BLOCK: entries [dnum][q_limbs+K][2][N], encrypting P * E_i * sigma(s)
+//   RELIN_BOUNDED  : entries [D][2][q_limbs][N], NTT domain, encrypting B^j * s^2
+//                    over Q (bounded_key_switch.rs:22-120)
+struct ckks_ksk {
+    ckks_ctx* ctx = nullptr;
+    int kind = 0;
+    bool with_p = true;
+    u32 q_limbs = 0, base_log = 0, D = 0;
+    u64 exponent = 1;
+    std::vector<u32> blocks;    // RNS-block sizes
+    u64* d_entries = nullptr;
+    size_t words = 0;
+    u64* d_block_const = nullptr;  // RNS-block ModUp constants
+};
+
+u32 ksk_limbs(const ckks_ksk* k);
+int32_t ksk_alloc(ckks_ctx* ctx, ckks_ksk* key);
+int32_t ksk_generate(ckks_ctx* ctx, ckks_ksk* key, const int8_t* secret, u64 seed, double sigma,
+                     const std::vector<u64>& factors, const std::vector<int8_t>& s_target, bool comp_major, u64 tag_a,
+                     u64 tag_e, cudaStream_t st, const u64* d_target_limbs = nullptr);
+int32_t relin_generate(ckks_ctx* ctx, ckks_ksk* key, const int8_t* secret, u64 seed, double sigma, cudaStream_t st);
+std::vector<u64> hybrid_factors(ckks_ctx* ctx, const ckks_ksk* key);
+std::vector<u64> rnsblock_factors(ckks_ctx* ctx, const ckks_ksk* key);
+std::vector<u64> relin_factors(ckks_ctx* ctx, const ckks_ksk* key);
+std::vector<int8_t> host_secret_automorphism(const int8_t* s, u32 n, u64 k);
+int32_t rnsblock_prepare(ckks_ctx* ctx, ckks_ksk* key);
+int32_t rnsblock_modup_launch(ckks_ctx* ctx, const ckks_ksk* key, const u64* a, u64* Y, cudaStream_t st);
+
+int32_t ks_mac_launch(ckks_ctx* ctx, const u64* Y, const u64* key, const u64* base, u64* acc, u32 q_limbs, u32 D,
+                      bool with_p, u64 perm_y, u64 perm_b, cudaStream_t st);
+int32_t rotate_hybrid(ckks_ctx* ctx, const ckks_ksk* key, const u64* ct_in, u64* ct_out, u32 n_ct, cudaStream_t st);
+int32_t rotate_hybrid_hoisted(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_keys, const u64* ct_in, u64* ct_out,
+                              u32 n_ct, cudaStream_t st);
+
+// sampling stream tags (shared with the oracle's restatement)
+constexpr u64 TAG_KEY_A = 1ull << 56, TAG_KEY_E = 2ull << 56, TAG_ENC_A = 3ull << 56, TAG_ENC_E = 4ull << 56,
+              TAG_RLK_A = 5ull << 56, TAG_RLK_E = 6ull << 56;

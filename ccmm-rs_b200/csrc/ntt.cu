@@ -12,12 +12,11 @@
 // (__umul64hi); outputs are canonical. Result values equal the reference's
 // PreparedNttPlan::forward (ring/prepared_ntt.rs:200-231) word for word:
 // both compute the unique A[k] = a(psi^(2k+1)) mod q.
-#include "context.cuh"
+#include "kernels.cuh"
 
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kMaxC = 16;
 
 __device__ __forceinline__ u32 bitrev(u32 x, int bits) { return __brev(x) >> (32 - bits); }
 
@@ -25,21 +24,37 @@ __device__ __forceinline__ u32 bitrev(u32 x, int bits) { return __brev(x) >> (32
 // that reading one column across bit-reversed rows is bank-conflict free.
 __device__ __forceinline__ int swz(u32 row, int log_rows, int C) { return (int)(bitrev(row, log_rows) & (C - 1)); }
 
-// Forward pass 1: tile of C columns j1, N2 rows j2.
-__global__ void __launch_bounds__(kThreads) k_ntt_fwd_pass1(const u64* __restrict__ in, u64* __restrict__ out,
-                                                            const NttTab* __restrict__ tabs, int limb_begin,
+// Forward pass 1: tile of C columns j1, N2 rows j2. With kDigits the input is
+// a signed digit polynomial [D][N] (int64) shared by every limb, lifted to
+// [0, q) on load (signed_mod, hybrid_rns_galois_key.rs:55-57); blockIdx.z
+// then indexes the digit.
+template <bool kDigits>
+__global__ void __launch_bounds__(kThreads) k_ntt_fwd_pass1(const void* __restrict__ in_, u64* __restrict__ out,
+                                                            const NttTab* __restrict__ tabs, LimbMap lm,
                                                             int limb_count, int log_n1, int log_n2, int log_c) {
     extern __shared__ u64 sm[];
-    const int N1 = 1 << log_n1, N2 = 1 << log_n2, C = 1 << log_c;
+    const int N2 = 1 << log_n2, C = 1 << log_c;
     const int limb = blockIdx.y;
-    const NttTab T = tabs[limb_begin + limb];
+    const NttTab T = tabs[lm(limb)];
     const u64 q = T.q, q2 = q << 1;
     const size_t base = ((size_t)blockIdx.z * limb_count + limb) << (log_n1 + log_n2);
     const int j1_0 = blockIdx.x << log_c;
 
-    for (int idx = threadIdx.x; idx < (N2 << log_c); idx += blockDim.x) {
-        int j2 = idx >> log_c, c = idx & (C - 1);
-        sm[(j2 << log_c) + (c ^ swz(j2, log_n2, C))] = in[base + j1_0 + c + ((size_t)j2 << log_n1)];
+    if (kDigits) {
+        const i64* in = (const i64*)in_ + ((size_t)blockIdx.z << (log_n1 + log_n2));
+        for (int idx = threadIdx.x; idx < (N2 << log_c); idx += blockDim.x) {
+            int j2 = idx >> log_c, c = idx & (C - 1);
+            i64 d = in[j1_0 + c + ((size_t)j2 << log_n1)];
+            u64 a = d < 0 ? (u64)(-d) : (u64)d;
+            a = a >= q ? a % q : a;
+            sm[(j2 << log_c) + (c ^ swz(j2, log_n2, C))] = (d < 0 && a) ? q - a : a;
+        }
+    } else {
+        const u64* in = (const u64*)in_;
+        for (int idx = threadIdx.x; idx < (N2 << log_c); idx += blockDim.x) {
+            int j2 = idx >> log_c, c = idx & (C - 1);
+            sm[(j2 << log_c) + (c ^ swz(j2, log_n2, C))] = in[base + j1_0 + c + ((size_t)j2 << log_n1)];
+        }
     }
     __syncthreads();
     // merged CT: natural in -> bit-reversed out (psi_rev holds psi2^bitrev(i))
@@ -72,12 +87,12 @@ __global__ void __launch_bounds__(kThreads) k_ntt_fwd_pass1(const u64* __restric
 // Forward pass 2: tile of C columns k2, N1 rows j1. The CTA reads its whole
 // tile before writing the same addresses, so src may equal dst.
 __global__ void __launch_bounds__(kThreads) k_ntt_fwd_pass2(const u64* src, u64* dst, const NttTab* __restrict__ tabs,
-                                                            int limb_begin, int limb_count, int log_n1, int log_n2,
+                                                            LimbMap lm, int limb_count, int log_n1, int log_n2,
                                                             int log_c) {
     extern __shared__ u64 sm[];
     const int N1 = 1 << log_n1, N2 = 1 << log_n2, C = 1 << log_c;
     const int limb = blockIdx.y;
-    const NttTab T = tabs[limb_begin + limb];
+    const NttTab T = tabs[lm(limb)];
     const u64 q = T.q, q2 = q << 1;
     const size_t base = ((size_t)blockIdx.z * limb_count + limb) << (log_n1 + log_n2);
     const int k2_0 = blockIdx.x << log_c;
@@ -116,12 +131,12 @@ __global__ void __launch_bounds__(kThreads) k_ntt_fwd_pass2(const u64* src, u64*
 // Inverse pass A: tile of C columns k2; cyclic GS over k1 (natural in ->
 // bit-reversed out), times N^-1 psi^-((2k2+1) j1), stored as rows [k2][j1].
 __global__ void __launch_bounds__(kThreads) k_ntt_inv_passA(const u64* __restrict__ in, u64* __restrict__ out,
-                                                            const NttTab* __restrict__ tabs, int limb_begin,
+                                                            const NttTab* __restrict__ tabs, LimbMap lm,
                                                             int limb_count, int log_n1, int log_n2, int log_c) {
     extern __shared__ u64 sm[];
     const int N1 = 1 << log_n1, C = 1 << log_c;
     const int limb = blockIdx.y;
-    const NttTab T = tabs[limb_begin + limb];
+    const NttTab T = tabs[lm(limb)];
     const u64 q = T.q, q2 = q << 1;
     const size_t base = ((size_t)blockIdx.z * limb_count + limb) << (log_n1 + log_n2);
     const int k2_0 = blockIdx.x << log_c;
@@ -161,12 +176,12 @@ __global__ void __launch_bounds__(kThreads) k_ntt_inv_passA(const u64* __restric
 // Inverse pass B: tile of C columns j1; merged GS negacyclic over k2
 // (bit-reversed in -> natural out). src may equal dst (same address set per CTA).
 __global__ void __launch_bounds__(kThreads) k_ntt_inv_passB(const u64* src, u64* dst, const NttTab* __restrict__ tabs,
-                                                            int limb_begin, int limb_count, int log_n1, int log_n2,
+                                                            LimbMap lm, int limb_count, int log_n1, int log_n2,
                                                             int log_c) {
     extern __shared__ u64 sm[];
     const int N2 = 1 << log_n2, C = 1 << log_c;
     const int limb = blockIdx.y;
-    const NttTab T = tabs[limb_begin + limb];
+    const NttTab T = tabs[lm(limb)];
     const u64 q = T.q, q2 = q << 1;
     const size_t base = ((size_t)blockIdx.z * limb_count + limb) << (log_n1 + log_n2);
     const int j1_0 = blockIdx.x << log_c;
@@ -205,7 +220,8 @@ void ntt_set_smem_limits() {
     static bool done = false;
     if (done) return;
     int bytes = 96 * 1024;
-    cudaFuncSetAttribute(k_ntt_fwd_pass1, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaFuncSetAttribute(k_ntt_fwd_pass1<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaFuncSetAttribute(k_ntt_fwd_pass1<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     cudaFuncSetAttribute(k_ntt_fwd_pass2, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     cudaFuncSetAttribute(k_ntt_inv_passA, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     cudaFuncSetAttribute(k_ntt_inv_passB, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
@@ -214,38 +230,63 @@ void ntt_set_smem_limits() {
 
 int32_t ntt_forward_launch(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, u32 limb_begin, u32 limb_count,
                            cudaStream_t st) {
+    return ntt_forward_launch_map(ctx, in, out, n_polys, LimbMap::range(limb_begin, limb_count), limb_count, st);
+}
+
+int32_t ntt_inverse_launch(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, u32 limb_begin, u32 limb_count,
+                           cudaStream_t st) {
+    return ntt_inverse_launch_map(ctx, in, out, n_polys, LimbMap::range(limb_begin, limb_count), limb_count, st);
+}
+
+int32_t ntt_forward_launch_map(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, LimbMap lm, u32 limb_count,
+                               cudaStream_t st) {
     if (n_polys == 0 || limb_count == 0) return CKKS_OK;
     const int l1 = ctx->log_n1, l2 = ctx->log_n2;
     u64* mid = out;
-    if (in == out) {  // pass 1 reads columns and writes rows: stage through scratch
-        int32_t rc = ctx_scratch(ctx, (size_t)n_polys * limb_count * ctx->n, &mid);
-        if (rc) return rc;
+    Workspace<u64> tmp;
+    if (in == out) {  // pass 1 reads columns and writes rows: stage through a workspace
+        if (int32_t rc = tmp.alloc((size_t)n_polys * limb_count * ctx->n, st)) return rc;
+        mid = tmp.p;
     }
     int lc1 = log2_min(l1, 4), lc2 = log2_min(l2, 4);
     dim3 g1(1u << (l1 - lc1), limb_count, n_polys), g2(1u << (l2 - lc2), limb_count, n_polys);
-    k_ntt_fwd_pass1<<<g1, kThreads, (sizeof(u64) << (l2 + lc1)), st>>>(in, mid, ctx->d_tabs, limb_begin, limb_count,
+    k_ntt_fwd_pass1<false><<<g1, kThreads, (sizeof(u64) << (l2 + lc1)), st>>>(in, mid, ctx->d_tabs, lm, limb_count,
                                                                        l1, l2, lc1);
-    k_ntt_fwd_pass2<<<g2, kThreads, (sizeof(u64) << (l1 + lc2)), st>>>(mid, out, ctx->d_tabs, limb_begin,
+    k_ntt_fwd_pass2<<<g2, kThreads, (sizeof(u64) << (l1 + lc2)), st>>>(mid, out, ctx->d_tabs, lm,
                                                                        limb_count, l1, l2, lc2);
     CKKS_CUDA_TRY(cudaGetLastError());
     return CKKS_OK;
 }
 
-int32_t ntt_inverse_launch(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, u32 limb_begin, u32 limb_count,
-                           cudaStream_t st) {
+int32_t ntt_inverse_launch_map(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, LimbMap lm, u32 limb_count,
+                               cudaStream_t st) {
     if (n_polys == 0 || limb_count == 0) return CKKS_OK;
     const int l1 = ctx->log_n1, l2 = ctx->log_n2;
     u64* mid = out;
+    Workspace<u64> tmp;
     if (in == out) {
-        int32_t rc = ctx_scratch(ctx, (size_t)n_polys * limb_count * ctx->n, &mid);
-        if (rc) return rc;
+        if (int32_t rc = tmp.alloc((size_t)n_polys * limb_count * ctx->n, st)) return rc;
+        mid = tmp.p;
     }
     int lcA = log2_min(l2, 4), lcB = log2_min(l1, 4);
     dim3 gA(1u << (l2 - lcA), limb_count, n_polys), gB(1u << (l1 - lcB), limb_count, n_polys);
-    k_ntt_inv_passA<<<gA, kThreads, (sizeof(u64) << (l1 + lcA)), st>>>(in, mid, ctx->d_tabs, limb_begin, limb_count,
+    k_ntt_inv_passA<<<gA, kThreads, (sizeof(u64) << (l1 + lcA)), st>>>(in, mid, ctx->d_tabs, lm, limb_count,
                                                                        l1, l2, lcA);
-    k_ntt_inv_passB<<<gB, kThreads, (sizeof(u64) << (l2 + lcB)), st>>>(mid, out, ctx->d_tabs, limb_begin,
+    k_ntt_inv_passB<<<gB, kThreads, (sizeof(u64) << (l2 + lcB)), st>>>(mid, out, ctx->d_tabs, lm,
                                                                        limb_count, l1, l2, lcB);
+    CKKS_CUDA_TRY(cudaGetLastError());
+    return CKKS_OK;
+}
+
+int32_t ntt_forward_digits_launch(ckks_ctx* ctx, const i64* digits, u64* out, u32 D, LimbMap lm, u32 limbs,
+                                  cudaStream_t st) {
+    if (D == 0 || limbs == 0) return CKKS_OK;
+    const int l1 = ctx->log_n1, l2 = ctx->log_n2;
+    int lc1 = log2_min(l1, 4), lc2 = log2_min(l2, 4);
+    dim3 g1(1u << (l1 - lc1), limbs, D), g2(1u << (l2 - lc2), limbs, D);
+    k_ntt_fwd_pass1<true><<<g1, kThreads, (sizeof(u64) << (l2 + lc1)), st>>>(digits, out, ctx->d_tabs, lm, limbs, l1,
+                                                                             l2, lc1);
+    k_ntt_fwd_pass2<<<g2, kThreads, (sizeof(u64) << (l1 + lc2)), st>>>(out, out, ctx->d_tabs, lm, limbs, l1, l2, lc2);
     CKKS_CUDA_TRY(cudaGetLastError());
     return CKKS_OK;
 }

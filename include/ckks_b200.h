@@ -20,9 +20,10 @@
  *     trailing limb is dropped first by rescale, ring/modulus_chain.rs:19-27)
  *     followed by auxiliary limbs p_0..p_{K-1}. Limb indices in the calls
  *     below index that combined list.
- *   - stream: a cudaStream_t passed as void*; NULL selects the context's own
- *     stream. Calls on one context are thread-safe when given distinct
- *     streams, except where noted.
+ *   - stream: a cudaStream_t passed as void*; NULL selects the CUDA default
+ *     stream. Work is stream-ordered; workspaces come from the stream-ordered
+ *     allocator (cudaMallocAsync). Calls on one context are thread-safe when
+ *     given distinct streams.
  */
 #ifndef CKKS_B200_H
 #define CKKS_B200_H
@@ -90,6 +91,109 @@ int32_t ckks_ntt_forward_host(ckks_ctx* ctx, const uint64_t* in_host, uint64_t* 
                               uint32_t limb_begin, uint32_t limb_count);
 int32_t ckks_ntt_inverse_host(ckks_ctx* ctx, const uint64_t* in_host, uint64_t* out_host, uint32_t n_polys,
                               uint32_t limb_begin, uint32_t limb_count);
+
+
+/* ------------------------------------------------------------ ring ops ----
+ * Polynomial batches [n_polys][limbs][N] over the context limbs
+ * [limb_begin, limb_begin + limbs). */
+
+/* Coefficient-domain Galois automorphism X -> X^k, k odd mod 2N
+ * (ckks/automorphism.rs:8-48, ckks/rns_automorphism.rs:12-28). in != out. */
+int32_t ckks_automorphism_coef(ckks_ctx* ctx, const uint64_t* in, uint64_t* out, uint32_t n_polys,
+                               uint32_t limb_begin, uint32_t limbs, uint64_t exponent, void* stream);
+/* NTT-domain automorphism as an index permutation
+ * (ring/ntt_galois_permutation.rs:5-19). in != out. */
+int32_t ckks_automorphism_ntt(ckks_ctx* ctx, const uint64_t* in, uint64_t* out, uint32_t n_polys,
+                              uint32_t limb_begin, uint32_t limbs, uint64_t exponent, void* stream);
+/* Galois exponents for slot rotations and conjugation (ckks/automorphism.rs:179-240). */
+uint64_t ckks_rotation_exponent_left(uint32_t degree, uint64_t steps);
+uint64_t ckks_rotation_exponent_right(uint32_t degree, uint64_t steps);
+uint64_t ckks_conjugation_exponent(uint32_t degree);
+
+/* Element-wise out = a op b (op 0: product, NTT domain, ring/ntt_polynomial.rs:186;
+ * 1: sum; 2: difference). out may alias a or b. */
+int32_t ckks_pointwise(ckks_ctx* ctx, const uint64_t* a, const uint64_t* b, uint64_t* out, uint32_t n_polys,
+                       uint32_t limb_begin, uint32_t limbs, int32_t op, void* stream);
+
+/* CKKS rescale: drop the trailing limb of the Q prefix q_0..q_{limbs_in-1}:
+ * out_i = ((x_i - centered(x mod q_d)) * q_d^-1) mod q_i, coefficient domain
+ * (ckks/rns_rescale.rs:107-167). in [n][limbs_in][N] -> out [n][limbs_in-1][N]. */
+int32_t ckks_rescale(ckks_ctx* ctx, const uint64_t* in, uint64_t* out, uint32_t n_polys, uint32_t limbs_in,
+                     void* stream);
+
+/* Exact ModDown by P: in [n][q_limbs + K][N] (Q prefix then all K auxiliary
+ * limbs, coefficient domain) -> out [n][q_limbs][N]
+ * (ring/auxiliary_modulus.rs:89-171 auxiliary_mod_down_rns_candidate). */
+int32_t ckks_mod_down(ckks_ctx* ctx, const uint64_t* in, uint64_t* out, uint32_t n_polys, uint32_t q_limbs,
+                      void* stream);
+
+/* ------------------------------------------------------------- gadgets ----
+ * Balanced base-2^base_log digits (grafting/bounded_gadget.rs): count
+ * ceil((bits(Q)+1)/base_log) (:17-37); decomposition of the centred exact CRT
+ * value (:59-118) of n_polys polynomials over the Q prefix of q_limbs limbs,
+ * digits [n][D][N] as int64; base_log in [1, 62] (the reference allows 63). */
+int32_t ckks_bounded_digit_count(ckks_ctx* ctx, uint32_t q_limbs, uint32_t base_log, uint32_t* out);
+int32_t ckks_bounded_decompose(ckks_ctx* ctx, const uint64_t* poly, uint32_t n_polys, uint32_t q_limbs,
+                               uint32_t base_log, int64_t* digits, void* stream);
+/* BoundedGadgetDecomposition::automorphism_hoisted (bounded_gadget.rs:273-312):
+ * digits [n][D][N] -> digits of sigma_k of the decomposed value. */
+int32_t ckks_bounded_digits_automorphism(ckks_ctx* ctx, const int64_t* in, int64_t* out, uint32_t n_polys,
+                                         uint32_t digit_count, uint32_t base_log, uint64_t exponent, void* stream);
+
+/* ------------------------------------------------ key-switching keys -----
+ * Key kinds:
+ *   CKKS_KSK_HYBRID_BOUNDED : hybrid-QP Galois key, entries [D][q_limbs+K][2][N]
+ *     (b_ntt, a_ntt) encrypting P * B^j * sigma(s) -- the reference's
+ *     PreparedHybridRnsGaloisKey (ckks/hybrid_rns_galois_key.rs:20-170).
+ *   CKKS_KSK_HYBRID_RNS_BLOCK : hybrid Galois key over RNS blocks ("dnum"),
+ *     entries [dnum][q_limbs+K][2][N] encrypting P * E_i * sigma(s) with E_i the
+ *     CRT idempotent of block i (grafting/rns_gadget.rs:92-135).
+ *   CKKS_KSK_RELIN_BOUNDED : bounded relinearization key over Q only,
+ *     BoundedRnsMultiplicationKey (grafting/bounded_key_switch.rs:22-120);
+ *     uploaded in the reference's coefficient-domain layout [D][2][q_limbs][N],
+ *     stored NTT-domain.
+ * Generation samples a counter-based stream (seed) on the GPU: uniform a in
+ * the NTT domain, discrete Gaussian e of width sigma shared across limbs;
+ * secret_host is the ternary secret (int8 in {-1,0,1}, N entries). */
+enum { CKKS_KSK_HYBRID_BOUNDED = 0, CKKS_KSK_HYBRID_RNS_BLOCK = 1, CKKS_KSK_RELIN_BOUNDED = 2 };
+typedef struct ckks_ksk ckks_ksk;
+
+int32_t ckks_hybrid_key_generate(ckks_ctx* ctx, uint32_t q_limbs, uint32_t base_log, uint64_t exponent,
+                                 const int8_t* secret_host, uint64_t seed, double sigma, ckks_ksk** out);
+int32_t ckks_hybrid_key_upload(ckks_ctx* ctx, uint32_t q_limbs, uint32_t base_log, uint64_t exponent,
+                               const uint64_t* entries_host, ckks_ksk** out);
+int32_t ckks_rnsblock_key_generate(ckks_ctx* ctx, uint32_t q_limbs, const uint32_t* block_sizes, uint32_t n_blocks,
+                                   uint64_t exponent, const int8_t* secret_host, uint64_t seed, double sigma,
+                                   ckks_ksk** out);
+int32_t ckks_rnsblock_key_upload(ckks_ctx* ctx, uint32_t q_limbs, const uint32_t* block_sizes, uint32_t n_blocks,
+                                 uint64_t exponent, const uint64_t* entries_host, ckks_ksk** out);
+int32_t ckks_relin_key_generate(ckks_ctx* ctx, uint32_t q_limbs, uint32_t base_log, const int8_t* secret_host,
+                                uint64_t seed, double sigma, ckks_ksk** out);
+int32_t ckks_relin_key_upload(ckks_ctx* ctx, uint32_t q_limbs, uint32_t base_log, const uint64_t* entries_host,
+                              ckks_ksk** out);
+/* digits/blocks, words of HBM payload, stored entries (NTT domain) to host */
+int32_t ckks_ksk_info(const ckks_ksk* key, uint32_t* digits, uint64_t* words);
+int32_t ckks_ksk_download(const ckks_ksk* key, uint64_t* entries_host);
+int32_t ckks_ksk_destroy(ckks_ksk* key);
+
+/* ---------------------------------------------------------- rotations ----
+ * Key-switched Galois automorphism of n_ct ciphertexts [n_ct][2][q_limbs][N]
+ * (coefficient domain) with one key; the output stays at the same level.
+ * Replaces apply_hybrid_rns_galois_automorphism_{with_prepared_ntt,
+ * prepared_qp} and rotate_{left,right}_hybrid_rns_ckks_with_prepared_ntt
+ * (ckks/hybrid_rns_galois_key.rs:202-273, 293-521). in != out. */
+int32_t ckks_rotate(ckks_ctx* ctx, const ckks_ksk* key, const uint64_t* ct_in, uint64_t* ct_out, uint32_t n_ct,
+                    void* stream);
+/* Hoisted rotations: one decomposition per ciphertext shared by n_keys Galois
+ * keys (all of one kind, level and gadget). out [n_ct][n_keys][2][q_limbs][N].
+ * Bounded keys: digits re-normalised per key exactly as
+ * BoundedGadgetDecomposition::automorphism_hoisted (bounded_gadget.rs:273-312),
+ * so every word equals the non-hoisted rotation. */
+int32_t ckks_rotate_hoisted(ckks_ctx* ctx, const ckks_ksk* const* keys, uint32_t n_keys, const uint64_t* ct_in,
+                            uint64_t* ct_out, uint32_t n_ct, void* stream);
+/* Host-buffer form of ckks_rotate_hoisted (copies in, rotates, copies out). */
+int32_t ckks_rotate_hoisted_host(ckks_ctx* ctx, const ckks_ksk* const* keys, uint32_t n_keys,
+                                 const uint64_t* ct_in_host, uint64_t* ct_out_host, uint32_t n_ct);
 
 #ifdef __cplusplus
 }
