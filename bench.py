@@ -282,12 +282,103 @@ def reference_arm(args, world, rank):
     }
 
 
+# -------------------------------------------------------------- rotations
+ROT_LOG_N, ROT_L, ROT_K, ROT_QBITS, ROT_PBITS, ROT_BASE_LOG, ROT_NCT = 16, 24, 3, 50, 60, 32, 16
+# 32 distinct Galois steps: powers of two 1..2^14 and odd steps 3, 5, .., 35
+ROT_STEPS = [1 << i for i in range(15)] + list(range(3, 37, 2))
+
+
+def rot_config():
+    return {"workload": "hoisted key-switched rotations, N=2^16, 24x50-bit Q + 3x60-bit P, "
+                        "bounded hybrid-QP gadget base 2^32 (38 digits), 16 ct x 32 Galois steps",
+            "log_n": ROT_LOG_N, "q_limbs": ROT_L, "p_limbs": ROT_K, "base_log": ROT_BASE_LOG,
+            "ciphertexts": ROT_NCT, "galois_steps": ROT_STEPS, "scale": "2^50", "secret": "ternary",
+            "sigma": 3.2, "l2": "keys (34 GB) and outputs larger than L2", "parallelism": "replicas"}
+
+
+def bench_rot_gpu(args, world, rank, local):
+    import torch
+    import ckks_b200 as cb
+    import ckks_b200.params as params
+    dev = torch.device("cuda", local)
+    n = 1 << ROT_LOG_N
+    q = params.primes_below_bits(ROT_QBITS, n, ROT_L)
+    p = params.primes_below_bits(ROT_PBITS, n, ROT_K)
+    ctx = cb.Context(ROT_LOG_N, q, p)
+    rng = np.random.default_rng(4321 + rank)
+    secret = rng.integers(-1, 2, n).astype(np.int8)
+    exps = [ctx.rotation_exponent_left(r) for r in ROT_STEPS]
+    keys = [cb.KeySwitchKey.hybrid_generate(ctx, ROT_L, ROT_BASE_LOG, k, secret, seed=1000 + i)
+            for i, k in enumerate(exps)]
+    D, words = keys[0].info()
+    # ciphertexts: uniform residues (the distribution of fresh RLWE ciphertexts)
+    host = np.stack([np.stack([rng.integers(0, m, (2, n), dtype=np.uint64) for m in q], axis=1)
+                     for _ in range(ROT_NCT)])
+    cts = cb.as_u64_tensor(host, dev)
+    out = torch.empty((ROT_NCT, len(keys), 2, ROT_L, n), dtype=torch.int64, device=dev)
+    st = torch.cuda.current_stream()
+
+    def step():
+        cb.rotate_hoisted(ctx, keys, cts, out=out)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(st)
+    for _ in range(args.steps):
+        step()
+    t1.record(st)
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = t0.elapsed_time(t1)
+    clk = clocks.stop()
+    ms_max = max_over_ranks(world, ms)
+    rots = ROT_NCT * len(keys)
+    value = rots * args.steps * world / (ms_max / 1000.0)
+    # roofline of the whole rotation: key + ciphertext in/out bytes per rotation
+    key_bytes = words * 8
+    ct_bytes = 2 * ROT_L * n * 8
+    alg_bytes = key_bytes + 2 * ct_bytes
+    peak, kind = peaks()
+    achieved = alg_bytes * rots * args.steps / (ms / 1000.0) / 1e9
+    # end to end through the C ABI host-buffer call (pinned host memory)
+    pin_in = torch.from_numpy(host.view(np.int64)).pin_memory()
+    pin_out = torch.empty(tuple(out.shape), dtype=torch.int64).pin_memory()
+    hin, hout = pin_in.numpy().view(np.uint64), pin_out.numpy().view(np.uint64)
+    cb.rotate_hoisted_host(ctx, keys, hin, hout)
+    barrier(world)
+    e2e_steps = max(1, min(args.steps, 3))
+    t = time.perf_counter()
+    for _ in range(e2e_steps):
+        cb.rotate_hoisted_host(ctx, keys, hin, hout)
+    e2e_s = max_over_ranks(world, time.perf_counter() - t)
+    line = {
+        "metric": "key-switched rotations/s (N=2^16, 24 limbs, hoisted, bit-exact)", "value": value,
+        "unit": "rotations/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u64", "data": "synthetic (seeded uniform ciphertexts, GPU-generated keys)", "config": rot_config(),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_kind": kind,
+                     "kernel": "whole rotation: %d-digit key (%.3f GB) + ct in/out per rotation" % (D, key_bytes / 1e9)},
+        "e2e": {"value": rots * e2e_steps * world / e2e_s, "unit": "rotations/s",
+                "h2d_bytes_per_step": int(host.nbytes), "d2h_bytes_per_step": int(hout.nbytes),
+                "path": "ckks_rotate_hoisted_host"},
+        "gpu_launches": None, "clocks": clk,
+    }
+    return line
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="ntt", choices=["ntt"])
+    ap.add_argument("--workload", default="rotation", choices=["rotation", "ntt"])
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -298,7 +389,13 @@ def main():
         if line:
             print(json.dumps(line), flush=True)
         return
-    line = bench_ntt_gpu(args, world, rank, local)
+    if args.workload == "ntt":
+        line = bench_ntt_gpu(args, world, rank, local)
+    else:
+        line = bench_rot_gpu(args, world, rank, local)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        return
     if rank == 0:
         threads = os.cpu_count() or 1
         v, sample = ntt_cpu_sample(threads, seconds_target=10.0)

@@ -71,45 +71,43 @@ u32 brev(u32 x, int bits) {
 
 // Host tables of one modulus, in the order of the device layout.
 struct HostTables {
-    std::vector<u64> psi_rev, psi_inv_rev, w, w_inv, mid, imid;
+    std::vector<u64> psiA, psiA_inv, psiB, psiB_inv, mid, midi;
 };
 
-void build_tables(u64 q, u64 psi, u32 log_n1, u32 log_n2, HostTables& t) {
-    const u32 N1 = 1u << log_n1, N2 = 1u << log_n2, N = N1 * N2;
-    u64 psi_inv = invmod(psi, q), n_inv = invmod(N % q, q);
-    u64 psi2 = powmod(psi, N1, q), psi2_inv = invmod(psi2, q);
-    u64 w1 = powmod(psi, 2ull * N2, q), w1_inv = invmod(w1, q);
-    t.psi_rev.resize(N2);
-    t.psi_inv_rev.resize(N2);
-    for (u32 i = 0; i < N2; ++i) {
-        t.psi_rev[i] = powmod(psi2, brev(i, log_n2), q);
-        t.psi_inv_rev[i] = powmod(psi2_inv, brev(i, log_n2), q);
+void build_tables(u64 q, u64 psi, u32 log_n, HostTables& t) {
+    const u32 la = log_n - log_n / 2, lb = log_n / 2, A = 1u << la, B = 1u << lb, N = A * B;
+    const u64 two_n = 2ull * N;
+    std::vector<u64> pw(two_n);
+    u64 v = 1;
+    for (u64 e = 0; e < two_n; ++e) {
+        pw[e] = v;
+        v = mulmod(v, psi, q);
     }
-    t.w.resize(N1 / 2);
-    t.w_inv.resize(N1 / 2);
-    u64 a = 1, b = 1;
-    for (u32 i = 0; i < N1 / 2; ++i) {
-        t.w[i] = a;
-        t.w_inv[i] = b;
-        a = mulmod(a, w1, q);
-        b = mulmod(b, w1_inv, q);
+    auto P = [&](u64 e) { return pw[e % two_n]; };
+    t.psiA.resize(A);
+    t.psiA_inv.resize(A);
+    for (u32 i = 0; i < A; ++i) {  // psi_A = psi^B
+        u64 r = brev(i, (int)la);
+        t.psiA[i] = P((u64)B * r);
+        t.psiA_inv[i] = P(two_n - ((u64)B * r) % two_n);
     }
+    t.psiB.resize(B);
+    t.psiB_inv.resize(B);
+    for (u32 i = 0; i < B; ++i) {  // psi_2B = psi^A
+        u64 r = brev(i, (int)lb);
+        t.psiB[i] = P((u64)A * r);
+        t.psiB_inv[i] = P(two_n - ((u64)A * r) % two_n);
+    }
+    u64 ninv = invmod(N % q, q);
     t.mid.resize(N);
-    t.imid.resize(N);
-    for (u32 j1 = 0; j1 < N1; ++j1) {  // psi^((2k2+1) j1)
-        u64 v = powmod(psi, j1, q), step = mulmod(v, v, q);
-        for (u32 k2 = 0; k2 < N2; ++k2) {
-            t.mid[(size_t)j1 * N2 + k2] = v;
-            v = mulmod(v, step, q);
+    t.midi.resize(N);
+    for (u32 jl = 0; jl < B; ++jl)
+        for (u32 ka = 0; ka < A; ++ka) {
+            // exponent (2k_a + 1 - A) j_lo mod 2N
+            u64 e = ((2ull * ka + 1 + two_n - A) % two_n) * jl % two_n;
+            t.mid[(size_t)jl * A + ka] = P(e);
+            t.midi[(size_t)ka * B + jl] = mulmod(ninv, P((two_n - e) % two_n), q);
         }
-    }
-    for (u32 k2 = 0; k2 < N2; ++k2) {  // N^-1 psi^-((2k2+1) j1)
-        u64 base = powmod(psi_inv, 2ull * k2 + 1, q), v = n_inv;
-        for (u32 j1 = 0; j1 < N1; ++j1) {
-            t.imid[(size_t)k2 * N1 + j1] = v;
-            v = mulmod(v, base, q);
-        }
-    }
 }
 
 // Rescale, ModDown, P-factor and Q-Garner constants (device copies).
@@ -281,13 +279,12 @@ int32_t ckks_ctx_create(uint32_t log_n, const uint64_t* q, uint32_t L, const uin
         for (size_t i = 0; i < M; ++i)
             th.emplace_back([&, i]() {
                 ctx->psi[i] = find_root(mod[i], n);
-                build_tables(mod[i], ctx->psi[i], ctx->log_n1, ctx->log_n2, ht[i]);
+                build_tables(mod[i], ctx->psi[i], ctx->log_n, ht[i]);
             });
         for (auto& t : th) t.join();
     }
-    const u32 N1 = 1u << ctx->log_n1, N2 = 1u << ctx->log_n2;
-    // per modulus: 2*(N2 + N2 + N1/2 + N1/2 + N + N) words (value + Shoup)
-    const size_t per = 2 * (2 * (size_t)N2 + N1 + 2 * (size_t)n);
+    // per modulus: value + Shoup of psiA, psiA_inv (A), psiB, psiB_inv (B), mid, midi (N)
+    const size_t per = 4 * ((size_t)(1u << ctx->log_n1) + (1u << ctx->log_n2) + n);
     std::vector<u64> host(per * M);
     ctx->h_tabs.resize(M);
     if (cudaMalloc(&ctx->d_table_mem, host.size() * sizeof(u64)) != cudaSuccess ||
@@ -312,12 +309,12 @@ int32_t ckks_ctx_create(uint32_t log_n, const uint64_t* q, uint32_t L, const uin
             *quo = ctx->d_table_mem + off + v.size();
             off += 2 * v.size();
         };
-        put(ht[i].psi_rev, &T.psi_rev, &T.psi_rev_q);
-        put(ht[i].psi_inv_rev, &T.psi_inv_rev, &T.psi_inv_rev_q);
-        put(ht[i].w, &T.w, &T.w_q);
-        put(ht[i].w_inv, &T.w_inv, &T.w_inv_q);
+        put(ht[i].psiA, &T.psiA, &T.psiA_q);
+        put(ht[i].psiA_inv, &T.psiA_inv, &T.psiA_inv_q);
+        put(ht[i].psiB, &T.psiB, &T.psiB_q);
+        put(ht[i].psiB_inv, &T.psiB_inv, &T.psiB_inv_q);
         put(ht[i].mid, &T.mid, &T.mid_q);
-        put(ht[i].imid, &T.imid, &T.imid_q);
+        put(ht[i].midi, &T.midi, &T.midi_q);
     }
     if (cudaMemcpy(ctx->d_table_mem, host.data(), host.size() * sizeof(u64), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(ctx->d_tabs, ctx->h_tabs.data(), M * sizeof(NttTab), cudaMemcpyHostToDevice) != cudaSuccess ||

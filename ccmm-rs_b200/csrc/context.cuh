@@ -12,20 +12,17 @@
 #include "../../include/ckks_b200.h"
 
 
-// Per-modulus NTT tables (device pointers). N = N1 * N2 with N2 = 2^floor(logN/2).
-// The forward transform is the two-pass decomposition
-//   A[k2 + N2 k1] = sum_j1 w1^(j1 k1) psi^((2k2+1) j1) sum_j2 a[j1 + N1 j2] psi2^((2k2+1) j2)
-// with psi2 = psi^N1 (order 2 N2) and w1 = psi^(2 N2) (order N1), which equals
-// the reference definition A[k] = a(psi^(2k+1)) (ring/ntt.rs:101-127).
+// Per-modulus NTT tables (device pointers) of the twisted four-step
+// transform N = A * B: psi_A^bitrev and psi_A^-bitrev (A entries, psi_A =
+// psi^B), psi_2B^bitrev and psi_2B^-bitrev (B entries, psi_2B = psi^A), the
+// twist mid[j_lo][k_a] = psi^((2k_a+1-A) j_lo) and the inverse twist
+// midi[k_a][j_lo] = N^-1 psi^-((2k_a+1-A) j_lo), each with Shoup companions.
 struct NttTab {
     u64 q;
-    u64 mu_hi, mu_lo;                       // Barrett floor(2^128/q)
-    const u64 *psi_rev, *psi_rev_q;         // [N2] psi2^bitrev(i)     (forward pass 1)
-    const u64 *psi_inv_rev, *psi_inv_rev_q; // [N2] psi2^-bitrev(i)    (inverse pass B)
-    const u64 *w, *w_q;                     // [N1/2] w1^i             (forward pass 2)
-    const u64 *w_inv, *w_inv_q;             // [N1/2] w1^-i            (inverse pass A)
-    const u64 *mid, *mid_q;                 // [N1][N2] psi^((2k2+1) j1)
-    const u64 *imid, *imid_q;               // [N2][N1] N^-1 psi^-((2k2+1) j1)
+    u64 mu_hi, mu_lo;  // Barrett floor(2^128/q)
+    const u64 *psiA, *psiA_q, *psiA_inv, *psiA_inv_q;
+    const u64 *psiB, *psiB_q, *psiB_inv, *psiB_inv_q;
+    const u64 *mid, *mid_q, *midi, *midi_q;
 };
 
 constexpr int kMaxAux = 8;  // auxiliary (P) limbs

@@ -157,7 +157,11 @@ __global__ void __launch_bounds__(kT) k_bounded_decompose(const u64* __restrict_
         if (d == -half) flag = 1;
         digits[dbase + ((size_t)j << log_n) + c] = d;
     }
-    if (flags) flags[(size_t)blockIdx.y * n + c] = flag;
+    if (flags && flag) {  // list of coefficients holding a -B/2 digit: [count][indices]
+        u32* fl = flags + (size_t)blockIdx.y * (n + 1);
+        u32 slot = atomicAdd(fl, 1u);
+        fl[1 + slot] = c;
+    }
 }
 
 // automorphism_hoisted (bounded_gadget.rs:273-312), output-driven:

@@ -1,0 +1,273 @@
+// hoisted.cu -- NTT-domain hoisting of the bounded hybrid-QP rotation.
+//
+// The reference hoists at the digit level (BoundedGadgetDecomposition::
+// automorphism_hoisted, grafting/bounded_gadget.rs:273-312) and transforms the
+// re-normalised digits for every Galois element. Those digits equal the
+// signed automorphism of the digits of a, sigma(d_j), except at coefficients
+// whose source value is negated and holds a digit equal to -B/2: there the
+// carry re-normalisation changes a few digits by Delta. Since
+// NTT(sigma(d_j)) is the NTT-domain permutation of NTT(d_j)
+// (ring/ntt_galois_permutation.rs:5-19), the exact key-switch sum is
+//   sum_j NTT(d_j)[pi(k)] K_j[k] + sum_{(t,j,Delta)} Delta psi^((2k+1) t) K_j[k],
+// so the digit transforms are done once per ciphertext, and every Galois
+// element costs one MAC pass plus the (rare, sparse) correction terms. A
+// (ciphertext, Galois element) pair whose corrections exceed the list
+// capacity is recomputed by the non-hoisted path, so every output word equals
+// the reference's.
+//
+// The MAC streams each key slice once per group of G ciphertexts (evict-first
+// loads) while the hoisted digit transforms of the group stay L2-resident
+// and are gathered through the permutation.
+#include "keyswitch.cuh"
+
+namespace {
+
+constexpr int kT = 256;
+
+struct Exc {
+    u32 t, j;
+    i64 delta;
+};
+
+// Reduce x = xhi * 2^64 + xlo (xhi < q) modulo q (Barrett, mu = floor(2^128/q)).
+__device__ __forceinline__ u64 reduce_wide(u64 xhi, u64 xlo, u64 q, u64 mu_hi, u64 mu_lo) {
+    u64 p0_hi = __umul64hi(xlo, mu_lo);
+    u64 p1_lo = xlo * mu_hi, p1_hi = __umul64hi(xlo, mu_hi);
+    u64 p2_lo = xhi * mu_lo, p2_hi = __umul64hi(xhi, mu_lo);
+    u64 mid = p0_hi + p1_lo;
+    u64 c = mid < p0_hi;
+    u64 mid2 = mid + p2_lo;
+    c += mid2 < mid;
+    u64 qt = xhi * mu_hi + p1_hi + p2_hi + c;
+    u64 r = xlo - qt * q;
+    while (r >= q) r -= q;
+    return r;
+}
+
+struct Acc {
+    u64 hi, lo;
+    __device__ __forceinline__ void mac(u64 a, u64 b) {
+        u64 pl = a * b, ph = __umul64hi(a, b);
+        lo += pl;
+        hi += ph + (lo < pl);
+    }
+    __device__ __forceinline__ void fold(u64 q, u64 mh, u64 ml) {
+        u64 h = hi >= q ? reduce_wide(0, hi, q, mh, ml) : hi;
+        lo = reduce_wide(h, lo, q, mh, ml);
+        hi = 0;
+    }
+};
+
+__device__ __forceinline__ u64 pow_mod_dev(u64 b, u64 e, const Barrett& m) {
+    u64 r = 1;
+    while (e) {
+        if (e & 1) r = mul_barrett(r, b, m);
+        b = mul_barrett(b, b, m);
+        e >>= 1;
+    }
+    return r;
+}
+
+// Flagged source coefficients (a digit equals -B/2) of G ciphertexts ->
+// exception lists per (ciphertext, key): entries (t, j, Delta) where the
+// reference's re-normalised digit differs from -d_j[s].
+__global__ void k_hoist_exceptions(const i64* __restrict__ digits, size_t dig_stride, const u32* __restrict__ flags,
+                                   size_t flag_stride, const u64* __restrict__ exps, int n_keys, int D, int base_log,
+                                   int log_n, Exc* __restrict__ exc, u32* __restrict__ exc_count, int cap) {
+    const int c = blockIdx.z, g = blockIdx.y;
+    const u32* fl = flags + c * flag_stride;
+    const u32 nflag = fl[0];
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nflag) return;
+    const u32 n = 1u << log_n;
+    const u32 s = fl[1 + i];
+    const u64 mapped = ((u64)s * exps[g]) & (2ull * n - 1);
+    if (mapped < n) return;  // not negated: digits move unchanged
+    const u32 t = (u32)(mapped - n);
+    const i64* d = digits + c * dig_stride;
+    const i64 B = (i64)1 << base_log, half = B >> 1;
+    i64 carry = 0;
+    Exc* list = exc + ((size_t)c * n_keys + g) * cap;
+    u32* cnt = exc_count + (size_t)c * n_keys + g;
+    for (int j = 0; j < D; ++j) {
+        i64 dj = d[((size_t)j << log_n) + s];
+        i64 value = -dj + carry;
+        i64 m = (value + half) & (B - 1);
+        i64 normalized = m - half;
+        carry = (value - normalized) >> base_log;
+        i64 delta = normalized + dj;  // reference digit minus the naive -d_j
+        if (delta != 0) {
+            u32 slot = atomicAdd(cnt, 1u);
+            if ((int)slot < cap) list[slot] = Exc{t, (u32)j, delta};
+        }
+    }
+}
+
+// acc[c][g][0][l][k] = pf_l Bhat_c[l][pi_g(k)] + sum_j Yhat_c[j][l][pi_g(k)] key_g[j][l][0][k] + corrections
+// acc[c][g][1][l][k] =                             sum_j Yhat_c[j][l][pi_g(k)] key_g[j][l][1][k] + corrections
+template <int G>
+__global__ void __launch_bounds__(kT) k_mac_hoisted(const u64* __restrict__ Yhat, size_t y_stride,
+                                                    const u64* __restrict__ Bhat, size_t b_stride,
+                                                    const u64* const* __restrict__ keys, const u64* __restrict__ exps,
+                                                    const u64* __restrict__ pf, const u64* __restrict__ pf_q,
+                                                    u64* __restrict__ acc, const NttTab* __restrict__ tabs, LimbMap lm,
+                                                    int n_ct, int n_keys, int Lq, int LK, int D, int log_n,
+                                                    const Exc* __restrict__ exc, const u32* __restrict__ exc_count,
+                                                    int cap, const u64* __restrict__ psi) {
+    const u32 n = 1u << log_n;
+    const u32 k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int g = blockIdx.y, l = blockIdx.z;
+    if (k >= n) return;
+    const NttTab& T = tabs[lm(l)];
+    const u64 q = T.q, mh = T.mu_hi, ml = T.mu_lo;
+    const u32 src = galois_src(k, exps[g], log_n);
+    const u64* key = keys[g];
+    Acc ab[G], aa[G];
+#pragma unroll
+    for (int c = 0; c < G; ++c) ab[c] = aa[c] = Acc{0, 0};
+    int since = 0;
+    for (int j = 0; j < D; ++j) {
+        const size_t kofs = (((size_t)j * LK + l) * 2) << log_n;
+        const u64 kb = __ldcs(key + kofs + k), ka = __ldcs(key + kofs + n + k);
+        const size_t yofs = (((size_t)j * LK + l) << log_n) + src;
+#pragma unroll
+        for (int c = 0; c < G; ++c) {
+            if (c < n_ct) {
+                u64 y = __ldg(Yhat + c * y_stride + yofs);
+                ab[c].mac(y, kb);
+                aa[c].mac(y, ka);
+            }
+        }
+        if (++since == 15) {
+#pragma unroll
+            for (int c = 0; c < G; ++c) {
+                ab[c].fold(q, mh, ml);
+                aa[c].fold(q, mh, ml);
+            }
+            since = 0;
+        }
+    }
+    const Barrett bm{q, mh, ml};
+#pragma unroll
+    for (int c = 0; c < G; ++c) {
+        if (c >= n_ct) break;
+        ab[c].fold(q, mh, ml);
+        aa[c].fold(q, mh, ml);
+        u64 b = ab[c].lo, a = aa[c].lo;
+        if (l < Lq) b = add_mod(b, mul_shoup(__ldg(Bhat + c * b_stride + ((size_t)l << log_n) + src), pf[l], pf_q[l], q), q);
+        const u32 cnt = min(exc_count[(size_t)c * n_keys + g], (u32)cap);
+        if (cnt) {
+            const Exc* list = exc + ((size_t)c * n_keys + g) * cap;
+            const u64 ps = psi[lm(l)];
+            for (u32 e = 0; e < cnt; ++e) {
+                const Exc x = list[e];
+                // NTT of Delta * X^t at slot k: Delta * psi^((2k+1) t)
+                u64 w = pow_mod_dev(ps, ((2ull * k + 1) * x.t) & (2ull * n - 1), bm);
+                u64 dm = x.delta < 0 ? q - ((u64)(-x.delta) % q) : ((u64)x.delta % q);
+                dm = dm == q ? 0 : dm;
+                u64 v = mul_barrett(w, dm, bm);
+                const size_t kofs = (((size_t)x.j * LK + l) * 2) << log_n;
+                b = add_mod(b, mul_barrett(v, key[kofs + k], bm), q);
+                a = add_mod(a, mul_barrett(v, key[kofs + n + k], bm), q);
+            }
+        }
+        const size_t obase = (((size_t)c * n_keys + g) * 2 * LK) << log_n;
+        acc[obase + ((size_t)l << log_n) + k] = b;
+        acc[obase + (((size_t)LK + l) << log_n) + k] = a;
+    }
+}
+
+}  // namespace
+
+// Hoisted hybrid rotations of n_ct ciphertexts by n_keys Galois keys (bounded
+// or RNS-block gadget), out [n_ct][n_keys][2][Lq][N]. Ciphertexts are
+// processed in groups of up to 4 sharing each streamed key slice.
+int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_keys, const u64* ct_in,
+                                   u64* ct_out, u32 n_ct, cudaStream_t st) {
+    const ckks_ksk* k0 = keys[0];
+    const u32 Lq = k0->q_limbs, LK = ksk_limbs(k0), D = k0->D, n = ctx->n;
+    const size_t ct_words = (size_t)2 * Lq * n;
+    const bool bounded = k0->kind == CKKS_KSK_HYBRID_BOUNDED;
+    const u32 G = n_ct >= 4 ? 4 : n_ct;
+    const int cap = 1024;
+    const LimbMap lq = LimbMap::range(0, Lq), lqp = LimbMap::qp(ctx, Lq);
+    const size_t y_stride = (size_t)D * LK * n, b_stride = (size_t)Lq * n, d_stride = (size_t)D * n,
+                 f_stride = (size_t)n + 1;
+    Workspace<u64> Y, Bh, acc, Z, karr;
+    Workspace<i64> dig;
+    Workspace<u32> flags, cnt;
+    Workspace<Exc> exc;
+    int32_t rc;
+    if ((rc = Y.alloc(G * y_stride, st)) || (rc = Bh.alloc(G * b_stride, st)) ||
+        (rc = acc.alloc((size_t)G * n_keys * 2 * LK * n, st)) || (rc = Z.alloc((size_t)G * n_keys * 2 * LK * n, st)) ||
+        (rc = karr.alloc(2 * (size_t)n_keys + ctx->moduli.size(), st)) || (rc = dig.alloc(G * d_stride, st)) ||
+        (rc = flags.alloc(G * f_stride, st)) || (rc = cnt.alloc((size_t)G * n_keys, st)) ||
+        (rc = exc.alloc((size_t)G * n_keys * cap, st)))
+        return rc;
+    // key pointers, exponents and psi per modulus
+    std::vector<u64> hk(2 * (size_t)n_keys + ctx->moduli.size());
+    for (u32 g = 0; g < n_keys; ++g) {
+        hk[g] = (u64)(uintptr_t)keys[g]->d_entries;
+        hk[n_keys + g] = keys[g]->exponent;
+    }
+    for (size_t i = 0; i < ctx->moduli.size(); ++i) hk[2 * n_keys + i] = ctx->psi[i];
+    CKKS_CUDA_TRY(cudaMemcpyAsync(karr.p, hk.data(), hk.size() * 8, cudaMemcpyHostToDevice, st));
+    const u64* const* d_keys = (const u64* const*)karr.p;
+    const u64* d_exps = karr.p + n_keys;
+    const u64* d_psi = karr.p + 2 * n_keys;
+    std::vector<u32> overflow;
+    std::vector<u32> h_cnt((size_t)G * n_keys);
+    for (u32 c0 = 0; c0 < n_ct; c0 += G) {
+        const u32 gn = (n_ct - c0) < G ? (n_ct - c0) : G;
+        CKKS_CUDA_TRY(cudaMemsetAsync(flags.p, 0, G * f_stride * sizeof(u32), st));
+        CKKS_CUDA_TRY(cudaMemsetAsync(cnt.p, 0, (size_t)G * n_keys * sizeof(u32), st));
+        for (u32 c = 0; c < gn; ++c) {
+            const u64* in = ct_in + (size_t)(c0 + c) * ct_words;
+            if (bounded) {
+                if ((rc = bounded_decompose_launch(ctx, in + (size_t)Lq * n, 1, Lq, k0->base_log, dig.p + c * d_stride,
+                                                   flags.p + c * f_stride, st)))
+                    return rc;
+                if ((rc = ntt_forward_digits_launch(ctx, dig.p + c * d_stride, Y.p + c * y_stride, D, lqp, LK, st)))
+                    return rc;
+            } else {  // RNS blocks: ModUp of a, then transform (the permutation is the whole automorphism)
+                if ((rc = rnsblock_modup_launch(ctx, k0, in + (size_t)Lq * n, Y.p + c * y_stride, st))) return rc;
+                if ((rc = ntt_forward_launch_map(ctx, Y.p + c * y_stride, Y.p + c * y_stride, D, lqp, LK, st))) return rc;
+            }
+            if ((rc = ntt_forward_launch_map(ctx, in, Bh.p + c * b_stride, 1, lq, Lq, st))) return rc;
+        }
+        if (bounded) {
+            dim3 g((n + kT - 1) / kT, n_keys, gn);
+            k_hoist_exceptions<<<g, kT, 0, st>>>(dig.p, d_stride, flags.p, f_stride, d_exps, n_keys, D,
+                                                 k0->base_log, ctx->log_n, exc.p, cnt.p, cap);
+        }
+        {
+            dim3 g((n + kT - 1) / kT, n_keys, LK);
+#define CKKS_MAC(GG)                                                                                               \
+    k_mac_hoisted<GG><<<g, kT, 0, st>>>(Y.p, y_stride, Bh.p, b_stride, d_keys, d_exps, ctx->d_pmodq,                \
+                                        ctx->d_pmodq + ctx->L, acc.p, ctx->d_tabs, lqp, gn, n_keys, Lq, LK, D,      \
+                                        ctx->log_n, exc.p, cnt.p, cap, d_psi)
+            if (G >= 3) CKKS_MAC(4);
+            else if (G == 2) CKKS_MAC(2);
+            else CKKS_MAC(1);
+#undef CKKS_MAC
+        }
+        CKKS_CUDA_TRY(cudaGetLastError());
+        if ((rc = ntt_inverse_launch_map(ctx, acc.p, Z.p, gn * n_keys * 2, lqp, LK, st))) return rc;
+        // ModDown of every (ciphertext, key) pair straight into the output
+        if ((rc = mod_down_launch(ctx, Z.p, ct_out + (size_t)c0 * n_keys * ct_words, gn * n_keys * 2, Lq, st)))
+            return rc;
+        // pairs whose correction lists overflowed are recomputed exactly
+        CKKS_CUDA_TRY(cudaMemcpyAsync(h_cnt.data(), cnt.p, (size_t)G * n_keys * sizeof(u32), cudaMemcpyDeviceToHost, st));
+        CKKS_CUDA_TRY(cudaStreamSynchronize(st));
+        for (u32 c = 0; c < gn; ++c)
+            for (u32 g = 0; g < n_keys; ++g)
+                if (h_cnt[(size_t)c * n_keys + g] > (u32)cap) overflow.push_back(((c0 + c) << 16) | g);
+    }
+    for (u32 code : overflow) {
+        const u32 c = code >> 16, g = code & 0xffff;
+        if ((rc = rotate_hybrid(ctx, keys[g], ct_in + (size_t)c * ct_words,
+                                ct_out + ((size_t)c * n_keys + g) * ct_words, 1, st)))
+            return rc;
+    }
+    return CKKS_OK;
+}

@@ -376,6 +376,14 @@ int32_t rotate_hybrid(ckks_ctx* ctx, const ckks_ksk* key, const u64* ct_in, u64*
 // and the key switch. out layout [n_ct][n_keys][2][Lq][N].
 int32_t rotate_hybrid_hoisted(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_keys, const u64* ct_in, u64* ct_out,
                               u32 n_ct, cudaStream_t st) {
+    return rotate_hoisted_ntt(ctx, keys, n_keys, ct_in, ct_out, n_ct, st);
+}
+
+// Digit-level hoisting (the reference's own structure): one decomposition per
+// ciphertext, re-normalised digits and their transforms per Galois element.
+// Kept as the reference-order path for differential tests.
+int32_t rotate_hybrid_hoisted_digits(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_keys, const u64* ct_in,
+                                     u64* ct_out, u32 n_ct, cudaStream_t st) {
     const ckks_ksk* k0 = keys[0];
     const u32 Lq = k0->q_limbs, LK = ksk_limbs(k0), D = k0->D, n = ctx->n;
     const size_t ct_words = (size_t)2 * Lq * n;

@@ -38,6 +38,10 @@ int32_t rnsblock_modup_launch(ckks_ctx* ctx, const ckks_ksk* key, const u64* a, 
 int32_t ks_mac_launch(ckks_ctx* ctx, const u64* Y, const u64* key, const u64* base, u64* acc, u32 q_limbs, u32 D,
                       bool with_p, u64 perm_y, u64 perm_b, cudaStream_t st);
 int32_t rotate_hybrid(ckks_ctx* ctx, const ckks_ksk* key, const u64* ct_in, u64* ct_out, u32 n_ct, cudaStream_t st);
+int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_keys, const u64* ct_in, u64* ct_out,
+                           u32 n_ct, cudaStream_t st);
+int32_t rotate_hybrid_hoisted_digits(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_keys, const u64* ct_in,
+                                     u64* ct_out, u32 n_ct, cudaStream_t st);
 int32_t rotate_hybrid_hoisted(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_keys, const u64* ct_in, u64* ct_out,
                               u32 n_ct, cudaStream_t st);
 

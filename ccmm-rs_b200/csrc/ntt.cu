@@ -1,232 +1,298 @@
 // ntt.cu -- batched negacyclic NTT / inverse NTT for sm_100a.
 //
-// Two passes over HBM per transform (N = N1 * N2, both <= 512 for N <= 2^17):
-//   forward pass 1: per column j1, a merged Cooley-Tukey negacyclic N2-point
-//                   transform along j2 (psi2 = psi^N1), times psi^((2k2+1) j1);
-//                   written as rows [j1][k2];
-//   forward pass 2: per column k2, a cyclic N1-point DIT transform along j1
-//                   (w1 = psi^(2 N2)); written in natural order k2 + N2 k1.
-// The inverse runs the mirror image (Gentleman-Sande).
-// Each CTA stages a tile of C (<= 16) columns in shared memory; butterflies
-// keep values lazily reduced in [0, 4q) with Shoup multiplication
-// (__umul64hi); outputs are canonical. Result values equal the reference's
-// PreparedNttPlan::forward (ring/prepared_ntt.rs:200-231) word for word:
-// both compute the unique A[k] = a(psi^(2k+1)) mod q.
-#include "kernels.cuh"
+// Twisted four-step form, N = A * B (A = 2^ceil(logN/2), B = 2^floor(logN/2)),
+// input index j = j_lo + B i, output index k = k_a + A k_b:
+//   A[k_a + A k_b] = sum_{j_lo} psi_2B^((2k_b+1) j_lo) * [psi^((2k_a+1-A) j_lo)
+//                    * sum_i a[j_lo + B i] psi_A^((2k_a+1) i)]
+// with psi_A = psi^B and psi_2B = psi^A, which is the reference definition
+// A[k] = a(psi^(2k+1)) (ring/ntt.rs:101-127) regrouped.
+//   forward pass 1 (column j_lo): A-point negacyclic merged CT, twist, store
+//     row j_lo (A contiguous words);
+//   forward pass 2 (unit k_a): B-point negacyclic merged CT over {k_a + A j_lo},
+//     written back to the same addresses in natural order (in-place safe).
+//   The inverse runs the merged GS networks in the opposite order with the
+//   inverse twist (N^-1 folded in).
+// Both passes use small tables (A or B entries of psi^bitrev with Shoup
+// companions, staged in shared memory); the twist is one coalesced N-entry
+// table. Each CTA handles C columns (or units); a thread holds R1 points in
+// registers for the first half of the stages and R2 for the second, with one
+// shared-memory exchange, and every global access is a 128-byte segment.
+// Butterflies are Harvey-lazy in [0, 4q) with Shoup multiplication
+// (__umul64hi); outputs are canonical.
+#include "ntt_core.cuh"
 
 namespace {
 
-constexpr int kThreads = 256;
+using nttc::brev;
 
-__device__ __forceinline__ u32 bitrev(u32 x, int bits) { return __brev(x) >> (32 - bits); }
+constexpr int kMaxThreads = 256;
 
-// Row-dependent XOR swizzle of the column index inside a [rows][C] tile so
-// that reading one column across bit-reversed rows is bank-conflict free.
-__device__ __forceinline__ int swz(u32 row, int log_rows, int C) { return (int)(bitrev(row, log_rows) & (C - 1)); }
+template <int LOG_M>
+struct Split {
+    static constexpr int M = 1 << LOG_M;
+    static constexpr int LR1 = (LOG_M + 1) / 2, LR2 = LOG_M / 2;
+    static constexpr int R1 = 1 << LR1, R2 = 1 << LR2;
+    static constexpr int RMAX = R1 > R2 ? R1 : R2;
+};
 
-// Forward pass 1: tile of C columns j1, N2 rows j2. With kDigits the input is
-// a signed digit polynomial [D][N] (int64) shared by every limb, lifted to
-// [0, q) on load (signed_mod, hybrid_rns_galois_key.rs:55-57); blockIdx.z
-// then indexes the digit.
-template <bool kDigits>
-__global__ void __launch_bounds__(kThreads) k_ntt_fwd_pass1(const void* __restrict__ in_, u64* __restrict__ out,
-                                                            const NttTab* __restrict__ tabs, LimbMap lm,
-                                                            int limb_count, int log_n1, int log_n2, int log_c) {
-    extern __shared__ u64 sm[];
-    const int N2 = 1 << log_n2, C = 1 << log_c;
-    const int limb = blockIdx.y;
-    const NttTab T = tabs[lm(limb)];
-    const u64 q = T.q, q2 = q << 1;
-    const size_t base = ((size_t)blockIdx.z * limb_count + limb) << (log_n1 + log_n2);
-    const int j1_0 = blockIdx.x << log_c;
+__device__ __forceinline__ u64 lift_digit(i64 d, u64 q) {
+    u64 a = d < 0 ? (u64)(-d) : (u64)d;
+    a = a >= q ? a % q : a;
+    return (d < 0 && a) ? q - a : a;
+}
 
-    if (kDigits) {
-        const i64* in = (const i64*)in_ + ((size_t)blockIdx.z << (log_n1 + log_n2));
-        for (int idx = threadIdx.x; idx < (N2 << log_c); idx += blockDim.x) {
-            int j2 = idx >> log_c, c = idx & (C - 1);
-            i64 d = in[j1_0 + c + ((size_t)j2 << log_n1)];
-            u64 a = d < 0 ? (u64)(-d) : (u64)d;
-            a = a >= q ? a % q : a;
-            sm[(j2 << log_c) + (c ^ swz(j2, log_n2, C))] = (d < 0 && a) ? q - a : a;
-        }
-    } else {
-        const u64* in = (const u64*)in_;
-        for (int idx = threadIdx.x; idx < (N2 << log_c); idx += blockDim.x) {
-            int j2 = idx >> log_c, c = idx & (C - 1);
-            sm[(j2 << log_c) + (c ^ swz(j2, log_n2, C))] = in[base + j1_0 + c + ((size_t)j2 << log_n1)];
-        }
-    }
-    __syncthreads();
-    // merged CT: natural in -> bit-reversed out (psi_rev holds psi2^bitrev(i))
-    for (int m = 1, lt = log_n2 - 1; m < N2; m <<= 1, --lt) {
-        for (int idx = threadIdx.x; idx < ((N2 >> 1) << log_c); idx += blockDim.x) {
-            int c = idx & (C - 1), b = idx >> log_c;
-            int i = b >> lt;
-            int r0 = (i << (lt + 1)) + (b & ((1 << lt) - 1)), r1 = r0 + (1 << lt);
-            u64 S = __ldg(T.psi_rev + m + i), Sq = __ldg(T.psi_rev_q + m + i);
-            u64* p0 = &sm[(r0 << log_c) + (c ^ swz(r0, log_n2, C))];
-            u64* p1 = &sm[(r1 << log_c) + (c ^ swz(r1, log_n2, C))];
-            u64 X = *p0, Y = *p1;
-            X = X >= q2 ? X - q2 : X;
-            u64 t = mul_shoup_lazy(Y, S, Sq, q);
-            *p0 = X + t;
-            *p1 = X - t + q2;
-        }
-        __syncthreads();
-    }
-    // twiddle psi^((2k2+1) j1), store rows [j1][k2] (lazy, [0, 2q))
-    for (int idx = threadIdx.x; idx < (N2 << log_c); idx += blockDim.x) {
-        int k2 = idx & (N2 - 1), c = idx >> log_n2;
-        u32 r = bitrev(k2, log_n2);
-        u64 v = sm[(r << log_c) + (c ^ (k2 & (C - 1)))];
-        size_t t = ((size_t)(j1_0 + c) << log_n2) + k2;
-        out[base + t] = mul_shoup_lazy(v, __ldg(T.mid + t), __ldg(T.mid_q + t), q);
+// Stage a small twiddle table (M values then M Shoup companions) in shared memory.
+__device__ __forceinline__ void stage_table(u64* st, const u64* __restrict__ v, const u64* __restrict__ vq, int M) {
+    for (int i = threadIdx.x; i < M; i += blockDim.x) {
+        st[i] = __ldg(v + i);
+        st[M + i] = __ldg(vq + i);
     }
 }
 
-// Forward pass 2: tile of C columns k2, N1 rows j1. The CTA reads its whole
-// tile before writing the same addresses, so src may equal dst.
-__global__ void __launch_bounds__(kThreads) k_ntt_fwd_pass2(const u64* src, u64* dst, const NttTab* __restrict__ tabs,
-                                                            LimbMap lm, int limb_count, int log_n1, int log_n2,
-                                                            int log_c) {
+// Forward pass 1 over columns j_lo: negacyclic A-point merged CT with
+// psi_A = psi^B (natural in, bit-reversed out), times the twist
+// psi^((2k_a+1-A) j_lo), stored as row j_lo in natural k_a order.
+// kDigits: the input is a signed digit polynomial [D][N] shared by every limb
+// (blockIdx.z = digit), lifted on load (signed_mod, hybrid_rns_galois_key.rs:55-57).
+template <int LOG_M, bool kDigits>
+__global__ void __launch_bounds__(kMaxThreads) k_fwd1(const void* __restrict__ in_, u64* __restrict__ out,
+                                                      const NttTab* __restrict__ tabs, LimbMap lm, int limb_count,
+                                                      int log_b, int log_c) {
+    using S = Split<LOG_M>;
     extern __shared__ u64 sm[];
-    const int N1 = 1 << log_n1, N2 = 1 << log_n2, C = 1 << log_c;
+    const int C = 1 << log_c, tid = threadIdx.x;
     const int limb = blockIdx.y;
-    const NttTab T = tabs[lm(limb)];
-    const u64 q = T.q, q2 = q << 1;
-    const size_t base = ((size_t)blockIdx.z * limb_count + limb) << (log_n1 + log_n2);
-    const int k2_0 = blockIdx.x << log_c;
-
-    for (int idx = threadIdx.x; idx < (N1 << log_c); idx += blockDim.x) {
-        int j1 = idx >> log_c, c = idx & (C - 1);
-        sm[(bitrev(j1, log_n1) << log_c) + c] = src[base + ((size_t)j1 << log_n2) + k2_0 + c];
+    const NttTab& T = tabs[lm(limb)];
+    const u64 q = T.q;
+    u64* st = sm + (S::M << log_c);
+    stage_table(st, T.psiA, T.psiA_q, S::M);
+    const size_t base = ((size_t)blockIdx.z * limb_count + limb) << (LOG_M + log_b);
+    const int c0 = blockIdx.x << log_c;
+    auto tw = [&](int s, u32 blk, u64& W, u64& Wq) {
+        u32 idx = (1u << s) + blk;
+        W = st[idx];
+        Wq = st[S::M + idx];
+    };
+    __syncthreads();
+    if (tid < (C << S::LR2)) {
+        const int c = tid & (C - 1), i0 = tid >> log_c;
+        u64 x[S::R1];
+        if (kDigits) {
+            const i64* in = (const i64*)in_ + ((size_t)blockIdx.z << (LOG_M + log_b));
+#pragma unroll
+            for (int e = 0; e < S::R1; ++e) x[e] = lift_digit(in[c0 + c + ((size_t)(i0 + S::R2 * e) << log_b)], q);
+        } else {
+            const u64* in = (const u64*)in_ + base;
+#pragma unroll
+            for (int e = 0; e < S::R1; ++e) x[e] = in[c0 + c + ((size_t)(i0 + S::R2 * e) << log_b)];
+        }
+        nttc::ct_stages<S::LR1>(x, 0, 0, tw, q);
+#pragma unroll
+        for (int e = 0; e < S::R1; ++e) sm[((i0 + S::R2 * e) << log_c) + (c ^ (e & (C - 1)))] = x[e];
     }
     __syncthreads();
-    // cyclic DIT: bit-reversed in -> natural out
-    for (int lh = 0; lh < log_n1; ++lh) {
-        const int half = 1 << lh;
-        const int tw_shift = log_n1 - lh - 1;  // w1^(o * N1/len), len = 2*half
-        for (int idx = threadIdx.x; idx < ((N1 >> 1) << log_c); idx += blockDim.x) {
-            int c = idx & (C - 1), b = idx >> log_c;
-            int o = b & (half - 1), blk = b >> lh;
-            int r0 = (blk << (lh + 1)) + o, r1 = r0 + half;
-            int ti = o << tw_shift;
-            u64 W = __ldg(T.w + ti), Wq = __ldg(T.w_q + ti);
-            u64* p0 = &sm[(r0 << log_c) + c];
-            u64* p1 = &sm[(r1 << log_c) + c];
-            u64 X = *p0, Y = *p1;
-            X = X >= q2 ? X - q2 : X;
-            u64 t = mul_shoup_lazy(Y, W, Wq, q);
-            *p0 = X + t;
-            *p1 = X - t + q2;
+    if (tid < (C << S::LR1)) {
+        const int g = tid & (S::R1 - 1), c = tid >> S::LR1;
+        u64 y[S::R2];
+#pragma unroll
+        for (int e = 0; e < S::R2; ++e) y[e] = sm[((S::R2 * g + e) << log_c) + (c ^ (g & (C - 1)))];
+        nttc::ct_stages<S::LR2>(y, S::LR1, g, tw, q);
+        const size_t row = (size_t)(c0 + c) << LOG_M;
+#pragma unroll
+        for (int e = 0; e < S::R2; ++e) {
+            const size_t p = row + brev(S::R2 * g + e, LOG_M);
+            out[base + p] = mul_shoup_lazy(y[e], __ldg(T.mid + p), __ldg(T.mid_q + p), q);
         }
-        __syncthreads();
-    }
-    for (int idx = threadIdx.x; idx < (N1 << log_c); idx += blockDim.x) {
-        int k1 = idx >> log_c, c = idx & (C - 1);
-        dst[base + ((size_t)k1 << log_n2) + k2_0 + c] = reduce_4q(sm[(k1 << log_c) + c], q);
     }
 }
 
-// Inverse pass A: tile of C columns k2; cyclic GS over k1 (natural in ->
-// bit-reversed out), times N^-1 psi^-((2k2+1) j1), stored as rows [k2][j1].
-__global__ void __launch_bounds__(kThreads) k_ntt_inv_passA(const u64* __restrict__ in, u64* __restrict__ out,
-                                                            const NttTab* __restrict__ tabs, LimbMap lm,
-                                                            int limb_count, int log_n1, int log_n2, int log_c) {
+// Forward pass 2 over units k_a: negacyclic B-point merged CT with
+// psi_2B = psi^A on {k_a + A j_lo}; output k_b = brev(r) stored at k_a + A k_b
+// (natural order). src may equal dst; values < 4q in, canonical out.
+template <int LOG_M>
+__global__ void __launch_bounds__(kMaxThreads) k_fwd2(const u64* src, u64* dst, const NttTab* __restrict__ tabs,
+                                                      LimbMap lm, int limb_count, int log_a, int log_c) {
+    using S = Split<LOG_M>;
     extern __shared__ u64 sm[];
-    const int N1 = 1 << log_n1, C = 1 << log_c;
+    const int C = 1 << log_c, tid = threadIdx.x;
     const int limb = blockIdx.y;
-    const NttTab T = tabs[lm(limb)];
-    const u64 q = T.q, q2 = q << 1;
-    const size_t base = ((size_t)blockIdx.z * limb_count + limb) << (log_n1 + log_n2);
-    const int k2_0 = blockIdx.x << log_c;
-
-    for (int idx = threadIdx.x; idx < (N1 << log_c); idx += blockDim.x) {
-        int k1 = idx >> log_c, c = idx & (C - 1);
-        sm[(k1 << log_c) + (c ^ swz(k1, log_n1, C))] = in[base + ((size_t)k1 << log_n2) + k2_0 + c];
+    const NttTab& T = tabs[lm(limb)];
+    const u64 q = T.q;
+    u64* st = sm + (S::M << log_c);
+    stage_table(st, T.psiB, T.psiB_q, S::M);
+    const size_t base = ((size_t)blockIdx.z * limb_count + limb) << (LOG_M + log_a);
+    const int b0 = blockIdx.x << log_c;
+    const int c = tid & (C - 1);
+    auto tw = [&](int s, u32 blk, u64& W, u64& Wq) {
+        u32 idx = (1u << s) + blk;
+        W = st[idx];
+        Wq = st[S::M + idx];
+    };
+    __syncthreads();
+    if (tid < (C << S::LR2)) {
+        const int i0 = tid >> log_c;
+        u64 x[S::R1];
+#pragma unroll
+        for (int e = 0; e < S::R1; ++e) x[e] = src[base + ((size_t)(i0 + S::R2 * e) << log_a) + b0 + c];
+        nttc::ct_stages<S::LR1>(x, 0, 0, tw, q);
+#pragma unroll
+        for (int e = 0; e < S::R1; ++e) sm[((i0 + S::R2 * e) << log_c) + c] = x[e];
     }
     __syncthreads();
-    for (int lh = log_n1 - 1; lh >= 0; --lh) {
-        const int half = 1 << lh;
-        const int tw_shift = log_n1 - lh - 1;
-        for (int idx = threadIdx.x; idx < ((N1 >> 1) << log_c); idx += blockDim.x) {
-            int c = idx & (C - 1), b = idx >> log_c;
-            int o = b & (half - 1), blk = b >> lh;
-            int r0 = (blk << (lh + 1)) + o, r1 = r0 + half;
-            int ti = o << tw_shift;
-            u64 W = __ldg(T.w_inv + ti), Wq = __ldg(T.w_inv_q + ti);
-            u64* p0 = &sm[(r0 << log_c) + (c ^ swz(r0, log_n1, C))];
-            u64* p1 = &sm[(r1 << log_c) + (c ^ swz(r1, log_n1, C))];
-            u64 X = *p0, Y = *p1;
-            u64 s = X + Y;
-            *p0 = s >= q2 ? s - q2 : s;
-            *p1 = mul_shoup_lazy(X - Y + q2, W, Wq, q);
-        }
-        __syncthreads();
-    }
-    for (int idx = threadIdx.x; idx < (N1 << log_c); idx += blockDim.x) {
-        int j1 = idx & (N1 - 1), c = idx >> log_n1;
-        u32 r = bitrev(j1, log_n1);
-        u64 v = sm[(r << log_c) + (c ^ (j1 & (C - 1)))];
-        size_t t = ((size_t)(k2_0 + c) << log_n1) + j1;
-        out[base + t] = mul_shoup_lazy(v, __ldg(T.imid + t), __ldg(T.imid_q + t), q);
+    if (tid < (C << S::LR1)) {
+        const int g = tid >> log_c;
+        u64 y[S::R2];
+#pragma unroll
+        for (int e = 0; e < S::R2; ++e) y[e] = sm[((S::R2 * g + e) << log_c) + c];
+        nttc::ct_stages<S::LR2>(y, S::LR1, g, tw, q);
+#pragma unroll
+        for (int e = 0; e < S::R2; ++e)
+            dst[base + ((size_t)brev(S::R2 * g + e, LOG_M) << log_a) + b0 + c] = reduce_4q(y[e], q);
     }
 }
 
-// Inverse pass B: tile of C columns j1; merged GS negacyclic over k2
-// (bit-reversed in -> natural out). src may equal dst (same address set per CTA).
-__global__ void __launch_bounds__(kThreads) k_ntt_inv_passB(const u64* src, u64* dst, const NttTab* __restrict__ tabs,
-                                                            LimbMap lm, int limb_count, int log_n1, int log_n2,
-                                                            int log_c) {
+// Inverse pass 1 over units k_a: negacyclic B-point merged GS with psi_2B^-1
+// on the bit-reversed input {k_a + A brev(r)}, times the inverse twist
+// N^-1 psi^-((2k_a+1-A) j_lo), stored as row k_a (lazy, [0, 2q)). in != out.
+template <int LOG_M>
+__global__ void __launch_bounds__(kMaxThreads) k_inv1(const u64* __restrict__ in, u64* __restrict__ out,
+                                                      const NttTab* __restrict__ tabs, LimbMap lm, int limb_count,
+                                                      int log_a, int log_c) {
+    using S = Split<LOG_M>;
     extern __shared__ u64 sm[];
-    const int N2 = 1 << log_n2, C = 1 << log_c;
+    const int C = 1 << log_c, tid = threadIdx.x;
     const int limb = blockIdx.y;
-    const NttTab T = tabs[lm(limb)];
-    const u64 q = T.q, q2 = q << 1;
-    const size_t base = ((size_t)blockIdx.z * limb_count + limb) << (log_n1 + log_n2);
-    const int j1_0 = blockIdx.x << log_c;
-
-    for (int idx = threadIdx.x; idx < (N2 << log_c); idx += blockDim.x) {
-        int k2 = idx >> log_c, c = idx & (C - 1);
-        sm[(bitrev(k2, log_n2) << log_c) + c] = src[base + ((size_t)k2 << log_n1) + j1_0 + c];
+    const NttTab& T = tabs[lm(limb)];
+    const u64 q = T.q;
+    u64* st = sm + (S::M << log_c);
+    stage_table(st, T.psiB_inv, T.psiB_inv_q, S::M);
+    const size_t base = ((size_t)blockIdx.z * limb_count + limb) << (LOG_M + log_a);
+    const int b0 = blockIdx.x << log_c;
+    auto tw = [&](int s, u32 blk, u64& W, u64& Wq) {
+        u32 idx = (S::M >> (s + 1)) + blk;
+        W = st[idx];
+        Wq = st[S::M + idx];
+    };
+    __syncthreads();
+    if (tid < (C << S::LR1)) {
+        const int c = tid & (C - 1), g = tid >> log_c;
+        u64 x[S::R2];
+#pragma unroll
+        for (int e = 0; e < S::R2; ++e) x[e] = in[base + ((size_t)brev(S::R2 * g + e, LOG_M) << log_a) + b0 + c];
+        nttc::gs_stages<S::LR2>(x, 0, g, tw, q);
+#pragma unroll
+        for (int e = 0; e < S::R2; ++e) {
+            const int r = S::R2 * g + e;
+            sm[(r << log_c) + (c ^ (r & (C - 1)))] = x[e];
+        }
     }
     __syncthreads();
-    for (int lt = 0, h = N2 >> 1; h >= 1; ++lt, h >>= 1) {
-        for (int idx = threadIdx.x; idx < ((N2 >> 1) << log_c); idx += blockDim.x) {
-            int c = idx & (C - 1), b = idx >> log_c;
-            int i = b >> lt;
-            int r0 = (i << (lt + 1)) + (b & ((1 << lt) - 1)), r1 = r0 + (1 << lt);
-            u64 S = __ldg(T.psi_inv_rev + h + i), Sq = __ldg(T.psi_inv_rev_q + h + i);
-            u64* p0 = &sm[(r0 << log_c) + c];
-            u64* p1 = &sm[(r1 << log_c) + c];
-            u64 X = *p0, Y = *p1;
-            u64 s = X + Y;
-            *p0 = s >= q2 ? s - q2 : s;
-            *p1 = mul_shoup_lazy(X - Y + q2, S, Sq, q);
+    if (tid < (C << S::LR2)) {
+        const int i0 = tid & (S::R2 - 1), c = tid >> S::LR2;
+        u64 y[S::R1];
+#pragma unroll
+        for (int e = 0; e < S::R1; ++e) {
+            const int r = i0 + S::R2 * e;
+            y[e] = sm[(r << log_c) + (c ^ (r & (C - 1)))];
         }
-        __syncthreads();
-    }
-    for (int idx = threadIdx.x; idx < (N2 << log_c); idx += blockDim.x) {
-        int j2 = idx >> log_c, c = idx & (C - 1);
-        dst[base + j1_0 + c + ((size_t)j2 << log_n1)] = reduce_2q(sm[(j2 << log_c) + c], q);
+        nttc::gs_stages<S::LR1>(y, S::LR2, 0, tw, q);
+        const size_t row = (size_t)(b0 + c) << LOG_M;
+#pragma unroll
+        for (int e = 0; e < S::R1; ++e) {
+            const size_t p = row + i0 + S::R2 * e;
+            out[base + p] = mul_shoup_lazy(y[e], __ldg(T.midi + p), __ldg(T.midi_q + p), q);
+        }
     }
 }
 
-int log2_min(int log_dim, int log_cmax) { return log_dim < log_cmax ? log_dim : log_cmax; }
+// Inverse pass 2 over columns j_lo: negacyclic A-point merged GS with
+// psi_A^-1 on {j_lo + B brev(r)}; natural output j_lo + B i, canonical.
+// src may equal dst.
+template <int LOG_M>
+__global__ void __launch_bounds__(kMaxThreads) k_inv2(const u64* src, u64* dst, const NttTab* __restrict__ tabs,
+                                                      LimbMap lm, int limb_count, int log_b, int log_c) {
+    using S = Split<LOG_M>;
+    extern __shared__ u64 sm[];
+    const int C = 1 << log_c, tid = threadIdx.x;
+    const int limb = blockIdx.y;
+    const NttTab& T = tabs[lm(limb)];
+    const u64 q = T.q;
+    u64* st = sm + (S::M << log_c);
+    stage_table(st, T.psiA_inv, T.psiA_inv_q, S::M);
+    const size_t base = ((size_t)blockIdx.z * limb_count + limb) << (LOG_M + log_b);
+    const int c0 = blockIdx.x << log_c;
+    const int c = tid & (C - 1);
+    auto tw = [&](int s, u32 blk, u64& W, u64& Wq) {
+        u32 idx = (S::M >> (s + 1)) + blk;
+        W = st[idx];
+        Wq = st[S::M + idx];
+    };
+    __syncthreads();
+    if (tid < (C << S::LR1)) {
+        const int g = tid >> log_c;
+        u64 x[S::R2];
+#pragma unroll
+        for (int e = 0; e < S::R2; ++e) x[e] = src[base + c0 + c + ((size_t)brev(S::R2 * g + e, LOG_M) << log_b)];
+        nttc::gs_stages<S::LR2>(x, 0, g, tw, q);
+#pragma unroll
+        for (int e = 0; e < S::R2; ++e) sm[((S::R2 * g + e) << log_c) + c] = x[e];
+    }
+    __syncthreads();
+    if (tid < (C << S::LR2)) {
+        const int i0 = tid >> log_c;
+        u64 y[S::R1];
+#pragma unroll
+        for (int e = 0; e < S::R1; ++e) y[e] = sm[((i0 + S::R2 * e) << log_c) + c];
+        nttc::gs_stages<S::LR1>(y, S::LR2, 0, tw, q);
+#pragma unroll
+        for (int e = 0; e < S::R1; ++e) dst[base + c0 + c + ((size_t)(i0 + S::R2 * e) << log_b)] = reduce_2q(y[e], q);
+    }
+}
+
+// columns per CTA: min(16, available, 256 / RMAX)
+template <int LOG_M>
+int pick_log_c(int log_avail) {
+    int lc = 4;
+    while ((Split<LOG_M>::RMAX << lc) > kMaxThreads) --lc;
+    return lc < log_avail ? lc : log_avail;
+}
+
+template <int LOG_M>
+int32_t launch_pass(int which, const void* in, u64* out, const NttTab* tabs, LimbMap lm, u32 limbs, u32 polys,
+                    int log_other, cudaStream_t st) {
+    const int lc = pick_log_c<LOG_M>(log_other);
+    const int threads = Split<LOG_M>::RMAX << lc;
+    const size_t smem = (sizeof(u64) << (LOG_M + lc)) + 2 * sizeof(u64) * (1u << LOG_M);
+    dim3 grid(1u << (log_other - lc), limbs, polys);
+    switch (which) {
+        case 0: k_fwd1<LOG_M, false><<<grid, threads, smem, st>>>(in, out, tabs, lm, limbs, log_other, lc); break;
+        case 1: k_fwd1<LOG_M, true><<<grid, threads, smem, st>>>(in, out, tabs, lm, limbs, log_other, lc); break;
+        case 2: k_fwd2<LOG_M><<<grid, threads, smem, st>>>((const u64*)in, out, tabs, lm, limbs, log_other, lc); break;
+        case 3: k_inv1<LOG_M><<<grid, threads, smem, st>>>((const u64*)in, out, tabs, lm, limbs, log_other, lc); break;
+        default: k_inv2<LOG_M><<<grid, threads, smem, st>>>((const u64*)in, out, tabs, lm, limbs, log_other, lc); break;
+    }
+    return CKKS_OK;
+}
+
+int32_t pass(int which, int log_m, const void* in, u64* out, const NttTab* tabs, LimbMap lm, u32 limbs, u32 polys,
+             int log_other, cudaStream_t st) {
+    switch (log_m) {
+        case 1: return launch_pass<1>(which, in, out, tabs, lm, limbs, polys, log_other, st);
+        case 2: return launch_pass<2>(which, in, out, tabs, lm, limbs, polys, log_other, st);
+        case 3: return launch_pass<3>(which, in, out, tabs, lm, limbs, polys, log_other, st);
+        case 4: return launch_pass<4>(which, in, out, tabs, lm, limbs, polys, log_other, st);
+        case 5: return launch_pass<5>(which, in, out, tabs, lm, limbs, polys, log_other, st);
+        case 6: return launch_pass<6>(which, in, out, tabs, lm, limbs, polys, log_other, st);
+        case 7: return launch_pass<7>(which, in, out, tabs, lm, limbs, polys, log_other, st);
+        case 8: return launch_pass<8>(which, in, out, tabs, lm, limbs, polys, log_other, st);
+        case 9: return launch_pass<9>(which, in, out, tabs, lm, limbs, polys, log_other, st);
+        default: ckks_set_error("NTT: unsupported transform size"); return CKKS_ERR_BAD_ARG;
+    }
+}
 
 }  // namespace
 
-void ntt_set_smem_limits() {
-    static bool done = false;
-    if (done) return;
-    int bytes = 96 * 1024;
-    cudaFuncSetAttribute(k_ntt_fwd_pass1<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    cudaFuncSetAttribute(k_ntt_fwd_pass1<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    cudaFuncSetAttribute(k_ntt_fwd_pass2, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    cudaFuncSetAttribute(k_ntt_inv_passA, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    cudaFuncSetAttribute(k_ntt_inv_passB, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    done = true;
-}
+void ntt_set_smem_limits() {}
 
 int32_t ntt_forward_launch(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, u32 limb_begin, u32 limb_count,
                            cudaStream_t st) {
@@ -241,19 +307,15 @@ int32_t ntt_inverse_launch(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, 
 int32_t ntt_forward_launch_map(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, LimbMap lm, u32 limb_count,
                                cudaStream_t st) {
     if (n_polys == 0 || limb_count == 0) return CKKS_OK;
-    const int l1 = ctx->log_n1, l2 = ctx->log_n2;
+    const int la = ctx->log_n1, lb = ctx->log_n2;
     u64* mid = out;
     Workspace<u64> tmp;
     if (in == out) {  // pass 1 reads columns and writes rows: stage through a workspace
         if (int32_t rc = tmp.alloc((size_t)n_polys * limb_count * ctx->n, st)) return rc;
         mid = tmp.p;
     }
-    int lc1 = log2_min(l1, 4), lc2 = log2_min(l2, 4);
-    dim3 g1(1u << (l1 - lc1), limb_count, n_polys), g2(1u << (l2 - lc2), limb_count, n_polys);
-    k_ntt_fwd_pass1<false><<<g1, kThreads, (sizeof(u64) << (l2 + lc1)), st>>>(in, mid, ctx->d_tabs, lm, limb_count,
-                                                                       l1, l2, lc1);
-    k_ntt_fwd_pass2<<<g2, kThreads, (sizeof(u64) << (l1 + lc2)), st>>>(mid, out, ctx->d_tabs, lm,
-                                                                       limb_count, l1, l2, lc2);
+    if (int32_t rc = pass(0, la, in, mid, ctx->d_tabs, lm, limb_count, n_polys, lb, st)) return rc;
+    if (int32_t rc = pass(2, lb, mid, out, ctx->d_tabs, lm, limb_count, n_polys, la, st)) return rc;
     CKKS_CUDA_TRY(cudaGetLastError());
     return CKKS_OK;
 }
@@ -261,19 +323,15 @@ int32_t ntt_forward_launch_map(ckks_ctx* ctx, const u64* in, u64* out, u32 n_pol
 int32_t ntt_inverse_launch_map(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, LimbMap lm, u32 limb_count,
                                cudaStream_t st) {
     if (n_polys == 0 || limb_count == 0) return CKKS_OK;
-    const int l1 = ctx->log_n1, l2 = ctx->log_n2;
+    const int la = ctx->log_n1, lb = ctx->log_n2;
     u64* mid = out;
     Workspace<u64> tmp;
     if (in == out) {
         if (int32_t rc = tmp.alloc((size_t)n_polys * limb_count * ctx->n, st)) return rc;
         mid = tmp.p;
     }
-    int lcA = log2_min(l2, 4), lcB = log2_min(l1, 4);
-    dim3 gA(1u << (l2 - lcA), limb_count, n_polys), gB(1u << (l1 - lcB), limb_count, n_polys);
-    k_ntt_inv_passA<<<gA, kThreads, (sizeof(u64) << (l1 + lcA)), st>>>(in, mid, ctx->d_tabs, lm, limb_count,
-                                                                       l1, l2, lcA);
-    k_ntt_inv_passB<<<gB, kThreads, (sizeof(u64) << (l2 + lcB)), st>>>(mid, out, ctx->d_tabs, lm,
-                                                                       limb_count, l1, l2, lcB);
+    if (int32_t rc = pass(3, lb, in, mid, ctx->d_tabs, lm, limb_count, n_polys, la, st)) return rc;
+    if (int32_t rc = pass(4, la, mid, out, ctx->d_tabs, lm, limb_count, n_polys, lb, st)) return rc;
     CKKS_CUDA_TRY(cudaGetLastError());
     return CKKS_OK;
 }
@@ -281,12 +339,9 @@ int32_t ntt_inverse_launch_map(ckks_ctx* ctx, const u64* in, u64* out, u32 n_pol
 int32_t ntt_forward_digits_launch(ckks_ctx* ctx, const i64* digits, u64* out, u32 D, LimbMap lm, u32 limbs,
                                   cudaStream_t st) {
     if (D == 0 || limbs == 0) return CKKS_OK;
-    const int l1 = ctx->log_n1, l2 = ctx->log_n2;
-    int lc1 = log2_min(l1, 4), lc2 = log2_min(l2, 4);
-    dim3 g1(1u << (l1 - lc1), limbs, D), g2(1u << (l2 - lc2), limbs, D);
-    k_ntt_fwd_pass1<true><<<g1, kThreads, (sizeof(u64) << (l2 + lc1)), st>>>(digits, out, ctx->d_tabs, lm, limbs, l1,
-                                                                             l2, lc1);
-    k_ntt_fwd_pass2<<<g2, kThreads, (sizeof(u64) << (l1 + lc2)), st>>>(out, out, ctx->d_tabs, lm, limbs, l1, l2, lc2);
+    const int la = ctx->log_n1, lb = ctx->log_n2;
+    if (int32_t rc = pass(1, la, digits, out, ctx->d_tabs, lm, limbs, D, lb, st)) return rc;
+    if (int32_t rc = pass(2, lb, out, out, ctx->d_tabs, lm, limbs, D, la, st)) return rc;
     CKKS_CUDA_TRY(cudaGetLastError());
     return CKKS_OK;
 }

@@ -1,0 +1,81 @@
+// ntt_core.cuh -- register-tiled radix-2 networks used by the NTT passes.
+//
+// The forward transform is the merged Cooley-Tukey network over all N points
+// (natural in, bit-reversed out) with twiddles psi^bitrev(i) (the SEAL/
+// Longa-Naehrig form); the inverse is the merged Gentleman-Sande network
+// (bit-reversed in, natural out) with psi^-bitrev(i). A pass runs the stages
+// that touch one "column" (or "row") of the N = A x B index matrix: M = A or
+// B points, held R1 per thread in registers for the first log R1 stages and
+// R2 per thread for the rest, with one shared-memory exchange in between.
+#pragma once
+#include "kernels.cuh"
+
+namespace nttc {
+
+__device__ __forceinline__ u32 brev(u32 x, int bits) { return bits ? (__brev(x) >> (32 - bits)) : 0; }
+
+// Harvey butterflies on lazily reduced values.
+// CT: X, Y in [0, 4q) -> X' = X + W Y, Y' = X - W Y, both in [0, 4q).
+__device__ __forceinline__ void ct_bfly(u64& X, u64& Y, u64 W, u64 Wq, u64 q, u64 q2) {
+    u64 x = X >= q2 ? X - q2 : X;
+    u64 t = mul_shoup_lazy(Y, W, Wq, q);
+    X = x + t;
+    Y = x - t + q2;
+}
+// GS: X, Y in [0, 2q) -> X' = X + Y, Y' = (X - Y) W, both in [0, 2q).
+__device__ __forceinline__ void gs_bfly(u64& X, u64& Y, u64 W, u64 Wq, u64 q, u64 q2) {
+    u64 s = X + Y;
+    u64 d = X - Y + q2;
+    X = s >= q2 ? s - q2 : s;
+    Y = mul_shoup_lazy(d, W, Wq, q);
+}
+
+// Merged CT stages s0 .. s0 + LR - 1 on R = 2^LR register values with pair
+// distance R/2, R/4, .., 1; the twiddle block of register e at stage ls is
+// (base << ls) + (e >> (LR - ls)); tw(stage, block, W, Wq) supplies the twiddle.
+// Compile-time recursion keeps every register index static.
+template <int LR, int LS, typename TW>
+__device__ __forceinline__ void ct_stage(u64 (&x)[1 << LR], int s0, u32 base, TW& tw, u64 q, u64 q2) {
+    if constexpr (LS < LR) {
+        constexpr int half = (1 << LR) >> (LS + 1);
+#pragma unroll
+        for (int b = 0; b < (1 << LS); ++b) {
+            u64 W, Wq;
+            tw(s0 + LS, (base << LS) + b, W, Wq);
+#pragma unroll
+            for (int o = 0; o < half; ++o) ct_bfly(x[b * 2 * half + o], x[b * 2 * half + o + half], W, Wq, q, q2);
+        }
+        ct_stage<LR, LS + 1>(x, s0, base, tw, q, q2);
+    }
+}
+
+template <int LR, typename TW>
+__device__ __forceinline__ void ct_stages(u64 (&x)[1 << LR], int s0, u32 base, TW tw, u64 q) {
+    ct_stage<LR, 0>(x, s0, base, tw, q, q << 1);
+}
+
+template <int LR, int LS, typename TW>
+__device__ __forceinline__ void gs_stage(u64 (&x)[1 << LR], int s0, u32 blk0, TW& tw, u64 q, u64 q2) {
+    if constexpr (LS < LR) {
+        constexpr int t = 1 << LS;
+        constexpr int nblk = (1 << LR) >> (LS + 1);
+#pragma unroll
+        for (int b = 0; b < nblk; ++b) {
+            u64 W, Wq;
+            tw(s0 + LS, (blk0 << (LR - LS - 1)) + b, W, Wq);
+#pragma unroll
+            for (int o = 0; o < t; ++o) gs_bfly(x[b * 2 * t + o], x[b * 2 * t + o + t], W, Wq, q, q2);
+        }
+        gs_stage<LR, LS + 1>(x, s0, blk0, tw, q, q2);
+    }
+}
+
+// Merged GS stages with register distance t = 1, 2, .., 2^(LR-1) (local stages
+// s0 .. s0 + LR - 1 of the network whose t = 2^s); block of register e at
+// stage ls is (blk0 << (LR - ls - 1)) + (e >> (ls + 1)).
+template <int LR, typename TW>
+__device__ __forceinline__ void gs_stages(u64 (&x)[1 << LR], int s0, u32 blk0, TW tw, u64 q) {
+    gs_stage<LR, 0>(x, s0, blk0, tw, q, q << 1);
+}
+
+}  // namespace nttc

@@ -218,3 +218,29 @@ def test_key_errors(oracle, cuda, small):
     with pytest.raises(cb.CkksError) as e:
         cb.rotate_hoisted(ctx, [k1, k2], ct)
     assert e.value.status == -2
+
+
+@pytest.mark.parametrize("base_log", [4, 8, 32])
+def test_hoisted_ntt_domain_corrections(oracle, cuda, small, base_log):
+    # NTT-domain hoisting must equal the reference's digit-level hoisting word
+    # for word, including coefficients whose digits hit -B/2 (frequent for
+    # small bases; base 2^4 also overflows the correction lists and takes the
+    # exact fallback).
+    n, q, p, ctx = small
+    rng = np.random.default_rng(50 + base_log)
+    s = rng.integers(-1, 2, n).astype(np.int8)
+    cts = np.stack([encode_encrypt(oracle, q, s, rng, 2.0 ** 40, seed=60 + i)[1] for i in range(5)])
+    Q = 1
+    for m in q:
+        Q *= m
+    # plant values whose balanced digits contain -B/2 in the first ciphertext's a-part
+    for c in range(0, n, 7):
+        v = (Q - (1 << (base_log - 1)) * (1 + (c % 3) * (1 << base_log))) % Q
+        cts[0, 1, :, c] = [v % m for m in q]
+    ks = [ctx.rotation_exponent_left(r) for r in (1, 3, 16)] + [2 * n - 1]
+    keys_ref = [oracle.hybrid_key(q, p, s, k, base_log, seed=300 + i) for i, k in enumerate(ks)]
+    keys = [cb.KeySwitchKey.hybrid_upload(ctx, len(q), base_log, k, kr) for k, kr in zip(ks, keys_ref)]
+    got = host(cb.rotate_hoisted(ctx, keys, dev(cts)))
+    for i in range(len(cts)):
+        want = oracle.hybrid_rotate_hoisted(q, p, keys_ref, ks, base_log, cts[i])
+        assert np.array_equal(got[i], want), i
