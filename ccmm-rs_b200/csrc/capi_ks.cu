@@ -97,6 +97,14 @@ int32_t finish_key(ckks_ksk* k, int32_t rc, ckks_ksk** out) {
     return rc;
 }
 
+// Reference layout [D][LK][2][N] from the host into the permuted storage.
+int32_t upload_galois(ckks_ctx* ctx, ckks_ksk* k, const uint64_t* entries_host) {
+    Workspace<u64> tmp;
+    if (int32_t rc = tmp.alloc(k->words, nullptr)) return rc;
+    CKKS_CUDA_TRY(cudaMemcpy(tmp.p, entries_host, k->words * 8, cudaMemcpyHostToDevice));
+    return ksk_permute_entries(ctx, tmp.p, k->d_entries, k->words / ctx->n, k->exponent, true, nullptr);
+}
+
 }  // namespace
 
 extern "C" {
@@ -201,9 +209,7 @@ int32_t ckks_hybrid_key_upload(ckks_ctx* ctx, uint32_t q_limbs, uint32_t base_lo
     if (int32_t rc = new_key(ctx, CKKS_KSK_HYBRID_BOUNDED, q_limbs, base_log, exponent, {}, &k, "ckks_hybrid_key_upload"))
         return rc;
     *out = k;
-    cudaError_t e = cudaMemcpy(k->d_entries, entries_host, k->words * 8, cudaMemcpyHostToDevice);
-    if (e != cudaSuccess) ckks_set_error(cudaGetErrorString(e));
-    return finish_key(k, e == cudaSuccess ? CKKS_OK : CKKS_ERR_CUDA, out);
+    return finish_key(k, upload_galois(ctx, k, entries_host), out);
 }
 
 int32_t ckks_rnsblock_key_generate(ckks_ctx* ctx, uint32_t q_limbs, const uint32_t* block_sizes, uint32_t n_blocks,
@@ -231,9 +237,7 @@ int32_t ckks_rnsblock_key_upload(ckks_ctx* ctx, uint32_t q_limbs, const uint32_t
     if (int32_t rc = new_key(ctx, CKKS_KSK_HYBRID_RNS_BLOCK, q_limbs, 0, exponent, bs, &k, "ckks_rnsblock_key_upload"))
         return rc;
     *out = k;
-    cudaError_t e = cudaMemcpy(k->d_entries, entries_host, k->words * 8, cudaMemcpyHostToDevice);
-    if (e != cudaSuccess) ckks_set_error(cudaGetErrorString(e));
-    return finish_key(k, e == cudaSuccess ? CKKS_OK : CKKS_ERR_CUDA, out);
+    return finish_key(k, upload_galois(ctx, k, entries_host), out);
 }
 
 int32_t ckks_relin_key_generate(ckks_ctx* ctx, uint32_t q_limbs, uint32_t base_log, const int8_t* secret_host,
@@ -272,7 +276,20 @@ int32_t ckks_ksk_info(const ckks_ksk* key, uint32_t* digits, uint64_t* words) {
 
 int32_t ckks_ksk_download(const ckks_ksk* key, uint64_t* entries_host) {
     CKKS_CHECK_ARG(key && entries_host, "ckks_ksk_download: null argument");
-    CKKS_CUDA_TRY(cudaMemcpy(entries_host, key->d_entries, key->words * 8, cudaMemcpyDeviceToHost));
+    if (key->kind == CKKS_KSK_RELIN_BOUNDED) {
+        CKKS_CUDA_TRY(cudaMemcpy(entries_host, key->d_entries, key->words * 8, cudaMemcpyDeviceToHost));
+        return CKKS_OK;
+    }
+    int32_t rc;
+    {
+        Workspace<u64> tmp;
+        if ((rc = tmp.alloc(key->words, nullptr))) return rc;
+        if ((rc = ksk_permute_entries(key->ctx, key->d_entries, tmp.p, key->words / key->ctx->n, key->exponent, false,
+                                      nullptr)))
+            return rc;
+        CKKS_CUDA_TRY(cudaMemcpy(entries_host, tmp.p, key->words * 8, cudaMemcpyDeviceToHost));
+    }
+    CKKS_CUDA_TRY(cudaDeviceSynchronize());
     return CKKS_OK;
 }
 

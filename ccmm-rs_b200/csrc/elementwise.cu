@@ -70,17 +70,20 @@ __global__ void k_rescale(const u64* __restrict__ in, u64* __restrict__ out, con
 }
 
 // ring/auxiliary_modulus.rs:89-171: centered CRT over P from the K auxiliary
-// residues (mixed-radix Garner, exact), then (x_i - r) * P^-1 mod q_i.
+// residues (mixed-radix Garner, exact), then (x_i - r) * P^-1 mod q_i for every
+// Q limb. One thread per coefficient s; with exps, the result is scattered by
+// the coefficient automorphism X -> X^k (k = exps[(poly / 2) % n_keys]):
+// out[t] = +-value[s], t = s k mod 2N (negated when t >= N). ModDown commutes
+// exactly with that signed permutation because P is odd.
 __global__ void k_mod_down(const u64* __restrict__ in, u64* __restrict__ out, ModDownConst md, int q_limbs,
-                           int log_n) {
+                           int log_n, const u64* __restrict__ exps, int n_keys) {
     const u32 n = 1u << log_n;
     const u32 c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n) return;
     const int K = md.K;
-    const size_t src = (size_t)blockIdx.z * (q_limbs + K) << log_n;
-    const size_t dst = (size_t)blockIdx.z * q_limbs << log_n;
+    const size_t src = (size_t)blockIdx.y * (q_limbs + K) << log_n;
+    const size_t dst = (size_t)blockIdx.y * q_limbs << log_n;
     u64 v[kMaxAux];
-    // Garner: v_i = (x_i - sum_{j<i} v_j * (p_0..p_{j-1} mod p_i)) * (p_0..p_{i-1})^-1 mod p_i
     for (int i = 0; i < K; ++i) {
         const u64 p = md.p[i];
         u64 x = in[src + ((size_t)(q_limbs + i) << log_n) + c];
@@ -93,14 +96,23 @@ __global__ void k_mod_down(const u64* __restrict__ in, u64* __restrict__ out, Mo
     for (int i = K - 1; i >= 0; --i) {
         if (v[i] != md.half[i]) { neg = v[i] > md.half[i]; break; }
     }
-    const int i = blockIdx.y;
-    const u64 qi = md.q[i];
-    u64 r = 0;
-    for (int j = 0; j < K; ++j)
-        r = add_mod(r, mul_shoup(v[j], md.pre[i * kMaxAux + j], md.pre_q[i * kMaxAux + j], qi), qi);
-    if (neg) r = sub_mod(r, md.p_mod_q[i], qi);
-    u64 d = sub_mod(in[src + ((size_t)i << log_n) + c], r, qi);
-    out[dst + ((size_t)i << log_n) + c] = mul_shoup(d, md.pinv_mod_q[i], md.pinv_mod_q_q[i], qi);
+    u32 t = c;
+    bool flip = false;
+    if (exps) {
+        const u64 mapped = ((u64)c * exps[(blockIdx.y >> 1) % n_keys]) & (2ull * n - 1);
+        flip = mapped >= n;
+        t = (u32)(mapped & (n - 1));
+    }
+    for (int i = 0; i < q_limbs; ++i) {
+        const u64 qi = md.q[i];
+        u64 r = 0;
+        for (int j = 0; j < K; ++j)
+            r = add_mod(r, mul_shoup(v[j], md.pre[i * kMaxAux + j], md.pre_q[i * kMaxAux + j], qi), qi);
+        if (neg) r = sub_mod(r, md.p_mod_q[i], qi);
+        u64 d = sub_mod(in[src + ((size_t)i << log_n) + c], r, qi);
+        u64 o = mul_shoup(d, md.pinv_mod_q[i], md.pinv_mod_q_q[i], qi);
+        out[dst + ((size_t)i << log_n) + t] = flip ? neg_mod(o, qi) : o;
+    }
 }
 
 }  // namespace
@@ -154,9 +166,22 @@ int32_t rescale_launch(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, u32 
 }
 
 int32_t mod_down_launch(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, u32 q_limbs, cudaStream_t st) {
+    return mod_down_sigma_multi(ctx, in, out, n_polys, q_limbs, nullptr, 1, st);
+}
+
+int32_t mod_down_sigma_multi(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, u32 q_limbs, const u64* d_exps,
+                             u32 n_keys, cudaStream_t st) {
     if (!n_polys) return CKKS_OK;
-    dim3 g((ctx->n + kT - 1) / kT, q_limbs, n_polys);
-    k_mod_down<<<g, kT, 0, st>>>(in, out, ctx->mod_down, q_limbs, ctx->log_n);
+    // grid.y limit: chunks are multiples of 2 * n_keys so (poly / 2) % n_keys pairs stay aligned
+    const u32 unit = 2 * (n_keys ? n_keys : 1);
+    const u32 chunk = (65535 / unit) * unit;
+    for (u32 p0 = 0; p0 < n_polys; p0 += chunk) {
+        const u32 cnt = (n_polys - p0) < chunk ? (n_polys - p0) : chunk;
+        dim3 g((ctx->n + kT - 1) / kT, cnt);
+        k_mod_down<<<g, kT, 0, st>>>(in + ((size_t)p0 * (q_limbs + ctx->K) << ctx->log_n),
+                                     out + ((size_t)p0 * q_limbs << ctx->log_n), ctx->mod_down, q_limbs, ctx->log_n,
+                                     d_exps, n_keys ? n_keys : 1);
+    }
     CKKS_CUDA_TRY(cudaGetLastError());
     return CKKS_OK;
 }

@@ -103,24 +103,28 @@ __global__ void k_hoist_exceptions(const i64* __restrict__ digits, size_t dig_st
     }
 }
 
-// acc[c][g][0][l][k] = pf_l Bhat_c[l][pi_g(k)] + sum_j Yhat_c[j][l][pi_g(k)] key_g[j][l][0][k] + corrections
-// acc[c][g][1][l][k] =                             sum_j Yhat_c[j][l][pi_g(k)] key_g[j][l][1][k] + corrections
+// MAC in the permuted index s = pi_g(k) (keys are stored permuted):
+// acc'[c][g][0][l][s] = pf_l Bhat_c[l][s] + sum_j Yhat_c[j][l][s] key'_g[j][l][0][s] + corrections
+// acc'[c][g][1][l][s] =                      sum_j Yhat_c[j][l][s] key'_g[j][l][1][s] + corrections
+// so acc = perm_g(acc'); the caller applies sigma_g after the inverse transform.
+// Every load is contiguous: keys stream once per group (evict-first), the
+// group's digit transforms are re-read from L2 by every key.
 template <int G>
 __global__ void __launch_bounds__(kT) k_mac_hoisted(const u64* __restrict__ Yhat, size_t y_stride,
                                                     const u64* __restrict__ Bhat, size_t b_stride,
-                                                    const u64* const* __restrict__ keys, const u64* __restrict__ exps,
-                                                    const u64* __restrict__ pf, const u64* __restrict__ pf_q,
-                                                    u64* __restrict__ acc, const NttTab* __restrict__ tabs, LimbMap lm,
-                                                    int n_ct, int n_keys, int Lq, int LK, int D, int log_n,
-                                                    const Exc* __restrict__ exc, const u32* __restrict__ exc_count,
-                                                    int cap, const u64* __restrict__ psi) {
+                                                    const u64* const* __restrict__ keys,
+                                                    const u64* __restrict__ exps_inv, const u64* __restrict__ pf,
+                                                    const u64* __restrict__ pf_q, u64* __restrict__ acc,
+                                                    const NttTab* __restrict__ tabs, LimbMap lm, int n_ct, int n_keys,
+                                                    int Lq, int LK, int D, int log_n, const Exc* __restrict__ exc,
+                                                    const u32* __restrict__ exc_count, int cap,
+                                                    const u64* __restrict__ psi) {
     const u32 n = 1u << log_n;
-    const u32 k = blockIdx.x * blockDim.x + threadIdx.x;
+    const u32 s = blockIdx.x * blockDim.x + threadIdx.x;
     const int g = blockIdx.y, l = blockIdx.z;
-    if (k >= n) return;
+    if (s >= n) return;
     const NttTab& T = tabs[lm(l)];
     const u64 q = T.q, mh = T.mu_hi, ml = T.mu_lo;
-    const u32 src = galois_src(k, exps[g], log_n);
     const u64* key = keys[g];
     Acc ab[G], aa[G];
 #pragma unroll
@@ -128,8 +132,8 @@ __global__ void __launch_bounds__(kT) k_mac_hoisted(const u64* __restrict__ Yhat
     int since = 0;
     for (int j = 0; j < D; ++j) {
         const size_t kofs = (((size_t)j * LK + l) * 2) << log_n;
-        const u64 kb = __ldcs(key + kofs + k), ka = __ldcs(key + kofs + n + k);
-        const size_t yofs = (((size_t)j * LK + l) << log_n) + src;
+        const u64 kb = __ldcs(key + kofs + s), ka = __ldcs(key + kofs + n + s);
+        const size_t yofs = (((size_t)j * LK + l) << log_n) + s;
 #pragma unroll
         for (int c = 0; c < G; ++c) {
             if (c < n_ct) {
@@ -154,27 +158,40 @@ __global__ void __launch_bounds__(kT) k_mac_hoisted(const u64* __restrict__ Yhat
         ab[c].fold(q, mh, ml);
         aa[c].fold(q, mh, ml);
         u64 b = ab[c].lo, a = aa[c].lo;
-        if (l < Lq) b = add_mod(b, mul_shoup(__ldg(Bhat + c * b_stride + ((size_t)l << log_n) + src), pf[l], pf_q[l], q), q);
+        if (l < Lq) b = add_mod(b, mul_shoup(__ldg(Bhat + c * b_stride + ((size_t)l << log_n) + s), pf[l], pf_q[l], q), q);
         const u32 cnt = min(exc_count[(size_t)c * n_keys + g], (u32)cap);
         if (cnt) {
             const Exc* list = exc + ((size_t)c * n_keys + g) * cap;
             const u64 ps = psi[lm(l)];
+            const u32 k = galois_src(s, exps_inv[g], log_n);  // unpermuted slot of s
             for (u32 e = 0; e < cnt; ++e) {
                 const Exc x = list[e];
                 // NTT of Delta * X^t at slot k: Delta * psi^((2k+1) t)
                 u64 w = pow_mod_dev(ps, ((2ull * k + 1) * x.t) & (2ull * n - 1), bm);
-                u64 dm = x.delta < 0 ? q - ((u64)(-x.delta) % q) : ((u64)x.delta % q);
-                dm = dm == q ? 0 : dm;
+                u64 dm = x.delta < 0 ? (u64)(-x.delta) % q : (u64)x.delta % q;
+                if (x.delta < 0 && dm) dm = q - dm;
                 u64 v = mul_barrett(w, dm, bm);
                 const size_t kofs = (((size_t)x.j * LK + l) * 2) << log_n;
-                b = add_mod(b, mul_barrett(v, key[kofs + k], bm), q);
-                a = add_mod(a, mul_barrett(v, key[kofs + n + k], bm), q);
+                b = add_mod(b, mul_barrett(v, key[kofs + s], bm), q);
+                a = add_mod(a, mul_barrett(v, key[kofs + n + s], bm), q);
             }
         }
         const size_t obase = (((size_t)c * n_keys + g) * 2 * LK) << log_n;
-        acc[obase + ((size_t)l << log_n) + k] = b;
-        acc[obase + (((size_t)LK + l) << log_n) + k] = a;
+        acc[obase + ((size_t)l << log_n) + s] = b;
+        acc[obase + (((size_t)LK + l) << log_n) + s] = a;
     }
+}
+
+u64 galois_inverse_host(u64 k, u32 n) {
+    const u64 two_n = 2ull * n;
+    k %= two_n;
+    u64 r = 1, b = k, e = n - 1;
+    while (e) {
+        if (e & 1) r = (r * b) % two_n;
+        b = (b * b) % two_n;
+        e >>= 1;
+    }
+    return r;
 }
 
 }  // namespace
@@ -200,21 +217,23 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
     int32_t rc;
     if ((rc = Y.alloc(G * y_stride, st)) || (rc = Bh.alloc(G * b_stride, st)) ||
         (rc = acc.alloc((size_t)G * n_keys * 2 * LK * n, st)) || (rc = Z.alloc((size_t)G * n_keys * 2 * LK * n, st)) ||
-        (rc = karr.alloc(2 * (size_t)n_keys + ctx->moduli.size(), st)) || (rc = dig.alloc(G * d_stride, st)) ||
+        (rc = karr.alloc(3 * (size_t)n_keys + ctx->moduli.size(), st)) || (rc = dig.alloc(G * d_stride, st)) ||
         (rc = flags.alloc(G * f_stride, st)) || (rc = cnt.alloc((size_t)G * n_keys, st)) ||
         (rc = exc.alloc((size_t)G * n_keys * cap, st)))
         return rc;
     // key pointers, exponents and psi per modulus
-    std::vector<u64> hk(2 * (size_t)n_keys + ctx->moduli.size());
+    std::vector<u64> hk(3 * (size_t)n_keys + ctx->moduli.size());
     for (u32 g = 0; g < n_keys; ++g) {
         hk[g] = (u64)(uintptr_t)keys[g]->d_entries;
         hk[n_keys + g] = keys[g]->exponent;
+        hk[2 * n_keys + ctx->moduli.size() + g] = galois_inverse_host(keys[g]->exponent, n);
     }
     for (size_t i = 0; i < ctx->moduli.size(); ++i) hk[2 * n_keys + i] = ctx->psi[i];
     CKKS_CUDA_TRY(cudaMemcpyAsync(karr.p, hk.data(), hk.size() * 8, cudaMemcpyHostToDevice, st));
     const u64* const* d_keys = (const u64* const*)karr.p;
     const u64* d_exps = karr.p + n_keys;
     const u64* d_psi = karr.p + 2 * n_keys;
+    const u64* d_exps_inv = karr.p + 2 * n_keys + ctx->moduli.size();
     std::vector<u32> overflow;
     std::vector<u32> h_cnt((size_t)G * n_keys);
     for (u32 c0 = 0; c0 < n_ct; c0 += G) {
@@ -243,7 +262,7 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
         {
             dim3 g((n + kT - 1) / kT, n_keys, LK);
 #define CKKS_MAC(GG)                                                                                               \
-    k_mac_hoisted<GG><<<g, kT, 0, st>>>(Y.p, y_stride, Bh.p, b_stride, d_keys, d_exps, ctx->d_pmodq,                \
+    k_mac_hoisted<GG><<<g, kT, 0, st>>>(Y.p, y_stride, Bh.p, b_stride, d_keys, d_exps_inv, ctx->d_pmodq,            \
                                         ctx->d_pmodq + ctx->L, acc.p, ctx->d_tabs, lqp, gn, n_keys, Lq, LK, D,      \
                                         ctx->log_n, exc.p, cnt.p, cap, d_psi)
             if (G >= 3) CKKS_MAC(4);
@@ -253,8 +272,9 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
         }
         CKKS_CUDA_TRY(cudaGetLastError());
         if ((rc = ntt_inverse_launch_map(ctx, acc.p, Z.p, gn * n_keys * 2, lqp, LK, st))) return rc;
-        // ModDown of every (ciphertext, key) pair straight into the output
-        if ((rc = mod_down_launch(ctx, Z.p, ct_out + (size_t)c0 * n_keys * ct_words, gn * n_keys * 2, Lq, st)))
+        // ModDown of every (ciphertext, key) pair, then sigma_g, straight into the output
+        if ((rc = mod_down_sigma_multi(ctx, Z.p, ct_out + (size_t)c0 * n_keys * ct_words, gn * n_keys * 2, Lq, d_exps,
+                                       n_keys, st)))
             return rc;
         // pairs whose correction lists overflowed are recomputed exactly
         CKKS_CUDA_TRY(cudaMemcpyAsync(h_cnt.data(), cnt.p, (size_t)G * n_keys * sizeof(u32), cudaMemcpyDeviceToHost, st));

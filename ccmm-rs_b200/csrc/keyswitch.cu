@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(kT) k_ks_mac(const u64* __restrict__ Y, const 
                                                const u64* __restrict__ base, const u64* __restrict__ pf,
                                                const u64* __restrict__ pf_q, u64* __restrict__ acc,
                                                const NttTab* __restrict__ tabs, LimbMap lm, int Lq, int LK, int D,
-                                               int log_n, u64 perm_y, u64 perm_b) {
+                                               int log_n, u64 perm_y, u64 perm_b, u64 perm_key) {
     const u32 n = 1u << log_n;
     const u32 k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
@@ -64,13 +64,14 @@ __global__ void __launch_bounds__(kT) k_ks_mac(const u64* __restrict__ Y, const 
     const NttTab& T = tabs[lm(l)];
     const u64 q = T.q, mu_hi = T.mu_hi, mu_lo = T.mu_lo;
     const u32 ky = perm_y ? galois_src(k, perm_y, log_n) : k;
+    const u32 kk = perm_key ? galois_src(k, perm_key, log_n) : k;  // key slot of k in permuted storage
     Acc128 ab, aa;
     int since = 0;
     for (int j = 0; j < D; ++j) {
         u64 y = Y[(((size_t)j * LK + l) << log_n) + ky];
         const u64* kp = key + ((((size_t)j * LK + l) * 2) << log_n);
-        ab.mac(y, kp[k]);
-        aa.mac(y, kp[n + k]);
+        ab.mac(y, kp[kk]);
+        aa.mac(y, kp[n + kk]);
         if (++since == 15) {
             ab.fold(q, mu_hi, mu_lo);
             aa.fold(q, mu_hi, mu_lo);
@@ -136,7 +137,7 @@ __global__ void k_keygen_target(u64* __restrict__ T, const int8_t* __restrict__ 
 // entries[j][l][0] = That - a * s_hat, entries[j][l][1] = a (a uniform, sampled in the NTT domain)
 __global__ void k_keygen_finish(const u64* __restrict__ That, const u64* __restrict__ s_hat, u64* __restrict__ entries,
                                 const NttTab* __restrict__ tabs, LimbMap lm, int LK, int log_n, u64 seed, u64 tag_a,
-                                int comp_major) {
+                                int comp_major, u64 perm) {
     const u32 n = 1u << log_n;
     const u32 c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n) return;
@@ -148,9 +149,10 @@ __global__ void k_keygen_finish(const u64* __restrict__ That, const u64* __restr
     if (comp_major) {  // [j][2][LK][N] (relinearization key layout)
         entries[((((size_t)j * 2 + 0) * LK + l) << log_n) + c] = b;
         entries[((((size_t)j * 2 + 1) * LK + l) << log_n) + c] = a;
-    } else {  // [j][LK][2][N] (Galois key layout)
-        entries[((((size_t)j * LK + l) * 2 + 0) << log_n) + c] = b;
-        entries[((((size_t)j * LK + l) * 2 + 1) << log_n) + c] = a;
+    } else {  // [j][LK][2][N] (Galois key layout), stored at the permuted slot
+        const u32 sl = perm ? galois_src(c, perm, log_n) : c;
+        entries[((((size_t)j * LK + l) * 2 + 0) << log_n) + sl] = b;
+        entries[((((size_t)j * LK + l) * 2 + 1) << log_n) + sl] = a;
     }
 }
 
@@ -233,7 +235,7 @@ int32_t ksk_generate(ckks_ctx* ctx, ckks_ksk* key, const int8_t* secret, u64 see
     k_lift_ternary<<<gs, kT, 0, st>>>(d_sec.p, d_s.p, ctx->d_tabs, lm, ctx->log_n);
     if ((rc = ntt_forward_launch_map(ctx, d_s.p, d_s.p + (size_t)LK * n, 1, lm, LK, st))) return rc;
     k_keygen_finish<<<g, kT, 0, st>>>(d_That.p, d_s.p + (size_t)LK * n, key->d_entries, ctx->d_tabs, lm, LK,
-                                      ctx->log_n, seed, tag_a, comp_major ? 1 : 0);
+                                      ctx->log_n, seed, tag_a, comp_major ? 1 : 0, comp_major ? 0 : key->exponent);
     CKKS_CUDA_TRY(cudaGetLastError());
     return CKKS_OK;
 }
@@ -322,17 +324,29 @@ std::vector<int8_t> host_secret_automorphism(const int8_t* s, u32 n, u64 k) { re
 
 // --------------------------------------------------------------- pipelines
 int32_t ks_mac_launch(ckks_ctx* ctx, const u64* Y, const u64* key, const u64* base, u64* acc, u32 q_limbs, u32 D,
-                      bool with_p, u64 perm_y, u64 perm_b, cudaStream_t st) {
+                      bool with_p, u64 perm_y, u64 perm_b, cudaStream_t st, u64 perm_key) {
     const u32 LK = with_p ? q_limbs + ctx->K : q_limbs;
     const LimbMap lm = with_p ? LimbMap::qp(ctx, q_limbs) : LimbMap::range(0, q_limbs);
     dim3 g((ctx->n + kT - 1) / kT, LK, 1);
     k_ks_mac<<<g, kT, 0, st>>>(Y, key, base, ctx->d_pmodq, ctx->d_pmodq + ctx->L, acc, ctx->d_tabs, lm, q_limbs, LK,
-                               D, ctx->log_n, perm_y, perm_b);
+                               D, ctx->log_n, perm_y, perm_b, perm_key);
     CKKS_CUDA_TRY(cudaGetLastError());
     return CKKS_OK;
 }
 
+// Non-hoisted bounded rotation in the reference's order (sigma on (b, a),
+// decompose sigma(a), transform every digit): the exact fallback of the hoisted
+// path. The permuted key storage is read through the permutation.
 int32_t rotate_hybrid(ckks_ctx* ctx, const ckks_ksk* key, const u64* ct_in, u64* ct_out, u32 n_ct, cudaStream_t st) {
+    if (key->kind != CKKS_KSK_HYBRID_BOUNDED) {
+        const ckks_ksk* keys[1] = {key};
+        for (u32 i = 0; i < n_ct; ++i) {
+            const size_t ct_words = (size_t)2 * key->q_limbs * ctx->n;
+            if (int32_t rc = rotate_hoisted_ntt(ctx, keys, 1, ct_in + i * ct_words, ct_out + i * ct_words, 1, st))
+                return rc;
+        }
+        return CKKS_OK;
+    }
     const u32 Lq = key->q_limbs, LK = ksk_limbs(key), D = key->D, n = ctx->n;
     const size_t ct_words = (size_t)2 * Lq * n;
     Workspace<u64> ws;
@@ -349,84 +363,45 @@ int32_t rotate_hybrid(ckks_ctx* ctx, const ckks_ksk* key, const u64* ct_in, u64*
     for (u32 i = 0; i < n_ct; ++i) {
         const u64* in = ct_in + (size_t)i * ct_words;
         u64* out = ct_out + (size_t)i * ct_words;
-        u64 perm = 0;
-        if (key->kind == CKKS_KSK_HYBRID_BOUNDED) {
-            // exact reference order: sigma on (b, a), decompose sigma(a)
-            if ((rc = automorphism_coef_launch(ctx, in, sct, 2, lq, Lq, key->exponent, st))) return rc;
-            if ((rc = bounded_decompose_launch(ctx, sct + (size_t)Lq * n, 1, Lq, key->base_log, dg.p, nullptr, st)))
-                return rc;
-            if ((rc = ntt_forward_digits_launch(ctx, dg.p, Y, D, lqp, LK, st))) return rc;
-            if ((rc = ntt_forward_launch_map(ctx, sct, b_hat, 1, lq, Lq, st))) return rc;
-        } else {
-            // RNS blocks: ModUp of a, sigma applied as the NTT-domain permutation
-            if ((rc = rnsblock_modup_launch(ctx, key, in + (size_t)Lq * n, Y, st))) return rc;
-            if ((rc = ntt_forward_launch_map(ctx, Y, Y, D, lqp, LK, st))) return rc;
-            if ((rc = ntt_forward_launch_map(ctx, in, b_hat, 1, lq, Lq, st))) return rc;
-            perm = key->exponent;
-        }
-        if ((rc = ks_mac_launch(ctx, Y, key->d_entries, b_hat, acc, Lq, D, true, perm, perm, st))) return rc;
+        if ((rc = automorphism_coef_launch(ctx, in, sct, 2, lq, Lq, key->exponent, st))) return rc;
+        if ((rc = bounded_decompose_launch(ctx, sct + (size_t)Lq * n, 1, Lq, key->base_log, dg.p, nullptr, st)))
+            return rc;
+        if ((rc = ntt_forward_digits_launch(ctx, dg.p, Y, D, lqp, LK, st))) return rc;
+        if ((rc = ntt_forward_launch_map(ctx, sct, b_hat, 1, lq, Lq, st))) return rc;
+        if ((rc = ks_mac_launch(ctx, Y, key->d_entries, b_hat, acc, Lq, D, true, 0, 0, st, key->exponent))) return rc;
         if ((rc = ntt_inverse_launch_map(ctx, acc, Z, 2, lqp, LK, st))) return rc;
         if ((rc = mod_down_launch(ctx, Z, out, 2, Lq, st))) return rc;
     }
     return CKKS_OK;
 }
 
-// Hoisted rotations: one decomposition of a (and one NTT of b) per ciphertext,
-// then per Galois element the exact digit automorphism (bounded_gadget.rs:273-312)
-// and the key switch. out layout [n_ct][n_keys][2][Lq][N].
 int32_t rotate_hybrid_hoisted(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_keys, const u64* ct_in, u64* ct_out,
                               u32 n_ct, cudaStream_t st) {
     return rotate_hoisted_ntt(ctx, keys, n_keys, ct_in, ct_out, n_ct, st);
 }
 
-// Digit-level hoisting (the reference's own structure): one decomposition per
-// ciphertext, re-normalised digits and their transforms per Galois element.
-// Kept as the reference-order path for differential tests.
-int32_t rotate_hybrid_hoisted_digits(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_keys, const u64* ct_in,
-                                     u64* ct_out, u32 n_ct, cudaStream_t st) {
-    const ckks_ksk* k0 = keys[0];
-    const u32 Lq = k0->q_limbs, LK = ksk_limbs(k0), D = k0->D, n = ctx->n;
-    const size_t ct_words = (size_t)2 * Lq * n;
-    Workspace<u64> ws;
-    Workspace<i64> dg;
-    int32_t rc;
-    if ((rc = ws.alloc((size_t)Lq * n + (size_t)D * LK * n + 4 * (size_t)LK * n, st)) ||
-        (rc = dg.alloc((size_t)2 * D * n, st)))
-        return rc;
-    u64* b_hat = ws.p;
-    u64* Y = b_hat + (size_t)Lq * n;
-    u64* acc = Y + (size_t)D * LK * n;
-    u64* Z = acc + (size_t)2 * LK * n;
-    i64* d0 = dg.p;
-    i64* dk = dg.p + (size_t)D * n;
-    const LimbMap lq = LimbMap::range(0, Lq), lqp = LimbMap::qp(ctx, Lq);
-    for (u32 i = 0; i < n_ct; ++i) {
-        const u64* in = ct_in + (size_t)i * ct_words;
-        if ((rc = ntt_forward_launch_map(ctx, in, b_hat, 1, lq, Lq, st))) return rc;
-        if (k0->kind == CKKS_KSK_HYBRID_BOUNDED) {
-            if ((rc = bounded_decompose_launch(ctx, in + (size_t)Lq * n, 1, Lq, k0->base_log, d0, nullptr, st)))
-                return rc;
-        } else {
-            // RNS blocks: ModUp and transform once; each Galois element permutes in the NTT domain
-            if ((rc = rnsblock_modup_launch(ctx, k0, in + (size_t)Lq * n, Y, st))) return rc;
-            if ((rc = ntt_forward_launch_map(ctx, Y, Y, D, lqp, LK, st))) return rc;
-        }
-        for (u32 g = 0; g < n_keys; ++g) {
-            const ckks_ksk* key = keys[g];
-            u64* out = ct_out + ((size_t)i * n_keys + g) * ct_words;
-            if (k0->kind == CKKS_KSK_HYBRID_BOUNDED) {
-                if ((rc = digits_automorphism_launch(ctx, d0, dk, 1, D, key->base_log, key->exponent, st))) return rc;
-                if ((rc = ntt_forward_digits_launch(ctx, dk, Y, D, lqp, LK, st))) return rc;
-                if ((rc = ks_mac_launch(ctx, Y, key->d_entries, b_hat, acc, Lq, D, true, 0, key->exponent, st)))
-                    return rc;
-            } else {
-                if ((rc = ks_mac_launch(ctx, Y, key->d_entries, b_hat, acc, Lq, D, true, key->exponent,
-                                        key->exponent, st)))
-                    return rc;
-            }
-            if ((rc = ntt_inverse_launch_map(ctx, acc, Z, 2, lqp, LK, st))) return rc;
-            if ((rc = mod_down_launch(ctx, Z, out, 2, Lq, st))) return rc;
-        }
+// Galois key entries [polys][N] (each poly one (digit, limb, component)):
+// storage[pi_g(k)] = reference[k] (to_storage) or the inverse.
+namespace {
+__global__ void k_permute_entries(const u64* __restrict__ src, u64* __restrict__ dst, int log_n, u64 g, int to_storage) {
+    const u32 n = 1u << log_n;
+    const u32 k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const size_t base = (size_t)blockIdx.y << log_n;
+    const u32 s = galois_src(k, g, log_n);
+    if (to_storage) dst[base + s] = src[base + k];
+    else dst[base + k] = src[base + s];
+}
+}  // namespace
+
+int32_t ksk_permute_entries(ckks_ctx* ctx, const u64* src, u64* dst, size_t polys, u64 exponent, bool to_storage,
+                            cudaStream_t st) {
+    for (size_t p0 = 0; p0 < polys; p0 += 65535) {
+        const u32 cnt = (u32)((polys - p0) < 65535 ? (polys - p0) : 65535);
+        dim3 g((ctx->n + kT - 1) / kT, cnt);
+        k_permute_entries<<<g, kT, 0, st>>>(src + (p0 << ctx->log_n), dst + (p0 << ctx->log_n), ctx->log_n, exponent,
+                                            to_storage ? 1 : 0);
     }
+    CKKS_CUDA_TRY(cudaGetLastError());
     return CKKS_OK;
 }

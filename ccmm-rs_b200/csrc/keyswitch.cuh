@@ -10,6 +10,11 @@
 //   HYBRID_RNS_BLOCK: entries [dnum][q_limbs+K][2][N], encrypting P * E_i * sigma(s)
 //   RELIN_BOUNDED  : entries [D][2][q_limbs][N], NTT domain, encrypting B^j * s^2
 //                    over Q (bounded_key_switch.rs:22-120)
+// Galois keys are stored permuted by their own automorphism: slot pi_g(k)
+// (ring/ntt_galois_permutation.rs:5-19 source index) holds the reference
+// entry of slot k, so the key-switch MAC runs contiguously in the permuted
+// index and sigma_g is applied as the final coefficient scatter. Upload and
+// download convert from and to the reference layout.
 struct ckks_ksk {
     ckks_ctx* ctx = nullptr;
     int kind = 0;
@@ -36,12 +41,14 @@ int32_t rnsblock_prepare(ckks_ctx* ctx, ckks_ksk* key);
 int32_t rnsblock_modup_launch(ckks_ctx* ctx, const ckks_ksk* key, const u64* a, u64* Y, cudaStream_t st);
 
 int32_t ks_mac_launch(ckks_ctx* ctx, const u64* Y, const u64* key, const u64* base, u64* acc, u32 q_limbs, u32 D,
-                      bool with_p, u64 perm_y, u64 perm_b, cudaStream_t st);
+                      bool with_p, u64 perm_y, u64 perm_b, cudaStream_t st, u64 perm_key = 0);
+// Galois key entries [D][LK][2][N]: reference layout <-> permuted storage.
+int32_t ksk_permute_entries(ckks_ctx* ctx, const u64* src, u64* dst, size_t polys, u64 exponent, bool to_storage,
+                            cudaStream_t st);
+
 int32_t rotate_hybrid(ckks_ctx* ctx, const ckks_ksk* key, const u64* ct_in, u64* ct_out, u32 n_ct, cudaStream_t st);
 int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_keys, const u64* ct_in, u64* ct_out,
                            u32 n_ct, cudaStream_t st);
-int32_t rotate_hybrid_hoisted_digits(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_keys, const u64* ct_in,
-                                     u64* ct_out, u32 n_ct, cudaStream_t st);
 int32_t rotate_hybrid_hoisted(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_keys, const u64* ct_in, u64* ct_out,
                               u32 n_ct, cudaStream_t st);
 
