@@ -1,6 +1,15 @@
 """Throughput benchmark of the B200 RNS-CKKS hot path.
 
-python bench.py [--gpus N] [--steps K] [--warmup W] [--workload ntt] [--impl reference]
+python bench.py [--gpus N] [--steps K] [--warmup W] [--workload rotation|ntt] [--impl reference]
+
+Workload "rotation" (default): hoisted key-switched Galois rotations at
+N=2^16 over 24 Q limbs of 50-bit primes and 3 auxiliary 60-bit primes (the
+reference's prime search), the reference's bounded hybrid-QP gadget with base
+2^32 (38 digits, tests/r30_9a_13_hybrid_65536.rs default), 16 ciphertexts each
+rotated by the same 32 Galois steps (powers of two 1..2^14 and odd steps
+3..35) sharing one decomposition per ciphertext. One step = all 512
+rotations; outputs are word-for-word the reference algorithm's. Metric:
+rotations per second.
 
 Workload "ntt": batched forward + inverse negacyclic NTT at N=2^16 over 32
 limbs of 50-bit primes q = 1 mod 2N (the reference's prime search), 64
@@ -262,6 +271,25 @@ def ntt_cpu_sample(threads, seconds_target=10.0):
 def reference_arm(args, world, rank):
     if rank != 0:
         return None
+    if args.workload == "rotation":
+        threads = os.cpu_count() or 1
+        vals, sample = [], None
+        for i in range(args.warmup + args.steps):
+            if i < args.warmup and i > 0:
+                continue  # one untimed warm-up pass: the key generation dominates and is not timed
+            v, sample = rot_cpu_sample(threads, n_keys=1 if i < args.warmup else 2)
+            if i >= args.warmup:
+                vals.append(v)
+        value = float(np.median(vals))
+        return {
+            "metric": "key-switched rotations/s (N=2^16, 24 limbs, hoisted, bit-exact)", "value": value,
+            "unit": "rotations/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * ROT_NCT * len(ROT_STEPS) / value, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded uniform ciphertexts)",
+            "config": rot_config(), "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "rotations/s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "rotations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
     threads = os.cpu_count() or 1
     per_step = []
     sample = None
@@ -373,6 +401,39 @@ def bench_rot_gpu(args, world, rank, local):
     return line
 
 
+def rot_cpu_sample(threads, n_keys=2):
+    """Times the oracle's restatement of the reference's hoisted hybrid-QP
+    rotation (hybrid_rns_galois_key.rs:550-780 with bounded_gadget.rs:273-312
+    hoisting) on the host: one ciphertext per thread, n_keys Galois keys each,
+    each rotation single-threaded (the reference's rayon granularity)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import ctypes
+    from oracle_lib import Oracle, P, arr, u64p
+    o = Oracle()
+    n = 1 << ROT_LOG_N
+    q = arr(o.primes_below_bits(ROT_QBITS, n, ROT_L))
+    p = arr(o.primes_below_bits(ROT_PBITS, n, ROT_K))
+    rng = np.random.default_rng(77)
+    secret = rng.integers(-1, 2, n).astype(np.int8)
+    exps = [int(o.L.oracle_rotation_exponent_left(n, r)) for r in ROT_STEPS[:n_keys]]
+    import concurrent.futures as cf
+    with cf.ThreadPoolExecutor(n_keys) as ex:
+        keys = list(ex.map(lambda ik: o.hybrid_key(q, p, secret, ik[1], ROT_BASE_LOG, seed=500 + ik[0]),
+                           enumerate(exps)))
+    cts = np.stack([np.stack([rng.integers(0, m, (2, n), dtype=np.uint64) for m in q], axis=1)
+                    for _ in range(threads)])
+    out = np.zeros((threads, n_keys, 2, ROT_L, n), np.uint64)
+    kp = (u64p * n_keys)(*[P(k) for k in keys])
+    ex_arr = arr(exps)
+    t = time.perf_counter()
+    o.L.oracle_hybrid_rotate_hoisted_batch(P(q), ROT_L, P(p), ROT_K, n, ROT_BASE_LOG, n_keys, P(ex_arr), kp,
+                                           threads, P(cts), P(out), threads)
+    dt = time.perf_counter() - t
+    rots = threads * n_keys
+    return rots / dt, ("%d ciphertexts x %d Galois keys (one ciphertext per thread), N=2^16, 24+3 limbs, "
+                       "base 2^32, %.1f s" % (threads, n_keys, dt))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -394,7 +455,14 @@ def main():
     else:
         line = bench_rot_gpu(args, world, rank, local)
         if rank == 0:
+            threads = os.cpu_count() or 1
+            v, sample = rot_cpu_sample(threads)
+            line["cpu_baseline"] = {"value": v, "unit": "rotations/s", "cores": threads, "kind": "port",
+                                    "sample": sample}
             print(json.dumps(line), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
         return
     if rank == 0:
         threads = os.cpu_count() or 1
