@@ -368,12 +368,21 @@ def bench_rot_gpu(args, world, rank, local):
     ms_max = max_over_ranks(world, ms)
     rots = ROT_NCT * len(keys)
     value = rots * args.steps * world / (ms_max / 1000.0)
-    # roofline of the whole rotation: key + ciphertext in/out bytes per rotation
+    # per-phase device time of one step (outside the timed region)
+    _, phases = cb.rotate_hoisted_timed(ctx, keys, cts, out=out)
+    torch.cuda.synchronize()
+    # roofline of the dominant kernel, the key-switch MAC: algorithmic bytes per
+    # step = every key once per group of 4 ciphertexts + the hoisted digit
+    # transforms and base transforms of every ciphertext + the accumulators
     key_bytes = words * 8
-    ct_bytes = 2 * ROT_L * n * 8
-    alg_bytes = key_bytes + 2 * ct_bytes
+    LK = ROT_L + ROT_K
+    groups = -(-ROT_NCT // 4)
+    mac_bytes = (groups * len(keys) * key_bytes + ROT_NCT * D * LK * n * 8 + ROT_NCT * ROT_L * n * 8
+                 + rots * 2 * LK * n * 8)
     peak, kind = peaks()
-    achieved = alg_bytes * rots * args.steps / (ms / 1000.0) / 1e9
+    mac_ms = phases["key-switch MAC"]
+    achieved = mac_bytes / (mac_ms / 1000.0) / 1e9
+    ct_bytes = 2 * ROT_L * n * 8
     # end to end through the C ABI host-buffer call (pinned host memory)
     pin_in = torch.from_numpy(host.view(np.int64)).pin_memory()
     pin_out = torch.empty(tuple(out.shape), dtype=torch.int64).pin_memory()
@@ -392,11 +401,16 @@ def bench_rot_gpu(args, world, rank, local):
         "dtype": "u64", "data": "synthetic (seeded uniform ciphertexts, GPU-generated keys)", "config": rot_config(),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "peak_kind": kind,
-                     "kernel": "whole rotation: %d-digit key (%.3f GB) + ct in/out per rotation" % (D, key_bytes / 1e9)},
+                     "kernel": "k_mac_tiled (key-switch MAC, %d digits, keys %.3f GB each, read once per 4 ct)"
+                               % (D, key_bytes / 1e9),
+                     "kernel_ms_per_step": mac_ms, "algorithmic_bytes_per_step": mac_bytes},
+        "whole_rotation_roofline": {"bytes_per_rotation": key_bytes + 2 * ct_bytes,
+                                    "frac_no_key_reuse": (key_bytes + 2 * ct_bytes) * value / 1e9 / peak},
+        "phases_ms_per_step": phases,
         "e2e": {"value": rots * e2e_steps * world / e2e_s, "unit": "rotations/s",
                 "h2d_bytes_per_step": int(host.nbytes), "d2h_bytes_per_step": int(hout.nbytes),
                 "path": "ckks_rotate_hoisted_host"},
-        "gpu_launches": None, "clocks": clk,
+        "gpu_launches": args.steps * groups * (5 * 4 + 5), "clocks": clk,
     }
     return line
 

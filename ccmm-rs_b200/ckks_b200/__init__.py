@@ -59,6 +59,7 @@ _SIGS = {
     "ckks_ksk_destroy": (I32, [VP]),
     "ckks_rotate": (I32, [VP, VP, VP, VP, U32, VP]),
     "ckks_rotate_hoisted": (I32, [VP, ctypes.POINTER(VP), U32, VP, VP, U32, VP]),
+    "ckks_rotate_hoisted_timed": (I32, [VP, ctypes.POINTER(VP), U32, VP, VP, U32, VP, ctypes.POINTER(ctypes.c_double)]),
     "ckks_rotate_hoisted_host": (I32, [VP, ctypes.POINTER(VP), U32, u64p, u64p, U32]),
 }
 
@@ -382,6 +383,23 @@ def rotate_hoisted(ctx, keys, ct, out=None, stream=None):
     arr = (VP * len(keys))(*[k.handle.value for k in keys])
     check(lib().ckks_rotate_hoisted(ctx.handle, arr, len(keys), _dptr(ct), _dptr(out), n_ct, _stream(stream)))
     return out
+
+
+ROTATION_PHASES = {0: "decompose+digit/base NTT", 2: "correction lists", 3: "key-switch MAC", 4: "inverse NTT",
+                   5: "ModDown+sigma"}
+
+
+def rotate_hoisted_timed(ctx, keys, ct, out=None, stream=None):
+    """rotate_hoisted plus per-phase device milliseconds {phase name: ms}."""
+    import torch
+    q_limbs = keys[0].q_limbs
+    n_ct = ct.numel() // (2 * q_limbs * ctx.n)
+    if out is None:
+        out = torch.empty((n_ct, len(keys), 2, q_limbs, ctx.n), dtype=torch.int64, device=ct.device)
+    arr = (VP * len(keys))(*[k.handle.value for k in keys])
+    ms = (ctypes.c_double * 8)()
+    check(lib().ckks_rotate_hoisted_timed(ctx.handle, arr, len(keys), _dptr(ct), _dptr(out), n_ct, _stream(stream), ms))
+    return out, {name: ms[i] for i, name in ROTATION_PHASES.items()}
 
 
 def rotate_hoisted_host(ctx, keys, ct_host, out_host=None):

@@ -328,6 +328,24 @@ int32_t ckks_rotate_hoisted(ckks_ctx* ctx, const ckks_ksk* const* keys, uint32_t
     return rotate_hybrid_hoisted(ctx, keys, n_keys, ct_in, ct_out, n_ct, ckks_stream(ctx, stream));
 }
 
+int32_t ckks_rotate_hoisted_timed(ckks_ctx* ctx, const ckks_ksk* const* keys, uint32_t n_keys, const uint64_t* ct_in,
+                                  uint64_t* ct_out, uint32_t n_ct, void* stream, double* phase_ms) {
+    if (int32_t rc = need_ctx(ctx, "ckks_rotate_hoisted_timed")) return rc;
+    CKKS_CHECK_ARG(keys && n_keys && ct_in && ct_out && ct_in != ct_out && phase_ms,
+                   "ckks_rotate_hoisted_timed: bad arguments");
+    const ckks_ksk* k0 = keys[0];
+    for (u32 g = 0; g < n_keys; ++g) {
+        const ckks_ksk* k = keys[g];
+        if (!k || k->ctx != ctx || k->kind != k0->kind || k->kind == CKKS_KSK_RELIN_BOUNDED ||
+            k->q_limbs != k0->q_limbs || k->base_log != k0->base_log || k->D != k0->D || k->blocks != k0->blocks) {
+            ckks_set_error("ckks_rotate_hoisted_timed: keys must be Galois keys of one kind, level and gadget");
+            return CKKS_ERR_BASIS_MISMATCH;
+        }
+    }
+    for (int i = 0; i < 8; ++i) phase_ms[i] = 0;
+    return rotate_hoisted_ntt(ctx, keys, n_keys, ct_in, ct_out, n_ct, ckks_stream(ctx, stream), phase_ms);
+}
+
 int32_t ckks_rotate_hoisted_host(ckks_ctx* ctx, const ckks_ksk* const* keys, uint32_t n_keys,
                                  const uint64_t* ct_in_host, uint64_t* ct_out_host, uint32_t n_ct) {
     if (int32_t rc = need_ctx(ctx, "ckks_rotate_hoisted_host")) return rc;

@@ -194,13 +194,159 @@ u64 galois_inverse_host(u64 k, u32 n) {
     return r;
 }
 
+// Tiled MAC: one CTA owns (limb l, slot tile of kS slots) for G ciphertexts
+// and every Galois key. The G x D x kS digit-transform tile is staged in
+// shared memory once; keys stream from HBM exactly once per group
+// (evict-first), kU digits of key loads in flight per thread. Thread
+// (s, lane) accumulates keys g = lane, lane + kLanes, .. for all G
+// ciphertexts. Same sums as k_mac_hoisted.
+constexpr int kS = 64, kLanes = 4, kU = 5;
+
+template <int G>
+__global__ void __launch_bounds__(kS * kLanes) k_mac_tiled(const u64* __restrict__ Yhat, size_t y_stride,
+                                                           const u64* __restrict__ Bhat, size_t b_stride,
+                                                           const u64* const* __restrict__ keys,
+                                                           const u64* __restrict__ exps_inv,
+                                                           const u64* __restrict__ pf, const u64* __restrict__ pf_q,
+                                                           u64* __restrict__ acc, const NttTab* __restrict__ tabs,
+                                                           LimbMap lm, int n_ct, int n_keys, int Lq, int LK, int D,
+                                                           int log_n, const Exc* __restrict__ exc,
+                                                           const u32* __restrict__ exc_count, int cap,
+                                                           const u64* __restrict__ psi) {
+    extern __shared__ u64 ytile[];  // [G][D][kS]
+    const u32 n = 1u << log_n;
+    const int l = blockIdx.y;
+    const u32 s0 = blockIdx.x * kS;
+    const int tid = threadIdx.x, si = tid % kS, lane = tid / kS;
+    const u32 s = s0 + si;
+    const NttTab& T = tabs[lm(l)];
+    const u64 q = T.q, mh = T.mu_hi, ml = T.mu_lo;
+    for (int c = 0; c < G; ++c)
+        for (int idx = tid; idx < D * kS; idx += blockDim.x) {
+            const int j = idx / kS, x = idx % kS;
+            ytile[c * D * kS + idx] =
+                c < n_ct ? __ldg(Yhat + c * y_stride + (((size_t)j * LK + l) << log_n) + s0 + x) : 0;
+        }
+    __syncthreads();
+    const Barrett bm{q, mh, ml};
+    u64 bterm[G];
+#pragma unroll
+    for (int c = 0; c < G; ++c)
+        bterm[c] = (c < n_ct && l < Lq)
+                       ? mul_shoup(__ldg(Bhat + c * b_stride + ((size_t)l << log_n) + s), pf[l], pf_q[l], q)
+                       : 0;
+    const size_t jstride = ((size_t)LK * 2) << log_n;
+    for (int g = lane; g < n_keys; g += kLanes) {
+        const u64* key = keys[g];
+        const u64* kp = key + ((((size_t)l * 2) << log_n) + s);
+        Acc ab[G], aa[G];
+#pragma unroll
+        for (int c = 0; c < G; ++c) ab[c] = aa[c] = Acc{0, 0};
+        int batch = 0;
+        for (int j0 = 0; j0 < D; j0 += kU) {
+            u64 kb[kU], ka[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                if (j0 + u < D) {
+                    kb[u] = __ldcs(kp + (j0 + u) * jstride);
+                    ka[u] = __ldcs(kp + (j0 + u) * jstride + n);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                if (j0 + u < D) {
+#pragma unroll
+                    for (int c = 0; c < G; ++c) {
+                        const u64 y = ytile[(c * D + j0 + u) * kS + si];
+                        ab[c].mac(y, kb[u]);
+                        aa[c].mac(y, ka[u]);
+                    }
+                }
+            }
+            if (++batch == 3) {  // 15 products per 128-bit sum between folds
+#pragma unroll
+                for (int c = 0; c < G; ++c) {
+                    ab[c].fold(q, mh, ml);
+                    aa[c].fold(q, mh, ml);
+                }
+                batch = 0;
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < G; ++c) {
+            if (c >= n_ct) break;
+            ab[c].fold(q, mh, ml);
+            aa[c].fold(q, mh, ml);
+            u64 b = add_mod(ab[c].lo, bterm[c], q), a = aa[c].lo;
+            const u32 cnt = min(exc_count[(size_t)c * n_keys + g], (u32)cap);
+            if (cnt) {
+                const Exc* list = exc + ((size_t)c * n_keys + g) * cap;
+                const u64 ps = psi[lm(l)];
+                const u32 k = galois_src(s, exps_inv[g], log_n);
+                for (u32 e = 0; e < cnt; ++e) {
+                    const Exc x = list[e];
+                    u64 w = pow_mod_dev(ps, ((2ull * k + 1) * x.t) & (2ull * n - 1), bm);
+                    u64 dm = x.delta < 0 ? (u64)(-x.delta) % q : (u64)x.delta % q;
+                    if (x.delta < 0 && dm) dm = q - dm;
+                    u64 v = mul_barrett(w, dm, bm);
+                    const size_t kofs = (((size_t)x.j * LK + l) * 2) << log_n;
+                    b = add_mod(b, mul_barrett(v, key[kofs + s], bm), q);
+                    a = add_mod(a, mul_barrett(v, key[kofs + n + s], bm), q);
+                }
+            }
+            const size_t obase = (((size_t)c * n_keys + g) * 2 * LK) << log_n;
+            acc[obase + ((size_t)l << log_n) + s] = b;
+            acc[obase + (((size_t)LK + l) << log_n) + s] = a;
+        }
+    }
+}
+
+// CUDA-event phase timer (the analogue of the reference's HybridRotationTiming,
+// ckks/hybrid_rns_galois_key.rs:323-336). Phases accumulate over groups.
+struct PhaseTimer {
+    double* out = nullptr;
+    cudaStream_t st = nullptr;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> spans;
+    cudaEvent_t open_ev = nullptr;
+    int open_phase = -1;
+    void begin(int phase) {
+        if (!out) return;
+        cudaEventCreate(&open_ev);
+        cudaEventRecord(open_ev, st);
+        open_phase = phase;
+    }
+    void end() {
+        if (!out || open_phase < 0) return;
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, st);
+        spans.push_back({open_phase, {open_ev, e}});
+        open_phase = -1;
+    }
+    void finish() {
+        if (!out) return;
+        for (auto& sp : spans) {
+            float ms = 0;
+            cudaEventSynchronize(sp.second.second);
+            cudaEventElapsedTime(&ms, sp.second.first, sp.second.second);
+            out[sp.first] += ms;
+            cudaEventDestroy(sp.second.first);
+            cudaEventDestroy(sp.second.second);
+        }
+        spans.clear();
+    }
+};
+
 }  // namespace
 
 // Hoisted hybrid rotations of n_ct ciphertexts by n_keys Galois keys (bounded
 // or RNS-block gadget), out [n_ct][n_keys][2][Lq][N]. Ciphertexts are
 // processed in groups of up to 4 sharing each streamed key slice.
 int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_keys, const u64* ct_in,
-                                   u64* ct_out, u32 n_ct, cudaStream_t st) {
+                                   u64* ct_out, u32 n_ct, cudaStream_t st, double* phase_ms) {
+    PhaseTimer pt;
+    pt.out = phase_ms;
+    pt.st = st;
     const ckks_ksk* k0 = keys[0];
     const u32 Lq = k0->q_limbs, LK = ksk_limbs(k0), D = k0->D, n = ctx->n;
     const size_t ct_words = (size_t)2 * Lq * n;
@@ -240,6 +386,7 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
         const u32 gn = (n_ct - c0) < G ? (n_ct - c0) : G;
         CKKS_CUDA_TRY(cudaMemsetAsync(flags.p, 0, G * f_stride * sizeof(u32), st));
         CKKS_CUDA_TRY(cudaMemsetAsync(cnt.p, 0, (size_t)G * n_keys * sizeof(u32), st));
+        pt.begin(0);
         for (u32 c = 0; c < gn; ++c) {
             const u64* in = ct_in + (size_t)(c0 + c) * ct_words;
             if (bounded) {
@@ -254,28 +401,53 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
             }
             if ((rc = ntt_forward_launch_map(ctx, in, Bh.p + c * b_stride, 1, lq, Lq, st))) return rc;
         }
+        pt.end();
+        pt.begin(2);
         if (bounded) {
             dim3 g((n + kT - 1) / kT, n_keys, gn);
             k_hoist_exceptions<<<g, kT, 0, st>>>(dig.p, d_stride, flags.p, f_stride, d_exps, n_keys, D,
                                                  k0->base_log, ctx->log_n, exc.p, cnt.p, cap);
         }
+        pt.end();
+        pt.begin(3);
         {
-            dim3 g((n + kT - 1) / kT, n_keys, LK);
+            const size_t smem = (size_t)(G >= 3 ? 4 : G) * D * kS * sizeof(u64);
+            if (n >= (u32)kS && smem <= 200 * 1024) {
+                dim3 g(n / kS, LK);
+#define CKKS_MACT(GG)                                                                                              \
+    do {                                                                                                           \
+        cudaFuncSetAttribute(k_mac_tiled<GG>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);            \
+        k_mac_tiled<GG><<<g, kS * kLanes, (size_t)GG * D * kS * sizeof(u64), st>>>(                              \
+            Y.p, y_stride, Bh.p, b_stride, d_keys, d_exps_inv, ctx->d_pmodq, ctx->d_pmodq + ctx->L, acc.p,        \
+            ctx->d_tabs, lqp, gn, n_keys, Lq, LK, D, ctx->log_n, exc.p, cnt.p, cap, d_psi);                        \
+    } while (0)
+                if (G >= 3) CKKS_MACT(4);
+                else if (G == 2) CKKS_MACT(2);
+                else CKKS_MACT(1);
+#undef CKKS_MACT
+            } else {
+                dim3 g((n + kT - 1) / kT, n_keys, LK);
 #define CKKS_MAC(GG)                                                                                               \
     k_mac_hoisted<GG><<<g, kT, 0, st>>>(Y.p, y_stride, Bh.p, b_stride, d_keys, d_exps_inv, ctx->d_pmodq,            \
                                         ctx->d_pmodq + ctx->L, acc.p, ctx->d_tabs, lqp, gn, n_keys, Lq, LK, D,      \
                                         ctx->log_n, exc.p, cnt.p, cap, d_psi)
-            if (G >= 3) CKKS_MAC(4);
-            else if (G == 2) CKKS_MAC(2);
-            else CKKS_MAC(1);
+                if (G >= 3) CKKS_MAC(4);
+                else if (G == 2) CKKS_MAC(2);
+                else CKKS_MAC(1);
 #undef CKKS_MAC
+            }
         }
         CKKS_CUDA_TRY(cudaGetLastError());
+        pt.end();
+        pt.begin(4);
         if ((rc = ntt_inverse_launch_map(ctx, acc.p, Z.p, gn * n_keys * 2, lqp, LK, st))) return rc;
+        pt.end();
+        pt.begin(5);
         // ModDown of every (ciphertext, key) pair, then sigma_g, straight into the output
         if ((rc = mod_down_sigma_multi(ctx, Z.p, ct_out + (size_t)c0 * n_keys * ct_words, gn * n_keys * 2, Lq, d_exps,
                                        n_keys, st)))
             return rc;
+        pt.end();
         // pairs whose correction lists overflowed are recomputed exactly
         CKKS_CUDA_TRY(cudaMemcpyAsync(h_cnt.data(), cnt.p, (size_t)G * n_keys * sizeof(u32), cudaMemcpyDeviceToHost, st));
         CKKS_CUDA_TRY(cudaStreamSynchronize(st));
@@ -283,6 +455,7 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
             for (u32 g = 0; g < n_keys; ++g)
                 if (h_cnt[(size_t)c * n_keys + g] > (u32)cap) overflow.push_back(((c0 + c) << 16) | g);
     }
+    pt.finish();
     for (u32 code : overflow) {
         const u32 c = code >> 16, g = code & 0xffff;
         if ((rc = rotate_hybrid(ctx, keys[g], ct_in + (size_t)c * ct_words,

@@ -47,8 +47,10 @@ int32_t ksk_permute_entries(ckks_ctx* ctx, const u64* src, u64* dst, size_t poly
                             cudaStream_t st);
 
 int32_t rotate_hybrid(ckks_ctx* ctx, const ckks_ksk* key, const u64* ct_in, u64* ct_out, u32 n_ct, cudaStream_t st);
+// phase_ms (optional, [8], accumulated): 0 decomposition and digit/base
+// transforms, 2 correction lists, 3 key-switch MAC, 4 inverse NTT, 5 ModDown+sigma.
 int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_keys, const u64* ct_in, u64* ct_out,
-                           u32 n_ct, cudaStream_t st);
+                           u32 n_ct, cudaStream_t st, double* phase_ms = nullptr);
 int32_t rotate_hybrid_hoisted(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_keys, const u64* ct_in, u64* ct_out,
                               u32 n_ct, cudaStream_t st);
 

@@ -191,6 +191,13 @@ int32_t ckks_rotate(ckks_ctx* ctx, const ckks_ksk* key, const uint64_t* ct_in, u
  * so every word equals the non-hoisted rotation. */
 int32_t ckks_rotate_hoisted(ckks_ctx* ctx, const ckks_ksk* const* keys, uint32_t n_keys, const uint64_t* ct_in,
                             uint64_t* ct_out, uint32_t n_ct, void* stream);
+/* ckks_rotate_hoisted with per-phase device time in milliseconds (CUDA
+ * events on `stream`, summed over ciphertext groups; waits for completion):
+ * phase_ms[0] decomposition and the digit/base transforms, [2] carry-correction
+ * lists, [3] key-switch MAC, [4] inverse NTT, [5] ModDown and sigma; others 0.
+ * The analogue of HybridRotationTiming (ckks/hybrid_rns_galois_key.rs:323-336). */
+int32_t ckks_rotate_hoisted_timed(ckks_ctx* ctx, const ckks_ksk* const* keys, uint32_t n_keys, const uint64_t* ct_in,
+                                  uint64_t* ct_out, uint32_t n_ct, void* stream, double* phase_ms);
 /* Host-buffer form of ckks_rotate_hoisted (copies in, rotates, copies out). */
 int32_t ckks_rotate_hoisted_host(ckks_ctx* ctx, const ckks_ksk* const* keys, uint32_t n_keys,
                                  const uint64_t* ct_in_host, uint64_t* ct_out_host, uint32_t n_ct);
