@@ -35,6 +35,7 @@ _SIGS = {
     "ckks_ctx_psi": (I32, [VP, u64p]),
     "ckks_ntt_forward": (I32, [VP, VP, VP, U32, U32, U32, VP]),
     "ckks_ntt_inverse": (I32, [VP, VP, VP, U32, U32, U32, VP]),
+    "ckks_ntt_forward_inplace_static": (I32, [VP, VP, U32, U32, U32, VP]),
     "ckks_ntt_forward_host": (I32, [VP, u64p, u64p, U32, U32, U32]),
     "ckks_ntt_inverse_host": (I32, [VP, u64p, u64p, U32, U32, U32]),
     "ckks_automorphism_coef": (I32, [VP, VP, VP, U32, U32, U32, U64, VP]),

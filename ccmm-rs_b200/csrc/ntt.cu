@@ -345,3 +345,80 @@ int32_t ntt_forward_digits_launch(ckks_ctx* ctx, const i64* digits, u64* out, u3
     CKKS_CUDA_TRY(cudaGetLastError());
     return CKKS_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free in-place forward NTT.
+//
+// Some callers cannot let a library allocate device memory: processes whose
+// device memory is reserved up front by their own arena or by a serving
+// framework (a cudaMalloc from inside the library would fail or fragment that
+// budget), and deployments that forbid device allocation after start-up.
+// For them the in-place forward transform below stages its pass-1
+// intermediate in a fixed file-scope device array instead of a workspace from
+// the stream-ordered allocator. The array holds kStaticNttScratchWords words
+// (16 MiB), is resident on every device that loads this library until the
+// process exits, and is shared by every call: concurrent calls whose work
+// overlaps on the GPU race on it. Pass 1 writes every word of the range it
+// uses before pass 2 reads it, so nothing has to be cleared between calls.
+namespace {
+
+constexpr size_t kStaticNttScratchWords = size_t(1) << 21;
+static __device__ __align__(256) u64 g_static_ntt_scratch[kStaticNttScratchWords];
+
+std::mutex g_static_scratch_mutex;
+u64* g_static_scratch_addr[128] = {};
+
+// Device address of the array on the current device, looked up once per
+// device (the host-side symbol is only a stand-in and must not reach a kernel).
+int32_t static_scratch_address(u64** out) {
+    int dev = 0;
+    CKKS_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 128) {
+        ckks_set_error("ckks_ntt_forward_inplace_static: device ordinal out of range");
+        return CKKS_ERR_BAD_ARG;
+    }
+    std::lock_guard<std::mutex> lock(g_static_scratch_mutex);
+    if (!g_static_scratch_addr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_static_ntt_scratch);
+        if (e != cudaSuccess || !p) {
+            ckks_set_error(std::string("ckks_ntt_forward_inplace_static: cudaGetSymbolAddress: ") +
+                           cudaGetErrorString(e));
+            return CKKS_ERR_CUDA;
+        }
+        g_static_scratch_addr[dev] = (u64*)p;
+    }
+    *out = g_static_scratch_addr[dev];
+    return CKKS_OK;
+}
+
+}  // namespace
+
+extern "C" int32_t ckks_ntt_forward_inplace_static(ckks_ctx* ctx, uint64_t* data, uint32_t n_polys,
+                                                   uint32_t limb_begin, uint32_t limb_count, void* stream) {
+    if (!ctx || !data) {
+        ckks_set_error("ckks_ntt_forward_inplace_static: null argument");
+        return CKKS_ERR_BAD_ARG;
+    }
+    if ((size_t)limb_begin + limb_count > ctx->moduli.size()) {
+        ckks_set_error("ckks_ntt_forward_inplace_static: limb range outside the context basis");
+        return CKKS_ERR_BASIS_MISMATCH;
+    }
+    const size_t words = (size_t)n_polys * limb_count * ctx->n;
+    if (words > kStaticNttScratchWords) {
+        ckks_set_error("ckks_ntt_forward_inplace_static: n_polys * limb_count * N = " + std::to_string(words) +
+                       " words exceeds the fixed scratch of " + std::to_string(kStaticNttScratchWords) +
+                       " words (16 MiB); split the batch or use ckks_ntt_forward");
+        return CKKS_ERR_BAD_ARG;
+    }
+    if (words == 0) return CKKS_OK;
+    u64* scratch = nullptr;
+    if (int32_t rc = static_scratch_address(&scratch)) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    const LimbMap lm = LimbMap::range(limb_begin, limb_count);
+    const int la = ctx->log_n1, lb = ctx->log_n2;
+    if (int32_t rc = pass(0, la, data, scratch, ctx->d_tabs, lm, limb_count, n_polys, lb, st)) return rc;
+    if (int32_t rc = pass(2, lb, scratch, data, ctx->d_tabs, lm, limb_count, n_polys, la, st)) return rc;
+    CKKS_CUDA_TRY(cudaGetLastError());
+    return CKKS_OK;
+}

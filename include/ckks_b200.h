@@ -86,6 +86,19 @@ int32_t ckks_ntt_forward(ckks_ctx* ctx, const uint64_t* in, uint64_t* out, uint3
  * (ring/prepared_ntt.rs:327-398), PreparedRnsNttPlan::inverse (:62-83). */
 int32_t ckks_ntt_inverse(ckks_ctx* ctx, const uint64_t* in, uint64_t* out, uint32_t n_polys,
                          uint32_t limb_begin, uint32_t limb_count, void* stream);
+/* In-place forward NTT that allocates no device memory (no counterpart in
+ * the reference). For callers that cannot let a library allocate device
+ * memory -- their device memory is reserved up front by their own arena or a
+ * serving framework, or their deployment forbids device allocation after
+ * start-up. The pass-1 intermediate lives in a fixed 16 MiB device array
+ * compiled into the library (resident on every device that loads it until the
+ * process exits); batches with n_polys * limb_count * N > 2^21 words are
+ * rejected with CKKS_ERR_BAD_ARG. The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress); make that first call before
+ * any stream capture. All calls share the array: calls whose work overlaps on
+ * the GPU race. Output equals ckks_ntt_forward word for word. */
+int32_t ckks_ntt_forward_inplace_static(ckks_ctx* ctx, uint64_t* data, uint32_t n_polys, uint32_t limb_begin,
+                                        uint32_t limb_count, void* stream);
 /* Host-buffer forms: copy in, transform, copy out (synchronous). */
 int32_t ckks_ntt_forward_host(ckks_ctx* ctx, const uint64_t* in_host, uint64_t* out_host, uint32_t n_polys,
                               uint32_t limb_begin, uint32_t limb_count);
