@@ -29,34 +29,6 @@ struct Exc {
     i64 delta;
 };
 
-// Reduce x = xhi * 2^64 + xlo (xhi < q) modulo q (Barrett, mu = floor(2^128/q)).
-__device__ __forceinline__ u64 reduce_wide(u64 xhi, u64 xlo, u64 q, u64 mu_hi, u64 mu_lo) {
-    u64 p0_hi = __umul64hi(xlo, mu_lo);
-    u64 p1_lo = xlo * mu_hi, p1_hi = __umul64hi(xlo, mu_hi);
-    u64 p2_lo = xhi * mu_lo, p2_hi = __umul64hi(xhi, mu_lo);
-    u64 mid = p0_hi + p1_lo;
-    u64 c = mid < p0_hi;
-    u64 mid2 = mid + p2_lo;
-    c += mid2 < mid;
-    u64 qt = xhi * mu_hi + p1_hi + p2_hi + c;
-    u64 r = xlo - qt * q;
-    while (r >= q) r -= q;
-    return r;
-}
-
-struct Acc {
-    u64 hi, lo;
-    __device__ __forceinline__ void mac(u64 a, u64 b) {
-        u64 pl = a * b, ph = __umul64hi(a, b);
-        lo += pl;
-        hi += ph + (lo < pl);
-    }
-    __device__ __forceinline__ void fold(u64 q, u64 mh, u64 ml) {
-        u64 h = hi >= q ? reduce_wide(0, hi, q, mh, ml) : hi;
-        lo = reduce_wide(h, lo, q, mh, ml);
-        hi = 0;
-    }
-};
 
 __device__ __forceinline__ u64 pow_mod_dev(u64 b, u64 e, const Barrett& m) {
     u64 r = 1;
@@ -126,9 +98,9 @@ __global__ void __launch_bounds__(kT) k_mac_hoisted(const u64* __restrict__ Yhat
     const NttTab& T = tabs[lm(l)];
     const u64 q = T.q, mh = T.mu_hi, ml = T.mu_lo;
     const u64* key = keys[g];
-    Acc ab[G], aa[G];
+    Acc128 ab[G], aa[G];
 #pragma unroll
-    for (int c = 0; c < G; ++c) ab[c] = aa[c] = Acc{0, 0};
+    for (int c = 0; c < G; ++c) ab[c] = aa[c] = Acc128{0, 0};
     int since = 0;
     for (int j = 0; j < D; ++j) {
         const size_t kofs = (((size_t)j * LK + l) * 2) << log_n;
@@ -194,16 +166,42 @@ u64 galois_inverse_host(u64 k, u32 n) {
     return r;
 }
 
+// Split-operand accumulator: with sb = ceil(bits(q - 1) / 2), an operand
+// x < q is x1 * 2^sb + x0 (x0, x1 < 2^sb) and a product is
+// x0 y0 + (x0 y1 + x1 y0) 2^sb + x1 y1 2^(2 sb). Three 64-bit partial sums
+// take each 32 x 32 -> 64 multiply with accumulate (IMAD.WIDE.U32) without
+// carry handling; they are reduced mod q every `fold` terms (chosen so the
+// middle sum cannot overflow) and combined with 2^sb, 2^2sb mod q. The value
+// is the canonical residue of the same exact sum of products.
+struct SplitAcc {
+    u64 s0, s1, s2;
+    __device__ __forceinline__ void mac(u32 x0, u32 x1, u32 y0, u32 y1) {
+        s0 += (u64)x0 * y0;
+        s1 += (u64)x0 * y1;
+        s1 += (u64)x1 * y0;
+        s2 += (u64)x1 * y1;
+    }
+    // Reduce to the canonical residue, kept in s0 (s0 stays below
+    // q + fold * 2^(2 sb) < 2^64 until the next fold).
+    __device__ __forceinline__ void fold(u64 q, u64 one_q, u64 r1, u64 r1q, u64 r2, u64 r2q) {
+        u64 t = reduce_2q(mul_shoup_lazy(s0, 1, one_q, q), q);
+        t = add_mod(t, reduce_2q(mul_shoup_lazy(s1, r1, r1q, q), q), q);
+        t = add_mod(t, reduce_2q(mul_shoup_lazy(s2, r2, r2q, q), q), q);
+        s0 = t;
+        s1 = s2 = 0;
+    }
+};
+
 // Tiled MAC: one CTA owns (limb l, slot tile of kS slots) for G ciphertexts
 // and every Galois key. The G x D x kS digit-transform tile is staged in
-// shared memory once; keys stream from HBM exactly once per group
-// (evict-first), kU digits of key loads in flight per thread. Thread
-// (s, lane) accumulates keys g = lane, lane + kLanes, .. for all G
-// ciphertexts. Same sums as k_mac_hoisted.
-constexpr int kS = 64, kLanes = 4, kU = 5;
+// shared memory once (pre-split into its two sb-bit halves); keys stream from
+// HBM exactly once per group (evict-first), kU digits of key loads in flight
+// per thread. Thread (s, lane) accumulates keys g = lane, lane + kLanes, ..
+// for all G ciphertexts. Same sums as k_mac_hoisted.
+constexpr int kS = 64, kLanes = 4, kU = 4;
 
 template <int G>
-__global__ void __launch_bounds__(kS * kLanes) k_mac_tiled(const u64* __restrict__ Yhat, size_t y_stride,
+__global__ void __launch_bounds__(kS * kLanes, 2) k_mac_tiled(const u64* __restrict__ Yhat, size_t y_stride,
                                                            const u64* __restrict__ Bhat, size_t b_stride,
                                                            const u64* const* __restrict__ keys,
                                                            const u64* __restrict__ exps_inv,
@@ -213,7 +211,7 @@ __global__ void __launch_bounds__(kS * kLanes) k_mac_tiled(const u64* __restrict
                                                            int log_n, const Exc* __restrict__ exc,
                                                            const u32* __restrict__ exc_count, int cap,
                                                            const u64* __restrict__ psi) {
-    extern __shared__ u64 ytile[];  // [G][D][kS]
+    extern __shared__ u64 ytile[];  // [G][D][kS], each word (y >> sb) << 32 | (y & mask)
     const u32 n = 1u << log_n;
     const int l = blockIdx.y;
     const u32 s0 = blockIdx.x * kS;
@@ -221,11 +219,19 @@ __global__ void __launch_bounds__(kS * kLanes) k_mac_tiled(const u64* __restrict
     const u32 s = s0 + si;
     const NttTab& T = tabs[lm(l)];
     const u64 q = T.q, mh = T.mu_hi, ml = T.mu_lo;
+    const int sb = (65 - __clzll(q - 1)) / 2;  // ceil(bits(q - 1) / 2)
+    const u64 mask = (1ull << sb) - 1;
+    // middle sum grows by < 2^(2 sb + 1) per product: fold before 2^64
+    const u64 fold_lim = (~0ull) >> (2 * sb + 1);
+    const int fold_every = fold_lim > 8191 ? 8191 : (int)fold_lim;
+    const u64 one_q = shoup_quotient_dev(1, q);
+    const u64 r1 = (1ull << sb) % q, r2 = mul_barrett(r1, r1, Barrett{q, mh, ml});
+    const u64 r1q = shoup_quotient_dev(r1, q), r2q = shoup_quotient_dev(r2, q);
     for (int c = 0; c < G; ++c)
         for (int idx = tid; idx < D * kS; idx += blockDim.x) {
             const int j = idx / kS, x = idx % kS;
-            ytile[c * D * kS + idx] =
-                c < n_ct ? __ldg(Yhat + c * y_stride + (((size_t)j * LK + l) << log_n) + s0 + x) : 0;
+            u64 y = c < n_ct ? __ldg(Yhat + c * y_stride + (((size_t)j * LK + l) << log_n) + s0 + x) : 0;
+            ytile[c * D * kS + idx] = ((y >> sb) << 32) | (y & mask);
         }
     __syncthreads();
     const Barrett bm{q, mh, ml};
@@ -239,10 +245,10 @@ __global__ void __launch_bounds__(kS * kLanes) k_mac_tiled(const u64* __restrict
     for (int g = lane; g < n_keys; g += kLanes) {
         const u64* key = keys[g];
         const u64* kp = key + ((((size_t)l * 2) << log_n) + s);
-        Acc ab[G], aa[G];
+        SplitAcc ab[G], aa[G];
 #pragma unroll
-        for (int c = 0; c < G; ++c) ab[c] = aa[c] = Acc{0, 0};
-        int batch = 0;
+        for (int c = 0; c < G; ++c) ab[c] = aa[c] = SplitAcc{0, 0, 0};
+        int since = 0;
         for (int j0 = 0; j0 < D; j0 += kU) {
             u64 kb[kU], ka[kU];
 #pragma unroll
@@ -255,29 +261,32 @@ __global__ void __launch_bounds__(kS * kLanes) k_mac_tiled(const u64* __restrict
 #pragma unroll
             for (int u = 0; u < kU; ++u) {
                 if (j0 + u < D) {
+                    const u32 b0 = (u32)(kb[u] & mask), b1 = (u32)(kb[u] >> sb);
+                    const u32 a0 = (u32)(ka[u] & mask), a1 = (u32)(ka[u] >> sb);
 #pragma unroll
                     for (int c = 0; c < G; ++c) {
                         const u64 y = ytile[(c * D + j0 + u) * kS + si];
-                        ab[c].mac(y, kb[u]);
-                        aa[c].mac(y, ka[u]);
+                        const u32 y0 = (u32)y, y1 = (u32)(y >> 32);
+                        ab[c].mac(y0, y1, b0, b1);
+                        aa[c].mac(y0, y1, a0, a1);
+                    }
+                    if (++since == fold_every) {
+#pragma unroll
+                        for (int c = 0; c < G; ++c) {
+                            ab[c].fold(q, one_q, r1, r1q, r2, r2q);
+                            aa[c].fold(q, one_q, r1, r1q, r2, r2q);
+                        }
+                        since = 0;
                     }
                 }
-            }
-            if (++batch == 3) {  // 15 products per 128-bit sum between folds
-#pragma unroll
-                for (int c = 0; c < G; ++c) {
-                    ab[c].fold(q, mh, ml);
-                    aa[c].fold(q, mh, ml);
-                }
-                batch = 0;
             }
         }
 #pragma unroll
         for (int c = 0; c < G; ++c) {
             if (c >= n_ct) break;
-            ab[c].fold(q, mh, ml);
-            aa[c].fold(q, mh, ml);
-            u64 b = add_mod(ab[c].lo, bterm[c], q), a = aa[c].lo;
+            ab[c].fold(q, one_q, r1, r1q, r2, r2q);
+            aa[c].fold(q, one_q, r1, r1q, r2, r2q);
+            u64 b = add_mod(ab[c].s0, bterm[c], q), a = aa[c].s0;
             const u32 cnt = min(exc_count[(size_t)c * n_keys + g], (u32)cap);
             if (cnt) {
                 const Exc* list = exc + ((size_t)c * n_keys + g) * cap;

@@ -20,35 +20,6 @@ namespace {
 
 constexpr int kT = 256;
 
-// Reduce x = xhi * 2^64 + xlo (xhi < q) modulo q (Barrett, mu = floor(2^128 / q)).
-__device__ __forceinline__ u64 reduce_wide(u64 xhi, u64 xlo, u64 q, u64 mu_hi, u64 mu_lo) {
-    u64 p0_hi = __umul64hi(xlo, mu_lo);
-    u64 p1_lo = xlo * mu_hi, p1_hi = __umul64hi(xlo, mu_hi);
-    u64 p2_lo = xhi * mu_lo, p2_hi = __umul64hi(xhi, mu_lo);
-    u64 mid = p0_hi + p1_lo;
-    u64 c = mid < p0_hi;
-    u64 mid2 = mid + p2_lo;
-    c += mid2 < mid;
-    u64 qt = xhi * mu_hi + p1_hi + p2_hi + c;
-    u64 r = xlo - qt * q;
-    while (r >= q) r -= q;
-    return r;
-}
-
-struct Acc128 {
-    u64 hi = 0, lo = 0;
-    __device__ __forceinline__ void mac(u64 a, u64 b) {
-        u64 pl = a * b, ph = __umul64hi(a, b);
-        lo += pl;
-        hi += ph + (lo < pl);
-    }
-    __device__ __forceinline__ void fold(u64 q, u64 mu_hi, u64 mu_lo) {
-        u64 h = hi >= q ? reduce_wide(0, hi, q, mu_hi, mu_lo) : hi;
-        lo = reduce_wide(h, lo, q, mu_hi, mu_lo);
-        hi = 0;
-    }
-};
-
 // acc[0][l][k] = (l < Lq ? pf_l * base[l][pb(k)] : 0) + sum_j Y[j][l][py(k)] * key[j][l][0][k]
 // acc[1][l][k] =                                         sum_j Y[j][l][py(k)] * key[j][l][1][k]
 // py / pb: NTT-domain Galois source maps (k = 0: identity).
@@ -65,7 +36,7 @@ __global__ void __launch_bounds__(kT) k_ks_mac(const u64* __restrict__ Y, const 
     const u64 q = T.q, mu_hi = T.mu_hi, mu_lo = T.mu_lo;
     const u32 ky = perm_y ? galois_src(k, perm_y, log_n) : k;
     const u32 kk = perm_key ? galois_src(k, perm_key, log_n) : k;  // key slot of k in permuted storage
-    Acc128 ab, aa;
+    Acc128 ab{0, 0}, aa{0, 0};
     int since = 0;
     for (int j = 0; j < D; ++j) {
         u64 y = Y[(((size_t)j * LK + l) << log_n) + ky];

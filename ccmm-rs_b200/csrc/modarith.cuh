@@ -33,6 +33,10 @@ __device__ __forceinline__ u64 mul_shoup(u64 x, u64 w, u64 wq, u64 q) {
     return r >= q ? r - q : r;
 }
 __device__ __forceinline__ u64 reduce_2q(u64 x, u64 q) { return x >= q ? x - q : x; }
+// floor(w * 2^64 / q) on the device (w < q): one 128-by-64 division, setup use only.
+__device__ __forceinline__ u64 shoup_quotient_dev(u64 w, u64 q) {
+    return (u64)(((unsigned __int128)w << 64) / q);
+}
 __device__ __forceinline__ u64 reduce_4q(u64 x, u64 q) {
     u64 q2 = q << 1;
     x = x >= q2 ? x - q2 : x;
@@ -71,6 +75,38 @@ __device__ __forceinline__ u64 mul_barrett(u64 a, u64 b, const Barrett& m) {
     while (r >= m.q) r -= m.q;
     return r;
 }
+
+// x = xhi * 2^64 + xlo (xhi < q) modulo q, Barrett with mu = floor(2^128 / q).
+__device__ __forceinline__ u64 reduce_wide(u64 xhi, u64 xlo, u64 q, u64 mu_hi, u64 mu_lo) {
+    u64 p0_hi = __umul64hi(xlo, mu_lo);
+    u64 p1_lo = xlo * mu_hi, p1_hi = __umul64hi(xlo, mu_hi);
+    u64 p2_lo = xhi * mu_lo, p2_hi = __umul64hi(xhi, mu_lo);
+    u64 mid = p0_hi + p1_lo;
+    u64 c = mid < p0_hi;
+    u64 mid2 = mid + p2_lo;
+    c += mid2 < mid;
+    u64 qt = xhi * mu_hi + p1_hi + p2_hi + c;
+    u64 r = xlo - qt * q;
+    while (r >= q) r -= q;
+    return r;
+}
+
+// Exact 128-bit sum of products of canonical residues (each < q^2 < 2^124):
+// fold() reduces it to the canonical residue in lo; at most 15 products may
+// be added between folds.
+struct Acc128 {
+    u64 hi, lo;
+    __device__ __forceinline__ void mac(u64 a, u64 b) {
+        u64 pl = a * b, ph = __umul64hi(a, b);
+        lo += pl;
+        hi += ph + (lo < pl);
+    }
+    __device__ __forceinline__ void fold(u64 q, u64 mu_hi, u64 mu_lo) {
+        u64 h = hi >= q ? reduce_wide(0, hi, q, mu_hi, mu_lo) : hi;
+        lo = reduce_wide(h, lo, q, mu_hi, mu_lo);
+        hi = 0;
+    }
+};
 #endif
 
 inline void barrett_host(u64 q, u64* mu_hi, u64* mu_lo) {

@@ -276,6 +276,10 @@ int32_t launch_pass(int which, const void* in, u64* out, const NttTab* tabs, Lim
 
 int32_t pass(int which, int log_m, const void* in, u64* out, const NttTab* tabs, LimbMap lm, u32 limbs, u32 polys,
              int log_other, cudaStream_t st) {
+    if (polys > 65535 || limbs > 65535) {  // grid y / z limits
+        ckks_set_error("NTT: more than 65535 polynomials or limbs in one launch");
+        return CKKS_ERR_BAD_ARG;
+    }
     switch (log_m) {
         case 1: return launch_pass<1>(which, in, out, tabs, lm, limbs, polys, log_other, st);
         case 2: return launch_pass<2>(which, in, out, tabs, lm, limbs, polys, log_other, st);
