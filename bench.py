@@ -1,6 +1,6 @@
 """Throughput benchmark of the B200 RNS-CKKS hot path.
 
-python bench.py [--gpus N] [--steps K] [--warmup W] [--workload rotation|ntt] [--impl reference]
+python bench.py [--gpus N] [--steps K] [--warmup W] [--workload rotation|ntt|multiply] [--impl reference]
 
 Workload "rotation" (default): hoisted key-switched Galois rotations at
 N=2^16 over 24 Q limbs of 50-bit primes and 3 auxiliary 60-bit primes (the
@@ -16,6 +16,11 @@ limbs of 50-bit primes q = 1 mod 2N (the reference's prime search), 64
 polynomials per launch, residues uniform in [0, q). One step = one forward and
 one inverse transform of the whole batch. Metric: limb-polynomial transforms
 per second (forward and inverse each count once).
+
+Workload "multiply": the plain CKKS chain at N=2^12 (q = 60 + 40 + 40 bits,
+P = 60 bits, the reference's prime search): HMult -> bounded relinearization
+(base 2^20) -> rescale -> key-switched rotation by one slot, for 64
+ciphertext pairs. One step = 64 chains. Metric: chains per second.
 
 One JSON line on rank 0. Under torchrun each rank runs an independent replica
 (the path shards into independent polynomials/ciphertexts; no collective on
@@ -271,6 +276,23 @@ def ntt_cpu_sample(threads, seconds_target=10.0):
 def reference_arm(args, world, rank):
     if rank != 0:
         return None
+    if args.workload == "multiply":
+        threads = os.cpu_count() or 1
+        vals, sample = [], None
+        for i in range(args.warmup + args.steps):
+            v, sample = mul_cpu_sample(threads, pairs=4 * threads)
+            if i >= args.warmup:
+                vals.append(v)
+        value = float(np.median(vals))
+        return {
+            "metric": "HMult+relinearize+rescale+rotate chains/s (N=2^12, 3 limbs, bit-exact)", "value": value,
+            "unit": "chains/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * MUL_PAIRS / value, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded uniform ciphertexts)",
+            "config": mul_config(), "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "chains/s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "chains/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
     if args.workload == "rotation":
         threads = os.cpu_count() or 1
         vals, sample = [], None
@@ -448,12 +470,144 @@ def rot_cpu_sample(threads, n_keys=2):
                        "base 2^32, %.1f s" % (threads, n_keys, dt))
 
 
+# ------------------------------------------------- multiply chain (N=2^12)
+MUL_LOG_N, MUL_PAIRS, MUL_BASE_LOG = 12, 64, 20
+# the reference's prime search at N=2^12: one 60-bit and two 40-bit Q primes, one 60-bit P
+MUL_Q = [0xfffffffffffc001, 0xfffffdc001, 0xfffffc6001]
+MUL_P = [0xffffffffffe8001]
+
+
+def mul_config():
+    return {"workload": "HMult -> relinearize -> rescale -> rotate by 1 slot, N=2^12, q = 60+40+40 bits, "
+                        "P = 60 bits, bounded gadget base 2^20, 64 ciphertext pairs",
+            "log_n": MUL_LOG_N, "q_bits": [60, 40, 40], "p_bits": [60], "base_log": MUL_BASE_LOG,
+            "pairs": MUL_PAIRS, "scale": "2^40", "secret": "ternary", "sigma": 3.2,
+            "l2": "working set (12 MB) fits L2; latency-bound", "parallelism": "replicas"}
+
+
+def bench_mul_gpu(args, world, rank, local):
+    import torch
+    import ckks_b200 as cb
+    dev = torch.device("cuda", local)
+    n = 1 << MUL_LOG_N
+    ctx = cb.Context(MUL_LOG_N, MUL_Q, MUL_P)
+    rng = np.random.default_rng(99 + rank)
+    secret = rng.integers(-1, 2, n).astype(np.int8)
+    rk = cb.KeySwitchKey.relin_generate(ctx, 3, MUL_BASE_LOG, secret, seed=5)
+    gk = cb.KeySwitchKey.hybrid_generate(ctx, 2, MUL_BASE_LOG, ctx.rotation_exponent_left(1), secret, seed=6)
+    hx = np.stack([np.stack([rng.integers(0, m, (2, n), dtype=np.uint64) for m in MUL_Q], axis=1)
+                   for _ in range(MUL_PAIRS)])
+    hy = np.stack([np.stack([rng.integers(0, m, (2, n), dtype=np.uint64) for m in MUL_Q], axis=1)
+                   for _ in range(MUL_PAIRS)])
+    x, y = cb.as_u64_tensor(hx, dev), cb.as_u64_tensor(hy, dev)
+    prod = torch.empty((MUL_PAIRS, 2, 2, n), dtype=torch.int64, device=dev)
+    rot = torch.empty_like(prod)
+    st = torch.cuda.current_stream()
+
+    def step(xx, yy):
+        cb.multiply_relinearize_rescale(ctx, rk, xx, yy, out=prod)
+        cb.rotate(ctx, gk, prod, out=rot)
+
+    for _ in range(args.warmup):
+        step(x, y)
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(st)
+    for _ in range(args.steps):
+        step(x, y)
+    t1.record(st)
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = t0.elapsed_time(t1)
+    clk = clocks.stop()
+    ms_max = max_over_ranks(world, ms)
+    value = MUL_PAIRS * args.steps * world / (ms_max / 1000.0)
+    # end to end: pinned host inputs -> device, chain, result -> pinned host
+    px = torch.from_numpy(hx.view(np.int64)).pin_memory()
+    py = torch.from_numpy(hy.view(np.int64)).pin_memory()
+    pout = torch.empty(tuple(rot.shape), dtype=torch.int64).pin_memory()
+    dx, dy = torch.empty_like(x), torch.empty_like(y)
+
+    def e2e_step():
+        dx.copy_(px, non_blocking=True)
+        dy.copy_(py, non_blocking=True)
+        step(dx, dy)
+        pout.copy_(rot, non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    barrier(world)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(world, time.perf_counter() - t)
+    # roofline: bytes a chain must move at least (two input ciphertexts, both
+    # keys, the output ciphertext) per pair, against the HBM copy peak
+    ct_in, ct_out = 2 * 3 * n * 8, 2 * 2 * n * 8
+    D_r, w_r = rk.info()
+    D_g, w_g = gk.info()
+    bytes_step = MUL_PAIRS * (2 * ct_in + ct_out) + 8 * (w_r + w_g)
+    peak, kind = peaks()
+    achieved = bytes_step / (ms_max / args.steps / 1000.0) / 1e9
+    launches = 8 + 7 * MUL_PAIRS  # fused chain (8 launches per batch) + per-ciphertext rotation (7 each)
+    return {
+        "metric": "HMult+relinearize+rescale+rotate chains/s (N=2^12, 3 limbs, bit-exact)", "value": value,
+        "unit": "chains/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u64", "data": "synthetic (seeded uniform ciphertexts, GPU-generated keys)", "config": mul_config(),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_kind": kind,
+                     "kernel": "whole chain (working set fits L2: launch/latency-bound)",
+                     "algorithmic_bytes_per_step": bytes_step},
+        "e2e": {"value": MUL_PAIRS * args.steps * world / e2e_s, "unit": "chains/s",
+                "h2d_bytes_per_step": int(hx.nbytes + hy.nbytes), "d2h_bytes_per_step": int(pout.numel() * 8),
+                "path": "torch pinned copies + ckks_multiply_relin_rescale + ckks_rotate"},
+        "gpu_launches": args.steps * launches, "clocks": clk,
+    }
+
+
+def mul_cpu_sample(threads, pairs=None):
+    """Times the oracle's restatement of the reference chain (tensor, bounded
+    relinearize, rescale, hybrid rotate) on the host, one pair per thread."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import Oracle
+    import concurrent.futures as cf
+    o = Oracle()
+    n = 1 << MUL_LOG_N
+    pairs = pairs or threads
+    rng = np.random.default_rng(7)
+    secret = rng.integers(-1, 2, n).astype(np.int8)
+    rk = o.relin_key(MUL_Q, secret, MUL_BASE_LOG, seed=5)
+    k = int(o.L.oracle_rotation_exponent_left(n, 1))
+    gk = o.hybrid_key(MUL_Q[:2], MUL_P, secret, k, MUL_BASE_LOG, seed=6)
+    xs = [np.stack([rng.integers(0, m, (2, n), dtype=np.uint64) for m in MUL_Q], axis=1) for _ in range(pairs)]
+    ys = [np.stack([rng.integers(0, m, (2, n), dtype=np.uint64) for m in MUL_Q], axis=1) for _ in range(pairs)]
+
+    def chain(i):
+        quad = o.tensor(MUL_Q, xs[i], ys[i])
+        rel = o.relinearize(MUL_Q, quad, rk, MUL_BASE_LOG)
+        resc = o.rescale(MUL_Q, rel.reshape(2, 3, n))
+        return o.hybrid_rotate(MUL_Q[:2], MUL_P, gk, k, MUL_BASE_LOG, resc)
+
+    t = time.perf_counter()
+    with cf.ThreadPoolExecutor(threads) as ex:
+        list(ex.map(chain, range(pairs)))
+    dt = time.perf_counter() - t
+    return pairs / dt, "%d ciphertext pairs over %d threads (one chain per thread), N=2^12, %.2f s" % (
+        pairs, threads, dt)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="rotation", choices=["rotation", "ntt"])
+    ap.add_argument("--workload", default="rotation", choices=["rotation", "ntt", "multiply"])
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -463,6 +617,18 @@ def main():
         line = reference_arm(args, world, rank)
         if line:
             print(json.dumps(line), flush=True)
+        return
+    if args.workload == "multiply":
+        line = bench_mul_gpu(args, world, rank, local)
+        if rank == 0:
+            threads = os.cpu_count() or 1
+            v, sample = mul_cpu_sample(threads, pairs=4 * threads)
+            line["cpu_baseline"] = {"value": v, "unit": "chains/s", "cores": threads, "kind": "port",
+                                    "sample": sample}
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
         return
     if args.workload == "ntt":
         line = bench_ntt_gpu(args, world, rank, local)

@@ -7,6 +7,10 @@ the library or a GPU is missing, calls raise.
 
 Names follow the reference crate (ring/, ckks/, grafting/):
   RnsNttPlan / PreparedRnsNttPlan    ring/rns_ntt.rs, ring/prepared_rns_ntt.rs
+  rotate / rotate_hoisted            ckks/hybrid_rns_galois_key.rs
+  tensor / relinearize               grafting/rns_key_switch.rs, grafting/bounded_key_switch.rs
+  multiply_relinearize_rescale       ckks/rns_multiply.rs
+  multiply_plain                     ckks/rns_plain_multiply.rs
 """
 import ctypes
 import os
@@ -62,6 +66,12 @@ _SIGS = {
     "ckks_rotate_hoisted": (I32, [VP, ctypes.POINTER(VP), U32, VP, VP, U32, VP]),
     "ckks_rotate_hoisted_timed": (I32, [VP, ctypes.POINTER(VP), U32, VP, VP, U32, VP, ctypes.POINTER(ctypes.c_double)]),
     "ckks_rotate_hoisted_host": (I32, [VP, ctypes.POINTER(VP), U32, u64p, u64p, U32]),
+    "ckks_tensor": (I32, [VP, VP, VP, VP, U32, U32, VP]),
+    "ckks_relinearize": (I32, [VP, VP, VP, VP, U32, VP]),
+    "ckks_multiply_relin_rescale": (I32, [VP, VP, VP, VP, VP, U32, VP]),
+    "ckks_multiply_relin_rescale_host": (I32, [VP, VP, u64p, u64p, u64p, U32]),
+    "ckks_mul_plain": (I32, [VP, VP, VP, VP, U32, U32, U32, VP]),
+    "ckks_fft_stage": (I32, [VP, ctypes.POINTER(VP), U32, I32, VP, VP, VP, U32, U32, VP]),
 }
 
 STATUS = {0: "OK", -1: "BAD_ARG", -2: "BASIS_MISMATCH", -3: "EXPONENT_MISMATCH", -4: "OOM", -5: "CUDA",
@@ -429,3 +439,84 @@ class PreparedRnsNttPlan:
     def inverse(self, data, out=None):
         assert data.shape[-2] == self.limb_count
         return self.ctx.ntt_inverse(data, self.limb_begin, out)
+
+
+# ------------------------------------------------------------ products
+def _n_ct(ctx, t, polys, limbs):
+    return t.numel() // (polys * limbs * ctx.n)
+
+
+def tensor(ctx, lhs, rhs, out=None, stream=None):
+    """rns_tensor_with_ntt (grafting/rns_key_switch.rs:1675-1722):
+    [n][2][L][N] x [n][2][L][N] -> quadratic [n][3][L][N], coefficient domain."""
+    import torch
+    L = lhs.shape[-2]
+    n_ct = _n_ct(ctx, lhs, 2, L)
+    if out is None:
+        out = torch.empty((n_ct, 3, L, ctx.n), dtype=torch.int64, device=lhs.device)
+    check(lib().ckks_tensor(ctx.handle, _dptr(lhs), _dptr(rhs), _dptr(out), n_ct, L, _stream(stream)))
+    return out
+
+
+def relinearize(ctx, key, quad, out=None, stream=None):
+    """bounded_rns_relinearize_with_ntt (grafting/bounded_key_switch.rs:139-223):
+    [n][3][L][N] -> [n][2][L][N]."""
+    import torch
+    L = key.q_limbs
+    n_ct = _n_ct(ctx, quad, 3, L)
+    if out is None:
+        out = torch.empty((n_ct, 2, L, ctx.n), dtype=torch.int64, device=quad.device)
+    check(lib().ckks_relinearize(ctx.handle, key.handle, _dptr(quad), _dptr(out), n_ct, _stream(stream)))
+    return out
+
+
+def multiply_relinearize_rescale(ctx, key, lhs, rhs, out=None, stream=None):
+    """multiply_relinearize_rescale_rns_ckks_bounded_with_ntt (ckks/rns_multiply.rs:262-300):
+    [n][2][L][N] x [n][2][L][N] -> [n][2][L-1][N]."""
+    import torch
+    L = key.q_limbs
+    n_ct = _n_ct(ctx, lhs, 2, L)
+    if out is None:
+        out = torch.empty((n_ct, 2, L - 1, ctx.n), dtype=torch.int64, device=lhs.device)
+    check(lib().ckks_multiply_relin_rescale(ctx.handle, key.handle, _dptr(lhs), _dptr(rhs), _dptr(out), n_ct,
+                                            _stream(stream)))
+    return out
+
+
+def multiply_relinearize_rescale_host(ctx, key, lhs, rhs):
+    a, ap = _u64(lhs)
+    b, bp = _u64(rhs)
+    L = key.q_limbs
+    n_ct = a.size // (2 * L * ctx.n)
+    out = np.empty((n_ct, 2, L - 1, ctx.n), np.uint64)
+    check(lib().ckks_multiply_relin_rescale_host(ctx.handle, key.handle, ap, bp, out.ctypes.data_as(u64p), n_ct))
+    return out
+
+
+def multiply_plain(ctx, ct, plain_ntt, out=None, stream=None):
+    """multiply_plain_rns_ckks_with_prepared_ntt (ckks/rns_plain_multiply.rs:193-260):
+    ct [n][2][L][N] times the NTT-domain plaintext [L][N] (shared) or [n][L][N]."""
+    import torch
+    L = ct.shape[-2]
+    n_ct = _n_ct(ctx, ct, 2, L)
+    n_plain = plain_ntt.numel() // (L * ctx.n)
+    out = torch.empty_like(ct) if out is None else out
+    check(lib().ckks_mul_plain(ctx.handle, _dptr(ct), _dptr(plain_ntt), _dptr(out), n_ct, L, n_plain, _stream(stream)))
+    return out
+
+
+def fft_stage(ctx, keys, diag_ntt, ct, identity=True, out=None, stream=None):
+    """apply_stage (eblas/prepared_radix4_fft256.rs:744-822): rotations by
+    `keys` (one per nonzero offset) times their NTT-prepared diagonals, plus
+    the offset-0 diagonal times the input when `identity`, summed and
+    rescaled. diag_ntt [len(keys) + identity][L][N]; ct [n][2][L][N] ->
+    [n][2][L-1][N]."""
+    import torch
+    L = ct.shape[-2]
+    n_ct = _n_ct(ctx, ct, 2, L)
+    if out is None:
+        out = torch.empty((n_ct, 2, L - 1, ctx.n), dtype=torch.int64, device=ct.device)
+    arr = (VP * max(1, len(keys)))(*[k.handle.value for k in keys])
+    check(lib().ckks_fft_stage(ctx.handle, arr, len(keys), 1 if identity else 0, _dptr(diag_ntt), _dptr(ct),
+                               _dptr(out), n_ct, L, _stream(stream)))
+    return out

@@ -1,0 +1,122 @@
+// capi_mul.cu -- C ABI: tensor, relinearization, plaintext products and the
+// multiply -> relinearize -> rescale chain.
+#include "keyswitch.cuh"
+
+namespace {
+
+int32_t check_relin_key(ckks_ctx* ctx, const ckks_ksk* key, const char* who) {
+    CKKS_CHECK_ARG(ctx != nullptr && key != nullptr, std::string(who) + ": null context or key");
+    if (key->ctx != ctx || key->kind != CKKS_KSK_RELIN_BOUNDED) {
+        ckks_set_error(std::string(who) + ": key is not a bounded relinearization key of this context");
+        return CKKS_ERR_BASIS_MISMATCH;
+    }
+    return CKKS_OK;
+}
+
+bool overlaps(const void* a, size_t a_bytes, const void* b, size_t b_bytes) {
+    const char *x = (const char*)a, *y = (const char*)b;
+    return x < y + b_bytes && y < x + a_bytes;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t ckks_tensor(ckks_ctx* ctx, const uint64_t* lhs, const uint64_t* rhs, uint64_t* out, uint32_t n_ct,
+                    uint32_t q_limbs, void* stream) {
+    CKKS_CHECK_ARG(ctx != nullptr, "ckks_tensor: null context");
+    CKKS_CHECK_ARG(lhs && rhs && out, "ckks_tensor: null buffer");
+    if (q_limbs < 1 || q_limbs > ctx->L) {
+        ckks_set_error("ckks_tensor: q_limbs outside the context Q basis");
+        return CKKS_ERR_BASIS_MISMATCH;
+    }
+    const size_t ct = (size_t)2 * q_limbs * ctx->n * 8 * n_ct, o = ct / 2 * 3;
+    CKKS_CHECK_ARG(!overlaps(out, o, lhs, ct) && !overlaps(out, o, rhs, ct), "ckks_tensor: out overlaps an input");
+    if (!n_ct) return CKKS_OK;
+    return tensor_launch(ctx, lhs, rhs, out, n_ct, q_limbs, ckks_stream(ctx, stream));
+}
+
+int32_t ckks_relinearize(ckks_ctx* ctx, const ckks_ksk* key, const uint64_t* quad, uint64_t* out, uint32_t n_ct,
+                         void* stream) {
+    if (int32_t rc = check_relin_key(ctx, key, "ckks_relinearize")) return rc;
+    CKKS_CHECK_ARG(quad && out, "ckks_relinearize: null buffer");
+    const size_t poly = (size_t)key->q_limbs * ctx->n * 8 * n_ct;
+    CKKS_CHECK_ARG(!overlaps(out, 2 * poly, quad, 3 * poly), "ckks_relinearize: out overlaps the input");
+    if (!n_ct) return CKKS_OK;
+    return relinearize_launch(ctx, key, quad, out, n_ct, ckks_stream(ctx, stream));
+}
+
+int32_t ckks_multiply_relin_rescale(ckks_ctx* ctx, const ckks_ksk* key, const uint64_t* lhs, const uint64_t* rhs,
+                                    uint64_t* out, uint32_t n_ct, void* stream) {
+    if (int32_t rc = check_relin_key(ctx, key, "ckks_multiply_relin_rescale")) return rc;
+    CKKS_CHECK_ARG(lhs && rhs && out, "ckks_multiply_relin_rescale: null buffer");
+    CKKS_CHECK_ARG(key->q_limbs >= 2, "ckks_multiply_relin_rescale: no next level to rescale to");
+    const size_t in = (size_t)2 * key->q_limbs * ctx->n * 8 * n_ct, o = (size_t)2 * (key->q_limbs - 1) * ctx->n * 8 * n_ct;
+    CKKS_CHECK_ARG(!overlaps(out, o, lhs, in) && !overlaps(out, o, rhs, in),
+                   "ckks_multiply_relin_rescale: out overlaps an input");
+    if (!n_ct) return CKKS_OK;
+    return multiply_relin_rescale_launch(ctx, key, lhs, rhs, out, n_ct, ckks_stream(ctx, stream));
+}
+
+int32_t ckks_multiply_relin_rescale_host(ckks_ctx* ctx, const ckks_ksk* key, const uint64_t* lhs_host,
+                                         const uint64_t* rhs_host, uint64_t* out_host, uint32_t n_ct) {
+    if (int32_t rc = check_relin_key(ctx, key, "ckks_multiply_relin_rescale_host")) return rc;
+    CKKS_CHECK_ARG(lhs_host && rhs_host && out_host && key->q_limbs >= 2,
+                   "ckks_multiply_relin_rescale_host: bad arguments");
+    if (!n_ct) return CKKS_OK;
+    const size_t in = (size_t)2 * key->q_limbs * ctx->n * n_ct, o = (size_t)2 * (key->q_limbs - 1) * ctx->n * n_ct;
+    cudaStream_t st = ctx->own_stream;
+    int32_t rc;
+    {
+        Workspace<u64> d;
+        if ((rc = d.alloc(2 * in + o, st))) return rc;
+        CKKS_CUDA_TRY(cudaMemcpyAsync(d.p, lhs_host, in * 8, cudaMemcpyHostToDevice, st));
+        CKKS_CUDA_TRY(cudaMemcpyAsync(d.p + in, rhs_host, in * 8, cudaMemcpyHostToDevice, st));
+        rc = multiply_relin_rescale_launch(ctx, key, d.p, d.p + in, d.p + 2 * in, n_ct, st);
+        if (rc == CKKS_OK) CKKS_CUDA_TRY(cudaMemcpyAsync(out_host, d.p + 2 * in, o * 8, cudaMemcpyDeviceToHost, st));
+    }
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (rc == CKKS_OK && e != cudaSuccess) {
+        ckks_set_error(std::string("ckks_multiply_relin_rescale_host: ") + cudaGetErrorString(e));
+        return CKKS_ERR_CUDA;
+    }
+    return rc;
+}
+
+int32_t ckks_mul_plain(ckks_ctx* ctx, const uint64_t* ct, const uint64_t* plain_ntt, uint64_t* out, uint32_t n_ct,
+                       uint32_t q_limbs, uint32_t n_plain, void* stream) {
+    CKKS_CHECK_ARG(ctx != nullptr, "ckks_mul_plain: null context");
+    CKKS_CHECK_ARG(ct && plain_ntt && out, "ckks_mul_plain: null buffer");
+    if (q_limbs < 1 || q_limbs > ctx->L) {
+        ckks_set_error("ckks_mul_plain: q_limbs outside the context Q basis");
+        return CKKS_ERR_BASIS_MISMATCH;
+    }
+    CKKS_CHECK_ARG(n_plain == 1 || n_plain == n_ct, "ckks_mul_plain: n_plain must be 1 or n_ct");
+    if (!n_ct) return CKKS_OK;
+    return mul_plain_launch(ctx, ct, plain_ntt, out, n_ct, q_limbs, n_plain > 1, ckks_stream(ctx, stream));
+}
+
+int32_t ckks_fft_stage(ckks_ctx* ctx, const ckks_ksk* const* keys, uint32_t n_rot, int32_t identity,
+                       const uint64_t* diag_ntt, const uint64_t* ct_in, uint64_t* ct_out, uint32_t n_ct,
+                       uint32_t q_limbs, void* stream) {
+    CKKS_CHECK_ARG(ctx != nullptr, "ckks_fft_stage: null context");
+    CKKS_CHECK_ARG(diag_ntt && ct_in && ct_out && (n_rot == 0 || keys) && (n_rot || identity),
+                   "ckks_fft_stage: bad arguments");
+    CKKS_CHECK_ARG(q_limbs >= 2 && q_limbs <= ctx->L, "ckks_fft_stage: need 2..L limbs (the stage rescales)");
+    for (u32 g = 0; g < n_rot; ++g) {
+        const ckks_ksk* k = keys[g];
+        if (!k || k->ctx != ctx || k->kind == CKKS_KSK_RELIN_BOUNDED || k->kind != keys[0]->kind ||
+            k->q_limbs != q_limbs || k->base_log != keys[0]->base_log || k->D != keys[0]->D ||
+            k->blocks != keys[0]->blocks) {
+            ckks_set_error("ckks_fft_stage: keys must be Galois keys of one kind and gadget at level q_limbs");
+            return CKKS_ERR_BASIS_MISMATCH;
+        }
+    }
+    const size_t in = (size_t)2 * q_limbs * ctx->n * 8 * n_ct, o = (size_t)2 * (q_limbs - 1) * ctx->n * 8 * n_ct;
+    CKKS_CHECK_ARG(!overlaps(ct_out, o, ct_in, in), "ckks_fft_stage: out overlaps the input");
+    if (!n_ct) return CKKS_OK;
+    return fft_stage_launch(ctx, keys, n_rot, identity != 0, diag_ntt, ct_in, ct_out, n_ct, q_limbs,
+                            ckks_stream(ctx, stream));
+}
+
+}  // extern "C"

@@ -54,6 +54,20 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
 int32_t rotate_hybrid_hoisted(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_keys, const u64* ct_in, u64* ct_out,
                               u32 n_ct, cudaStream_t st);
 
+// Ciphertext products (multiply.cu). Layouts: ciphertexts [n][2][L][N],
+// quadratic ciphertexts [n][3][L][N], coefficient domain; prepared plaintexts
+// [n_plain][L][N], NTT domain.
+int32_t tensor_launch(ckks_ctx* ctx, const u64* lhs, const u64* rhs, u64* out, u32 n_ct, u32 L, cudaStream_t st);
+int32_t relinearize_launch(ckks_ctx* ctx, const ckks_ksk* key, const u64* quad, u64* out, u32 n_ct, cudaStream_t st);
+int32_t multiply_relin_rescale_launch(ckks_ctx* ctx, const ckks_ksk* key, const u64* lhs, const u64* rhs, u64* out,
+                                      u32 n_ct, cudaStream_t st);
+int32_t mul_plain_launch(ckks_ctx* ctx, const u64* ct_in, const u64* plain_ntt, u64* out, u32 n_ct, u32 L,
+                         bool plain_per_ct, cudaStream_t st);
+
+// One diagonal-rotation FFT stage (fft.cu): diag_ntt [n_rot + identity][L][N].
+int32_t fft_stage_launch(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_rot, bool identity, const u64* diag_ntt,
+                         const u64* ct_in, u64* ct_out, u32 n_ct, u32 L, cudaStream_t st);
+
 // sampling stream tags (shared with the oracle's restatement)
 constexpr u64 TAG_KEY_A = 1ull << 56, TAG_KEY_E = 2ull << 56, TAG_ENC_A = 3ull << 56, TAG_ENC_E = 4ull << 56,
               TAG_RLK_A = 5ull << 56, TAG_RLK_E = 6ull << 56;

@@ -215,6 +215,59 @@ int32_t ckks_rotate_hoisted_timed(ckks_ctx* ctx, const ckks_ksk* const* keys, ui
 int32_t ckks_rotate_hoisted_host(ckks_ctx* ctx, const ckks_ksk* const* keys, uint32_t n_keys,
                                  const uint64_t* ct_in_host, uint64_t* ct_out_host, uint32_t n_ct);
 
+
+/* ------------------------------------------------- ciphertext products ----
+ * Layouts: ciphertexts [n_ct][2][q_limbs][N] (b, a), quadratic ciphertexts
+ * [n_ct][3][q_limbs][N] (c0, c1, c2), coefficient domain, canonical residues
+ * over the Q prefix q_0..q_{q_limbs-1}. Every output word equals the
+ * reference's (exact modular arithmetic). */
+
+/* Tensor product of ciphertext pairs: c0 = b1 b2, c1 = b1 a2 + a1 b2,
+ * c2 = a1 a2 (negacyclic products per limb). Replaces rns_tensor_with_ntt
+ * (grafting/rns_key_switch.rs:1675-1722) and tensor (rlwe/quadratic.rs:70-140).
+ * out [n_ct][3][q_limbs][N] must not overlap the inputs. */
+int32_t ckks_tensor(ckks_ctx* ctx, const uint64_t* lhs, const uint64_t* rhs, uint64_t* out, uint32_t n_ct,
+                    uint32_t q_limbs, void* stream);
+/* Bounded relinearization with a CKKS_KSK_RELIN_BOUNDED key of the same
+ * level: b = c0 + sum_j d_j k_b[j], a = c1 + sum_j d_j k_a[j] with d_j the
+ * balanced base-2^base_log digits of c2. Replaces
+ * bounded_rns_relinearize_with_ntt(_observed) (grafting/bounded_key_switch.rs:139-223).
+ * quad [n_ct][3][L][N] -> out [n_ct][2][L][N] (no overlap). */
+int32_t ckks_relinearize(ckks_ctx* ctx, const ckks_ksk* key, const uint64_t* quad, uint64_t* out, uint32_t n_ct,
+                         void* stream);
+/* Multiply, relinearize, rescale: lhs, rhs [n_ct][2][L][N] at the key's level
+ * L >= 2 -> out [n_ct][2][L-1][N]. Replaces
+ * multiply_relinearize_rescale_rns_ckks_bounded_with_ntt (ckks/rns_multiply.rs:262-300);
+ * the CKKS scale bookkeeping (scale_l * scale_r / q_{L-1}) stays with the caller. */
+int32_t ckks_multiply_relin_rescale(ckks_ctx* ctx, const ckks_ksk* key, const uint64_t* lhs, const uint64_t* rhs,
+                                    uint64_t* out, uint32_t n_ct, void* stream);
+/* Host-buffer form of ckks_multiply_relin_rescale (copies in, runs, copies out). */
+int32_t ckks_multiply_relin_rescale_host(ckks_ctx* ctx, const ckks_ksk* key, const uint64_t* lhs_host,
+                                         const uint64_t* rhs_host, uint64_t* out_host, uint32_t n_ct);
+/* Plaintext multiply: out = INTT(NTT(ct) * plain_ntt) per component and limb.
+ * plain_ntt is the NTT-domain plaintext ([n_plain][q_limbs][N], n_plain 1 =
+ * one plaintext for every ciphertext, or n_ct), the reference's
+ * PreparedRnsPlaintextNtt. Replaces multiply_plain_rns_ckks_with_prepared_ntt
+ * (ckks/rns_plain_multiply.rs:193-260); the result scale is scale * plaintext_scale.
+ * out may equal ct. */
+int32_t ckks_mul_plain(ckks_ctx* ctx, const uint64_t* ct, const uint64_t* plain_ntt, uint64_t* out, uint32_t n_ct,
+                       uint32_t q_limbs, uint32_t n_plain, void* stream);
+
+
+/* One diagonal-rotation stage of the encrypted radix-4 FFT:
+ *   out = Rescale( sum_t multiply_plain(rotate(ct, offset_t), diag_t) ).
+ * keys: n_rot Galois keys, one per nonzero offset (one kind, level q_limbs
+ * and gadget); diag_ntt [n_rot + (identity ? 1 : 0)][q_limbs][N]: the
+ * NTT-prepared diagonals in the order of `keys`, then the offset-0 diagonal
+ * (applied to the unrotated input) when identity != 0. ct_in
+ * [n_ct][2][q_limbs][N] -> ct_out [n_ct][2][q_limbs-1][N]. The rotations of a
+ * ciphertext share one hoisted decomposition. Replaces apply_stage /
+ * apply_stage_canonical (eblas/prepared_radix4_fft256.rs:744-822); the scale
+ * becomes scale * plain_scale / q_{q_limbs-1} with the caller. */
+int32_t ckks_fft_stage(ckks_ctx* ctx, const ckks_ksk* const* keys, uint32_t n_rot, int32_t identity,
+                       const uint64_t* diag_ntt, const uint64_t* ct_in, uint64_t* ct_out, uint32_t n_ct,
+                       uint32_t q_limbs, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -161,3 +161,26 @@ def test_rotation_decodes_to_rotated_slots(oracle):
     out = oracle.hybrid_rotate(q, p, key, k, 20, ct)
     dec = oracle.decode(q, oracle.decrypt(q, s, out), 2.0 ** 40)
     assert np.linalg.norm(dec - np.roll(slots, -3)) / np.linalg.norm(slots) < 1e-6
+
+
+def test_multiply_chain_decodes(oracle):
+    # HMult -> bounded relinearize (base 2^20) -> rescale -> rotate by 1 on the
+    # N=2^12 chain q = 60 + 40 + 40 bits, P = 60 bits (ckks/rns_multiply.rs:262-300)
+    q = [0xfffffffffffc001, 0xfffffdc001, 0xfffffc6001]
+    p = [0xffffffffffe8001]
+    n = 4096
+    assert all(params.is_prime(m) and (m - 1) % (2 * n) == 0 for m in q + p)
+    rng = np.random.default_rng(12)
+    s = rng.integers(-1, 2, n).astype(np.int8)
+    scale = 2.0 ** 40
+    a = rng.uniform(-1, 1, n // 2) + 1j * rng.uniform(-1, 1, n // 2)
+    b = rng.uniform(-1, 1, n // 2) + 1j * rng.uniform(-1, 1, n // 2)
+    cx = oracle.encrypt(q, s, oracle.encode(a, q, scale), seed=1)
+    cy = oracle.encrypt(q, s, oracle.encode(b, q, scale), seed=2)
+    rel = oracle.relinearize(q, oracle.tensor(q, cx, cy), oracle.relin_key(q, s, 20, seed=3), 20)
+    resc = oracle.rescale(q, rel.reshape(2, 3, n))
+    k = int(oracle.L.oracle_rotation_exponent_left(n, 1))
+    rot = oracle.hybrid_rotate(q[:2], p, oracle.hybrid_key(q[:2], p, s, k, 20, seed=4), k, 20, resc)
+    dec = oracle.decode(q[:2], oracle.decrypt(q[:2], s, rot), scale * scale / q[-1])
+    err = np.linalg.norm(dec - np.roll(a * b, -1)) / np.linalg.norm(a * b)
+    assert err < 1e-4, err
