@@ -1,6 +1,6 @@
 """Throughput benchmark of the B200 RNS-CKKS hot path.
 
-python bench.py [--gpus N] [--steps K] [--warmup W] [--workload rotation|ntt|multiply] [--impl reference]
+python bench.py [--gpus N] [--steps K] [--warmup W] [--workload rotation|ntt|multiply|ccmm] [--impl reference]
 
 Workload "rotation" (default): hoisted key-switched Galois rotations at
 N=2^16 over 24 Q limbs of 50-bit primes and 3 auxiliary 60-bit primes (the
@@ -16,6 +16,11 @@ limbs of 50-bit primes q = 1 mod 2N (the reference's prime search), 64
 polynomials per launch, residues uniform in [0, q). One step = one forward and
 one inverse transform of the whole batch. Metric: limb-polynomial transforms
 per second (forward and inverse each count once).
+
+Workload "ccmm": structured encrypted matrix product of two 64 x 64 matrices
+of ciphertexts (one per entry) at N=2^15 over 14 x 50-bit limbs with the
+bounded relinearization key (base 2^20): sum of 64 tensors per output entry,
+relinearize, rescale. One step = one 64 x 64 CCMM. Metric: CCMM per second.
 
 Workload "multiply": the plain CKKS chain at N=2^12 (q = 60 + 40 + 40 bits,
 P = 60 bits, the reference's prime search): HMult -> bounded relinearization
@@ -276,6 +281,23 @@ def ntt_cpu_sample(threads, seconds_target=10.0):
 def reference_arm(args, world, rank):
     if rank != 0:
         return None
+    if args.workload == "ccmm":
+        threads = os.cpu_count() or 1
+        vals, sample = [], None
+        for i in range(1 + args.steps):
+            v, sample = ccmm_cpu_sample(threads)
+            if i >= 1:
+                vals.append(v)
+        value = float(np.median(vals))
+        return {
+            "metric": "64x64 structured CCMM/s (N=2^15, 14 limbs, both operands encrypted, bit-exact)",
+            "value": value, "unit": "CCMM/s", "n_gpus": world, "steps": args.steps, "warmup": 1,
+            "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u64", "data": "synthetic (seeded uniform ciphertext residues)", "config": ccmm_config(),
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "CCMM/s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "CCMM/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
     if args.workload == "multiply":
         threads = os.cpu_count() or 1
         vals, sample = [], None
@@ -602,12 +624,138 @@ def mul_cpu_sample(threads, pairs=None):
         pairs, threads, dt)
 
 
+# ------------------------------------------------------ structured CCMM
+CCMM_LOG_N, CCMM_L, CCMM_D, CCMM_BASE_LOG = 15, 14, 64, 20
+
+
+def ccmm_config():
+    return {"workload": "structured encrypted CCMM 64x64 by 64x64, one ciphertext per entry, N=2^15, "
+                        "14 x 50-bit Q limbs, bounded relinearization base 2^20",
+            "log_n": CCMM_LOG_N, "q_limbs": CCMM_L, "d": CCMM_D, "base_log": CCMM_BASE_LOG, "scale": "2^40",
+            "l2": "operands (2 x 30 GB) larger than L2", "parallelism": "replicas"}
+
+
+def ccmm_primes():
+    import ckks_b200.params as params
+    return params.primes_below_bits(50, 1 << CCMM_LOG_N, CCMM_L)
+
+
+def bench_ccmm_gpu(args, world, rank, local):
+    import torch
+    import ckks_b200 as cb
+    dev = torch.device("cuda", local)
+    n, d, L = 1 << CCMM_LOG_N, CCMM_D, CCMM_L
+    q = ccmm_primes()
+    ctx = cb.Context(CCMM_LOG_N, q)
+    rng = np.random.default_rng(31 + rank)
+    secret = rng.integers(-1, 2, n).astype(np.int8)
+    rk = cb.KeySwitchKey.relin_generate(ctx, L, CCMM_BASE_LOG, secret, seed=9)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(1234 + rank)
+    A = torch.empty((d * d, 2, L, n), dtype=torch.int64, device=dev)
+    B = torch.empty_like(A)
+    for l, m in enumerate(q):  # uniform residues per limb (fresh-ciphertext distribution)
+        A[:, :, l].random_(0, m, generator=gen)
+        B[:, :, l].random_(0, m, generator=gen)
+    C = torch.empty((d * d, 2, L - 1, n), dtype=torch.int64, device=dev)
+    st = torch.cuda.current_stream()
+
+    def step():
+        cb.matmul_structured(ctx, rk, A, B, d, d, d, out=C)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(st)
+    for _ in range(args.steps):
+        step()
+    t1.record(st)
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = t0.elapsed_time(t1)
+    clk = clocks.stop()
+    ms_max = max_over_ranks(world, ms)
+    value = args.steps * world / (ms_max / 1000.0)
+    D, key_words = rk.info()
+    ct_bytes = 2 * L * n * 8
+    # algorithmic bytes: both operand matrices read, the product written, and
+    # the relinearization key read once per group of four outputs
+    bytes_step = 2 * d * d * ct_bytes + d * d * 2 * (L - 1) * n * 8 + (d * d // 4) * key_words * 8
+    peak, kind = peaks()
+    achieved = bytes_step / (ms_max / args.steps / 1000.0) / 1e9
+    # end to end: pinned host operands in, product out, through the same call
+    hA = torch.empty(tuple(A.shape), dtype=torch.int64).pin_memory()
+    hB = torch.empty(tuple(B.shape), dtype=torch.int64).pin_memory()
+    hC = torch.empty(tuple(C.shape), dtype=torch.int64).pin_memory()
+    hA.copy_(A)
+    hB.copy_(B)
+    torch.cuda.synchronize()
+    barrier(world)
+    t = time.perf_counter()
+    A.copy_(hA, non_blocking=True)
+    B.copy_(hB, non_blocking=True)
+    step()
+    hC.copy_(C, non_blocking=True)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(world, time.perf_counter() - t)
+    return {
+        "metric": "64x64 structured CCMM/s (N=2^15, 14 limbs, both operands encrypted, bit-exact)", "value": value,
+        "unit": "CCMM/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u64", "data": "synthetic (seeded uniform ciphertext residues, GPU-generated key)",
+        "config": ccmm_config(),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_kind": kind, "kernel": "whole CCMM (operands, product, key stream)",
+                     "algorithmic_bytes_per_step": bytes_step},
+        "e2e": {"value": world / e2e_s, "unit": "CCMM/s", "h2d_bytes_per_step": int(2 * A.numel() * 8),
+                "d2h_bytes_per_step": int(C.numel() * 8), "path": "torch pinned copies + ckks_ccmm_structured"},
+        "gpu_launches": None, "clocks": clk,
+    }
+
+
+def ccmm_cpu_sample(threads):
+    """Times the oracle's restatement of one output entry of the reference
+    CCMM (64 tensors summed, bounded relinearization, rescale) per thread at
+    N=2^15, 14 limbs; CCMM/s = threads / (4096 x entry time)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import Oracle
+    import concurrent.futures as cf
+    o = Oracle()
+    n, d, L = 1 << CCMM_LOG_N, CCMM_D, CCMM_L
+    q = [int(x) for x in o.primes_below_bits(50, n, L)]
+    rng = np.random.default_rng(5)
+    secret = rng.integers(-1, 2, n).astype(np.int8)
+    key = o.relin_key(q, secret, CCMM_BASE_LOG, seed=9)
+    row = [np.stack([rng.integers(0, m, (2, n), dtype=np.uint64) for m in q], axis=1) for _ in range(d)]
+    col = [np.stack([rng.integers(0, m, (2, n), dtype=np.uint64) for m in q], axis=1) for _ in range(d)]
+
+    def entry(_):
+        acc = None
+        for kk in range(d):
+            t = o.tensor(q, row[kk], col[kk])
+            acc = t if acc is None else np.stack([(acc[:, l] + t[:, l]) % q[l] for l in range(L)], axis=1)
+        rel = o.relinearize(q, acc, key, CCMM_BASE_LOG)
+        return o.rescale(q, rel.reshape(2, L, n))
+
+    t = time.perf_counter()
+    with cf.ThreadPoolExecutor(threads) as ex:
+        list(ex.map(entry, range(threads)))
+    dt = time.perf_counter() - t
+    return threads / (d * d * dt), ("%d output entries (64 tensors + relinearize + rescale each, one per thread), "
+                                    "N=2^15, 14 limbs, %.1f s" % (threads, dt))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="rotation", choices=["rotation", "ntt", "multiply"])
+    ap.add_argument("--workload", default="rotation", choices=["rotation", "ntt", "multiply", "ccmm"])
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -617,6 +765,17 @@ def main():
         line = reference_arm(args, world, rank)
         if line:
             print(json.dumps(line), flush=True)
+        return
+    if args.workload == "ccmm":
+        line = bench_ccmm_gpu(args, world, rank, local)
+        if rank == 0:
+            threads = os.cpu_count() or 1
+            v, sample = ccmm_cpu_sample(threads)
+            line["cpu_baseline"] = {"value": v, "unit": "CCMM/s", "cores": threads, "kind": "port", "sample": sample}
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
         return
     if args.workload == "multiply":
         line = bench_mul_gpu(args, world, rank, local)

@@ -72,6 +72,9 @@ _SIGS = {
     "ckks_multiply_relin_rescale_host": (I32, [VP, VP, u64p, u64p, u64p, U32]),
     "ckks_mul_plain": (I32, [VP, VP, VP, VP, U32, U32, U32, VP]),
     "ckks_fft_stage": (I32, [VP, ctypes.POINTER(VP), U32, I32, VP, VP, VP, U32, U32, VP]),
+    "ckks_ccmm_structured": (I32, [VP, VP, VP, VP, VP, U32, U32, U32, VP]),
+    "ckks_encode": (I32, [VP, VP, VP, U32, U32, ctypes.c_double, VP]),
+    "ckks_decode": (I32, [VP, VP, VP, U32, U32, ctypes.c_double, VP]),
 }
 
 STATUS = {0: "OK", -1: "BAD_ARG", -2: "BASIS_MISMATCH", -3: "EXPONENT_MISMATCH", -4: "OOM", -5: "CUDA",
@@ -519,4 +522,44 @@ def fft_stage(ctx, keys, diag_ntt, ct, identity=True, out=None, stream=None):
     arr = (VP * max(1, len(keys)))(*[k.handle.value for k in keys])
     check(lib().ckks_fft_stage(ctx.handle, arr, len(keys), 1 if identity else 0, _dptr(diag_ntt), _dptr(ct),
                                _dptr(out), n_ct, L, _stream(stream)))
+    return out
+
+
+def matmul_structured(ctx, key, A, B, m, k, n, out=None, stream=None):
+    """matmul_structured_bounded_with_ntt (matrix/rns_ckks_ciphertext.rs:204-318):
+    A [k][m][2][L][N] and B [n][k][2][L][N] column-major ciphertext matrices ->
+    C [n][m][2][L-1][N]."""
+    import torch
+    L = key.q_limbs
+    if out is None:
+        out = torch.empty((n, m, 2, L - 1, ctx.n), dtype=torch.int64, device=A.device)
+    check(lib().ckks_ccmm_structured(ctx.handle, key.handle, _dptr(A), _dptr(B), _dptr(out), m, k, n,
+                                     _stream(stream)))
+    return out
+
+
+# ----------------------------------------------------- encode / decode
+def encode(ctx, slots, q_limbs, scale, stream=None):
+    """encode_rns (application_support/ckks.rs:39-62): complex slots [..., N/2]
+    (numpy or a complex128 CUDA tensor) -> plaintexts [..., q_limbs, N] on the GPU."""
+    import torch
+    if isinstance(slots, np.ndarray):
+        slots = torch.from_numpy(np.ascontiguousarray(slots, dtype=np.complex128)).cuda()
+    slots = slots.contiguous()
+    lead = tuple(slots.shape[:-1])
+    n_msg = int(np.prod(lead)) if lead else 1
+    out = torch.empty(lead + (q_limbs, ctx.n), dtype=torch.int64, device=slots.device)
+    check(lib().ckks_encode(ctx.handle, _dptr(slots), _dptr(out), n_msg, q_limbs, float(scale), _stream(stream)))
+    return out
+
+
+def decode(ctx, poly, scale, stream=None):
+    """Decode of application_support/ckks.rs:106-130: plaintexts [..., q_limbs, N]
+    -> complex128 slots [..., N/2] (CUDA tensor)."""
+    import torch
+    q_limbs = poly.shape[-2]
+    lead = tuple(poly.shape[:-2])
+    n_msg = int(np.prod(lead)) if lead else 1
+    out = torch.empty(lead + (ctx.n // 2,), dtype=torch.complex128, device=poly.device)
+    check(lib().ckks_decode(ctx.handle, _dptr(poly), _dptr(out), n_msg, q_limbs, float(scale), _stream(stream)))
     return out

@@ -1,5 +1,7 @@
 // capi_mul.cu -- C ABI: tensor, relinearization, plaintext products and the
 // multiply -> relinearize -> rescale chain.
+#include <cmath>
+
 #include "keyswitch.cuh"
 
 namespace {
@@ -117,6 +119,43 @@ int32_t ckks_fft_stage(ckks_ctx* ctx, const ckks_ksk* const* keys, uint32_t n_ro
     if (!n_ct) return CKKS_OK;
     return fft_stage_launch(ctx, keys, n_rot, identity != 0, diag_ntt, ct_in, ct_out, n_ct, q_limbs,
                             ckks_stream(ctx, stream));
+}
+
+int32_t ckks_ccmm_structured(ckks_ctx* ctx, const ckks_ksk* key, const uint64_t* A, const uint64_t* B, uint64_t* C,
+                             uint32_t m, uint32_t k, uint32_t n, void* stream) {
+    if (int32_t rc = check_relin_key(ctx, key, "ckks_ccmm_structured")) return rc;
+    CKKS_CHECK_ARG(A && B && C && m && k && n, "ckks_ccmm_structured: bad arguments");
+    CKKS_CHECK_ARG(key->q_limbs >= 2, "ckks_ccmm_structured: no next level to rescale to");
+    CKKS_CHECK_ARG((size_t)m * k <= 12288 && (size_t)k * n <= (size_t(1) << 24),
+                   "ckks_ccmm_structured: matrix too large for the slot blocks");
+    for (u32 l = 0; l < key->q_limbs; ++l)
+        CKKS_CHECK_ARG(ctx->moduli[l] < (1ull << 60), "ckks_ccmm_structured: Q moduli must be below 2^60");
+    const size_t ctb = (size_t)2 * key->q_limbs * ctx->n * 8, cto = (size_t)2 * (key->q_limbs - 1) * ctx->n * 8;
+    CKKS_CHECK_ARG(!overlaps(C, cto * m * n, A, ctb * m * k) && !overlaps(C, cto * m * n, B, ctb * k * n),
+                   "ckks_ccmm_structured: C overlaps an input");
+    return ccmm_structured_launch(ctx, key, A, B, C, m, k, n, ckks_stream(ctx, stream));
+}
+
+int32_t ckks_encode(ckks_ctx* ctx, const double* slots, uint64_t* out, uint32_t n_msg, uint32_t q_limbs, double scale,
+                    void* stream) {
+    CKKS_CHECK_ARG(ctx != nullptr, "ckks_encode: null context");
+    CKKS_CHECK_ARG(slots && out, "ckks_encode: null buffer");
+    CKKS_CHECK_ARG(q_limbs >= 1 && q_limbs <= ctx->L, "ckks_encode: q_limbs outside the context Q basis");
+    CKKS_CHECK_ARG(std::isfinite(scale) && scale > 0, "ckks_encode: scale must be finite and positive");
+    if (!n_msg) return CKKS_OK;
+    CKKS_CHECK_ARG(n_msg <= 65535, "ckks_encode: at most 65535 messages per call");
+    return encode_launch(ctx, slots, out, n_msg, q_limbs, scale, ckks_stream(ctx, stream));
+}
+
+int32_t ckks_decode(ckks_ctx* ctx, const uint64_t* poly, double* slots, uint32_t n_msg, uint32_t q_limbs,
+                    double scale, void* stream) {
+    CKKS_CHECK_ARG(ctx != nullptr, "ckks_decode: null context");
+    CKKS_CHECK_ARG(poly && slots, "ckks_decode: null buffer");
+    CKKS_CHECK_ARG(q_limbs >= 1 && q_limbs <= ctx->L, "ckks_decode: q_limbs outside the context Q basis");
+    CKKS_CHECK_ARG(std::isfinite(scale) && scale > 0, "ckks_decode: scale must be finite and positive");
+    if (!n_msg) return CKKS_OK;
+    CKKS_CHECK_ARG(n_msg <= 65535, "ckks_decode: at most 65535 messages per call");
+    return decode_launch(ctx, poly, slots, n_msg, q_limbs, scale, ckks_stream(ctx, stream));
 }
 
 }  // extern "C"

@@ -189,6 +189,78 @@ __global__ void k_digits_automorphism(const i64* __restrict__ in, i64* __restric
     }
 }
 
+// Decode support (application_support/ckks.rs:106-130): per coefficient the
+// exact CRT value, centred (wide_crt.rs:96-111), rounded to the nearest double
+// (ties to even; 64 leading bits plus a sticky bit round exactly as the whole
+// value) and divided by the scale.
+template <int W>
+__global__ void __launch_bounds__(kT) k_crt_to_double(const u64* __restrict__ poly, double* __restrict__ out,
+                                                      const NttTab* __restrict__ tabs, GarnerQ g,
+                                                      const u64* __restrict__ half_mr, const u64* __restrict__ q_words,
+                                                      int q_limbs, int L, int log_n, double scale) {
+    const u32 n = 1u << log_n;
+    const u32 c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const size_t pbase = (size_t)blockIdx.y * q_limbs << log_n;
+    u64 v[kMaxQ];
+    for (int i = 0; i < q_limbs; ++i) {
+        const u64 qi = tabs[i].q;
+        u64 acc = 0;
+        for (int j = 0; j < i; ++j) acc = add_mod(acc, mul_shoup(v[j], g.gq[i * L + j], g.gq_q[i * L + j], qi), qi);
+        v[i] = mul_shoup(sub_mod(poly[pbase + ((size_t)i << log_n) + c], acc, qi), g.ginv[i], g.ginv_q[i], qi);
+    }
+    bool neg = false;
+    for (int i = q_limbs - 1; i >= 0; --i) {
+        if (v[i] != half_mr[i]) { neg = v[i] > half_mr[i]; break; }
+    }
+    u64 x[W];
+#pragma unroll
+    for (int w = 0; w < W; ++w) x[w] = 0;
+    x[0] = v[q_limbs - 1];
+    for (int i = q_limbs - 2; i >= 0; --i) {
+        const u64 qi = tabs[i].q;
+        u64 carry = v[i];
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            u64 lo = x[w] * qi, hi = __umul64hi(x[w], qi);
+            lo += carry;
+            hi += lo < carry;
+            x[w] = lo;
+            carry = hi;
+        }
+    }
+    if (neg) {  // magnitude Q - x
+        u64 borrow = 0;
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            u64 b = x[w] + borrow;
+            u64 nb = (b < borrow) | (q_words[w] < b);
+            x[w] = q_words[w] - b;
+            borrow = nb;
+        }
+    }
+    int top = -1;
+#pragma unroll
+    for (int w = W - 1; w >= 0; --w)
+        if (top < 0 && x[w]) top = w * 64 + 63 - __clzll(x[w]);
+    double r = 0.0;
+    if (top >= 0 && top < 64) {
+        r = __ull2double_rn(x[0]);
+    } else if (top >= 64) {
+        const int shift = top - 63;
+        const int wi = shift >> 6, off = shift & 63;
+        u64 lead = off ? ((x[wi] >> off) | (x[wi + 1] << (64 - off))) : x[wi];
+        bool sticky = off ? (x[wi] << (64 - off)) != 0 : false;
+#pragma unroll
+        for (int w = 0; w < W; ++w)
+            if (w < wi && x[w]) sticky = true;
+        if (sticky) lead |= 1;
+        r = ldexp(__ull2double_rn(lead), shift);
+    }
+    r = neg ? -r : r;
+    out[(size_t)blockIdx.y * n + c] = __ddiv_rn(r, scale);
+}
+
 u64 galois_inverse(u64 k, u32 n) {
     const u64 two_n = 2ull * n;
     k %= two_n;
@@ -242,6 +314,28 @@ int32_t digits_automorphism_launch(ckks_ctx* ctx, const i64* in, i64* out, u32 n
     if (!n_polys || !D) return CKKS_OK;
     dim3 grid((ctx->n + kT - 1) / kT, n_polys);
     k_digits_automorphism<<<grid, kT, 0, st>>>(in, out, ctx->log_n, D, base_log, galois_inverse(k, ctx->n));
+    CKKS_CUDA_TRY(cudaGetLastError());
+    return CKKS_OK;
+}
+
+int32_t crt_to_double_launch(ckks_ctx* ctx, const u64* poly, u32 n_polys, u32 q_limbs, double scale, double* out,
+                             cudaStream_t st) {
+    CKKS_CHECK_ARG(q_limbs >= 1 && q_limbs <= ctx->L, "decode: Q prefix outside the context basis");
+    PrefixConst pc;
+    if (int32_t rc = prefix_const(ctx, q_limbs, &pc)) return rc;
+    if (!n_polys) return CKKS_OK;
+    dim3 grid((ctx->n + kT - 1) / kT, n_polys);
+#define CKKS_CRT(WW)                                                                                                \
+    k_crt_to_double<WW><<<grid, kT, 0, st>>>(poly, out, ctx->d_tabs, ctx->garner, pc.d_half_mr, pc.d_q_words,       \
+                                             q_limbs, ctx->L, ctx->log_n, scale)
+    if (pc.W <= 4) CKKS_CRT(4);
+    else if (pc.W <= 8) CKKS_CRT(8);
+    else if (pc.W <= 16) CKKS_CRT(16);
+    else if (pc.W <= 24) CKKS_CRT(24);
+    else if (pc.W <= 32) CKKS_CRT(32);
+    else if (pc.W <= 48) CKKS_CRT(48);
+    else CKKS_CRT(66);
+#undef CKKS_CRT
     CKKS_CUDA_TRY(cudaGetLastError());
     return CKKS_OK;
 }

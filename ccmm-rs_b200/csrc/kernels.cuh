@@ -32,3 +32,13 @@ int32_t digits_automorphism_launch(ckks_ctx* ctx, const i64* in, i64* out, u32 n
 // Forward NTT of signed digits lifted to every limb of `lm` ([D][limbs][N] out).
 int32_t ntt_forward_digits_launch(ckks_ctx* ctx, const i64* digits, u64* out, u32 D, LimbMap lm, u32 limbs,
                                   cudaStream_t st);
+
+// Exact centred CRT of [n][q_limbs][N] residues to nearest doubles divided by scale ([n][N]).
+int32_t crt_to_double_launch(ckks_ctx* ctx, const u64* poly, u32 n_polys, u32 q_limbs, double scale, double* out,
+                             cudaStream_t st);
+
+// FP64 canonical embedding (embed.cu).
+int32_t encode_launch(ckks_ctx* ctx, const double* slots, u64* out, u32 n_msg, u32 q_limbs, double scale,
+                      cudaStream_t st);
+int32_t decode_launch(ckks_ctx* ctx, const u64* poly, double* slots, u32 n_msg, u32 q_limbs, double scale,
+                      cudaStream_t st);

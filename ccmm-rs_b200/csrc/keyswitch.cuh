@@ -61,12 +61,21 @@ int32_t tensor_launch(ckks_ctx* ctx, const u64* lhs, const u64* rhs, u64* out, u
 int32_t relinearize_launch(ckks_ctx* ctx, const ckks_ksk* key, const u64* quad, u64* out, u32 n_ct, cudaStream_t st);
 int32_t multiply_relin_rescale_launch(ckks_ctx* ctx, const ckks_ksk* key, const u64* lhs, const u64* rhs, u64* out,
                                       u32 n_ct, cudaStream_t st);
+// Bounded relinearization key sum: c2 [n][L][N] coefficient domain; acc01
+// [n][2][L][N] holds the NTT-domain c0, c1 on entry and the NTT-domain
+// relinearized (b, a) on return.
+int32_t relin_core_launch(ckks_ctx* ctx, const ckks_ksk* key, const u64* c2, u64* acc01, u32 n, cudaStream_t st);
 int32_t mul_plain_launch(ckks_ctx* ctx, const u64* ct_in, const u64* plain_ntt, u64* out, u32 n_ct, u32 L,
                          bool plain_per_ct, cudaStream_t st);
 
 // One diagonal-rotation FFT stage (fft.cu): diag_ntt [n_rot + identity][L][N].
 int32_t fft_stage_launch(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_rot, bool identity, const u64* diag_ntt,
                          const u64* ct_in, u64* ct_out, u32 n_ct, u32 L, cudaStream_t st);
+
+// Structured CCMM (ccmm.cu): A [k][m], B [n][k], C [n][m] column-major
+// ciphertexts [2][L][N] at the key's level L; C one level down.
+int32_t ccmm_structured_launch(ckks_ctx* ctx, const ckks_ksk* key, const u64* A, const u64* B, u64* C, u32 m, u32 kd,
+                               u32 nd, cudaStream_t st);
 
 // sampling stream tags (shared with the oracle's restatement)
 constexpr u64 TAG_KEY_A = 1ull << 56, TAG_KEY_E = 2ull << 56, TAG_ENC_A = 3ull << 56, TAG_ENC_E = 4ull << 56,

@@ -133,9 +133,15 @@ int32_t tensor_ntt(ckks_ctx* ctx, const u64* Xh, const u64* Yh, u64* out01, size
     return CKKS_OK;
 }
 
+size_t relin_words_per_ct(const ckks_ctx* ctx, const ckks_ksk* key) {
+    return (size_t)key->D * ctx->n * (1 + key->q_limbs);
+}
+
+}  // namespace
+
 // c2: [n][L][N] coefficient domain; acc01: [n][2][L][N] NTT-domain c0, c1 on
 // entry, the NTT-domain relinearized (b, a) on return.
-int32_t relin_core(ckks_ctx* ctx, const ckks_ksk* key, const u64* c2, u64* acc01, u32 n, cudaStream_t st) {
+int32_t relin_core_launch(ckks_ctx* ctx, const ckks_ksk* key, const u64* c2, u64* acc01, u32 n, cudaStream_t st) {
     const u32 L = key->q_limbs, D = key->D, N = ctx->n;
     Workspace<i64> dg;
     Workspace<u64> Y;
@@ -149,12 +155,6 @@ int32_t relin_core(ckks_ctx* ctx, const ckks_ksk* key, const u64* c2, u64* acc01
     CKKS_CUDA_TRY(cudaGetLastError());
     return CKKS_OK;
 }
-
-size_t relin_words_per_ct(const ckks_ctx* ctx, const ckks_ksk* key) {
-    return (size_t)key->D * ctx->n * (1 + key->q_limbs);
-}
-
-}  // namespace
 
 int32_t tensor_launch(ckks_ctx* ctx, const u64* lhs, const u64* rhs, u64* out, u32 n_ct, u32 L, cudaStream_t st) {
     const size_t ct = (size_t)2 * L * ctx->n;
@@ -191,7 +191,7 @@ int32_t relinearize_launch(ckks_ctx* ctx, const ckks_ksk* key, const u64* quad, 
         CKKS_CUDA_TRY(cudaMemcpy2DAsync(acc, 2 * poly * 8, q, 3 * poly * 8, 2 * poly * 8, m, cudaMemcpyDeviceToDevice, st));
         CKKS_CUDA_TRY(cudaMemcpy2DAsync(c2, poly * 8, q + 2 * poly, 3 * poly * 8, poly * 8, m, cudaMemcpyDeviceToDevice, st));
         if ((rc = ntt_forward_launch(ctx, acc, acc, 2 * m, 0, L, st))) return rc;
-        if ((rc = relin_core(ctx, key, c2, acc, m, st))) return rc;
+        if ((rc = relin_core_launch(ctx, key, c2, acc, m, st))) return rc;
         if ((rc = ntt_inverse_launch(ctx, acc, out + (size_t)c0 * 2 * poly, 2 * m, 0, L, st))) return rc;
     }
     return CKKS_OK;
@@ -215,7 +215,7 @@ int32_t multiply_relin_rescale_launch(ckks_ctx* ctx, const ckks_ksk* key, const 
         if ((rc = ntt_forward_launch(ctx, rhs + c0 * ct, Yh, 2 * m, 0, L, st))) return rc;
         if ((rc = tensor_ntt(ctx, Xh, Yh, acc, ct, c2, poly, m, L, st))) return rc;
         if ((rc = ntt_inverse_launch(ctx, c2, Xh, m, 0, L, st))) return rc;  // c2 to the coefficient domain
-        if ((rc = relin_core(ctx, key, Xh, acc, m, st))) return rc;
+        if ((rc = relin_core_launch(ctx, key, Xh, acc, m, st))) return rc;
         if ((rc = ntt_inverse_launch(ctx, acc, Yh, 2 * m, 0, L, st))) return rc;
         if ((rc = rescale_launch(ctx, Yh, out + (size_t)c0 * 2 * (L - 1) * N, 2 * m, L, st))) return rc;
     }

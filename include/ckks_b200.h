@@ -268,6 +268,36 @@ int32_t ckks_fft_stage(ckks_ctx* ctx, const ckks_ksk* const* keys, uint32_t n_ro
                        const uint64_t* diag_ntt, const uint64_t* ct_in, uint64_t* ct_out, uint32_t n_ct,
                        uint32_t q_limbs, void* stream);
 
+
+/* Structured encrypted matrix product (one ciphertext per entry):
+ *   C[r][c] = Rescale( Relinearize( sum_k tensor(A[r][k], B[k][c]) ) )
+ * with the bounded relinearization key at the entries' level L = key q_limbs
+ * (>= 2). Matrices are column-major arrays of ciphertexts [2][L][N] (entry
+ * row + col * rows): A m x k, B k x n, C m x n at level L-1. Requires every Q
+ * modulus below 2^60 and 2 * 8 * (m * k + k) bytes of shared memory per slot
+ * block (m * k <= 12288). Replaces matmul_structured_bounded_with_ntt(_observed)
+ * (matrix/rns_ckks_ciphertext.rs:204-318); results equal it word for word. */
+int32_t ckks_ccmm_structured(ckks_ctx* ctx, const ckks_ksk* key, const uint64_t* A, const uint64_t* B, uint64_t* C,
+                             uint32_t m, uint32_t k, uint32_t n, void* stream);
+
+
+/* ------------------------------------------------------ encode / decode ----
+ * FP64 canonical embedding on the GPU with the reference's rounding (every
+ * double equals the reference operation sequence bit for bit).
+ * Encode: n_msg messages of N/2 complex slots (device, interleaved re, im
+ * doubles) -> plaintexts [n_msg][q_limbs][N] (device, coefficient domain),
+ * round(coefficient * scale) (half away from zero) mod q_l. Replaces
+ * encode_rns (application_support/ckks.rs:39-62) with
+ * CkksCanonicalEmbedding::slots_to_coefficients (ckks/embedding.rs:261-349). */
+int32_t ckks_encode(ckks_ctx* ctx, const double* slots, uint64_t* out, uint32_t n_msg, uint32_t q_limbs, double scale,
+                    void* stream);
+/* Decode: plaintexts [n_msg][q_limbs][N] -> slots [n_msg][N/2][2] (device):
+ * exact CRT, centred, rounded to the nearest double (ties to even), divided by
+ * scale, then coefficients_to_slots (ckks/embedding.rs:174-258). Replaces the
+ * decode of application_support/ckks.rs:106-130. */
+int32_t ckks_decode(ckks_ctx* ctx, const uint64_t* poly, double* slots, uint32_t n_msg, uint32_t q_limbs,
+                    double scale, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
