@@ -1,6 +1,6 @@
 """Throughput benchmark of the B200 RNS-CKKS hot path.
 
-python bench.py [--gpus N] [--steps K] [--warmup W] [--workload rotation|ntt|multiply|ccmm] [--impl reference]
+python bench.py [--gpus N] [--steps K] [--warmup W] [--workload rotation|ntt|multiply|ccmm|fft2] [--impl reference]
 
 Workload "rotation" (default): hoisted key-switched Galois rotations at
 N=2^16 over 24 Q limbs of 50-bit primes and 3 auxiliary 60-bit primes (the
@@ -21,6 +21,11 @@ Workload "ccmm": structured encrypted matrix product of two 64 x 64 matrices
 of ciphertexts (one per entry) at N=2^15 over 14 x 50-bit limbs with the
 bounded relinearization key (base 2^20): sum of 64 tensors per output entry,
 relinearize, rescale. One step = one 64 x 64 CCMM. Metric: CCMM per second.
+
+Workload "fft2": encrypted 2-D FFT of eight 256 x 256 real images, two
+ciphertexts per image at N=2^16 (24 x 50-bit Q, 3 x 60-bit P), with the
+radix-4 diagonal-rotation schedule: 4 row and 4 column stages, each
+sum(diagonal * rotation) + rescale. One step = 8 images. Metric: images/s.
 
 Workload "multiply": the plain CKKS chain at N=2^12 (q = 60 + 40 + 40 bits,
 P = 60 bits, the reference's prime search): HMult -> bounded relinearization
@@ -281,6 +286,23 @@ def ntt_cpu_sample(threads, seconds_target=10.0):
 def reference_arm(args, world, rank):
     if rank != 0:
         return None
+    if args.workload == "fft2":
+        threads = os.cpu_count() or 1
+        vals, sample = [], None
+        for i in range(1 + args.steps):
+            v, sample = fft2_cpu_sample(threads)
+            if i >= 1:
+                vals.append(v)
+        value = float(np.median(vals))
+        return {
+            "metric": "encrypted 256x256 FFT2 images/s (N=2^16, 24 limbs, radix-4 schedule, bit-exact)",
+            "value": value, "unit": "images/s", "n_gpus": world, "steps": args.steps, "warmup": 1,
+            "ms_per_step": 1000.0 * FFT2_IMAGES / value, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded uniform ciphertexts)",
+            "config": fft2_config(), "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "images/s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "images/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
     if args.workload == "ccmm":
         threads = os.cpu_count() or 1
         vals, sample = [], None
@@ -750,12 +772,144 @@ def ccmm_cpu_sample(threads):
                                     "N=2^15, 14 limbs, %.1f s" % (threads, dt))
 
 
+# -------------------------------------------------------------- FFT2 (images)
+FFT2_LOG_N, FFT2_S, FFT2_L, FFT2_K, FFT2_IMAGES, FFT2_BASE_LOG = 16, 256, 24, 3, 8, 32
+
+
+def fft2_config():
+    return {"workload": "encrypted 2-D FFT of 256x256 real images, 2 ciphertexts per image at N=2^16, "
+                        "24 x 50-bit Q + 3 x 60-bit P, radix-4 diagonal-rotation schedule (4 row + 4 column "
+                        "stages, 6 rotations + 7 plaintext products per stage), 8 images per step",
+            "log_n": FFT2_LOG_N, "image": [FFT2_S, FFT2_S], "images": FFT2_IMAGES, "q_limbs": FFT2_L,
+            "p_limbs": FFT2_K, "base_log": FFT2_BASE_LOG, "scale": "2^50",
+            "l2": "keys (about 35 GB) larger than L2", "parallelism": "replicas"}
+
+
+def bench_fft2_gpu(args, world, rank, local):
+    import torch
+    import ckks_b200 as cb
+    import ckks_b200.params as params
+    from ckks_b200 import fft2
+    dev = torch.device("cuda", local)
+    n = 1 << FFT2_LOG_N
+    q = params.primes_below_bits(50, n, FFT2_L)
+    p = params.primes_below_bits(60, n, FFT2_K)
+    ctx = cb.Context(FFT2_LOG_N, q, p)
+    rng = np.random.default_rng(55 + rank)
+    secret = rng.integers(-1, 2, n).astype(np.int8)
+    plan = fft2.Fft2Plan(ctx, FFT2_S, FFT2_L, secret, base_log=FFT2_BASE_LOG)
+    key_bytes = sum(8 * k.info()[1] for st in plan.stages for k in st[2])
+    host = np.stack([np.stack([np.stack([rng.integers(0, m, (2, n), dtype=np.uint64) for m in q], axis=1)
+                               for _ in range(2)]) for _ in range(FFT2_IMAGES)])
+    cts = cb.as_u64_tensor(host, dev)
+    st = torch.cuda.current_stream()
+
+    def step(x):
+        return plan.apply(x)
+
+    for _ in range(args.warmup):
+        step(cts)
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(st)
+    for _ in range(args.steps):
+        out = step(cts)
+    t1.record(st)
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = t0.elapsed_time(t1)
+    clk = clocks.stop()
+    ms_max = max_over_ranks(world, ms)
+    value = FFT2_IMAGES * args.steps * world / (ms_max / 1000.0)
+    rotations = sum(len(st_[2]) for st_ in plan.stages[:-1]) * 2 * FFT2_IMAGES + 2 * FFT2_IMAGES
+    # algorithmic bytes: every key once per stage batch, ciphertexts in and out of every stage
+    ct_bytes = lambda lvl: 2 * lvl * n * 8
+    lv = [st_[1] for st_ in plan.stages]
+    bytes_step = key_bytes + sum(2 * FFT2_IMAGES * (ct_bytes(l) + ct_bytes(l - 1)) for l in lv)
+    peak, kind = peaks()
+    achieved = bytes_step / (ms_max / args.steps / 1000.0) / 1e9
+    pin_in = torch.from_numpy(host.view(np.int64)).pin_memory()
+    pin_out = torch.empty(tuple(out.shape), dtype=torch.int64).pin_memory()
+    d_in = torch.empty_like(cts)
+    torch.cuda.synchronize()
+    barrier(world)
+    t = time.perf_counter()
+    d_in.copy_(pin_in, non_blocking=True)
+    o2 = step(d_in)
+    pin_out.copy_(o2, non_blocking=True)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(world, time.perf_counter() - t)
+    return {
+        "metric": "encrypted 256x256 FFT2 images/s (N=2^16, 24 limbs, radix-4 schedule, bit-exact)",
+        "value": value, "unit": "images/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u64", "data": "synthetic (seeded uniform ciphertexts, GPU-generated keys, GPU-encoded diagonals)",
+        "config": fft2_config(),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_kind": kind,
+                     "kernel": "whole FFT2 (key streams and stage ciphertexts; rotations per step: %d)" % rotations,
+                     "algorithmic_bytes_per_step": bytes_step},
+        "e2e": {"value": FFT2_IMAGES * world / e2e_s, "unit": "images/s", "h2d_bytes_per_step": int(host.nbytes),
+                "d2h_bytes_per_step": int(pin_out.numel() * 8), "path": "torch pinned copies + ckks_fft_stage(_multi)"},
+        "gpu_launches": None, "clocks": clk,
+    }
+
+
+def fft2_cpu_sample(threads):
+    """Times the oracle's restatement of one radix-4 row stage (6 hoisted
+    rotations, 7 plaintext products, sum, rescale) on one ciphertext per
+    thread at level 20 (the middle of the 24 .. 17 levels the 8 stages use);
+    images/s = threads / (16 x stage time)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import Oracle, P, arr, u64p
+    import concurrent.futures as cf
+    o = Oracle()
+    n, lvl = 1 << FFT2_LOG_N, 20
+    q = arr(o.primes_below_bits(50, n, FFT2_L))[:lvl]
+    p = arr(o.primes_below_bits(60, n, FFT2_K))
+    rng = np.random.default_rng(3)
+    secret = rng.integers(-1, 2, n).astype(np.int8)
+    offs = [-3, -2, -1, 1, 2, 3]
+    exps = [int(o.L.oracle_rotation_exponent_left(n, x)) if x > 0 else int(o.L.oracle_rotation_exponent_right(n, -x))
+            for x in offs]
+    with cf.ThreadPoolExecutor(6) as ex:
+        keys = list(ex.map(lambda ie: o.hybrid_key(q, p, secret, ie[1], FFT2_BASE_LOG, seed=900 + ie[0]),
+                           enumerate(exps)))
+    plains = [np.stack([rng.integers(0, m, n, dtype=np.uint64) for m in q]) for _ in range(7)]
+    cts = np.stack([np.stack([rng.integers(0, m, (2, n), dtype=np.uint64) for m in q], axis=1)
+                    for _ in range(threads)])
+    rot = np.zeros((threads, 6, 2, lvl, n), np.uint64)
+    kp = (u64p * 6)(*[P(k) for k in keys])
+    ex_arr = arr(exps)
+
+    def finish(c):
+        acc = o.mul_plain(q, cts[c], plains[6]).astype(object)
+        for g in range(6):
+            acc = acc + o.mul_plain(q, rot[c, g], plains[g]).astype(object)
+        acc = np.stack([acc[:, l] % int(q[l]) for l in range(lvl)], axis=1).astype(np.uint64)
+        return o.rescale(q, acc)
+
+    t = time.perf_counter()
+    o.L.oracle_hybrid_rotate_hoisted_batch(P(q), lvl, P(p), FFT2_K, n, FFT2_BASE_LOG, 6, P(ex_arr), kp, threads,
+                                           P(cts), P(rot), threads)
+    with cf.ThreadPoolExecutor(threads) as ex:
+        list(ex.map(finish, range(threads)))
+    dt = time.perf_counter() - t
+    return threads / (16 * dt), ("%d ciphertexts x one radix-4 stage at level 20 (6 hoisted rotations, 7 plaintext "
+                                 "products, rescale; one ciphertext per thread), %.1f s; x16 stage-ciphertexts "
+                                 "per image" % (threads, dt))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="rotation", choices=["rotation", "ntt", "multiply", "ccmm"])
+    ap.add_argument("--workload", default="rotation", choices=["rotation", "ntt", "multiply", "ccmm", "fft2"])
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -765,6 +919,18 @@ def main():
         line = reference_arm(args, world, rank)
         if line:
             print(json.dumps(line), flush=True)
+        return
+    if args.workload == "fft2":
+        line = bench_fft2_gpu(args, world, rank, local)
+        if rank == 0:
+            threads = os.cpu_count() or 1
+            v, sample = fft2_cpu_sample(threads)
+            line["cpu_baseline"] = {"value": v, "unit": "images/s", "cores": threads, "kind": "port",
+                                    "sample": sample}
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
         return
     if args.workload == "ccmm":
         line = bench_ccmm_gpu(args, world, rank, local)

@@ -73,6 +73,7 @@ _SIGS = {
     "ckks_mul_plain": (I32, [VP, VP, VP, VP, U32, U32, U32, VP]),
     "ckks_fft_stage": (I32, [VP, ctypes.POINTER(VP), U32, I32, VP, VP, VP, U32, U32, VP]),
     "ckks_ccmm_structured": (I32, [VP, VP, VP, VP, VP, U32, U32, U32, VP]),
+    "ckks_fft_stage_multi": (I32, [VP, ctypes.POINTER(VP), U32, u32p, U32, VP, VP, U32, VP, U32, U32, VP]),
     "ckks_encode": (I32, [VP, VP, VP, U32, U32, ctypes.c_double, VP]),
     "ckks_decode": (I32, [VP, VP, VP, U32, U32, ctypes.c_double, VP]),
 }
@@ -535,6 +536,22 @@ def matmul_structured(ctx, key, A, B, m, k, n, out=None, stream=None):
         out = torch.empty((n, m, 2, L - 1, ctx.n), dtype=torch.int64, device=A.device)
     check(lib().ckks_ccmm_structured(ctx.handle, key.handle, _dptr(A), _dptr(B), _dptr(out), m, k, n,
                                      _stream(stream)))
+    return out
+
+
+def fft_stage_multi(ctx, keys, terms, diag_ntt, cts, n_out, out=None, stream=None):
+    """Diagonal stage over several ciphertexts: out[a] = Rescale(sum over terms
+    (a, src, key) of diag * rotate(cts[src], keys[key])); key == len(keys)
+    selects the unrotated input. diag_ntt [len(terms)][L][N] in term order."""
+    import torch
+    L = cts.shape[-2]
+    n_in = _n_ct(ctx, cts, 2, L)
+    t = np.ascontiguousarray(np.asarray(terms, dtype=np.uint32).reshape(-1, 3))
+    if out is None:
+        out = torch.empty((n_out, 2, L - 1, ctx.n), dtype=torch.int64, device=cts.device)
+    arr = (VP * max(1, len(keys)))(*[k.handle.value for k in keys])
+    check(lib().ckks_fft_stage_multi(ctx.handle, arr, len(keys), t.ctypes.data_as(u32p), len(t), _dptr(diag_ntt),
+                                     _dptr(cts), n_in, _dptr(out), n_out, L, _stream(stream)))
     return out
 
 

@@ -136,6 +136,32 @@ int32_t ckks_ccmm_structured(ckks_ctx* ctx, const ckks_ksk* key, const uint64_t*
     return ccmm_structured_launch(ctx, key, A, B, C, m, k, n, ckks_stream(ctx, stream));
 }
 
+int32_t ckks_fft_stage_multi(ckks_ctx* ctx, const ckks_ksk* const* keys, uint32_t n_rot, const uint32_t* terms_host,
+                             uint32_t n_terms, const uint64_t* diag_ntt, const uint64_t* ct_in, uint32_t n_in,
+                             uint64_t* ct_out, uint32_t n_out, uint32_t q_limbs, void* stream) {
+    CKKS_CHECK_ARG(ctx != nullptr, "ckks_fft_stage_multi: null context");
+    CKKS_CHECK_ARG(terms_host && diag_ntt && ct_in && ct_out && n_terms && n_in && n_out && (n_rot == 0 || keys),
+                   "ckks_fft_stage_multi: bad arguments");
+    CKKS_CHECK_ARG(q_limbs >= 2 && q_limbs <= ctx->L, "ckks_fft_stage_multi: need 2..L limbs (the stage rescales)");
+    CKKS_CHECK_ARG(n_out <= 65535 && (size_t)2 * n_in * (n_rot + 1) <= 65535, "ckks_fft_stage_multi: batch too large");
+    for (u32 t = 0; t < n_terms; ++t)
+        CKKS_CHECK_ARG(terms_host[3 * t] < n_out && terms_host[3 * t + 1] < n_in && terms_host[3 * t + 2] <= n_rot,
+                       "ckks_fft_stage_multi: term index out of range");
+    for (u32 g = 0; g < n_rot; ++g) {
+        const ckks_ksk* k = keys[g];
+        if (!k || k->ctx != ctx || k->kind == CKKS_KSK_RELIN_BOUNDED || k->kind != keys[0]->kind ||
+            k->q_limbs != q_limbs || k->base_log != keys[0]->base_log || k->D != keys[0]->D ||
+            k->blocks != keys[0]->blocks) {
+            ckks_set_error("ckks_fft_stage_multi: keys must be Galois keys of one kind and gadget at level q_limbs");
+            return CKKS_ERR_BASIS_MISMATCH;
+        }
+    }
+    const size_t in = (size_t)2 * q_limbs * ctx->n * 8 * n_in, o = (size_t)2 * (q_limbs - 1) * ctx->n * 8 * n_out;
+    CKKS_CHECK_ARG(!overlaps(ct_out, o, ct_in, in), "ckks_fft_stage_multi: out overlaps the input");
+    return fft_stage_multi_launch(ctx, keys, n_rot, terms_host, n_terms, diag_ntt, ct_in, n_in, ct_out, n_out,
+                                  q_limbs, ckks_stream(ctx, stream));
+}
+
 int32_t ckks_encode(ckks_ctx* ctx, const double* slots, uint64_t* out, uint32_t n_msg, uint32_t q_limbs, double scale,
                     void* stream) {
     CKKS_CHECK_ARG(ctx != nullptr, "ckks_encode: null context");

@@ -4,6 +4,7 @@
 #include <thread>
 
 #include "context.cuh"
+#include "kernels.cuh"
 
 namespace {
 
@@ -374,7 +375,9 @@ int32_t ckks_primes_below_bits(uint32_t bits, uint32_t degree, uint32_t count, u
 
 int32_t ckks_ctx_destroy(ckks_ctx* ctx) {
     if (!ctx) return CKKS_OK;
-    if (ctx->own_stream) cudaStreamSynchronize(ctx->own_stream);
+    cudaDeviceSynchronize();
+    gadget_release_ctx(ctx);
+    embed_release_ctx(ctx);
     if (ctx->d_tabs) cudaFree(ctx->d_tabs);
     if (ctx->d_table_mem) cudaFree(ctx->d_table_mem);
     if (ctx->d_const_mem) cudaFree(ctx->d_const_mem);

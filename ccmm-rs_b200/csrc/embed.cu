@@ -265,3 +265,16 @@ int32_t decode_launch(ckks_ctx* ctx, const u64* poly, double* slots, u32 n_msg, 
     CKKS_CUDA_TRY(cudaGetLastError());
     return CKKS_OK;
 }
+
+// Drops the cached tables of a context that is being destroyed.
+void embed_release_ctx(const ckks_ctx* ctx) {
+    std::lock_guard<std::mutex> lock(g_embed_mutex);
+    auto it = g_embed.find(ctx);
+    if (it == g_embed.end()) return;
+    cudaFree(it->second.idx);
+    cudaFree(it->second.tw_fwd);
+    cudaFree(it->second.tw_inv);
+    cudaFree(it->second.tw_enc);
+    cudaFree(it->second.tw_dec);
+    g_embed.erase(it);
+}

@@ -11,6 +11,8 @@
 // and one rescale. The sum of products is linear mod q, so the result equals
 // the reference's per-term inverse transforms and sequential additions word
 // for word.
+#include <vector>
+
 #include "keyswitch.cuh"
 
 namespace {
@@ -53,7 +55,93 @@ __global__ void __launch_bounds__(kT) k_diag_mac(const u64* __restrict__ R, cons
     acc[c * 2 * poly + poly + lk] = aa.lo;
 }
 
+// Multi-ciphertext stage: out[a] = sum over the terms t of output a of
+// R[src_t][key_t] * P[t] (key_t = n_rot: the unrotated input X[src_t]).
+// terms: [n_terms][3] (output, source, key) sorted by output; first[a] .. first[a+1]
+// index the terms of output a. R: [n_in][n_rot][2][L][N], X: [n_in][2][L][N].
+__global__ void __launch_bounds__(kT) k_diag_mac_multi(const u64* __restrict__ R, const u64* __restrict__ X,
+                                                       const u64* __restrict__ P, const u32* __restrict__ terms,
+                                                       const u32* __restrict__ first, u64* __restrict__ acc,
+                                                       const NttTab* __restrict__ tabs, int n_rot, int L, int log_n) {
+    const u32 n = 1u << log_n;
+    const u32 k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int l = blockIdx.y;
+    const u32 a = blockIdx.z;
+    const NttTab& T = tabs[l];
+    const size_t poly = (size_t)L << log_n, lk = ((size_t)l << log_n) + k;
+    Acc128 ab{0, 0}, aa{0, 0};
+    int since = 0;
+    for (u32 t = first[a]; t < first[a + 1]; ++t) {
+        const u32 src = terms[3 * t + 1], key = terms[3 * t + 2];
+        const u64 p = __ldg(P + (size_t)t * poly + lk);
+        const u64* r = key < (u32)n_rot ? R + ((size_t)src * n_rot + key) * 2 * poly + lk : X + (size_t)src * 2 * poly + lk;
+        ab.mac(r[0], p);
+        aa.mac(r[poly], p);
+        if (++since == 15) {
+            ab.fold(T.q, T.mu_hi, T.mu_lo);
+            aa.fold(T.q, T.mu_hi, T.mu_lo);
+            since = 0;
+        }
+    }
+    ab.fold(T.q, T.mu_hi, T.mu_lo);
+    aa.fold(T.q, T.mu_hi, T.mu_lo);
+    acc[(size_t)a * 2 * poly + lk] = ab.lo;
+    acc[(size_t)a * 2 * poly + poly + lk] = aa.lo;
+}
+
 }  // namespace
+
+int32_t fft_stage_multi_launch(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_rot, const u32* terms_host,
+                               u32 n_terms, const u64* diag_ntt, const u64* ct_in, u32 n_in, u64* ct_out, u32 n_out,
+                               u32 L, cudaStream_t st) {
+    const u32 N = ctx->n;
+    const size_t poly = (size_t)L * N, ct = 2 * poly;
+    std::vector<u32> first(n_out + 1, 0), tl(3 * (size_t)n_terms);
+    {   // stable order by output
+        u32 w = 0;
+        for (u32 a = 0; a < n_out; ++a) {
+            first[a] = w;
+            for (u32 t = 0; t < n_terms; ++t)
+                if (terms_host[3 * t] == a) {
+                    for (int i = 0; i < 3; ++i) tl[3 * (size_t)w + i] = terms_host[3 * t + i];
+                    ++w;
+                }
+        }
+        first[n_out] = w;
+    }
+    // diagonals follow the caller's term order: remap to the sorted order
+    std::vector<u32> perm(n_terms);
+    {
+        u32 w = 0;
+        for (u32 a = 0; a < n_out; ++a)
+            for (u32 t = 0; t < n_terms; ++t)
+                if (terms_host[3 * t] == a) perm[w++] = t;
+    }
+    Workspace<u64> R, X, acc, P;
+    Workspace<u32> dterms;
+    int32_t rc;
+    if ((rc = R.alloc(ct * n_in * (n_rot ? n_rot : 1), st)) || (rc = X.alloc(ct * n_in, st)) ||
+        (rc = acc.alloc(ct * n_out, st)) || (rc = P.alloc(poly * n_terms, st)) ||
+        (rc = dterms.alloc(tl.size() + first.size(), st)))
+        return rc;
+    for (u32 w = 0; w < n_terms; ++w)
+        CKKS_CUDA_TRY(cudaMemcpyAsync(P.p + (size_t)w * poly, diag_ntt + (size_t)perm[w] * poly, poly * 8,
+                                      cudaMemcpyDeviceToDevice, st));
+    CKKS_CUDA_TRY(cudaMemcpyAsync(dterms.p, tl.data(), tl.size() * 4, cudaMemcpyHostToDevice, st));
+    CKKS_CUDA_TRY(cudaMemcpyAsync(dterms.p + tl.size(), first.data(), first.size() * 4, cudaMemcpyHostToDevice, st));
+    if (n_rot) {
+        if ((rc = rotate_hoisted_ntt(ctx, keys, n_rot, ct_in, R.p, n_in, st))) return rc;
+        if ((rc = ntt_forward_launch(ctx, R.p, R.p, 2 * n_in * n_rot, 0, L, st))) return rc;
+    }
+    if ((rc = ntt_forward_launch(ctx, ct_in, X.p, 2 * n_in, 0, L, st))) return rc;
+    dim3 g((N + kT - 1) / kT, L, n_out);
+    k_diag_mac_multi<<<g, kT, 0, st>>>(R.p, X.p, P.p, dterms.p, dterms.p + tl.size(), acc.p, ctx->d_tabs, (int)n_rot,
+                                       (int)L, (int)ctx->log_n);
+    CKKS_CUDA_TRY(cudaGetLastError());
+    if ((rc = ntt_inverse_launch(ctx, acc.p, acc.p, 2 * n_out, 0, L, st))) return rc;
+    return rescale_launch(ctx, acc.p, ct_out, 2 * n_out, L, st);
+}
 
 int32_t fft_stage_launch(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_rot, bool identity, const u64* diag_ntt,
                          const u64* ct_in, u64* ct_out, u32 n_ct, u32 L, cudaStream_t st) {

@@ -29,6 +29,7 @@ std::map<std::pair<const ckks_ctx*, u32>, PrefixConst> g_prefix;
 typedef unsigned __int128 u128;
 
 int words_for_bits(u32 bits) { return (int)(bits / 64) + 2; }
+constexpr int kMaxWords = 66;  // widest k_bounded_decompose / k_crt_to_double instantiation
 
 // Host helpers on little-endian word vectors.
 void mul_small_add(std::vector<u64>& x, u64 m, u64 a) {
@@ -73,14 +74,18 @@ int32_t prefix_const(ckks_ctx* ctx, u32 q_limbs, PrefixConst* out) {
     PrefixConst pc;
     pc.W = W;
     pc.bits = bits;
+    // Q as words, zero-padded to the widest kernel instantiation (kernels of
+    // width W' >= W read all W' words)
+    std::vector<u64> qpad(kMaxWords, 0);
+    std::copy(Q.begin(), Q.end(), qpad.begin());
     if (cudaMalloc(&pc.d_half_mr, q_limbs * sizeof(u64)) != cudaSuccess ||
-        cudaMalloc(&pc.d_q_words, W * sizeof(u64)) != cudaSuccess) {
+        cudaMalloc(&pc.d_q_words, kMaxWords * sizeof(u64)) != cudaSuccess) {
         cudaGetLastError();
         ckks_set_error("out of device memory for gadget constants");
         return CKKS_ERR_OOM;
     }
     cudaMemcpy(pc.d_half_mr, mr.data(), q_limbs * sizeof(u64), cudaMemcpyHostToDevice);
-    cudaMemcpy(pc.d_q_words, Q.data(), W * sizeof(u64), cudaMemcpyHostToDevice);
+    cudaMemcpy(pc.d_q_words, qpad.data(), kMaxWords * sizeof(u64), cudaMemcpyHostToDevice);
     g_prefix[key] = pc;
     *out = pc;
     return CKKS_OK;
@@ -338,4 +343,19 @@ int32_t crt_to_double_launch(ckks_ctx* ctx, const u64* poly, u32 n_polys, u32 q_
 #undef CKKS_CRT
     CKKS_CUDA_TRY(cudaGetLastError());
     return CKKS_OK;
+}
+
+// Drops the cached prefix constants of a context that is being destroyed (a
+// later context may be created at the same address).
+void gadget_release_ctx(const ckks_ctx* ctx) {
+    std::lock_guard<std::mutex> lock(g_prefix_mutex);
+    for (auto it = g_prefix.begin(); it != g_prefix.end();) {
+        if (it->first.first == ctx) {
+            cudaFree(it->second.d_half_mr);
+            cudaFree(it->second.d_q_words);
+            it = g_prefix.erase(it);
+        } else {
+            ++it;
+        }
+    }
 }

@@ -42,3 +42,7 @@ int32_t encode_launch(ckks_ctx* ctx, const double* slots, u64* out, u32 n_msg, u
                       cudaStream_t st);
 int32_t decode_launch(ckks_ctx* ctx, const u64* poly, double* slots, u32 n_msg, u32 q_limbs, double scale,
                       cudaStream_t st);
+
+// Per-context caches of gadget.cu and embed.cu, released by ckks_ctx_destroy.
+void gadget_release_ctx(const ckks_ctx* ctx);
+void embed_release_ctx(const ckks_ctx* ctx);

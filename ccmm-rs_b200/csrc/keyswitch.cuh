@@ -77,6 +77,12 @@ int32_t fft_stage_launch(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_rot, 
 int32_t ccmm_structured_launch(ckks_ctx* ctx, const ckks_ksk* key, const u64* A, const u64* B, u64* C, u32 m, u32 kd,
                                u32 nd, cudaStream_t st);
 
+// Multi-ciphertext diagonal stage: terms_host [n_terms][3] = (output, source, key or n_rot
+// for the unrotated source); diag_ntt [n_terms][L][N] in the caller's term order.
+int32_t fft_stage_multi_launch(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_rot, const u32* terms_host,
+                               u32 n_terms, const u64* diag_ntt, const u64* ct_in, u32 n_in, u64* ct_out, u32 n_out,
+                               u32 L, cudaStream_t st);
+
 // sampling stream tags (shared with the oracle's restatement)
 constexpr u64 TAG_KEY_A = 1ull << 56, TAG_KEY_E = 2ull << 56, TAG_ENC_A = 3ull << 56, TAG_ENC_E = 4ull << 56,
               TAG_RLK_A = 5ull << 56, TAG_RLK_E = 6ull << 56;

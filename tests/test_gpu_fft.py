@@ -130,3 +130,61 @@ def test_fft256_four_stages_decode_to_dft(oracle, cuda, setup):
     want = np.concatenate([np.fft.fft(x[b * 256:(b + 1) * 256]) for b in range(slots // 256)])
     err = np.linalg.norm(dec - want) / np.linalg.norm(want)
     assert err < 1e-6, err
+
+
+def test_cross_ciphertext_stage_bit_exact(oracle, cuda):
+    """fft_stage_multi over two ciphertexts (the last column stage of the 2-D
+    FFT) equals the oracle's rotations, plaintext products, sums and rescale."""
+    from ckks_b200 import fft2
+    log_n, n = 12, 1 << 12
+    q = [int(x) for x in oracle.primes_below_bits(50, n, 3)]
+    p = [int(x) for x in oracle.primes_below_bits(60, n, 1)]
+    ctx = cb.Context(log_n, q, p)
+    rng = np.random.default_rng(4)
+    s = rng.integers(-1, 2, n).astype(np.int8)
+    k = ctx.rotation_exponent_left(n // 4)
+    key_ref = oracle.hybrid_key(q, p, s, k, 20, seed=9)
+    key = cb.KeySwitchKey.hybrid_upload(ctx, 3, 20, k, key_ref)
+    terms = fft2.cross_stage_terms(64)
+    plains = [oracle.encode(t[3], q, float(q[-1])) for t in terms]
+    diag_ntt = np.stack([oracle.ntt_forward(q, x.copy()) for x in plains])
+    cts = np.stack([np.stack([np.stack([rng.integers(0, m, n, dtype=np.uint64) for m in q]) for _ in range(2)])
+                    for _ in range(2)])
+    tl = [(a, b, 0 if rot else 1) for a, b, rot, _ in terms]
+    got = host(cb.fft_stage_multi(ctx, [key], tl, dev(diag_ntt), dev(cts), 2))
+    rotated = [oracle.hybrid_rotate(q, p, key_ref, k, 20, cts[b]) for b in range(2)]
+    for a in range(2):
+        acc = None
+        for (aa, b, rot, _), pl in zip(terms, plains):
+            if aa != a:
+                continue
+            src = rotated[b] if rot else cts[b]
+            t = oracle.mul_plain(q, src, pl).astype(object)
+            acc = t if acc is None else acc + t
+        acc = np.stack([acc[:, l] % m for l, m in enumerate(q)], axis=1).astype(np.uint64)
+        assert np.array_equal(got[a], oracle.rescale(q, acc)), a
+
+
+def test_fft2_image_decodes_to_dft2(oracle, cuda):
+    """64 x 64 image in two ciphertexts at N=2^12: 3 row + 3 column radix-4
+    stages decode to numpy's 2-D DFT."""
+    from ckks_b200 import fft2
+    log_n, n, S = 12, 1 << 12, 64
+    q = [int(x) for x in oracle.primes_below_bits(50, n, 8)]
+    p = [int(x) for x in oracle.primes_below_bits(60, n, 2)]
+    ctx = cb.Context(log_n, q, p)
+    rng = np.random.default_rng(6)
+    s = rng.integers(-1, 2, n).astype(np.int8)
+    plan = fft2.Fft2Plan(ctx, S, len(q), s, base_log=20)
+    assert plan.out_level == len(q) - 6
+    img = rng.uniform(0, 1, (S, S))
+    scale = 2.0 ** 40
+    packed = fft2.pack_image(img)
+    cts = np.stack([oracle.encrypt(q, s, oracle.encode(packed[c], q, scale), seed=20 + c) for c in range(2)])
+    out = host(plan.apply(dev(cts[None]))[0])
+    ql = q[:plan.out_level]
+    slots = np.stack([oracle.decode(ql, oracle.decrypt(ql, s, out[c]), scale) for c in range(2)])
+    spec = fft2.unpack_spectrum(slots)
+    want = np.fft.fft2(img)
+    err = np.linalg.norm(spec - want) / np.linalg.norm(want)
+    assert err < 1e-6, err
