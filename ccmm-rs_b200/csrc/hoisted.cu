@@ -310,6 +310,20 @@ __global__ void __launch_bounds__(kS * kLanes, 2) k_mac_tiled(const u64* __restr
     }
 }
 
+// The tensor-core MAC runs on compute capability 10.0 devices (the library is
+// built for sm_100a only).
+bool tc_enabled() {
+    static int cached = -1;
+    if (cached < 0) {
+        int dev = 0, major = 0, minor = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+        cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
+        cached = (major == 10 && minor == 0) ? 1 : 0;
+    }
+    return cached == 1;
+}
+
 // CUDA-event phase timer (the analogue of the reference's HybridRotationTiming,
 // ckks/hybrid_rns_galois_key.rs:323-336). Phases accumulate over groups.
 struct PhaseTimer {
@@ -346,6 +360,389 @@ struct PhaseTimer {
     }
 };
 
+// ---------------------------------------------------------------------------
+// Key-switch MAC on the tcgen05 INT8 tensor cores.
+//
+// For one limb l and slot s the MAC of a ciphertext group and a set of
+// Galois keys is a matrix product over the digits j:
+//   acc[c][g][comp] = sum_j Y[c][j] * K_g[j][comp]        (mod q_l)
+// Both operands are split into bytes. With w_b = 2^(8b) Y mod q (canonical),
+//   sum_j Y K = sum_j sum_b byte_b(K) 2^(8b) Y  ==  sum_(j,b) byte_b(K) w_b   (mod q)
+// and w_b = sum_a 2^(8a) byte_a(w_b), so
+//   acc[c][g][comp] == sum_a 2^(8a) P[(g,comp)][(c,a)]  (mod q),
+//   P[(g,comp)][(c,a)] = sum_(j,b) byte_b(K_g[j][comp]) * byte_a(w_b(Y[c][j]))
+// an exact unsigned 8-bit product with K = 8 D' terms (D' = D rounded up to a
+// multiple of 4) and 32-bit accumulation (< 8 D' 255^2 < 2^31 for D' <= 4096).
+// One tcgen05.mma.kind::i8 per (slot, 4 digits): M = 64 rows (32 keys x 2
+// components), N = 128 columns (16 ciphertexts x 8 byte planes), K = 32 bytes.
+// A (keys) is K-major: row (g, comp) holds the key words of 4 digits; B is
+// MN-major: for each (digit j, weight b) the 16 words w_b(Y[c][j]) lie in
+// order, so each word is one 8-byte store. Both use the no-swizzle canonical
+// layout (8 x 16-byte core matrices). The epilogue reads the 8 planes of an
+// output from TMEM, forms the exact sum in 128 bits, reduces it mod q and adds
+// the base term and the sparse carry corrections exactly as k_mac_tiled.
+//
+// A CTA is persistent (one per SM, all 512 TMEM columns) and walks a flat
+// sequence of items (tile of 4 slots of one limb, key chunk, 4-digit chunk).
+// Key words and digit transforms of item i + 6 are fetched with cp.async into
+// an 8-deep ring while item i is expanded into its B operand and multiplied,
+// so a CTA keeps about 60 KB of loads in flight across tile boundaries; ring
+// slots are released by tcgen05.commit on per-stage mbarriers. The epilogue's
+// base terms and correction counts are staged in shared memory ahead of use.
+// Every wait is bounded; on a timeout the kernel records an error, waits
+// (bounded) for its MMAs and frees its TMEM.
+namespace tc {
+
+constexpr int kTS = 4;            // slots per tile
+constexpr int kCt = 16;           // ciphertexts per group (N = 8 kCt = 128)
+constexpr int kKeys = 32;         // keys per pass (M = 2 kKeys = 64)
+constexpr int kJc = 4;            // digits per chunk (K = 32 bytes)
+constexpr int kRing = 8;          // A / Y prefetch ring depth
+constexpr int kAhead = 6;         // items fetched ahead
+constexpr int kBStages = 2;       // B operand stages (kRing - kAhead)
+constexpr int kThreads = 256;
+// Strides are padded (slot and digit strides off multiples of 128 B) so the
+// 8-byte shared-memory stores of a warp fall on distinct banks.
+constexpr u32 kSboA = 256, kLboA = 128;        // A: row groups of 8 x 32 B, 16-byte K chunks
+constexpr u32 kSboB = 128, kLboB = 1088;       // B: ciphertext pairs, digits
+constexpr u32 kASlot = 2080;                   // 64 rows x 32 B (+32)
+constexpr u32 kBSlot = 4368;                   // 4 digits x 8 weights x 128 B (+padding)
+constexpr u32 kAStage = kTS * kASlot;          // 8320
+constexpr u32 kYStage = kCt * kJc * kTS * 8;   // 2048: Y words [c][jj][i]
+constexpr u32 kBStage = kTS * kBSlot;          // 17472
+constexpr u32 kOffY = kRing * kAStage;                     // 66560
+constexpr u32 kOffB = kOffY + kRing * kYStage;             // 82944
+constexpr u32 kOffE = kOffB + kBStages * kBStage;          // 117888: epilogue staging ring
+constexpr u32 kEStage = (kCt * kTS + 4) * 8;               // base terms [c][i] + pf, pf_q
+constexpr int kERing = kAhead + 1;                         // tiles whose staging may be live
+constexpr u32 kOffCnt = kOffE + kERing * kEStage;          // correction counts [c][g]
+constexpr u32 kSmemBytes = kOffCnt + kCt * kKeys * 4;      // 123,744 B: one CTA per SM
+constexpr u32 kTmemCols = 512;
+static_assert(kBStages == kRing - kAhead, "B stages follow the ring");
+constexpr long long kSpin = 1ll << 22;         // bounded waits (iterations)
+
+__device__ __forceinline__ u32 smem_u32(const void* p) { return (u32)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t sdesc(u32 saddr, u32 lbo, u32 sbo) {
+    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;  // descriptor version (sm_100); base offset 0, no swizzle
+    return d;
+}
+
+// kind::i8 instruction descriptor: D s32, A u8 K-major, B u8 MN-major, N = 128, M = 64.
+constexpr u32 kIdesc = (2u << 4) | (0u << 7) | (0u << 10) | (0u << 15) | (1u << 16) | ((128u >> 3) << 17) |
+                       ((64u >> 4) << 24);
+
+__device__ __forceinline__ void mma_i8(u32 d_tmem, uint64_t a, uint64_t b, u32 accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void commit(u32 bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+// true once the phase with the given parity has completed (bounded)
+__device__ __forceinline__ bool wait_parity(u32 bar, u32 parity) {
+    for (long long it = 0; it < kSpin; ++it) {
+        u32 done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// 8-byte asynchronous global -> shared copy; src_bytes 0 stores zeros
+__device__ __forceinline__ void cp8(u32 dst, const void* src, u32 src_bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(u32 taddr, u32 (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Position in a CTA's item sequence (tile_local-th tile of the CTA, key chunk,
+// digit chunk), advanced by counters instead of divisions.
+struct Item {
+    int tl, kc, ch;
+    __device__ __forceinline__ void next(int n_kc, int n_chunks) {
+        if (++ch == n_chunks) {
+            ch = 0;
+            if (++kc == n_kc) {
+                kc = 0;
+                ++tl;
+            }
+        }
+    }
+};
+
+}  // namespace tc
+
+// Same arguments and results as k_mac_tiled for bounded keys (up to 16
+// ciphertexts per call, any number of keys, D <= 4096, N >= 4).
+__global__ void __launch_bounds__(tc::kThreads, 1)
+    k_mac_tc(const u64* __restrict__ Yhat, size_t y_stride, const u64* __restrict__ Bhat, size_t b_stride,
+             const u64* const* __restrict__ keys, const u64* __restrict__ exps_inv, const u64* __restrict__ pf,
+             const u64* __restrict__ pf_q, u64* __restrict__ acc, const NttTab* __restrict__ tabs, LimbMap lm,
+             int n_ct, int n_keys, int Lq, int LK, int D, int log_n, const Exc* __restrict__ exc,
+             const u32* __restrict__ exc_count, int cap, const u64* __restrict__ psi, int* __restrict__ err) {
+    using namespace tc;
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ u32 s_tmem;
+    __shared__ int s_abort;
+    __shared__ __align__(8) uint64_t s_bar[kBStages];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const u32 n = 1u << log_n;
+    const int n_tiles_s = (int)(n / kTS), lts = log_n - 2;  // tiles per limb (a power of two)
+    const int n_tiles = LK * n_tiles_s;
+    const int n_chunks = (D + kJc - 1) / kJc;
+    const int n_kc = (n_keys + kKeys - 1) / kKeys;
+    const int per_tile = n_kc * n_chunks;
+    const int my_tiles = (int)blockIdx.x < n_tiles ? (n_tiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    const int n_items = my_tiles * per_tile;
+    if (tid == 0) {
+        s_abort = 0;
+        for (int i = 0; i < kBStages; ++i)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_bar[i])), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"(kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    // zero the operand rings once: A rows of absent keys and B columns of
+    // absent ciphertexts stay zero
+    for (u32 i = tid; i < kOffE / 16; i += kThreads) ((uint4*)smem)[i] = make_uint4(0, 0, 0, 0);
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const u32 tmem = s_tmem;
+    const u32 sbase = smem_u32(smem);
+    u32* s_cnt = (u32*)(smem + kOffCnt);
+
+    // issue the cp.async copies of item t (position it) into ring slot t % kRing
+    // (one commit group per call)
+    auto prefetch = [&](int t, const Item& it) {
+        if (t < n_items) {
+            const int tile = (int)blockIdx.x + it.tl * (int)gridDim.x;
+            const int l = tile >> lts;
+            const u32 s0 = (u32)(tile & (n_tiles_s - 1)) * kTS;
+            const int g0 = it.kc * kKeys;
+            const int gn = n_keys - g0 < kKeys ? n_keys - g0 : kKeys;
+            const int j0 = it.ch * kJc;
+            const u32 a_st = sbase + (u32)(t & (kRing - 1)) * kAStage;
+            for (int w = tid; w < gn * 2 * kJc * kTS; w += kThreads) {
+                const int i = w % kTS, jj = (w / kTS) % kJc, comp = (w / (kTS * kJc)) % 2, g = w / (kTS * kJc * 2);
+                const int j = j0 + jj;
+                const int m = 2 * g + comp;
+                const u64* src = keys[g0 + g] + ((((size_t)(j < D ? j : 0) * LK + l) * 2 + comp) << log_n) + s0 + i;
+                cp8(a_st + i * kASlot + (m >> 3) * kSboA + (jj >> 1) * kLboA + (m & 7) * 16 + (jj & 1) * 8, src,
+                    j < D ? 8u : 0u);
+            }
+            const u32 y_st = sbase + kOffY + (u32)(t & (kRing - 1)) * kYStage;
+            for (int w = tid; w < n_ct * kJc * kTS; w += kThreads) {
+                const int i = w % kTS, jj = (w / kTS) % kJc, c = w / (kTS * kJc);
+                const int j = j0 + jj;
+                const u64* src = Yhat + c * y_stride + (((size_t)(j < D ? j : 0) * LK + l) << log_n) + s0 + i;
+                cp8(y_st + (u32)w * 8, src, j < D ? 8u : 0u);
+            }
+            if (it.kc == 0 && it.ch == 0) {  // epilogue inputs of this tile: base terms, pf, pf_q
+                const u32 e_st = sbase + kOffE + (u32)(it.tl % kERing) * kEStage;
+                for (int w = tid; w < n_ct * kTS; w += kThreads) {
+                    const int i = w % kTS, c = w / kTS;
+                    const bool ok = l < Lq;
+                    cp8(e_st + (u32)w * 8, Bhat + c * b_stride + ((size_t)(ok ? l : 0) << log_n) + s0 + i, ok ? 8u : 0u);
+                }
+                if (tid == 0) {
+                    const bool ok = l < Lq;
+                    cp8(e_st + kCt * kTS * 8, pf + (ok ? l : 0), ok ? 8u : 0u);
+                    cp8(e_st + kCt * kTS * 8 + 8, pf_q + (ok ? l : 0), ok ? 8u : 0u);
+                }
+            }
+        }
+        cp_commit();
+    };
+
+    Item ahead{0, 0, 0};
+    for (int t = 0; t < kAhead; ++t) {
+        prefetch(t, ahead);
+        ahead.next(n_kc, n_chunks);
+    }
+    int cur_kc = -1, f_limb = -1;
+    u64 f256 = 0, f256q = 0;  // 2^8 mod q_l and its Shoup companion
+    Item it{0, 0, 0};
+    for (int t = 0; t < n_items; ++t, it.next(n_kc, n_chunks)) {
+        const int tile = (int)blockIdx.x + it.tl * (int)gridDim.x;
+        const int l = tile >> lts;
+        const u32 s0 = (u32)(tile & (n_tiles_s - 1)) * kTS;
+        const int g0 = it.kc * kKeys;
+        const int gn = n_keys - g0 < kKeys ? n_keys - g0 : kKeys;
+        const int bst = t & (kBStages - 1);
+        // the MMAs of item t - 2 read ring slot (t + kAhead) % kRing and B stage bst: wait before reuse
+        if (t >= kBStages) {
+            if (!wait_parity(smem_u32(&s_bar[bst]), (u32)(((t / kBStages) - 1) & 1))) {
+                if (tid == 0) atomicExch(err, 1);
+                s_abort = 1;
+            }
+        }
+        prefetch(t + kAhead, ahead);
+        ahead.next(n_kc, n_chunks);
+        cp_wait<kAhead>();  // this thread's copies of item t have landed
+        if (it.kc != cur_kc && it.ch == 0) {  // correction counts of this key chunk
+            for (int w = tid; w < kCt * kKeys; w += kThreads) {
+                const int c = w / kKeys, g = w % kKeys;
+                s_cnt[w] = (c < n_ct && g < gn) ? exc_count[(size_t)c * n_keys + g0 + g] : 0u;
+            }
+            cur_kc = it.kc;
+        }
+        __syncthreads();
+        if (s_abort) break;
+        const NttTab& T = tabs[lm(l)];
+        const u64 q = T.q;
+        // B: w_b(Y[c][j]) = 2^(8b) Y mod q for the 8 weights
+        {
+            const u64* ys = (const u64*)(smem + kOffY + (t & (kRing - 1)) * kYStage);
+            uint8_t* Bs = smem + kOffB + bst * kBStage;
+            if (l != f_limb) {
+                f256 = 256 % q;
+                f256q = shoup_quotient_dev(f256, q);
+                f_limb = l;
+            }
+            for (int w = tid; w < n_ct * kJc * kTS; w += kThreads) {
+                const int i = w % kTS, jj = (w / kTS) % kJc, c = w / (kTS * kJc);
+                uint8_t* dst = Bs + i * kBSlot + jj * kLboB + (c >> 1) * kSboB + (c & 1) * 8;
+                u64 wv = ys[w];
+#pragma unroll
+                for (int b = 0; b < 8; ++b) {
+                    *(u64*)(dst + b * 16) = wv;
+                    if (b < 7) wv = mul_shoup(wv, f256, f256q, q);
+                }
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            fence_after();
+            const u32 a0 = sbase + (u32)(t & (kRing - 1)) * kAStage, b0 = sbase + kOffB + (u32)bst * kBStage;
+#pragma unroll
+            for (int i = 0; i < kTS; ++i)
+                mma_i8(tmem + (u32)i * 128u, sdesc(a0 + i * kASlot, kLboA, kSboA),
+                       sdesc(b0 + i * kBSlot, kLboB, kSboB), it.ch > 0 ? 1u : 0u);
+            commit(smem_u32(&s_bar[bst]));
+        }
+        if (it.ch != n_chunks - 1) continue;
+        // ------------------------------------------------ epilogue of (tile, key chunk)
+        if (!wait_parity(smem_u32(&s_bar[bst]), (u32)((t / kBStages) & 1))) {
+            if (tid == 0) atomicExch(err, 1);
+            s_abort = 1;
+        }
+        fence_after();
+        {
+            const Barrett bm{q, T.mu_hi, T.mu_lo};
+            const u64* es = (const u64*)(smem + kOffE + (it.tl % kERing) * kEStage);
+            const u64 pfl = es[kCt * kTS], pfql = es[kCt * kTS + 1];
+            const int qd = warp & 3, half = warp >> 2;  // warps 0-3: slots 0, 1; warps 4-7: slots 2, 3
+            const int m = 16 * qd + lane;
+            const int gl = m >> 1, comp = m & 1, g = g0 + gl;
+            const bool row_ok = lane < 16 && gl < gn;
+            const u32 trow = tmem + ((u32)(32 * qd) << 16);
+            for (int cb = 0; cb < kCt; cb += 4) {
+                u32 r[2][32];
+#pragma unroll
+                for (int h = 0; h < 2; ++h) tmem_ld32(trow + (u32)((2 * half + h) * 128 + 8 * cb), r[h]);
+                tmem_wait_ld();
+                if (!row_ok) continue;
+#pragma unroll
+                for (int cc = 0; cc < 4; ++cc) {
+                    const int c = cb + cc;
+                    if (c >= n_ct) break;
+                    u64 outv[2];
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        u64 lo = 0, hi = 0;  // exact sum_a 2^(8a) P_a in 128 bits (< 2^90)
+#pragma unroll
+                        for (int a = 0; a < 8; ++a) {
+                            const u64 v = (u64)r[h][8 * cc + a];
+                            const u64 add_lo = a ? (v << (8 * a)) : v;
+                            const u64 add_hi = a > 1 ? (v >> (64 - 8 * a)) : 0;
+                            lo += add_lo;
+                            hi += add_hi + (lo < add_lo);
+                        }
+                        u64 v = reduce_wide(hi >= q ? hi % q : hi, lo, q, T.mu_hi, T.mu_lo);
+                        const int i = 2 * half + h;
+                        const u32 s = s0 + i;
+                        if (comp == 0 && l < Lq) v = add_mod(v, mul_shoup(es[c * kTS + i], pfl, pfql, q), q);
+                        const u32 cnt = min(s_cnt[c * kKeys + gl], (u32)cap);
+                        if (cnt) {
+                            const Exc* list = exc + ((size_t)c * n_keys + g) * cap;
+                            const u64 ps = psi[lm(l)];
+                            const u32 k = galois_src(s, exps_inv[g], log_n);
+                            const u64* key = keys[g];
+                            for (u32 e = 0; e < cnt; ++e) {
+                                const Exc x = list[e];
+                                u64 wv = pow_mod_dev(ps, ((2ull * k + 1) * x.t) & (2ull * n - 1), bm);
+                                u64 dm = x.delta < 0 ? (u64)(-x.delta) % q : (u64)x.delta % q;
+                                if (x.delta < 0 && dm) dm = q - dm;
+                                const u64 tv = mul_barrett(wv, dm, bm);
+                                const size_t kofs = (((size_t)x.j * LK + l) * 2 + comp) << log_n;
+                                v = add_mod(v, mul_barrett(tv, key[kofs + s], bm), q);
+                            }
+                        }
+                        outv[h] = v;
+                    }
+                    const size_t obase = ((((size_t)c * n_keys + g) * 2 + comp) * LK + l) << log_n;
+                    *(ulonglong2*)(acc + obase + s0 + 2 * half) = make_ulonglong2(outv[0], outv[1]);
+                }
+            }
+        }
+        fence_before();
+        __syncthreads();  // TMEM columns free for the next item's MMAs
+        if (s_abort) break;
+    }
+    // teardown: drain the copies, wait (bounded) for MMAs in flight, free TMEM
+    cp_wait<0>();
+    __syncthreads();
+    if (tid == 0) {
+        for (int bsi = 0; bsi < kBStages; ++bsi) {
+            // the last commit on each stage, if any
+            int last = -1;
+            for (int t = n_items - 1; t >= 0 && t >= n_items - kBStages; --t)
+                if ((t & (kBStages - 1)) == bsi) last = t;
+            if (last >= 0) wait_parity(smem_u32(&s_bar[bsi]), (u32)((last / kBStages) & 1));
+        }
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+}
+
 }  // namespace
 
 // Hoisted hybrid rotations of n_ct ciphertexts by n_keys Galois keys (bounded
@@ -360,7 +757,18 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
     const u32 Lq = k0->q_limbs, LK = ksk_limbs(k0), D = k0->D, n = ctx->n;
     const size_t ct_words = (size_t)2 * Lq * n;
     const bool bounded = k0->kind == CKKS_KSK_HYBRID_BOUNDED;
-    const u32 G = n_ct >= 4 ? 4 : n_ct;
+    // Bounded keys use the tensor-core MAC with up to 16 ciphertexts per group
+    // (each key word read once per group), as far as device memory allows;
+    // otherwise groups of 4 on the CUDA-core tiled MAC.
+    const bool use_tc = bounded && n >= (u32)tc::kTS && D <= 4096 && tc_enabled();
+    u32 G = n_ct >= 4 ? 4 : n_ct;
+    if (use_tc) {
+        const size_t per_ct = ((size_t)D * LK * n + (size_t)Lq * n + 4 * (size_t)n_keys * LK * n) * sizeof(u64);
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        G = n_ct < (u32)tc::kCt ? n_ct : (u32)tc::kCt;
+        while (G > 4 && (size_t)G * per_ct > free_b / 2) G -= 4;
+    }
     const int cap = 1024;
     const LimbMap lq = LimbMap::range(0, Lq), lqp = LimbMap::qp(ctx, Lq);
     const size_t y_stride = (size_t)D * LK * n, b_stride = (size_t)Lq * n, d_stride = (size_t)D * n,
@@ -369,7 +777,10 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
     Workspace<i64> dig;
     Workspace<u32> flags, cnt;
     Workspace<Exc> exc;
+    Workspace<int> terr;
     int32_t rc;
+    if ((rc = terr.alloc(1, st))) return rc;
+    CKKS_CUDA_TRY(cudaMemsetAsync(terr.p, 0, sizeof(int), st));
     if ((rc = Y.alloc(G * y_stride, st)) || (rc = Bh.alloc(G * b_stride, st)) ||
         (rc = acc.alloc((size_t)G * n_keys * 2 * LK * n, st)) || (rc = Z.alloc((size_t)G * n_keys * 2 * LK * n, st)) ||
         (rc = karr.alloc(3 * (size_t)n_keys + ctx->moduli.size(), st)) || (rc = dig.alloc(G * d_stride, st)) ||
@@ -419,7 +830,17 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
         }
         pt.end();
         pt.begin(3);
-        {
+        if (use_tc) {
+            static int n_sm = 0;
+            if (!n_sm) cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, ctx->device);
+            const int n_tiles = (int)(LK * (n / tc::kTS));
+            CKKS_CUDA_TRY(cudaFuncSetAttribute(k_mac_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)tc::kSmemBytes));
+            k_mac_tc<<<n_tiles < n_sm ? n_tiles : n_sm, tc::kThreads, tc::kSmemBytes, st>>>(
+                Y.p, y_stride, Bh.p, b_stride, d_keys, d_exps_inv, ctx->d_pmodq, ctx->d_pmodq + ctx->L, acc.p,
+                ctx->d_tabs, lqp, (int)gn, (int)n_keys, (int)Lq, (int)LK, (int)D, (int)ctx->log_n, exc.p, cnt.p, cap,
+                d_psi, terr.p);
+        } else {
             const size_t smem = (size_t)(G >= 3 ? 4 : G) * D * kS * sizeof(u64);
             if (n >= (u32)kS && smem <= 200 * 1024) {
                 dim3 g(n / kS, LK);
@@ -458,8 +879,14 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
             return rc;
         pt.end();
         // pairs whose correction lists overflowed are recomputed exactly
+        int h_err = 0;
         CKKS_CUDA_TRY(cudaMemcpyAsync(h_cnt.data(), cnt.p, (size_t)G * n_keys * sizeof(u32), cudaMemcpyDeviceToHost, st));
+        CKKS_CUDA_TRY(cudaMemcpyAsync(&h_err, terr.p, sizeof(int), cudaMemcpyDeviceToHost, st));
         CKKS_CUDA_TRY(cudaStreamSynchronize(st));
+        if (h_err) {
+            ckks_set_error("key-switch MAC: a tensor-core pipeline wait timed out");
+            return CKKS_ERR_TIMEOUT;
+        }
         for (u32 c = 0; c < gn; ++c)
             for (u32 g = 0; g < n_keys; ++g)
                 if (h_cnt[(size_t)c * n_keys + g] > (u32)cap) overflow.push_back(((c0 + c) << 16) | g);

@@ -86,7 +86,8 @@ __global__ void __launch_bounds__(kMaxThreads) k_fwd1(const void* __restrict__ i
 #pragma unroll
             for (int e = 0; e < S::R1; ++e) x[e] = in[c0 + c + ((size_t)(i0 + S::R2 * e) << log_b)];
         }
-        nttc::ct_stages<S::LR1>(x, 0, 0, tw, q);
+        if (q < nttc::kLazyCtBound) nttc::ct_stages<S::LR1, false>(x, 0, 0, tw, q);
+        else nttc::ct_stages<S::LR1, true>(x, 0, 0, tw, q);
 #pragma unroll
         for (int e = 0; e < S::R1; ++e) sm[((i0 + S::R2 * e) << log_c) + (c ^ (e & (C - 1)))] = x[e];
     }
@@ -96,7 +97,8 @@ __global__ void __launch_bounds__(kMaxThreads) k_fwd1(const void* __restrict__ i
         u64 y[S::R2];
 #pragma unroll
         for (int e = 0; e < S::R2; ++e) y[e] = sm[((S::R2 * g + e) << log_c) + (c ^ (g & (C - 1)))];
-        nttc::ct_stages<S::LR2>(y, S::LR1, g, tw, q);
+        if (q < nttc::kLazyCtBound) nttc::ct_stages<S::LR2, false>(y, S::LR1, g, tw, q);
+        else nttc::ct_stages<S::LR2, true>(y, S::LR1, g, tw, q);
         const size_t row = (size_t)(c0 + c) << LOG_M;
 #pragma unroll
         for (int e = 0; e < S::R2; ++e) {
@@ -134,7 +136,8 @@ __global__ void __launch_bounds__(kMaxThreads) k_fwd2(const u64* src, u64* dst, 
         u64 x[S::R1];
 #pragma unroll
         for (int e = 0; e < S::R1; ++e) x[e] = src[base + ((size_t)(i0 + S::R2 * e) << log_a) + b0 + c];
-        nttc::ct_stages<S::LR1>(x, 0, 0, tw, q);
+        if (q < nttc::kLazyCtBound) nttc::ct_stages<S::LR1, false>(x, 0, 0, tw, q);
+        else nttc::ct_stages<S::LR1, true>(x, 0, 0, tw, q);
 #pragma unroll
         for (int e = 0; e < S::R1; ++e) sm[((i0 + S::R2 * e) << log_c) + c] = x[e];
     }
@@ -144,10 +147,19 @@ __global__ void __launch_bounds__(kMaxThreads) k_fwd2(const u64* src, u64* dst, 
         u64 y[S::R2];
 #pragma unroll
         for (int e = 0; e < S::R2; ++e) y[e] = sm[((S::R2 * g + e) << log_c) + c];
-        nttc::ct_stages<S::LR2>(y, S::LR1, g, tw, q);
+        if (q < nttc::kLazyCtBound) {
+            nttc::ct_stages<S::LR2, false>(y, S::LR1, g, tw, q);
+            const u64 one_q = (~0ull) / q;  // floor(2^64 / q) for odd q
 #pragma unroll
-        for (int e = 0; e < S::R2; ++e)
-            dst[base + ((size_t)brev(S::R2 * g + e, LOG_M) << log_a) + b0 + c] = reduce_4q(y[e], q);
+            for (int e = 0; e < S::R2; ++e)
+                dst[base + ((size_t)brev(S::R2 * g + e, LOG_M) << log_a) + b0 + c] =
+                    reduce_2q(mul_shoup_lazy(y[e], 1, one_q, q), q);
+        } else {
+            nttc::ct_stages<S::LR2, true>(y, S::LR1, g, tw, q);
+#pragma unroll
+            for (int e = 0; e < S::R2; ++e)
+                dst[base + ((size_t)brev(S::R2 * g + e, LOG_M) << log_a) + b0 + c] = reduce_4q(y[e], q);
+        }
     }
 }
 

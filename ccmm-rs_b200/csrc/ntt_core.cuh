@@ -15,13 +15,19 @@ namespace nttc {
 __device__ __forceinline__ u32 brev(u32 x, int bits) { return bits ? (__brev(x) >> (32 - bits)) : 0; }
 
 // Harvey butterflies on lazily reduced values.
-// CT: X, Y in [0, 4q) -> X' = X + W Y, Y' = X - W Y, both in [0, 4q).
+// CT (kRed): X, Y in [0, 4q) -> X' = X + W Y, Y' = X - W Y, both in [0, 4q).
+// CT (!kRed): no conditional subtraction; each stage adds less than 2q to the
+// bound (W Y is reduced to [0, 2q) for any 64-bit Y), so a pass of s stages
+// from [0, B) ends below B + 2 s q. Used for q < 2^59, where even 2 passes of
+// 9 stages stay below 20 q < 2^64.
+template <bool kRed = true>
 __device__ __forceinline__ void ct_bfly(u64& X, u64& Y, u64 W, u64 Wq, u64 q, u64 q2) {
-    u64 x = X >= q2 ? X - q2 : X;
+    u64 x = kRed ? (X >= q2 ? X - q2 : X) : X;
     u64 t = mul_shoup_lazy(Y, W, Wq, q);
     X = x + t;
     Y = x - t + q2;
 }
+constexpr u64 kLazyCtBound = 1ull << 59;  // primes below this take the !kRed network
 // GS: X, Y in [0, 2q) -> X' = X + Y, Y' = (X - Y) W, both in [0, 2q).
 __device__ __forceinline__ void gs_bfly(u64& X, u64& Y, u64 W, u64 Wq, u64 q, u64 q2) {
     u64 s = X + Y;
@@ -34,7 +40,7 @@ __device__ __forceinline__ void gs_bfly(u64& X, u64& Y, u64 W, u64 Wq, u64 q, u6
 // distance R/2, R/4, .., 1; the twiddle block of register e at stage ls is
 // (base << ls) + (e >> (LR - ls)); tw(stage, block, W, Wq) supplies the twiddle.
 // Compile-time recursion keeps every register index static.
-template <int LR, int LS, typename TW>
+template <int LR, int LS, bool kRed, typename TW>
 __device__ __forceinline__ void ct_stage(u64 (&x)[1 << LR], int s0, u32 base, TW& tw, u64 q, u64 q2) {
     if constexpr (LS < LR) {
         constexpr int half = (1 << LR) >> (LS + 1);
@@ -43,15 +49,16 @@ __device__ __forceinline__ void ct_stage(u64 (&x)[1 << LR], int s0, u32 base, TW
             u64 W, Wq;
             tw(s0 + LS, (base << LS) + b, W, Wq);
 #pragma unroll
-            for (int o = 0; o < half; ++o) ct_bfly(x[b * 2 * half + o], x[b * 2 * half + o + half], W, Wq, q, q2);
+            for (int o = 0; o < half; ++o)
+                ct_bfly<kRed>(x[b * 2 * half + o], x[b * 2 * half + o + half], W, Wq, q, q2);
         }
-        ct_stage<LR, LS + 1>(x, s0, base, tw, q, q2);
+        ct_stage<LR, LS + 1, kRed>(x, s0, base, tw, q, q2);
     }
 }
 
-template <int LR, typename TW>
+template <int LR, bool kRed = true, typename TW>
 __device__ __forceinline__ void ct_stages(u64 (&x)[1 << LR], int s0, u32 base, TW tw, u64 q) {
-    ct_stage<LR, 0>(x, s0, base, tw, q, q << 1);
+    ct_stage<LR, 0, kRed>(x, s0, base, tw, q, q << 1);
 }
 
 template <int LR, int LS, typename TW>
