@@ -593,8 +593,9 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
         prefetch(t, ahead);
         ahead.next(n_kc, n_chunks);
     }
-    int cur_kc = -1, f_limb = -1;
-    u64 f256 = 0, f256q = 0;  // 2^8 mod q_l and its Shoup companion
+    int cur_kc = -1, f_limb = -1, r_limb = -1;
+    u64 f256 = 0, f256q = 0;             // 2^8 mod q_l and its Shoup companion
+    u64 one_q = 0, r64 = 0, r64q = 0;    // floor(2^64 / q_l), 2^64 mod q_l, Shoup companion
     Item it{0, 0, 0};
     for (int t = 0; t < n_items; ++t, it.next(n_kc, n_chunks)) {
         const int tile = (int)blockIdx.x + it.tl * (int)gridDim.x;
@@ -672,31 +673,36 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
             const int gl = m >> 1, comp = m & 1, g = g0 + gl;
             const bool row_ok = lane < 16 && gl < gn;
             const u32 trow = tmem + ((u32)(32 * qd) << 16);
+            if (l != r_limb) {  // 2^64 mod q and Shoup companions for the final reduction
+                one_q = (~0ull) / q;  // floor(2^64 / q), q odd
+                r64 = (u64)(-(q * one_q));  // 2^64 - q floor(2^64 / q) = 2^64 mod q
+                r64 = r64 >= q ? r64 - q : r64;
+                r64q = shoup_quotient_dev(r64, q);
+                r_limb = l;
+            }
             for (int cb = 0; cb < kCt; cb += 4) {
-                u32 r[2][32];
+                u64 outv[2][4];
 #pragma unroll
-                for (int h = 0; h < 2; ++h) tmem_ld32(trow + (u32)((2 * half + h) * 128 + 8 * cb), r[h]);
-                tmem_wait_ld();
-                if (!row_ok) continue;
+                for (int h = 0; h < 2; ++h) {
+                    const int i = 2 * half + h;
+                    const u32 s = s0 + i;
+                    u32 r[32];
+                    tmem_ld32(trow + (u32)(i * 128 + 8 * cb), r);
+                    tmem_wait_ld();
+                    if (!row_ok) continue;
 #pragma unroll
-                for (int cc = 0; cc < 4; ++cc) {
-                    const int c = cb + cc;
-                    if (c >= n_ct) break;
-                    u64 outv[2];
-#pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        u64 lo = 0, hi = 0;  // exact sum_a 2^(8a) P_a in 128 bits (< 2^90)
-#pragma unroll
-                        for (int a = 0; a < 8; ++a) {
-                            const u64 v = (u64)r[h][8 * cc + a];
-                            const u64 add_lo = a ? (v << (8 * a)) : v;
-                            const u64 add_hi = a > 1 ? (v >> (64 - 8 * a)) : 0;
-                            lo += add_lo;
-                            hi += add_hi + (lo < add_lo);
-                        }
-                        u64 v = reduce_wide(hi >= q ? hi % q : hi, lo, q, T.mu_hi, T.mu_lo);
-                        const int i = 2 * half + h;
-                        const u32 s = s0 + i;
+                    for (int cc = 0; cc < 4; ++cc) {
+                        const int c = cb + cc;
+                        if (c >= n_ct) break;
+                        // sum_a 2^(8a) P_a with P_a < 2^25: pairwise in 64 bits, then 128
+                        const u32* P = r + 8 * cc;
+                        const u64 p01 = (u64)P[0] + ((u64)P[1] << 8), p23 = (u64)P[2] + ((u64)P[3] << 8);
+                        const u64 p45 = (u64)P[4] + ((u64)P[5] << 8), p67 = (u64)P[6] + ((u64)P[7] << 8);
+                        const u64 lo4 = p01 + (p23 << 16), hi4 = p45 + (p67 << 16);  // each < 2^51
+                        const u64 lo = lo4 + (hi4 << 32);
+                        const u64 hi = (hi4 >> 32) + (lo < lo4);                    // < 2^20
+                        // (hi 2^64 + lo) mod q = lo mod q + hi (2^64 mod q) mod q
+                        u64 v = add_mod(reduce_2q(mul_shoup_lazy(lo, 1, one_q, q), q), mul_shoup(hi, r64, r64q, q), q);
                         if (comp == 0 && l < Lq) v = add_mod(v, mul_shoup(es[c * kTS + i], pfl, pfql, q), q);
                         const u32 cnt = min(s_cnt[c * kKeys + gl], (u32)cap);
                         if (cnt) {
@@ -714,10 +720,16 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                                 v = add_mod(v, mul_barrett(tv, key[kofs + s], bm), q);
                             }
                         }
-                        outv[h] = v;
+                        outv[h][cc] = v;
                     }
+                }
+                if (!row_ok) continue;
+#pragma unroll
+                for (int cc = 0; cc < 4; ++cc) {
+                    const int c = cb + cc;
+                    if (c >= n_ct) break;
                     const size_t obase = ((((size_t)c * n_keys + g) * 2 + comp) * LK + l) << log_n;
-                    *(ulonglong2*)(acc + obase + s0 + 2 * half) = make_ulonglong2(outv[0], outv[1]);
+                    *(ulonglong2*)(acc + obase + s0 + 2 * half) = make_ulonglong2(outv[0][cc], outv[1][cc]);
                 }
             }
         }
