@@ -71,18 +71,27 @@ __global__ void k_rescale(const u64* __restrict__ in, u64* __restrict__ out, con
 
 // ring/auxiliary_modulus.rs:89-171: centered CRT over P from the K auxiliary
 // residues (mixed-radix Garner, exact), then (x_i - r) * P^-1 mod q_i for every
-// Q limb. One thread per coefficient s; with exps, the result is scattered by
-// the coefficient automorphism X -> X^k (k = exps[(poly / 2) % n_keys]):
-// out[t] = +-value[s], t = s k mod 2N (negated when t >= N). ModDown commutes
-// exactly with that signed permutation because P is odd.
+// Q limb. One thread per output coefficient t; with exps_inv, the output is
+// the coefficient automorphism X -> X^k of the ModDown result
+// (k^-1 = exps_inv[(poly / 2) % n_keys]): out[t] = +-value[s] with
+// s = t k^-1 mod 2N (negated when s >= N), so the stores are coalesced and the
+// reads gather within one polynomial. ModDown commutes exactly with that
+// signed permutation because P is odd.
 __global__ void k_mod_down(const u64* __restrict__ in, u64* __restrict__ out, ModDownConst md, int q_limbs,
-                           int log_n, const u64* __restrict__ exps, int n_keys) {
+                           int log_n, const u64* __restrict__ exps_inv, int n_keys) {
     const u32 n = 1u << log_n;
-    const u32 c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= n) return;
+    const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
     const int K = md.K;
     const size_t src = (size_t)blockIdx.y * (q_limbs + K) << log_n;
     const size_t dst = (size_t)blockIdx.y * q_limbs << log_n;
+    u32 c = t;
+    bool flip = false;
+    if (exps_inv) {
+        const u64 s = ((u64)t * exps_inv[(blockIdx.y >> 1) % n_keys]) & (2ull * n - 1);
+        flip = s >= n;
+        c = (u32)(s & (n - 1));
+    }
     u64 v[kMaxAux];
     for (int i = 0; i < K; ++i) {
         const u64 p = md.p[i];
@@ -95,13 +104,6 @@ __global__ void k_mod_down(const u64* __restrict__ in, u64* __restrict__ out, Mo
     bool neg = false;
     for (int i = K - 1; i >= 0; --i) {
         if (v[i] != md.half[i]) { neg = v[i] > md.half[i]; break; }
-    }
-    u32 t = c;
-    bool flip = false;
-    if (exps) {
-        const u64 mapped = ((u64)c * exps[(blockIdx.y >> 1) % n_keys]) & (2ull * n - 1);
-        flip = mapped >= n;
-        t = (u32)(mapped & (n - 1));
     }
     for (int i = 0; i < q_limbs; ++i) {
         const u64 qi = md.q[i];
@@ -169,8 +171,8 @@ int32_t mod_down_launch(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, u32
     return mod_down_sigma_multi(ctx, in, out, n_polys, q_limbs, nullptr, 1, st);
 }
 
-int32_t mod_down_sigma_multi(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, u32 q_limbs, const u64* d_exps,
-                             u32 n_keys, cudaStream_t st) {
+int32_t mod_down_sigma_multi(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, u32 q_limbs,
+                             const u64* d_exps_inv, u32 n_keys, cudaStream_t st) {
     if (!n_polys) return CKKS_OK;
     // grid.y limit: chunks are multiples of 2 * n_keys so (poly / 2) % n_keys pairs stay aligned
     const u32 unit = 2 * (n_keys ? n_keys : 1);
@@ -180,7 +182,7 @@ int32_t mod_down_sigma_multi(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys
         dim3 g((ctx->n + kT - 1) / kT, cnt);
         k_mod_down<<<g, kT, 0, st>>>(in + ((size_t)p0 * (q_limbs + ctx->K) << ctx->log_n),
                                      out + ((size_t)p0 * q_limbs << ctx->log_n), ctx->mod_down, q_limbs, ctx->log_n,
-                                     d_exps, n_keys ? n_keys : 1);
+                                     d_exps_inv, n_keys ? n_keys : 1);
     }
     CKKS_CUDA_TRY(cudaGetLastError());
     return CKKS_OK;

@@ -377,20 +377,20 @@ struct PhaseTimer {
 // components), N = 128 columns (16 ciphertexts x 8 byte planes), K = 32 bytes.
 // A (keys) is K-major: row (g, comp) holds the key words of 4 digits; B is
 // MN-major: for each (digit j, weight b) the 16 words w_b(Y[c][j]) lie in
-// order, so each word is one 8-byte store. Both use the no-swizzle canonical
-// layout (8 x 16-byte core matrices). The epilogue reads the 8 planes of an
-// output from TMEM, forms the exact sum in 128 bits, reduces it mod q and adds
-// the base term and the sparse carry corrections exactly as k_mac_tiled.
+// order. Both use the no-swizzle canonical layout (8 x 16-byte core matrices).
 //
-// A CTA is persistent (one per SM, all 512 TMEM columns) and walks a flat
-// sequence of items (tile of 4 slots of one limb, key chunk, 4-digit chunk).
-// Key words and digit transforms of item i + 6 are fetched with cp.async into
-// an 8-deep ring while item i is expanded into its B operand and multiplied,
-// so a CTA keeps about 60 KB of loads in flight across tile boundaries; ring
-// slots are released by tcgen05.commit on per-stage mbarriers. The epilogue's
-// base terms and correction counts are staged in shared memory ahead of use.
-// Every wait is bounded; on a timeout the kernel records an error, waits
-// (bounded) for its MMAs and frees its TMEM.
+// Warp roles of a persistent CTA (one per SM, all 512 TMEM columns):
+//   warps 4-11 producers: cp.async of the key words and digit transforms of
+//              item t + 6 into an 8-deep ring, then the B operand of item t;
+//   warp 12    issues the MMAs of item t once its operands are ready;
+//   warps 0-3  epilogue: TMEM -> exact combine of the 8 planes, reduction mod
+//              q, base term and sparse carry corrections, stores.
+// An item is (tile of 4 slots of one limb, key chunk, 4-digit chunk); the
+// accumulators of consecutive (tile, key chunk) units alternate between TMEM
+// lanes 0-15 and 16-31 of every subpartition (the two M = 64 halves), so the
+// epilogue of one unit overlaps the MMAs of the next. Stages are handed over
+// with mbarriers (ready, empty, full, free); every wait is bounded and on a
+// timeout the kernel records an error, drains and frees its TMEM.
 namespace tc {
 
 constexpr int kTS = 4;            // slots per tile
@@ -400,9 +400,11 @@ constexpr int kJc = 4;            // digits per chunk (K = 32 bytes)
 constexpr int kRing = 8;          // A / Y prefetch ring depth
 constexpr int kAhead = 6;         // items fetched ahead
 constexpr int kBStages = 2;       // B operand stages (kRing - kAhead)
-constexpr int kThreads = 256;
+constexpr int kProdWarp0 = 4, kMmaWarp = 12;
+constexpr int kThreads = 416;     // 13 warps: 4 epilogue, 8 producer, 1 MMA
+constexpr int kProd = 256, kEpi = 128;
 // Strides are padded (slot and digit strides off multiples of 128 B) so the
-// 8-byte shared-memory stores of a warp fall on distinct banks.
+// shared-memory stores of a warp spread over the banks.
 constexpr u32 kSboA = 256, kLboA = 128;        // A: row groups of 8 x 32 B, 16-byte K chunks
 constexpr u32 kSboB = 128, kLboB = 1088;       // B: ciphertext pairs, digits
 constexpr u32 kASlot = 2080;                   // 64 rows x 32 B (+32)
@@ -414,9 +416,10 @@ constexpr u32 kOffY = kRing * kAStage;                     // 66560
 constexpr u32 kOffB = kOffY + kRing * kYStage;             // 82944
 constexpr u32 kOffE = kOffB + kBStages * kBStage;          // 117888: epilogue staging ring
 constexpr u32 kEStage = (kCt * kTS + 4) * 8;               // base terms [c][i] + pf, pf_q
-constexpr int kERing = kAhead + 1;                         // tiles whose staging may be live
-constexpr u32 kOffCnt = kOffE + kERing * kEStage;          // correction counts [c][g]
-constexpr u32 kSmemBytes = kOffCnt + kCt * kKeys * 4;      // 123,744 B: one CTA per SM
+constexpr int kERing = 12;                                 // tiles whose staging may be live
+constexpr u32 kOffCnt = kOffE + kERing * kEStage;          // correction counts [c][g], g < kCntKeys
+constexpr int kCntKeys = 256;
+constexpr u32 kSmemBytes = kOffCnt + kCt * kCntKeys * 4;   // 140,800 B: one CTA per SM
 constexpr u32 kTmemCols = 512;
 static_assert(kBStages == kRing - kAhead, "B stages follow the ring");
 constexpr long long kSpin = 1ll << 22;         // bounded waits (iterations)
@@ -447,6 +450,10 @@ __device__ __forceinline__ void commit(u32 bar) {
                  : "memory");
 }
 
+__device__ __forceinline__ void arrive(u32 bar) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}\n" ::"r"(bar) : "memory");
+}
+
 // true once the phase with the given parity has completed (bounded)
 __device__ __forceinline__ bool wait_parity(u32 bar, u32 parity) {
     for (long long it = 0; it < kSpin; ++it) {
@@ -464,6 +471,17 @@ __device__ __forceinline__ bool wait_parity(u32 bar, u32 parity) {
 
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void named_sync(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
+// barrier over the n threads of group `id` that returns the OR of v (one decision for the group)
+__device__ __forceinline__ bool group_any(int id, int n, bool v) {
+    u32 r;
+    asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.or.pred q, %2, %3, p;\n\t"
+                 "selp.u32 %0, 1, 0, q;\n\t}\n"
+                 : "=r"(r)
+                 : "r"((u32)v), "r"(id), "r"(n)
+                 : "memory");
+    return r != 0;
+}
 
 // 8-byte asynchronous global -> shared copy; src_bytes 0 stores zeros
 __device__ __forceinline__ void cp8(u32 dst, const void* src, u32 src_bytes) {
@@ -473,14 +491,13 @@ __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_grou
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-__device__ __forceinline__ void tmem_ld32(u32 taddr, u32 (&r)[32]) {
+// 16 TMEM lanes x 32 columns: thread t gets columns 8k + 2 (t % 4) + {0, 1} of
+// lanes t / 4 (registers 4k, 4k + 1) and t / 4 + 8 (registers 4k + 2, 4k + 3).
+__device__ __forceinline__ void tmem_ld16x4(u32 taddr, u32 (&r)[16]) {
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        "tcgen05.ld.sync.aligned.16x256b.x4.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
@@ -514,7 +531,9 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ u32 s_tmem;
     __shared__ int s_abort;
-    __shared__ __align__(8) uint64_t s_bar[kBStages];
+    // ready / empty: B stages (producers -> MMA, MMA -> producers);
+    // full / free: TMEM accumulator halves (MMA -> epilogue, epilogue -> MMA)
+    __shared__ __align__(8) uint64_t s_ready[kBStages], s_empty[kBStages], s_full[2], s_free[2];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const u32 n = 1u << log_n;
     const int n_tiles_s = (int)(n / kTS), lts = log_n - 2;  // tiles per limb (a power of two)
@@ -524,235 +543,314 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     const int per_tile = n_kc * n_chunks;
     const int my_tiles = (int)blockIdx.x < n_tiles ? (n_tiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
     const int n_items = my_tiles * per_tile;
+    const int n_units = my_tiles * n_kc;
+    const bool cnt_staged = n_keys <= kCntKeys;
     if (tid == 0) {
         s_abort = 0;
-        for (int i = 0; i < kBStages; ++i)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_bar[i])), "r"(1));
+        for (int i = 0; i < kBStages; ++i) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_ready[i])), "r"(1));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_empty[i])), "r"(1));
+        }
+        for (int i = 0; i < 2; ++i) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_full[i])), "r"(1));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_free[i])), "r"(1));
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 0) {
+    if (warp == kMmaWarp) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
                      "r"(kTmemCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
     }
     // zero the operand rings once: A rows of absent keys and B columns of
-    // absent ciphertexts stay zero
+    // absent ciphertexts stay zero; stage the correction counts
     for (u32 i = tid; i < kOffE / 16; i += kThreads) ((uint4*)smem)[i] = make_uint4(0, 0, 0, 0);
+    u32* s_cnt = (u32*)(smem + kOffCnt);
+    if (cnt_staged)
+        for (int w = tid; w < kCt * n_keys; w += kThreads)
+            s_cnt[w] = w / n_keys < n_ct ? exc_count[(size_t)(w / n_keys) * n_keys + w % n_keys] : 0u;
     fence_before();
     __syncthreads();
     fence_after();
     const u32 tmem = s_tmem;
     const u32 sbase = smem_u32(smem);
-    u32* s_cnt = (u32*)(smem + kOffCnt);
 
-    // issue the cp.async copies of item t (position it) into ring slot t % kRing
-    // (one commit group per call)
-    auto prefetch = [&](int t, const Item& it) {
-        if (t < n_items) {
+    if (warp >= kProdWarp0 && warp < kMmaWarp) {
+        // ------------------------------------------------------------ producers
+        const int ptid = tid - kProdWarp0 * 32;
+        auto prefetch = [&](int t, const Item& it) {
+            if (t < n_items) {
+                const int tile = (int)blockIdx.x + it.tl * (int)gridDim.x;
+                const int l = tile >> lts;
+                const u32 s0 = (u32)(tile & (n_tiles_s - 1)) * kTS;
+                const int g0 = it.kc * kKeys;
+                const int gn = n_keys - g0 < kKeys ? n_keys - g0 : kKeys;
+                const int j0 = it.ch * kJc;
+                const u32 a_st = sbase + (u32)(t & (kRing - 1)) * kAStage;
+                for (int w = ptid; w < gn * 2 * kJc * kTS; w += kProd) {
+                    const int i = w % kTS, jj = (w / kTS) % kJc, comp = (w / (kTS * kJc)) % 2,
+                              g = w / (kTS * kJc * 2);
+                    const int j = j0 + jj;
+                    const int m = 2 * g + comp;
+                    const u64* src =
+                        keys[g0 + g] + ((((size_t)(j < D ? j : 0) * LK + l) * 2 + comp) << log_n) + s0 + i;
+                    cp8(a_st + i * kASlot + (m >> 3) * kSboA + (jj >> 1) * kLboA + (m & 7) * 16 + (jj & 1) * 8, src,
+                        j < D ? 8u : 0u);
+                }
+                const u32 y_st = sbase + kOffY + (u32)(t & (kRing - 1)) * kYStage;
+                for (int w = ptid; w < n_ct * kJc * kTS; w += kProd) {
+                    const int i = w % kTS, jj = (w / kTS) % kJc, c = w / (kTS * kJc);
+                    const int j = j0 + jj;
+                    const u64* src = Yhat + c * y_stride + (((size_t)(j < D ? j : 0) * LK + l) << log_n) + s0 + i;
+                    cp8(y_st + (u32)w * 8, src, j < D ? 8u : 0u);
+                }
+                if (it.kc == 0 && it.ch == 0) {  // epilogue inputs of this tile: base terms, pf, pf_q
+                    const u32 e_st = sbase + kOffE + (u32)(it.tl % kERing) * kEStage;
+                    const bool ok = l < Lq;
+                    for (int w = ptid; w < n_ct * kTS; w += kProd) {
+                        const int i = w % kTS, c = w / kTS;
+                        cp8(e_st + (u32)w * 8, Bhat + c * b_stride + ((size_t)(ok ? l : 0) << log_n) + s0 + i,
+                            ok ? 8u : 0u);
+                    }
+                    if (ptid == 0) {
+                        cp8(e_st + kCt * kTS * 8, pf + (ok ? l : 0), ok ? 8u : 0u);
+                        cp8(e_st + kCt * kTS * 8 + 8, pf_q + (ok ? l : 0), ok ? 8u : 0u);
+                    }
+                }
+            }
+            cp_commit();
+        };
+        Item ahead{0, 0, 0};
+        for (int t = 0; t < kAhead; ++t) {
+            prefetch(t, ahead);
+            ahead.next(n_kc, n_chunks);
+        }
+        int f_limb = -1;
+        u64 f256[4], f256q[4];  // 2^(8b) mod q_l, b = 1, 2, 3, 4, with Shoup companions
+        Item it{0, 0, 0};
+        for (int t = 0; t < n_items; ++t, it.next(n_kc, n_chunks)) {
             const int tile = (int)blockIdx.x + it.tl * (int)gridDim.x;
             const int l = tile >> lts;
-            const u32 s0 = (u32)(tile & (n_tiles_s - 1)) * kTS;
-            const int g0 = it.kc * kKeys;
-            const int gn = n_keys - g0 < kKeys ? n_keys - g0 : kKeys;
-            const int j0 = it.ch * kJc;
-            const u32 a_st = sbase + (u32)(t & (kRing - 1)) * kAStage;
-            for (int w = tid; w < gn * 2 * kJc * kTS; w += kThreads) {
-                const int i = w % kTS, jj = (w / kTS) % kJc, comp = (w / (kTS * kJc)) % 2, g = w / (kTS * kJc * 2);
-                const int j = j0 + jj;
-                const int m = 2 * g + comp;
-                const u64* src = keys[g0 + g] + ((((size_t)(j < D ? j : 0) * LK + l) * 2 + comp) << log_n) + s0 + i;
-                cp8(a_st + i * kASlot + (m >> 3) * kSboA + (jj >> 1) * kLboA + (m & 7) * 16 + (jj & 1) * 8, src,
-                    j < D ? 8u : 0u);
-            }
-            const u32 y_st = sbase + kOffY + (u32)(t & (kRing - 1)) * kYStage;
-            for (int w = tid; w < n_ct * kJc * kTS; w += kThreads) {
-                const int i = w % kTS, jj = (w / kTS) % kJc, c = w / (kTS * kJc);
-                const int j = j0 + jj;
-                const u64* src = Yhat + c * y_stride + (((size_t)(j < D ? j : 0) * LK + l) << log_n) + s0 + i;
-                cp8(y_st + (u32)w * 8, src, j < D ? 8u : 0u);
-            }
-            if (it.kc == 0 && it.ch == 0) {  // epilogue inputs of this tile: base terms, pf, pf_q
-                const u32 e_st = sbase + kOffE + (u32)(it.tl % kERing) * kEStage;
-                for (int w = tid; w < n_ct * kTS; w += kThreads) {
-                    const int i = w % kTS, c = w / kTS;
-                    const bool ok = l < Lq;
-                    cp8(e_st + (u32)w * 8, Bhat + c * b_stride + ((size_t)(ok ? l : 0) << log_n) + s0 + i, ok ? 8u : 0u);
+            const int bst = t & (kBStages - 1);
+            bool bad = false;
+            if (t >= kBStages)  // the MMAs of item t - 2 released B stage bst and ring slot (t + kAhead) % kRing
+                bad = !wait_parity(smem_u32(&s_empty[bst]), (u32)(((t / kBStages) - 1) & 1));
+            if (group_any(1, kProd, bad || s_abort)) {  // one decision for all producers
+                if (ptid == 0) {
+                    atomicExch(err, 1);
+                    s_abort = 1;
                 }
-                if (tid == 0) {
-                    const bool ok = l < Lq;
-                    cp8(e_st + kCt * kTS * 8, pf + (ok ? l : 0), ok ? 8u : 0u);
-                    cp8(e_st + kCt * kTS * 8 + 8, pf_q + (ok ? l : 0), ok ? 8u : 0u);
-                }
+                break;
             }
-        }
-        cp_commit();
-    };
-
-    Item ahead{0, 0, 0};
-    for (int t = 0; t < kAhead; ++t) {
-        prefetch(t, ahead);
-        ahead.next(n_kc, n_chunks);
-    }
-    int cur_kc = -1, f_limb = -1, r_limb = -1;
-    u64 f256 = 0, f256q = 0;             // 2^8 mod q_l and its Shoup companion
-    u64 one_q = 0, r64 = 0, r64q = 0;    // floor(2^64 / q_l), 2^64 mod q_l, Shoup companion
-    Item it{0, 0, 0};
-    for (int t = 0; t < n_items; ++t, it.next(n_kc, n_chunks)) {
-        const int tile = (int)blockIdx.x + it.tl * (int)gridDim.x;
-        const int l = tile >> lts;
-        const u32 s0 = (u32)(tile & (n_tiles_s - 1)) * kTS;
-        const int g0 = it.kc * kKeys;
-        const int gn = n_keys - g0 < kKeys ? n_keys - g0 : kKeys;
-        const int bst = t & (kBStages - 1);
-        // the MMAs of item t - 2 read ring slot (t + kAhead) % kRing and B stage bst: wait before reuse
-        if (t >= kBStages) {
-            if (!wait_parity(smem_u32(&s_bar[bst]), (u32)(((t / kBStages) - 1) & 1))) {
-                if (tid == 0) atomicExch(err, 1);
-                s_abort = 1;
-            }
-        }
-        prefetch(t + kAhead, ahead);
-        ahead.next(n_kc, n_chunks);
-        cp_wait<kAhead>();  // this thread's copies of item t have landed
-        if (it.kc != cur_kc && it.ch == 0) {  // correction counts of this key chunk
-            for (int w = tid; w < kCt * kKeys; w += kThreads) {
-                const int c = w / kKeys, g = w % kKeys;
-                s_cnt[w] = (c < n_ct && g < gn) ? exc_count[(size_t)c * n_keys + g0 + g] : 0u;
-            }
-            cur_kc = it.kc;
-        }
-        __syncthreads();
-        if (s_abort) break;
-        const NttTab& T = tabs[lm(l)];
-        const u64 q = T.q;
-        // B: w_b(Y[c][j]) = 2^(8b) Y mod q for the 8 weights
-        {
-            const u64* ys = (const u64*)(smem + kOffY + (t & (kRing - 1)) * kYStage);
-            uint8_t* Bs = smem + kOffB + bst * kBStage;
+            prefetch(t + kAhead, ahead);
+            ahead.next(n_kc, n_chunks);
+            cp_wait<kAhead>();   // this thread's copies of item t have landed
+            named_sync(1, kProd);
+            const NttTab& T = tabs[lm(l)];
+            const u64 q = T.q;
             if (l != f_limb) {
-                f256 = 256 % q;
-                f256q = shoup_quotient_dev(f256, q);
+                const Barrett bm{q, T.mu_hi, T.mu_lo};
+                u64 w = 256 % q;
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    f256[b] = w;
+                    f256q[b] = shoup_quotient_dev(w, q);
+                    w = mul_barrett(w, 256 % q, bm);
+                }
                 f_limb = l;
             }
-            for (int w = tid; w < n_ct * kJc * kTS; w += kThreads) {
-                const int i = w % kTS, jj = (w / kTS) % kJc, c = w / (kTS * kJc);
-                uint8_t* dst = Bs + i * kBSlot + jj * kLboB + (c >> 1) * kSboB + (c & 1) * 8;
-                u64 wv = ys[w];
+            // B: w_b(Y[c][j]) = 2^(8b) Y mod q; a unit (slot, digit, ciphertext pair, weight half)
+            // writes 4 weights x 2 ciphertexts as 16-byte stores
+            {
+                const u64* ys = (const u64*)(smem + kOffY + (t & (kRing - 1)) * kYStage);
+                uint8_t* Bs = smem + kOffB + bst * kBStage;
+                for (int w = ptid; w < (n_ct + 1) / 2 * kJc * kTS * 2; w += kProd) {
+                    const int i = w % kTS, jj = (w / kTS) % kJc, bh = (w / (kTS * kJc)) & 1, cp = w / (kTS * kJc * 2);
+                    const int c0 = 2 * cp;
+                    const u64 y0 = ys[(c0 * kJc + jj) * kTS + i];
+                    const u64 y1 = c0 + 1 < n_ct ? ys[((c0 + 1) * kJc + jj) * kTS + i] : 0;
+                    uint8_t* dst = Bs + i * kBSlot + jj * kLboB + cp * kSboB + bh * 64;
 #pragma unroll
-                for (int b = 0; b < 8; ++b) {
-                    *(u64*)(dst + b * 16) = wv;
-                    if (b < 7) wv = mul_shoup(wv, f256, f256q, q);
+                    for (int b = 0; b < 4; ++b) {
+                        u64 v0, v1;
+                        if (bh == 0) {
+                            v0 = b ? mul_shoup(y0, f256[b - 1], f256q[b - 1], q) : y0;
+                            v1 = b ? mul_shoup(y1, f256[b - 1], f256q[b - 1], q) : y1;
+                        } else {  // weights 4 .. 7 = 2^32 * (1, 2^8, 2^16, 2^24)
+                            const u64 z0 = mul_shoup(y0, f256[3], f256q[3], q), z1 = mul_shoup(y1, f256[3], f256q[3], q);
+                            v0 = b ? mul_shoup(z0, f256[b - 1], f256q[b - 1], q) : z0;
+                            v1 = b ? mul_shoup(z1, f256[b - 1], f256q[b - 1], q) : z1;
+                        }
+                        *(ulonglong2*)(dst + b * 16) = make_ulonglong2(v0, v1);
+                    }
                 }
             }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            named_sync(1, kProd);
+            if (ptid == 0) arrive(smem_u32(&s_ready[bst]));
         }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        fence_before();
-        __syncthreads();
-        if (tid == 0) {
-            fence_after();
-            const u32 a0 = sbase + (u32)(t & (kRing - 1)) * kAStage, b0 = sbase + kOffB + (u32)bst * kBStage;
+        cp_wait<0>();
+    } else if (warp == kMmaWarp) {
+        // ------------------------------------------------------------- MMA issue
+        if (lane == 0) {
+            Item it{0, 0, 0};
+            int unit = -1, last_t = -1;
+            for (int t = 0; t < n_items; ++t, it.next(n_kc, n_chunks)) {
+                const int bst = t & (kBStages - 1);
+                if (!wait_parity(smem_u32(&s_ready[bst]), (u32)((t / kBStages) & 1))) {
+                    atomicExch(err, 2);
+                    s_abort = 1;
+                }
+                if (it.ch == 0) {
+                    ++unit;
+                    if (unit >= 2 && !wait_parity(smem_u32(&s_free[unit & 1]), (u32)(((unit >> 1) - 1) & 1))) {
+                        atomicExch(err, 3);
+                        s_abort = 1;
+                    }
+                }
+                if (s_abort) break;
+                fence_after();
+                const u32 a0 = sbase + (u32)(t & (kRing - 1)) * kAStage, b0 = sbase + kOffB + (u32)bst * kBStage;
+                const u32 dbase = tmem + ((u32)(16 * (unit & 1)) << 16);
 #pragma unroll
-            for (int i = 0; i < kTS; ++i)
-                mma_i8(tmem + (u32)i * 128u, sdesc(a0 + i * kASlot, kLboA, kSboA),
-                       sdesc(b0 + i * kBSlot, kLboB, kSboB), it.ch > 0 ? 1u : 0u);
-            commit(smem_u32(&s_bar[bst]));
+                for (int i = 0; i < kTS; ++i)
+                    mma_i8(dbase + (u32)i * 128u, sdesc(a0 + i * kASlot, kLboA, kSboA),
+                           sdesc(b0 + i * kBSlot, kLboB, kSboB), it.ch > 0 ? 1u : 0u);
+                commit(smem_u32(&s_empty[bst]));
+                if (it.ch == n_chunks - 1) commit(smem_u32(&s_full[unit & 1]));
+                last_t = t;
+            }
+            // drain: the last commit covers every MMA issued
+            if (last_t >= 0)
+                wait_parity(smem_u32(&s_empty[last_t & (kBStages - 1)]), (u32)((last_t / kBStages) & 1));
         }
-        if (it.ch != n_chunks - 1) continue;
-        // ------------------------------------------------ epilogue of (tile, key chunk)
-        if (!wait_parity(smem_u32(&s_bar[bst]), (u32)((t / kBStages) & 1))) {
-            if (tid == 0) atomicExch(err, 1);
-            s_abort = 1;
-        }
-        fence_after();
-        {
+        __syncwarp();
+    } else {
+        // -------------------------------------------------------------- epilogue
+        const int qd = warp;  // TMEM subpartition (lanes 32 qd ..)
+        const int t0 = lane & 3, t1 = lane >> 2;
+        int r_limb = -1;
+        u64 one_q = 0, r64 = 0, r64q = 0;  // floor(2^64 / q_l), 2^64 mod q_l, Shoup companion
+        for (int u = 0; u < n_units; ++u) {
+            const int tl = u / n_kc, kc = u - tl * n_kc;
+            const int tile = (int)blockIdx.x + tl * (int)gridDim.x;
+            const int l = tile >> lts;
+            const u32 s0 = (u32)(tile & (n_tiles_s - 1)) * kTS;
+            const int g0 = kc * kKeys;
+            const int gn = n_keys - g0 < kKeys ? n_keys - g0 : kKeys;
+            const bool bad = !wait_parity(smem_u32(&s_full[u & 1]), (u32)((u >> 1) & 1));
+            if (group_any(2, kEpi, bad || s_abort)) {  // one decision for all epilogue threads
+                if (tid == 0) {
+                    atomicExch(err, 4);
+                    s_abort = 1;
+                }
+                break;
+            }
+            fence_after();
+            const NttTab& T = tabs[lm(l)];
+            const u64 q = T.q;
             const Barrett bm{q, T.mu_hi, T.mu_lo};
-            const u64* es = (const u64*)(smem + kOffE + (it.tl % kERing) * kEStage);
-            const u64 pfl = es[kCt * kTS], pfql = es[kCt * kTS + 1];
-            const int qd = warp & 3, half = warp >> 2;  // warps 0-3: slots 0, 1; warps 4-7: slots 2, 3
-            const int m = 16 * qd + lane;
-            const int gl = m >> 1, comp = m & 1, g = g0 + gl;
-            const bool row_ok = lane < 16 && gl < gn;
-            const u32 trow = tmem + ((u32)(32 * qd) << 16);
-            if (l != r_limb) {  // 2^64 mod q and Shoup companions for the final reduction
-                one_q = (~0ull) / q;  // floor(2^64 / q), q odd
-                r64 = (u64)(-(q * one_q));  // 2^64 - q floor(2^64 / q) = 2^64 mod q
-                r64 = r64 >= q ? r64 - q : r64;
+            if (l != r_limb) {
+                one_q = (~0ull) / q;                 // floor(2^64 / q), q odd
+                r64 = (u64)(-(q * one_q));           // 2^64 mod q
                 r64q = shoup_quotient_dev(r64, q);
                 r_limb = l;
             }
+            const u64* es = (const u64*)(smem + kOffE + (tl % kERing) * kEStage);
+            const u64 pfl = es[kCt * kTS], pfql = es[kCt * kTS + 1];
+            const u32 taddr = tmem + ((u32)(32 * qd + 16 * (u & 1)) << 16);
+            // rows of this thread: m = 16 qd + t1 + 8 h (h = 0, 1); ciphertext cb + t0 after the exchange
             for (int cb = 0; cb < kCt; cb += 4) {
-                u64 outv[2][4];
+                u64 outv[2][kTS];
+#pragma unroll
+                for (int i = 0; i < kTS; ++i) {
+                    u32 r[16];
+                    __syncwarp();
+                    tmem_ld16x4(taddr + (u32)(i * 128 + 8 * cb), r);
+                    tmem_wait_ld();
+                    // exchange within each group of 4 lanes: lane t0 gathers ciphertext cb + t0
+                    // (registers 4k .. hold ciphertext cb + k; lane s holds planes 2 s, 2 s + 1).
+                    // Partial pk = plane(2k) + 2^8 plane(2k + 1) < 2^34 from lane k.
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        u64 pk[4];
+                        // own contribution: ciphertext t0 from registers 4 t0 + 2h
+                        const u32 a_lo[4] = {r[2 * h], r[4 + 2 * h], r[8 + 2 * h], r[12 + 2 * h]};
+                        const u32 a_hi[4] = {r[2 * h + 1], r[4 + 2 * h + 1], r[8 + 2 * h + 1], r[12 + 2 * h + 1]};
+                        auto pick = [&](const u32 (&v)[4], int k) -> u32 {
+                            const u32 x01 = (k & 1) ? v[1] : v[0], x23 = (k & 1) ? v[3] : v[2];
+                            return (k & 2) ? x23 : x01;
+                        };
+                        const u64 mine = (u64)pick(a_lo, t0) + ((u64)pick(a_hi, t0) << 8);
+                        pk[0] = pk[1] = pk[2] = pk[3] = 0;
+#pragma unroll
+                        for (int x = 1; x < 4; ++x) {
+                            const int k = t0 ^ x;  // the partner's ciphertext
+                            const u32 g_lo = __shfl_xor_sync(0xffffffffu, pick(a_lo, k), x);
+                            const u32 g_hi = __shfl_xor_sync(0xffffffffu, pick(a_hi, k), x);
+                            const u64 v = (u64)g_lo + ((u64)g_hi << 8);  // planes 2k', 2k'+1, k' = t0 ^ x
+                            const int src = t0 ^ x;
+                            pk[0] = src == 0 ? v : pk[0];
+                            pk[1] = src == 1 ? v : pk[1];
+                            pk[2] = src == 2 ? v : pk[2];
+                            pk[3] = src == 3 ? v : pk[3];
+                        }
+                        pk[0] = t0 == 0 ? mine : pk[0];
+                        pk[1] = t0 == 1 ? mine : pk[1];
+                        pk[2] = t0 == 2 ? mine : pk[2];
+                        pk[3] = t0 == 3 ? mine : pk[3];
+                        const u64 lo4 = pk[0] + (pk[1] << 16), hi4 = pk[2] + (pk[3] << 16);  // each < 2^51
+                        const u64 lo = lo4 + (hi4 << 32);
+                        const u64 hi = (hi4 >> 32) + (lo < lo4);                            // < 2^20
+                        outv[h][i] =
+                            add_mod(reduce_2q(mul_shoup_lazy(lo, 1, one_q, q), q), mul_shoup(hi, r64, r64q, q), q);
+                    }
+                }
+                const int c = cb + t0;
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
-                    const int i = 2 * half + h;
-                    const u32 s = s0 + i;
-                    u32 r[32];
-                    tmem_ld32(trow + (u32)(i * 128 + 8 * cb), r);
-                    tmem_wait_ld();
-                    if (!row_ok) continue;
+                    const int m = 16 * qd + t1 + 8 * h;
+                    const int gl = m >> 1, comp = m & 1, g = g0 + gl;
+                    if (c >= n_ct || gl >= gn) continue;
+                    const u32 cnt = min(cnt_staged ? s_cnt[c * n_keys + g] : exc_count[(size_t)c * n_keys + g],
+                                        (u32)cap);
 #pragma unroll
-                    for (int cc = 0; cc < 4; ++cc) {
-                        const int c = cb + cc;
-                        if (c >= n_ct) break;
-                        // sum_a 2^(8a) P_a with P_a < 2^25: pairwise in 64 bits, then 128
-                        const u32* P = r + 8 * cc;
-                        const u64 p01 = (u64)P[0] + ((u64)P[1] << 8), p23 = (u64)P[2] + ((u64)P[3] << 8);
-                        const u64 p45 = (u64)P[4] + ((u64)P[5] << 8), p67 = (u64)P[6] + ((u64)P[7] << 8);
-                        const u64 lo4 = p01 + (p23 << 16), hi4 = p45 + (p67 << 16);  // each < 2^51
-                        const u64 lo = lo4 + (hi4 << 32);
-                        const u64 hi = (hi4 >> 32) + (lo < lo4);                    // < 2^20
-                        // (hi 2^64 + lo) mod q = lo mod q + hi (2^64 mod q) mod q
-                        u64 v = add_mod(reduce_2q(mul_shoup_lazy(lo, 1, one_q, q), q), mul_shoup(hi, r64, r64q, q), q);
+                    for (int i = 0; i < kTS; ++i) {
+                        u64 v = outv[h][i];
                         if (comp == 0 && l < Lq) v = add_mod(v, mul_shoup(es[c * kTS + i], pfl, pfql, q), q);
-                        const u32 cnt = min(s_cnt[c * kKeys + gl], (u32)cap);
                         if (cnt) {
+                            const u32 s = s0 + i;
                             const Exc* list = exc + ((size_t)c * n_keys + g) * cap;
                             const u64 ps = psi[lm(l)];
                             const u32 k = galois_src(s, exps_inv[g], log_n);
                             const u64* key = keys[g];
                             for (u32 e = 0; e < cnt; ++e) {
-                                const Exc x = list[e];
-                                u64 wv = pow_mod_dev(ps, ((2ull * k + 1) * x.t) & (2ull * n - 1), bm);
-                                u64 dm = x.delta < 0 ? (u64)(-x.delta) % q : (u64)x.delta % q;
-                                if (x.delta < 0 && dm) dm = q - dm;
+                                const Exc xe = list[e];
+                                u64 wv = pow_mod_dev(ps, ((2ull * k + 1) * xe.t) & (2ull * n - 1), bm);
+                                u64 dm = xe.delta < 0 ? (u64)(-xe.delta) % q : (u64)xe.delta % q;
+                                if (xe.delta < 0 && dm) dm = q - dm;
                                 const u64 tv = mul_barrett(wv, dm, bm);
-                                const size_t kofs = (((size_t)x.j * LK + l) * 2 + comp) << log_n;
+                                const size_t kofs = (((size_t)xe.j * LK + l) * 2 + comp) << log_n;
                                 v = add_mod(v, mul_barrett(tv, key[kofs + s], bm), q);
                             }
                         }
-                        outv[h][cc] = v;
+                        outv[h][i] = v;
                     }
-                }
-                if (!row_ok) continue;
-#pragma unroll
-                for (int cc = 0; cc < 4; ++cc) {
-                    const int c = cb + cc;
-                    if (c >= n_ct) break;
                     const size_t obase = ((((size_t)c * n_keys + g) * 2 + comp) * LK + l) << log_n;
-                    *(ulonglong2*)(acc + obase + s0 + 2 * half) = make_ulonglong2(outv[0][cc], outv[1][cc]);
+                    *(ulonglong2*)(acc + obase + s0) = make_ulonglong2(outv[h][0], outv[h][1]);
+                    *(ulonglong2*)(acc + obase + s0 + 2) = make_ulonglong2(outv[h][2], outv[h][3]);
                 }
             }
-        }
-        fence_before();
-        __syncthreads();  // TMEM columns free for the next item's MMAs
-        if (s_abort) break;
-    }
-    // teardown: drain the copies, wait (bounded) for MMAs in flight, free TMEM
-    cp_wait<0>();
-    __syncthreads();
-    if (tid == 0) {
-        for (int bsi = 0; bsi < kBStages; ++bsi) {
-            // the last commit on each stage, if any
-            int last = -1;
-            for (int t = n_items - 1; t >= 0 && t >= n_items - kBStages; --t)
-                if ((t & (kBStages - 1)) == bsi) last = t;
-            if (last >= 0) wait_parity(smem_u32(&s_bar[bsi]), (u32)((last / kBStages) & 1));
+            fence_before();
+            named_sync(2, kEpi);
+            if (tid == 0) arrive(smem_u32(&s_free[u & 1]));
         }
     }
+    // teardown: every role has left its loop (on abort, after a bounded wait)
     fence_before();
     __syncthreads();
     fence_after();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+    if (warp == kMmaWarp) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
 }
 
 }  // namespace
@@ -886,8 +984,8 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
         pt.end();
         pt.begin(5);
         // ModDown of every (ciphertext, key) pair, then sigma_g, straight into the output
-        if ((rc = mod_down_sigma_multi(ctx, Z.p, ct_out + (size_t)c0 * n_keys * ct_words, gn * n_keys * 2, Lq, d_exps,
-                                       n_keys, st)))
+        if ((rc = mod_down_sigma_multi(ctx, Z.p, ct_out + (size_t)c0 * n_keys * ct_words, gn * n_keys * 2, Lq,
+                                       d_exps_inv, n_keys, st)))
             return rc;
         pt.end();
         // pairs whose correction lists overflowed are recomputed exactly

@@ -18,10 +18,10 @@ int32_t pointwise_launch(ckks_ctx* ctx, const u64* a, const u64* b, u64* out, u3
                          int op, cudaStream_t st);
 int32_t rescale_launch(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, u32 limbs_in, cudaStream_t st);
 int32_t mod_down_launch(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, u32 q_limbs, cudaStream_t st);
-// ModDown of n_polys polynomials; poly p is then mapped by X -> X^k with
-// k = d_exps[(p / 2) % n_keys] (device array; null: no automorphism).
-int32_t mod_down_sigma_multi(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, u32 q_limbs, const u64* d_exps,
-                             u32 n_keys, cudaStream_t st);
+// ModDown of n_polys polynomials; poly p is then mapped by X -> X^k where
+// d_exps_inv[(p / 2) % n_keys] = k^-1 mod 2N (device array; null: no automorphism).
+int32_t mod_down_sigma_multi(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, u32 q_limbs,
+                             const u64* d_exps_inv, u32 n_keys, cudaStream_t st);
 
 // Bounded (balanced base-2^base_log) gadget, grafting/bounded_gadget.rs.
 int32_t bounded_digit_count(ckks_ctx* ctx, u32 q_limbs, u32 base_log, u32* out);
