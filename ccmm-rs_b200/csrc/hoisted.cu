@@ -491,16 +491,19 @@ __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_grou
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-// 16 TMEM lanes x 32 columns: thread t gets columns 8k + 2 (t % 4) + {0, 1} of
-// lanes t / 4 (registers 4k, 4k + 1) and t / 4 + 8 (registers 4k + 2, 4k + 3).
-__device__ __forceinline__ void tmem_ld16x4(u32 taddr, u32 (&r)[16]) {
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// 32 TMEM lanes x 32 columns: lane L of the warp gets columns 0 .. 31 of lane L.
+__device__ __forceinline__ void tmem_ld32(u32 taddr, u32 (&r)[32]) {
     asm volatile(
-        "tcgen05.ld.sync.aligned.16x256b.x4.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
         : "r"(taddr));
 }
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 // Position in a CTA's item sequence (tile_local-th tile of the CTA, key chunk,
 // digit chunk), advanced by counters instead of divisions.
@@ -672,14 +675,16 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                     uint8_t* dst = Bs + i * kBSlot + jj * kLboB + cp * kSboB + bh * 64;
 #pragma unroll
                     for (int b = 0; b < 4; ++b) {
+                        // lazily reduced in [0, 2q): the byte-split sum needs only the residue class
                         u64 v0, v1;
                         if (bh == 0) {
-                            v0 = b ? mul_shoup(y0, f256[b - 1], f256q[b - 1], q) : y0;
-                            v1 = b ? mul_shoup(y1, f256[b - 1], f256q[b - 1], q) : y1;
+                            v0 = b ? mul_shoup_lazy(y0, f256[b - 1], f256q[b - 1], q) : y0;
+                            v1 = b ? mul_shoup_lazy(y1, f256[b - 1], f256q[b - 1], q) : y1;
                         } else {  // weights 4 .. 7 = 2^32 * (1, 2^8, 2^16, 2^24)
-                            const u64 z0 = mul_shoup(y0, f256[3], f256q[3], q), z1 = mul_shoup(y1, f256[3], f256q[3], q);
-                            v0 = b ? mul_shoup(z0, f256[b - 1], f256q[b - 1], q) : z0;
-                            v1 = b ? mul_shoup(z1, f256[b - 1], f256q[b - 1], q) : z1;
+                            const u64 z0 = mul_shoup_lazy(y0, f256[3], f256q[3], q),
+                                      z1 = mul_shoup_lazy(y1, f256[3], f256q[3], q);
+                            v0 = b ? mul_shoup_lazy(z0, f256[b - 1], f256q[b - 1], q) : z0;
+                            v1 = b ? mul_shoup_lazy(z1, f256[b - 1], f256q[b - 1], q) : z1;
                         }
                         *(ulonglong2*)(dst + b * 16) = make_ulonglong2(v0, v1);
                     }
@@ -711,11 +716,13 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                 if (s_abort) break;
                 fence_after();
                 const u32 a0 = sbase + (u32)(t & (kRing - 1)) * kAStage, b0 = sbase + kOffB + (u32)bst * kBStage;
-                const u32 dbase = tmem + ((u32)(16 * (unit & 1)) << 16);
+                // accumulator of slot i: columns 256 buf + 128 (i / 2), TMEM lanes 16 (i % 2) + ..
+                const u32 dbase = tmem + (u32)(256 * (unit & 1));
 #pragma unroll
                 for (int i = 0; i < kTS; ++i)
-                    mma_i8(dbase + (u32)i * 128u, sdesc(a0 + i * kASlot, kLboA, kSboA),
-                           sdesc(b0 + i * kBSlot, kLboB, kSboB), it.ch > 0 ? 1u : 0u);
+                    mma_i8(dbase + ((u32)(16 * (i & 1)) << 16) + (u32)(i >> 1) * 128u,
+                           sdesc(a0 + i * kASlot, kLboA, kSboA), sdesc(b0 + i * kBSlot, kLboB, kSboB),
+                           it.ch > 0 ? 1u : 0u);
                 commit(smem_u32(&s_empty[bst]));
                 if (it.ch == n_chunks - 1) commit(smem_u32(&s_full[unit & 1]));
                 last_t = t;
@@ -728,7 +735,6 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     } else {
         // -------------------------------------------------------------- epilogue
         const int qd = warp;  // TMEM subpartition (lanes 32 qd ..)
-        const int t0 = lane & 3, t1 = lane >> 2;
         int r_limb = -1;
         u64 one_q = 0, r64 = 0, r64q = 0;  // floor(2^64 / q_l), 2^64 mod q_l, Shoup companion
         for (int u = 0; u < n_units; ++u) {
@@ -758,68 +764,35 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
             }
             const u64* es = (const u64*)(smem + kOffE + (tl % kERing) * kEStage);
             const u64 pfl = es[kCt * kTS], pfql = es[kCt * kTS + 1];
-            const u32 taddr = tmem + ((u32)(32 * qd + 16 * (u & 1)) << 16);
-            // rows of this thread: m = 16 qd + t1 + 8 h (h = 0, 1); ciphertext cb + t0 after the exchange
-            for (int cb = 0; cb < kCt; cb += 4) {
-                u64 outv[2][kTS];
-#pragma unroll
-                for (int i = 0; i < kTS; ++i) {
-                    u32 r[16];
+            // lane L of warp qd: row m = 16 qd + (L % 16); slot 2 p + (L / 16) of slot pair p
+            const u32 taddr = tmem + ((u32)(32 * qd) << 16) + (u32)(256 * (u & 1));
+            const int m = 16 * qd + (lane & 15);
+            const int gl = m >> 1, comp = m & 1, g = g0 + gl;
+            const bool row_ok = gl < gn;
+            for (int pp = 0; pp < kTS / 2; ++pp) {
+                const int i = 2 * pp + (lane >> 4);
+                const u32 s = s0 + i;
+                for (int cb = 0; cb < kCt; cb += 4) {
+                    u32 r[32];
                     __syncwarp();
-                    tmem_ld16x4(taddr + (u32)(i * 128 + 8 * cb), r);
+                    tmem_ld32(taddr + (u32)(pp * 128 + 8 * cb), r);
                     tmem_wait_ld();
-                    // exchange within each group of 4 lanes: lane t0 gathers ciphertext cb + t0
-                    // (registers 4k .. hold ciphertext cb + k; lane s holds planes 2 s, 2 s + 1).
-                    // Partial pk = plane(2k) + 2^8 plane(2k + 1) < 2^34 from lane k.
 #pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        u64 pk[4];
-                        // own contribution: ciphertext t0 from registers 4 t0 + 2h
-                        const u32 a_lo[4] = {r[2 * h], r[4 + 2 * h], r[8 + 2 * h], r[12 + 2 * h]};
-                        const u32 a_hi[4] = {r[2 * h + 1], r[4 + 2 * h + 1], r[8 + 2 * h + 1], r[12 + 2 * h + 1]};
-                        auto pick = [&](const u32 (&v)[4], int k) -> u32 {
-                            const u32 x01 = (k & 1) ? v[1] : v[0], x23 = (k & 1) ? v[3] : v[2];
-                            return (k & 2) ? x23 : x01;
-                        };
-                        const u64 mine = (u64)pick(a_lo, t0) + ((u64)pick(a_hi, t0) << 8);
-                        pk[0] = pk[1] = pk[2] = pk[3] = 0;
-#pragma unroll
-                        for (int x = 1; x < 4; ++x) {
-                            const int k = t0 ^ x;  // the partner's ciphertext
-                            const u32 g_lo = __shfl_xor_sync(0xffffffffu, pick(a_lo, k), x);
-                            const u32 g_hi = __shfl_xor_sync(0xffffffffu, pick(a_hi, k), x);
-                            const u64 v = (u64)g_lo + ((u64)g_hi << 8);  // planes 2k', 2k'+1, k' = t0 ^ x
-                            const int src = t0 ^ x;
-                            pk[0] = src == 0 ? v : pk[0];
-                            pk[1] = src == 1 ? v : pk[1];
-                            pk[2] = src == 2 ? v : pk[2];
-                            pk[3] = src == 3 ? v : pk[3];
-                        }
-                        pk[0] = t0 == 0 ? mine : pk[0];
-                        pk[1] = t0 == 1 ? mine : pk[1];
-                        pk[2] = t0 == 2 ? mine : pk[2];
-                        pk[3] = t0 == 3 ? mine : pk[3];
-                        const u64 lo4 = pk[0] + (pk[1] << 16), hi4 = pk[2] + (pk[3] << 16);  // each < 2^51
+                    for (int cc = 0; cc < 4; ++cc) {
+                        const int c = cb + cc;
+                        if (!row_ok || c >= n_ct) continue;
+                        // sum_a 2^(8a) P_a with P_a < 2^25: pairwise in 64 bits, then 128
+                        const u32* P = r + 8 * cc;
+                        const u64 p01 = (u64)P[0] + ((u64)P[1] << 8), p23 = (u64)P[2] + ((u64)P[3] << 8);
+                        const u64 p45 = (u64)P[4] + ((u64)P[5] << 8), p67 = (u64)P[6] + ((u64)P[7] << 8);
+                        const u64 lo4 = p01 + (p23 << 16), hi4 = p45 + (p67 << 16);  // each < 2^51
                         const u64 lo = lo4 + (hi4 << 32);
-                        const u64 hi = (hi4 >> 32) + (lo < lo4);                            // < 2^20
-                        outv[h][i] =
-                            add_mod(reduce_2q(mul_shoup_lazy(lo, 1, one_q, q), q), mul_shoup(hi, r64, r64q, q), q);
-                    }
-                }
-                const int c = cb + t0;
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int m = 16 * qd + t1 + 8 * h;
-                    const int gl = m >> 1, comp = m & 1, g = g0 + gl;
-                    if (c >= n_ct || gl >= gn) continue;
-                    const u32 cnt = min(cnt_staged ? s_cnt[c * n_keys + g] : exc_count[(size_t)c * n_keys + g],
-                                        (u32)cap);
-#pragma unroll
-                    for (int i = 0; i < kTS; ++i) {
-                        u64 v = outv[h][i];
+                        const u64 hi = (hi4 >> 32) + (lo < lo4);                    // < 2^20
+                        u64 v = add_mod(reduce_2q(mul_shoup_lazy(lo, 1, one_q, q), q), mul_shoup(hi, r64, r64q, q), q);
                         if (comp == 0 && l < Lq) v = add_mod(v, mul_shoup(es[c * kTS + i], pfl, pfql, q), q);
+                        const u32 cnt =
+                            min(cnt_staged ? s_cnt[c * n_keys + g] : exc_count[(size_t)c * n_keys + g], (u32)cap);
                         if (cnt) {
-                            const u32 s = s0 + i;
                             const Exc* list = exc + ((size_t)c * n_keys + g) * cap;
                             const u64 ps = psi[lm(l)];
                             const u32 k = galois_src(s, exps_inv[g], log_n);
@@ -834,11 +807,8 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                                 v = add_mod(v, mul_barrett(tv, key[kofs + s], bm), q);
                             }
                         }
-                        outv[h][i] = v;
+                        acc[(((((size_t)c * n_keys + g) * 2 + comp) * LK + l) << log_n) + s] = v;
                     }
-                    const size_t obase = ((((size_t)c * n_keys + g) * 2 + comp) * LK + l) << log_n;
-                    *(ulonglong2*)(acc + obase + s0) = make_ulonglong2(outv[h][0], outv[h][1]);
-                    *(ulonglong2*)(acc + obase + s0 + 2) = make_ulonglong2(outv[h][2], outv[h][3]);
                 }
             }
             fence_before();
