@@ -439,12 +439,14 @@ def bench_rot_gpu(args, world, rank, local):
     # per-phase device time of one step (outside the timed region)
     _, phases = cb.rotate_hoisted_timed(ctx, keys, cts, out=out)
     torch.cuda.synchronize()
-    # roofline of the dominant kernel, the key-switch MAC: algorithmic bytes per
-    # step = every key once per group of 4 ciphertexts + the hoisted digit
-    # transforms and base transforms of every ciphertext + the accumulators
+    # roofline of the dominant kernel, the tensor-core key-switch MAC
+    # (k_mac_tc): algorithmic bytes per step = every key once per group of 16
+    # ciphertexts + the hoisted digit transforms and base transforms of every
+    # ciphertext + the accumulators it writes
     key_bytes = words * 8
     LK = ROT_L + ROT_K
-    groups = -(-ROT_NCT // 4)
+    group = 16
+    groups = -(-ROT_NCT // group)
     mac_bytes = (groups * len(keys) * key_bytes + ROT_NCT * D * LK * n * 8 + ROT_NCT * ROT_L * n * 8
                  + rots * 2 * LK * n * 8)
     peak, kind = peaks()
@@ -469,8 +471,8 @@ def bench_rot_gpu(args, world, rank, local):
         "dtype": "u64", "data": "synthetic (seeded uniform ciphertexts, GPU-generated keys)", "config": rot_config(),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "peak_kind": kind,
-                     "kernel": "k_mac_tiled (key-switch MAC, %d digits, keys %.3f GB each, read once per 4 ct)"
-                               % (D, key_bytes / 1e9),
+                     "kernel": "k_mac_tc (INT8 tcgen05 key-switch MAC, %d digits, keys %.3f GB each, read once "
+                               "per %d ct)" % (D, key_bytes / 1e9, min(group, ROT_NCT)),
                      "kernel_ms_per_step": mac_ms, "algorithmic_bytes_per_step": mac_bytes},
         "whole_rotation_roofline": {"bytes_per_rotation": key_bytes + 2 * ct_bytes,
                                     "frac_no_key_reuse": (key_bytes + 2 * ct_bytes) * value / 1e9 / peak},
@@ -478,7 +480,7 @@ def bench_rot_gpu(args, world, rank, local):
         "e2e": {"value": rots * e2e_steps * world / e2e_s, "unit": "rotations/s",
                 "h2d_bytes_per_step": int(host.nbytes), "d2h_bytes_per_step": int(hout.nbytes),
                 "path": "ckks_rotate_hoisted_host"},
-        "gpu_launches": args.steps * groups * (5 * 4 + 5), "clocks": clk,
+        "gpu_launches": args.steps * groups * (5 * min(group, ROT_NCT) + 5), "clocks": clk,
     }
     return line
 

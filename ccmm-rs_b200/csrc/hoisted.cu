@@ -581,6 +581,19 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     if (warp >= kProdWarp0 && warp < kMmaWarp) {
         // ------------------------------------------------------------ producers
         const int ptid = tid - kProdWarp0 * 32;
+        // A copies: producer thread ptid owns slot pi, digit pjj and component pcomp of the
+        // keys pg0 + 8 r (r < 4); Y copies: slot pi, digit pjj of ciphertext ptid / 16.
+        static_assert(kProd == 256 && kKeys == 32 && kTS * kJc * 2 * 8 == kProd, "producer work split");
+        const int pi = ptid & 3, pjj = (ptid >> 2) & 3, pcomp = (ptid >> 4) & 1, pg0 = ptid >> 5;
+        u32 a_dst[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int m = 2 * (pg0 + 8 * r) + pcomp;
+            a_dst[r] = pi * kASlot + (m >> 3) * kSboA + (pjj >> 1) * kLboA + (m & 7) * 16 + (pjj & 1) * 8;
+        }
+        const int yc = ptid >> 4;  // ciphertext of this thread's Y copy (kCt * kJc * kTS == kProd)
+        const u64* kp[4] = {nullptr, nullptr, nullptr, nullptr};
+        int kp_kc = -1;
         auto prefetch = [&](int t, const Item& it) {
             if (t < n_items) {
                 const int tile = (int)blockIdx.x + it.tl * (int)gridDim.x;
@@ -588,33 +601,30 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                 const u32 s0 = (u32)(tile & (n_tiles_s - 1)) * kTS;
                 const int g0 = it.kc * kKeys;
                 const int gn = n_keys - g0 < kKeys ? n_keys - g0 : kKeys;
-                const int j0 = it.ch * kJc;
-                const u32 a_st = sbase + (u32)(t & (kRing - 1)) * kAStage;
-                for (int w = ptid; w < gn * 2 * kJc * kTS; w += kProd) {
-                    const int i = w % kTS, jj = (w / kTS) % kJc, comp = (w / (kTS * kJc)) % 2,
-                              g = w / (kTS * kJc * 2);
-                    const int j = j0 + jj;
-                    const int m = 2 * g + comp;
-                    const u64* src =
-                        keys[g0 + g] + ((((size_t)(j < D ? j : 0) * LK + l) * 2 + comp) << log_n) + s0 + i;
-                    cp8(a_st + i * kASlot + (m >> 3) * kSboA + (jj >> 1) * kLboA + (m & 7) * 16 + (jj & 1) * 8, src,
-                        j < D ? 8u : 0u);
+                if (it.kc != kp_kc) {
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) kp[r] = pg0 + 8 * r < gn ? keys[g0 + pg0 + 8 * r] : keys[0];
+                    kp_kc = it.kc;
                 }
-                const u32 y_st = sbase + kOffY + (u32)(t & (kRing - 1)) * kYStage;
-                for (int w = ptid; w < n_ct * kJc * kTS; w += kProd) {
-                    const int i = w % kTS, jj = (w / kTS) % kJc, c = w / (kTS * kJc);
-                    const int j = j0 + jj;
-                    const u64* src = Yhat + c * y_stride + (((size_t)(j < D ? j : 0) * LK + l) << log_n) + s0 + i;
-                    cp8(y_st + (u32)w * 8, src, j < D ? 8u : 0u);
+                const int j = it.ch * kJc + pjj;
+                const bool jok = j < D;
+                const size_t koff = ((((size_t)(jok ? j : 0) * LK + l) * 2 + pcomp) << log_n) + s0 + pi;
+                const u32 a_st = sbase + (u32)(t & (kRing - 1)) * kAStage;
+#pragma unroll
+                for (int r = 0; r < 4; ++r)
+                    if (pg0 + 8 * r < gn) cp8(a_st + a_dst[r], kp[r] + koff, jok ? 8u : 0u);
+                if (yc < n_ct) {
+                    const u32 y_st = sbase + kOffY + (u32)(t & (kRing - 1)) * kYStage;
+                    cp8(y_st + (u32)ptid * 8, Yhat + yc * y_stride + (((size_t)(jok ? j : 0) * LK + l) << log_n) + s0 + pi,
+                        jok ? 8u : 0u);
                 }
                 if (it.kc == 0 && it.ch == 0) {  // epilogue inputs of this tile: base terms, pf, pf_q
                     const u32 e_st = sbase + kOffE + (u32)(it.tl % kERing) * kEStage;
                     const bool ok = l < Lq;
-                    for (int w = ptid; w < n_ct * kTS; w += kProd) {
-                        const int i = w % kTS, c = w / kTS;
-                        cp8(e_st + (u32)w * 8, Bhat + c * b_stride + ((size_t)(ok ? l : 0) << log_n) + s0 + i,
+                    if (ptid < n_ct * kTS)
+                        cp8(e_st + (u32)ptid * 8,
+                            Bhat + (ptid / kTS) * b_stride + ((size_t)(ok ? l : 0) << log_n) + s0 + (ptid % kTS),
                             ok ? 8u : 0u);
-                    }
                     if (ptid == 0) {
                         cp8(e_st + kCt * kTS * 8, pf + (ok ? l : 0), ok ? 8u : 0u);
                         cp8(e_st + kCt * kTS * 8 + 8, pf_q + (ok ? l : 0), ok ? 8u : 0u);
