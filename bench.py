@@ -383,10 +383,11 @@ ROT_STEPS = [1 << i for i in range(15)] + list(range(3, 37, 2))
 
 
 def rot_config():
-    default = ROT_L == 24 and ROT_NCT == 16 and len(ROT_STEPS) == 32
+    default = ROT_L == 24 and ROT_NCT == 16 and len(ROT_STEPS) == 32 and ROT_BASE_LOG == 32
     return {"workload": ("hoisted key-switched rotations, N=2^16, %dx50-bit Q + 3x60-bit P, bounded hybrid-QP "
-                         "gadget base 2^32, %d ct x %d Galois steps%s"
-                         % (ROT_L, ROT_NCT, len(ROT_STEPS), "" if default else " (reduced profiling size)")),
+                         "gadget base 2^%d, %d ct x %d Galois steps%s"
+                         % (ROT_L, ROT_BASE_LOG, ROT_NCT, len(ROT_STEPS),
+                            "" if default else " (reduced profiling size)")),
             "log_n": ROT_LOG_N, "q_limbs": ROT_L, "p_limbs": ROT_K, "base_log": ROT_BASE_LOG,
             "ciphertexts": ROT_NCT, "galois_steps": ROT_STEPS, "scale": "2^50", "secret": "ternary",
             "sigma": 3.2, "l2": "keys and outputs larger than L2", "parallelism": "replicas"}
@@ -920,9 +921,10 @@ def main():
     ap.add_argument("--rot-limbs", type=int, default=24)
     ap.add_argument("--rot-ct", type=int, default=16)
     ap.add_argument("--rot-keys", type=int, default=32)
+    ap.add_argument("--rot-base-log", type=int, default=32)
     args = ap.parse_args()
-    global ROT_L, ROT_NCT, ROT_STEPS
-    ROT_L, ROT_NCT = args.rot_limbs, args.rot_ct
+    global ROT_L, ROT_NCT, ROT_STEPS, ROT_BASE_LOG
+    ROT_L, ROT_NCT, ROT_BASE_LOG = args.rot_limbs, args.rot_ct, args.rot_base_log
     ROT_STEPS = ROT_STEPS[:args.rot_keys]
     args.warmup = max(3, args.warmup)
     world, rank, local = dist_setup() if args.impl == "b200" else (

@@ -131,7 +131,8 @@ __global__ void __launch_bounds__(kT) k_mac_hoisted(const u64* __restrict__ Yhat
         aa[c].fold(q, mh, ml);
         u64 b = ab[c].lo, a = aa[c].lo;
         if (l < Lq) b = add_mod(b, mul_shoup(__ldg(Bhat + c * b_stride + ((size_t)l << log_n) + s), pf[l], pf_q[l], q), q);
-        const u32 cnt = min(exc_count[(size_t)c * n_keys + g], (u32)cap);
+        u32 cnt = exc_count[(size_t)c * n_keys + g];
+            if (cnt > (u32)cap) cnt = 0;  // overflowed: recomputed by the exact fallback
         if (cnt) {
             const Exc* list = exc + ((size_t)c * n_keys + g) * cap;
             const u64 ps = psi[lm(l)];
@@ -287,7 +288,8 @@ __global__ void __launch_bounds__(kS * kLanes, 2) k_mac_tiled(const u64* __restr
             ab[c].fold(q, one_q, r1, r1q, r2, r2q);
             aa[c].fold(q, one_q, r1, r1q, r2, r2q);
             u64 b = add_mod(ab[c].s0, bterm[c], q), a = aa[c].s0;
-            const u32 cnt = min(exc_count[(size_t)c * n_keys + g], (u32)cap);
+            u32 cnt = exc_count[(size_t)c * n_keys + g];
+            if (cnt > (u32)cap) cnt = 0;  // overflowed: recomputed by the exact fallback
             if (cnt) {
                 const Exc* list = exc + ((size_t)c * n_keys + g) * cap;
                 const u64 ps = psi[lm(l)];
@@ -638,8 +640,9 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
             prefetch(t, ahead);
             ahead.next(n_kc, n_chunks);
         }
-        int f_limb = -1;
-        u64 f256[4], f256q[4];  // 2^(8b) mod q_l, b = 1, 2, 3, 4, with Shoup companions
+        int f_limb = -1, q_bits = 0;
+        bool near_pow2 = false;
+        u64 f256[1], f256q[1];  // 2^8 mod q_l with its Shoup companion
         Item it{0, 0, 0};
         for (int t = 0; t < n_items; ++t, it.next(n_kc, n_chunks)) {
             const int tile = (int)blockIdx.x + it.tl * (int)gridDim.x;
@@ -662,41 +665,36 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
             const NttTab& T = tabs[lm(l)];
             const u64 q = T.q;
             if (l != f_limb) {
-                const Barrett bm{q, T.mu_hi, T.mu_lo};
-                u64 w = 256 % q;
-#pragma unroll
-                for (int b = 0; b < 4; ++b) {
-                    f256[b] = w;
-                    f256q[b] = shoup_quotient_dev(w, q);
-                    w = mul_barrett(w, 256 % q, bm);
-                }
+                f256[0] = 256 % q;
+                f256q[0] = shoup_quotient_dev(f256[0], q);
+                q_bits = 64 - __clzll(q);
+                near_pow2 = q_bits <= 55 && ((1ull << q_bits) - q) < (1ull << (q_bits - 9));
                 f_limb = l;
             }
-            // B: w_b(Y[c][j]) = 2^(8b) Y mod q; a unit (slot, digit, ciphertext pair, weight half)
-            // writes 4 weights x 2 ciphertexts as 16-byte stores
+            // B: w_b(Y[c][j]) == 2^(8b) Y (mod q), lazily reduced below 2^64. A unit is one
+            // (ciphertext, slot, digit); the thread mapping (c & 1, slot, digit & 1 in the low
+            // bits) puts a half-warp's 8-byte stores on distinct banks.
             {
                 const u64* ys = (const u64*)(smem + kOffY + (t & (kRing - 1)) * kYStage);
                 uint8_t* Bs = smem + kOffB + bst * kBStage;
-                for (int w = ptid; w < (n_ct + 1) / 2 * kJc * kTS * 2; w += kProd) {
-                    const int i = w % kTS, jj = (w / kTS) % kJc, bh = (w / (kTS * kJc)) & 1, cp = w / (kTS * kJc * 2);
-                    const int c0 = 2 * cp;
-                    const u64 y0 = ys[(c0 * kJc + jj) * kTS + i];
-                    const u64 y1 = c0 + 1 < n_ct ? ys[((c0 + 1) * kJc + jj) * kTS + i] : 0;
-                    uint8_t* dst = Bs + i * kBSlot + jj * kLboB + cp * kSboB + bh * 64;
+                const int c = ((ptid >> 5) << 1) | (ptid & 1), i = (ptid >> 1) & 3, jj = (ptid >> 3) & 3;
+                if (c < n_ct) {
+                    uint8_t* dst = Bs + i * kBSlot + jj * kLboB + (c >> 1) * kSboB + (c & 1) * 8;
+                    u64 w = ys[(c * kJc + jj) * kTS + i];
+                    if (near_pow2) {
+                        // q in (2^e - 2^(e-9), 2^e), e <= 55: w < 2^(e+1) stays below 2^(e+1)
 #pragma unroll
-                    for (int b = 0; b < 4; ++b) {
-                        // lazily reduced in [0, 2q): the byte-split sum needs only the residue class
-                        u64 v0, v1;
-                        if (bh == 0) {
-                            v0 = b ? mul_shoup_lazy(y0, f256[b - 1], f256q[b - 1], q) : y0;
-                            v1 = b ? mul_shoup_lazy(y1, f256[b - 1], f256q[b - 1], q) : y1;
-                        } else {  // weights 4 .. 7 = 2^32 * (1, 2^8, 2^16, 2^24)
-                            const u64 z0 = mul_shoup_lazy(y0, f256[3], f256q[3], q),
-                                      z1 = mul_shoup_lazy(y1, f256[3], f256q[3], q);
-                            v0 = b ? mul_shoup_lazy(z0, f256[b - 1], f256q[b - 1], q) : z0;
-                            v1 = b ? mul_shoup_lazy(z1, f256[b - 1], f256q[b - 1], q) : z1;
+                        for (int b = 0; b < 8; ++b) {
+                            *(u64*)(dst + b * 16) = w;
+                            const u64 x = w << 8;
+                            w = x - (x >> q_bits) * q;
                         }
-                        *(ulonglong2*)(dst + b * 16) = make_ulonglong2(v0, v1);
+                    } else {
+#pragma unroll
+                        for (int b = 0; b < 8; ++b) {
+                            *(u64*)(dst + b * 16) = w;
+                            w = mul_shoup_lazy(w, f256[0], f256q[0], q);
+                        }
                     }
                 }
             }
@@ -800,8 +798,9 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                         const u64 hi = (hi4 >> 32) + (lo < lo4);                    // < 2^20
                         u64 v = add_mod(reduce_2q(mul_shoup_lazy(lo, 1, one_q, q), q), mul_shoup(hi, r64, r64q, q), q);
                         if (comp == 0 && l < Lq) v = add_mod(v, mul_shoup(es[c * kTS + i], pfl, pfql, q), q);
-                        const u32 cnt =
-                            min(cnt_staged ? s_cnt[c * n_keys + g] : exc_count[(size_t)c * n_keys + g], (u32)cap);
+                        // pairs whose list overflowed are recomputed by the exact fallback: skip them here
+                        u32 cnt = cnt_staged ? s_cnt[c * n_keys + g] : exc_count[(size_t)c * n_keys + g];
+                        if (cnt > (u32)cap) cnt = 0;
                         if (cnt) {
                             const Exc* list = exc + ((size_t)c * n_keys + g) * cap;
                             const u64 ps = psi[lm(l)];

@@ -298,6 +298,20 @@ int32_t ckks_encode(ckks_ctx* ctx, const double* slots, uint64_t* out, uint32_t 
 int32_t ckks_decode(ckks_ctx* ctx, const uint64_t* poly, double* slots, uint32_t n_msg, uint32_t q_limbs,
                     double scale, void* stream);
 
+
+/* Diagonal-rotation stage over several ciphertexts (a stage of a transform
+ * whose vectors span n_in ciphertexts, e.g. the last column stage of a 2-D
+ * FFT over two ciphertexts):
+ *   out[a] = Rescale( sum_{t: terms[t][0] = a} diag_t * rot_{terms[t][2]}(in[terms[t][1]]) )
+ * terms_host [n_terms][3] = (output index, input index, key index, or n_rot
+ * for the unrotated input); diag_ntt [n_terms][q_limbs][N] NTT-prepared, in
+ * term order. Every input is rotated by every key with one hoisted
+ * decomposition. ct_in [n_in][2][q_limbs][N] -> ct_out [n_out][2][q_limbs-1][N].
+ * With n_in = n_out = 1 it is ckks_fft_stage (eblas/prepared_radix4_fft256.rs:744-822). */
+int32_t ckks_fft_stage_multi(ckks_ctx* ctx, const ckks_ksk* const* keys, uint32_t n_rot, const uint32_t* terms_host,
+                             uint32_t n_terms, const uint64_t* diag_ntt, const uint64_t* ct_in, uint32_t n_in,
+                             uint64_t* ct_out, uint32_t n_out, uint32_t q_limbs, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
