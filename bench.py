@@ -383,10 +383,11 @@ ROT_STEPS = [1 << i for i in range(15)] + list(range(3, 37, 2))
 
 
 def rot_config():
-    default = ROT_L == 24 and ROT_NCT == 16 and len(ROT_STEPS) == 32 and ROT_BASE_LOG == 32
-    return {"workload": ("hoisted key-switched rotations, N=2^16, %dx50-bit Q + 3x60-bit P, bounded hybrid-QP "
+    default = (ROT_L == 24 and ROT_NCT == 16 and len(ROT_STEPS) == 32 and ROT_BASE_LOG == 32
+               and ROT_LOG_N == 16)
+    return {"workload": ("hoisted key-switched rotations, N=2^%d, %dx50-bit Q + 3x60-bit P, bounded hybrid-QP "
                          "gadget base 2^%d, %d ct x %d Galois steps%s"
-                         % (ROT_L, ROT_BASE_LOG, ROT_NCT, len(ROT_STEPS),
+                         % (ROT_LOG_N, ROT_L, ROT_BASE_LOG, ROT_NCT, len(ROT_STEPS),
                             "" if default else " (reduced profiling size)")),
             "log_n": ROT_LOG_N, "q_limbs": ROT_L, "p_limbs": ROT_K, "base_log": ROT_BASE_LOG,
             "ciphertexts": ROT_NCT, "galois_steps": ROT_STEPS, "scale": "2^50", "secret": "ternary",
@@ -451,6 +452,11 @@ def bench_rot_gpu(args, world, rank, local):
     mac_bytes = (groups * len(keys) * key_bytes + ROT_NCT * D * LK * n * 8 + ROT_NCT * ROT_L * n * 8
                  + rots * 2 * LK * n * 8)
     peak, kind = peaks()
+    # DRAM traffic per launch: an ncu capture of k_mac_tc on the same limbs,
+    # digits, keys and ciphertexts at N=2^11 read 1.424 GB and wrote 0.488 GB for
+    # 1.804 GB of algorithmic bytes; every term scales with N, so the full launch
+    # moves the same multiple of its algorithmic bytes
+    mac_traffic = mac_bytes * (1.424 + 0.488) / 1.804
     mac_ms = phases["key-switch MAC"]
     achieved = mac_bytes / (mac_ms / 1000.0) / 1e9
     ct_bytes = 2 * ROT_L * n * 8
@@ -465,19 +471,54 @@ def bench_rot_gpu(args, world, rank, local):
     for _ in range(e2e_steps):
         cb.rotate_hoisted_host(ctx, keys, hin, hout)
     e2e_s = max_over_ranks(world, time.perf_counter() - t)
+    # the plain GPU forms of the same rotations, outside the headline timing:
+    # one key switch per (ciphertext, key) with no hoisting (ckks_rotate, CUDA-core
+    # MAC) on a 4-key sample, and the hoisted schedule with the CUDA-core MAC
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sample_keys = keys[:4]
+    o1 = torch.empty_like(cts)
+    for k in sample_keys:
+        cb.rotate(ctx, k, cts, out=o1)
+    torch.cuda.synchronize()
+    e0.record(st)
+    for k in sample_keys:
+        cb.rotate(ctx, k, cts, out=o1)
+    e1.record(st)
+    torch.cuda.synchronize()
+    per_rot = ROT_NCT * len(sample_keys) / (e0.elapsed_time(e1) / 1000.0)
+    ctx.tensor_cores = False
+    step()
+    torch.cuda.synchronize()
+    e0.record(st)
+    step()
+    e1.record(st)
+    torch.cuda.synchronize()
+    cc_value = rots / (e0.elapsed_time(e1) / 1000.0)
+    _, cc_phases = cb.rotate_hoisted_timed(ctx, keys, cts, out=out)
+    ctx.tensor_cores = True
+    torch.cuda.synchronize()
+    plain_gpu = {
+        "per_rotation": {"value": per_rot, "unit": "rotations/s", "path": "ckks_rotate (no hoisting, CUDA-core MAC)",
+                         "sample": "%d ct x %d keys" % (ROT_NCT, len(sample_keys))},
+        "hoisted_cuda_core_mac": {"value": cc_value, "unit": "rotations/s", "path": "ckks_rotate_hoisted, "
+                                  "tensor cores off", "mac_ms_per_step": cc_phases["key-switch MAC"]},
+    }
     line = {
         "metric": "key-switched rotations/s (N=2^16, 24 limbs, hoisted, bit-exact)", "value": value,
         "unit": "rotations/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u64", "data": "synthetic (seeded uniform ciphertexts, GPU-generated keys)", "config": rot_config(),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "peak_kind": kind,
+                     "traffic": mac_traffic, "traffic_source": "ncu capture at N=2^11 scaled by N",
+                     "peak_kind": kind,
                      "kernel": "k_mac_tc (INT8 tcgen05 key-switch MAC, %d digits, keys %.3f GB each, read once "
                                "per %d ct)" % (D, key_bytes / 1e9, min(group, ROT_NCT)),
                      "kernel_ms_per_step": mac_ms, "algorithmic_bytes_per_step": mac_bytes},
         "whole_rotation_roofline": {"bytes_per_rotation": key_bytes + 2 * ct_bytes,
                                     "frac_no_key_reuse": (key_bytes + 2 * ct_bytes) * value / 1e9 / peak},
         "phases_ms_per_step": phases,
+        "tensor_cores": ctx.tensor_cores,
+        "plain_gpu": plain_gpu,
         "e2e": {"value": rots * e2e_steps * world / e2e_s, "unit": "rotations/s",
                 "h2d_bytes_per_step": int(host.nbytes), "d2h_bytes_per_step": int(hout.nbytes),
                 "path": "ckks_rotate_hoisted_host"},
@@ -515,8 +556,8 @@ def rot_cpu_sample(threads, n_keys=2):
                                            threads, P(cts), P(out), threads)
     dt = time.perf_counter() - t
     rots = threads * n_keys
-    return rots / dt, ("%d ciphertexts x %d Galois keys (one ciphertext per thread), N=2^16, 24+3 limbs, "
-                       "base 2^32, %.1f s" % (threads, n_keys, dt))
+    return rots / dt, ("%d ciphertexts x %d Galois keys (one ciphertext per thread), N=2^%d, %d+%d limbs, "
+                       "base 2^%d, %.1f s" % (threads, n_keys, ROT_LOG_N, ROT_L, ROT_K, ROT_BASE_LOG, dt))
 
 
 # ------------------------------------------------- multiply chain (N=2^12)
@@ -922,9 +963,10 @@ def main():
     ap.add_argument("--rot-ct", type=int, default=16)
     ap.add_argument("--rot-keys", type=int, default=32)
     ap.add_argument("--rot-base-log", type=int, default=32)
+    ap.add_argument("--rot-log-n", type=int, default=16)
     args = ap.parse_args()
-    global ROT_L, ROT_NCT, ROT_STEPS, ROT_BASE_LOG
-    ROT_L, ROT_NCT, ROT_BASE_LOG = args.rot_limbs, args.rot_ct, args.rot_base_log
+    global ROT_L, ROT_NCT, ROT_STEPS, ROT_BASE_LOG, ROT_LOG_N
+    ROT_L, ROT_NCT, ROT_BASE_LOG, ROT_LOG_N = args.rot_limbs, args.rot_ct, args.rot_base_log, args.rot_log_n
     ROT_STEPS = ROT_STEPS[:args.rot_keys]
     args.warmup = max(3, args.warmup)
     world, rank, local = dist_setup() if args.impl == "b200" else (

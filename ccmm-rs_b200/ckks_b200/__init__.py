@@ -36,6 +36,8 @@ _SIGS = {
     "ckks_is_prime": (I32, [U64]),
     "ckks_ctx_create": (I32, [U32, u64p, U32, u64p, U32, ctypes.POINTER(VP)]),
     "ckks_ctx_destroy": (I32, [VP]),
+    "ckks_ctx_set_tensor_cores": (I32, [VP, I32]),
+    "ckks_ctx_tensor_cores": (I32, [VP]),
     "ckks_ctx_psi": (I32, [VP, u64p]),
     "ckks_ntt_forward": (I32, [VP, VP, VP, U32, U32, U32, VP]),
     "ckks_ntt_inverse": (I32, [VP, VP, VP, U32, U32, U32, VP]),
@@ -171,6 +173,16 @@ class Context:
         out = np.zeros(len(self.moduli), np.uint64)
         check(lib().ckks_ctx_psi(self.handle, out.ctypes.data_as(u64p)))
         return [int(x) for x in out]
+
+    @property
+    def tensor_cores(self):
+        """True when bounded hoisted rotations run their key-switch MAC on the
+        INT8 tensor cores (enabled by default where the device has them)."""
+        return bool(lib().ckks_ctx_tensor_cores(self.handle))
+
+    @tensor_cores.setter
+    def tensor_cores(self, enable):
+        check(lib().ckks_ctx_set_tensor_cores(self.handle, 1 if enable else 0))
 
     def close(self):
         if getattr(self, "handle", None):

@@ -295,6 +295,7 @@ int32_t ckks_ksk_download(const ckks_ksk* key, uint64_t* entries_host) {
 
 int32_t ckks_ksk_destroy(ckks_ksk* key) {
     if (!key) return CKKS_OK;
+    keyset_forget_key(key);
     if (key->d_entries) cudaFree(key->d_entries);
     if (key->d_block_const) cudaFree(key->d_block_const);
     delete key;

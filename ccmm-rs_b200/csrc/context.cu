@@ -373,11 +373,23 @@ int32_t ckks_primes_below_bits(uint32_t bits, uint32_t degree, uint32_t count, u
     return CKKS_OK;
 }
 
+int32_t ckks_ctx_set_tensor_cores(ckks_ctx* ctx, int32_t enable) {
+    CKKS_CHECK_ARG(ctx != nullptr, "ckks_ctx_set_tensor_cores: ctx is null");
+    ctx->tensor_cores = enable != 0;
+    return CKKS_OK;
+}
+
+int32_t ckks_ctx_tensor_cores(const ckks_ctx* ctx) {
+    if (!ctx) return 0;
+    return ctx->tensor_cores && tc_enabled() ? 1 : 0;
+}
+
 int32_t ckks_ctx_destroy(ckks_ctx* ctx) {
     if (!ctx) return CKKS_OK;
     cudaDeviceSynchronize();
     gadget_release_ctx(ctx);
     embed_release_ctx(ctx);
+    keyset_release_ctx(ctx);
     if (ctx->d_tabs) cudaFree(ctx->d_tabs);
     if (ctx->d_table_mem) cudaFree(ctx->d_table_mem);
     if (ctx->d_const_mem) cudaFree(ctx->d_const_mem);

@@ -65,6 +65,9 @@ struct ckks_ctx {
     u64* d_const_mem = nullptr;
     ModDownConst mod_down{};
     GarnerQ garner{};
+    // key-switch MAC of bounded hoisted rotations: tcgen05 INT8 tensor cores
+    // (when the device has them) or the CUDA-core split-accumulator form
+    bool tensor_cores = true;
 };
 
 // ---------------------------------------------------------------- errors
@@ -114,6 +117,19 @@ int32_t ntt_forward_launch_map(ckks_ctx* ctx, const u64* in, u64* out, u32 n_pol
                                cudaStream_t st);
 int32_t ntt_inverse_launch_map(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, LimbMap lm, u32 limb_count,
                                cudaStream_t st);
+// Optional epilogue of the inverse transform for key-switch accumulators
+// [n_ct][n_keys][2][limbs][N]: the b component (even poly p) of ciphertext
+// c = p / (2 n_keys) gets P b_c added on its first q_limbs limbs, with
+// b_c = b + c * b_stride ([q_limbs][N], coefficient domain) and (P mod q_l,
+// Shoup) = (pf[l], pf_q[l]). ModDown then yields ModDown(x) + b_c exactly.
+struct InvBase {
+    const u64* b = nullptr;
+    size_t b_stride = 0;
+    u32 n_keys = 1, q_limbs = 0;
+    const u64 *pf = nullptr, *pf_q = nullptr;
+};
+int32_t ntt_inverse_base_launch(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, LimbMap lm, u32 limb_count,
+                                const InvBase& ib, cudaStream_t st);
 inline LimbMap LimbMap::qp(const ckks_ctx* c, u32 q_limbs) { return LimbMap{0, (int)q_limbs, (int)c->L}; }
 // Stream-ordered workspace (cudaMallocAsync / cudaFreeAsync on `st`).
 template <typename T>

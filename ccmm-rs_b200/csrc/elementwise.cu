@@ -77,12 +77,18 @@ __global__ void k_rescale(const u64* __restrict__ in, u64* __restrict__ out, con
 // s = t k^-1 mod 2N (negated when s >= N), so the stores are coalesced and the
 // reads gather within one polynomial. ModDown commutes exactly with that
 // signed permutation because P is odd.
+// KT > 0 fixes the number of auxiliary limbs at compile time (KT == 0: md.K at
+// run time). The Q-limb gathers are issued kBatch at a time so each thread keeps
+// several independent loads in flight (the reads are scattered under sigma).
+template <int KT>
 __global__ void k_mod_down(const u64* __restrict__ in, u64* __restrict__ out, ModDownConst md, int q_limbs,
                            int log_n, const u64* __restrict__ exps_inv, int n_keys) {
+    constexpr int kBatch = 8;
     const u32 n = 1u << log_n;
     const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
-    const int K = md.K;
+    const int K = KT > 0 ? KT : md.K;
+    constexpr int KM = KT > 0 ? KT : kMaxAux;
     const size_t src = (size_t)blockIdx.y * (q_limbs + K) << log_n;
     const size_t dst = (size_t)blockIdx.y * q_limbs << log_n;
     u32 c = t;
@@ -92,28 +98,52 @@ __global__ void k_mod_down(const u64* __restrict__ in, u64* __restrict__ out, Mo
         flip = s >= n;
         c = (u32)(s & (n - 1));
     }
-    u64 v[kMaxAux];
-    for (int i = 0; i < K; ++i) {
-        const u64 p = md.p[i];
-        u64 x = in[src + ((size_t)(q_limbs + i) << log_n) + c];
-        u64 acc = 0;
-        for (int j = 0; j < i; ++j) acc = add_mod(acc, mul_shoup(v[j], md.pp[i][j], md.pp_q[i][j], p), p);
-        v[i] = mul_shoup(sub_mod(x, acc, p), md.pinv[i], md.pinv_q[i], p);
+    const u64* x = in + src + c;
+    u64 v[KM];
+#pragma unroll
+    for (int i = 0; i < KM; ++i)
+        if (i < K) v[i] = __ldg(x + ((size_t)(q_limbs + i) << log_n));
+#pragma unroll
+    for (int i = 0; i < KM; ++i) {
+        if (i < K) {
+            const u64 p = md.p[i];
+            u64 acc = 0;
+#pragma unroll
+            for (int j = 0; j < i; ++j) acc = add_mod(acc, mul_shoup(v[j], md.pp[i][j], md.pp_q[i][j], p), p);
+            v[i] = mul_shoup(sub_mod(v[i], acc, p), md.pinv[i], md.pinv_q[i], p);
+        }
     }
     // centered: value > floor(P/2) -> negative (lexicographic mixed-radix compare)
-    bool neg = false;
-    for (int i = K - 1; i >= 0; --i) {
-        if (v[i] != md.half[i]) { neg = v[i] > md.half[i]; break; }
+    bool neg = false, decided = false;
+#pragma unroll
+    for (int i = KM - 1; i >= 0; --i) {
+        if (i < K && !decided && v[i] != md.half[i]) {
+            neg = v[i] > md.half[i];
+            decided = true;
+        }
     }
-    for (int i = 0; i < q_limbs; ++i) {
-        const u64 qi = md.q[i];
-        u64 r = 0;
-        for (int j = 0; j < K; ++j)
-            r = add_mod(r, mul_shoup(v[j], md.pre[i * kMaxAux + j], md.pre_q[i * kMaxAux + j], qi), qi);
-        if (neg) r = sub_mod(r, md.p_mod_q[i], qi);
-        u64 d = sub_mod(in[src + ((size_t)i << log_n) + c], r, qi);
-        u64 o = mul_shoup(d, md.pinv_mod_q[i], md.pinv_mod_q_q[i], qi);
-        out[dst + ((size_t)i << log_n) + t] = flip ? neg_mod(o, qi) : o;
+    u64* o = out + dst + t;
+    for (int i0 = 0; i0 < q_limbs; i0 += kBatch) {
+        u64 xin[kBatch];
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u)
+            if (i0 + u < q_limbs) xin[u] = __ldg(x + ((size_t)(i0 + u) << log_n));
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u) {
+            const int i = i0 + u;
+            if (i < q_limbs) {
+                const u64 qi = md.q[i];
+                const u64* pre = md.pre + (size_t)i * kMaxAux;
+                const u64* pre_q = md.pre_q + (size_t)i * kMaxAux;
+                u64 r = 0;
+#pragma unroll
+                for (int j = 0; j < KM; ++j)
+                    if (j < K) r = add_mod(r, mul_shoup(v[j], pre[j], pre_q[j], qi), qi);
+                if (neg) r = sub_mod(r, md.p_mod_q[i], qi);
+                const u64 w = mul_shoup(sub_mod(xin[u], r, qi), md.pinv_mod_q[i], md.pinv_mod_q_q[i], qi);
+                o[(size_t)i << log_n] = flip ? neg_mod(w, qi) : w;
+            }
+        }
     }
 }
 
@@ -180,9 +210,15 @@ int32_t mod_down_sigma_multi(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys
     for (u32 p0 = 0; p0 < n_polys; p0 += chunk) {
         const u32 cnt = (n_polys - p0) < chunk ? (n_polys - p0) : chunk;
         dim3 g((ctx->n + kT - 1) / kT, cnt);
-        k_mod_down<<<g, kT, 0, st>>>(in + ((size_t)p0 * (q_limbs + ctx->K) << ctx->log_n),
-                                     out + ((size_t)p0 * q_limbs << ctx->log_n), ctx->mod_down, q_limbs, ctx->log_n,
-                                     d_exps_inv, n_keys ? n_keys : 1);
+        const u64* pin = in + ((size_t)p0 * (q_limbs + ctx->K) << ctx->log_n);
+        u64* pout = out + ((size_t)p0 * q_limbs << ctx->log_n);
+        const int nk = n_keys ? (int)n_keys : 1;
+        switch (ctx->K) {
+            case 1: k_mod_down<1><<<g, kT, 0, st>>>(pin, pout, ctx->mod_down, q_limbs, ctx->log_n, d_exps_inv, nk); break;
+            case 2: k_mod_down<2><<<g, kT, 0, st>>>(pin, pout, ctx->mod_down, q_limbs, ctx->log_n, d_exps_inv, nk); break;
+            case 3: k_mod_down<3><<<g, kT, 0, st>>>(pin, pout, ctx->mod_down, q_limbs, ctx->log_n, d_exps_inv, nk); break;
+            default: k_mod_down<0><<<g, kT, 0, st>>>(pin, pout, ctx->mod_down, q_limbs, ctx->log_n, d_exps_inv, nk);
+        }
     }
     CKKS_CUDA_TRY(cudaGetLastError());
     return CKKS_OK;

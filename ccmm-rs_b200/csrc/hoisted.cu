@@ -20,6 +20,12 @@
 // and are gathered through the permutation.
 #include "keyswitch.cuh"
 
+#include <algorithm>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <vector>
+
 namespace {
 
 constexpr int kT = 256;
@@ -76,17 +82,16 @@ __global__ void k_hoist_exceptions(const i64* __restrict__ digits, size_t dig_st
 }
 
 // MAC in the permuted index s = pi_g(k) (keys are stored permuted):
-// acc'[c][g][0][l][s] = pf_l Bhat_c[l][s] + sum_j Yhat_c[j][l][s] key'_g[j][l][0][s] + corrections
-// acc'[c][g][1][l][s] =                      sum_j Yhat_c[j][l][s] key'_g[j][l][1][s] + corrections
-// so acc = perm_g(acc'); the caller applies sigma_g after the inverse transform.
+// acc'[c][g][comp][l][s] = sum_j Yhat_c[j][l][s] key'_g[j][l][comp][s] + corrections
+// so acc = perm_g(acc'); the caller applies sigma_g after the inverse transform
+// and the inverse transform adds the base term P b in the coefficient domain
+// (InvBase), so P NTT(b) is not accumulated here.
 // Every load is contiguous: keys stream once per group (evict-first), the
 // group's digit transforms are re-read from L2 by every key.
 template <int G>
 __global__ void __launch_bounds__(kT) k_mac_hoisted(const u64* __restrict__ Yhat, size_t y_stride,
-                                                    const u64* __restrict__ Bhat, size_t b_stride,
                                                     const u64* const* __restrict__ keys,
-                                                    const u64* __restrict__ exps_inv, const u64* __restrict__ pf,
-                                                    const u64* __restrict__ pf_q, u64* __restrict__ acc,
+                                                    const u64* __restrict__ exps_inv, u64* __restrict__ acc,
                                                     const NttTab* __restrict__ tabs, LimbMap lm, int n_ct, int n_keys,
                                                     int Lq, int LK, int D, int log_n, const Exc* __restrict__ exc,
                                                     const u32* __restrict__ exc_count, int cap,
@@ -130,9 +135,8 @@ __global__ void __launch_bounds__(kT) k_mac_hoisted(const u64* __restrict__ Yhat
         ab[c].fold(q, mh, ml);
         aa[c].fold(q, mh, ml);
         u64 b = ab[c].lo, a = aa[c].lo;
-        if (l < Lq) b = add_mod(b, mul_shoup(__ldg(Bhat + c * b_stride + ((size_t)l << log_n) + s), pf[l], pf_q[l], q), q);
         u32 cnt = exc_count[(size_t)c * n_keys + g];
-            if (cnt > (u32)cap) cnt = 0;  // overflowed: recomputed by the exact fallback
+        if (cnt > (u32)cap) cnt = 0;  // overflowed: recomputed by the exact fallback
         if (cnt) {
             const Exc* list = exc + ((size_t)c * n_keys + g) * cap;
             const u64 ps = psi[lm(l)];
@@ -203,10 +207,8 @@ constexpr int kS = 64, kLanes = 4, kU = 4;
 
 template <int G>
 __global__ void __launch_bounds__(kS * kLanes, 2) k_mac_tiled(const u64* __restrict__ Yhat, size_t y_stride,
-                                                           const u64* __restrict__ Bhat, size_t b_stride,
                                                            const u64* const* __restrict__ keys,
                                                            const u64* __restrict__ exps_inv,
-                                                           const u64* __restrict__ pf, const u64* __restrict__ pf_q,
                                                            u64* __restrict__ acc, const NttTab* __restrict__ tabs,
                                                            LimbMap lm, int n_ct, int n_keys, int Lq, int LK, int D,
                                                            int log_n, const Exc* __restrict__ exc,
@@ -236,12 +238,6 @@ __global__ void __launch_bounds__(kS * kLanes, 2) k_mac_tiled(const u64* __restr
         }
     __syncthreads();
     const Barrett bm{q, mh, ml};
-    u64 bterm[G];
-#pragma unroll
-    for (int c = 0; c < G; ++c)
-        bterm[c] = (c < n_ct && l < Lq)
-                       ? mul_shoup(__ldg(Bhat + c * b_stride + ((size_t)l << log_n) + s), pf[l], pf_q[l], q)
-                       : 0;
     const size_t jstride = ((size_t)LK * 2) << log_n;
     for (int g = lane; g < n_keys; g += kLanes) {
         const u64* key = keys[g];
@@ -287,7 +283,7 @@ __global__ void __launch_bounds__(kS * kLanes, 2) k_mac_tiled(const u64* __restr
             if (c >= n_ct) break;
             ab[c].fold(q, one_q, r1, r1q, r2, r2q);
             aa[c].fold(q, one_q, r1, r1q, r2, r2q);
-            u64 b = add_mod(ab[c].s0, bterm[c], q), a = aa[c].s0;
+            u64 b = ab[c].s0, a = aa[c].s0;
             u32 cnt = exc_count[(size_t)c * n_keys + g];
             if (cnt > (u32)cap) cnt = 0;  // overflowed: recomputed by the exact fallback
             if (cnt) {
@@ -312,6 +308,8 @@ __global__ void __launch_bounds__(kS * kLanes, 2) k_mac_tiled(const u64* __restr
     }
 }
 
+}  // namespace
+
 // The tensor-core MAC runs on compute capability 10.0 devices (the library is
 // built for sm_100a only).
 bool tc_enabled() {
@@ -325,6 +323,129 @@ bool tc_enabled() {
     }
     return cached == 1;
 }
+
+namespace {
+
+// ------------------------------------------------------------ packed key sets
+// The tensor-core MAC reads the A operand of an item (tile of 4 slots of one
+// limb, 32-key chunk, 4-digit chunk) as one contiguous block, brought into
+// shared memory by a single bulk copy. Blocks are in the MAC's shared-memory
+// image (K-major, no swizzle): row group rg (8 rows = 4 keys x 2 components) of
+// 1 KB, then slot i (256 B), K chunk kk (128 B: digits 2 kk, 2 kk + 1), row
+// (16 B), digit (8 B). Only the row groups of present keys are stored. A set is
+// packed once per ordered list of Galois keys and cached per context until a
+// key of the set or the context is destroyed.
+struct PackedSet {
+    std::vector<const ckks_ksk*> keys;
+    u64* d = nullptr;
+    u32 rg = 0, n_kc = 0, n_chunks = 0;
+};
+std::mutex g_sets_mu;
+std::map<const ckks_ctx*, std::vector<std::unique_ptr<PackedSet>>> g_sets;
+
+__global__ void k_pack_keys(const u64* const* __restrict__ keys, int n_keys, int LK, int D, int log_n, u32 rg,
+                            u32 n_kc, u32 n_chunks, u64* __restrict__ out, size_t total) {
+    const u32 block_words = rg * 128;
+    const u32 tiles_s = (1u << log_n) >> 2;
+    for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < total; w += (size_t)gridDim.x * blockDim.x) {
+        const size_t block = w / block_words;
+        const u32 off = (u32)(w - block * block_words);
+        const u32 r = off & 127;
+        const u32 m = ((off >> 7) << 3) | ((r >> 1) & 7);
+        const u32 i = r >> 5, jj = (((r >> 4) & 1) << 1) | (r & 1);
+        const u32 ch = (u32)(block % n_chunks);
+        const size_t rest = block / n_chunks;
+        const u32 kc = (u32)(rest % n_kc);
+        const size_t tile = rest / n_kc;
+        const u32 l = (u32)(tile / tiles_s), s = (u32)(tile % tiles_s) * 4 + i;
+        const u32 g = kc * 32 + (m >> 1), comp = m & 1, j = ch * 4 + jj;
+        out[w] = (g < (u32)n_keys && j < (u32)D)
+                     ? __ldg(keys[g] + (((((size_t)j * LK + l) * 2 + comp) << log_n) + s))
+                     : 0;
+    }
+}
+
+// The packed set of these keys, packed on first use when device memory allows
+// (null otherwise: the caller takes the CUDA-core MAC).
+const PackedSet* packed_set_get(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_keys, cudaStream_t st) {
+    std::lock_guard<std::mutex> lock(g_sets_mu);
+    std::vector<std::unique_ptr<PackedSet>>& sets = g_sets[ctx];
+    for (const auto& p : sets)
+        if (p->keys.size() == n_keys && std::equal(p->keys.begin(), p->keys.end(), keys)) return p.get();
+    const ckks_ksk* k0 = keys[0];
+    const u32 LK = ksk_limbs(k0), n = ctx->n;
+    std::unique_ptr<PackedSet> pp(new PackedSet);
+    PackedSet& p = *pp;
+    p.keys.assign(keys, keys + n_keys);
+    p.n_kc = (n_keys + 31) / 32;
+    p.n_chunks = (k0->D + 3) / 4;
+    p.rg = n_keys >= 32 ? 8 : (n_keys + 3) / 4;
+    const size_t total = (size_t)LK * (n / 4) * p.n_kc * p.n_chunks * p.rg * 128;
+    // unused stream-ordered workspace memory goes back to the device first
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess) {
+        cudaStreamSynchronize(st);
+        cudaMemPoolTrimTo(pool, 0);
+    }
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return nullptr;
+    // keep a quarter of the device free for the rotation workspaces
+    const size_t bytes = total * sizeof(u64);
+    if (bytes > free_b || free_b - bytes < total_b / 4) return nullptr;
+    std::vector<const u64*> hptr(n_keys);
+    for (u32 g = 0; g < n_keys; ++g) hptr[g] = keys[g]->d_entries;
+    const u64** d_ptr = nullptr;
+    if (cudaMalloc(&p.d, bytes) != cudaSuccess || cudaMalloc(&d_ptr, n_keys * sizeof(u64*)) != cudaSuccess ||
+        cudaMemcpy(d_ptr, hptr.data(), n_keys * sizeof(u64*), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaGetLastError();
+        if (p.d) cudaFree(p.d);
+        if (d_ptr) cudaFree(d_ptr);
+        return nullptr;
+    }
+    k_pack_keys<<<148 * 16, 256, 0, st>>>(d_ptr, (int)n_keys, (int)LK, (int)k0->D, (int)ctx->log_n, p.rg, p.n_kc,
+                                          p.n_chunks, p.d, total);
+    // ready for every stream of the context
+    const bool ok = cudaGetLastError() == cudaSuccess && cudaStreamSynchronize(st) == cudaSuccess;
+    cudaFree(d_ptr);
+    if (!ok) {
+        cudaFree(p.d);
+        return nullptr;
+    }
+    sets.push_back(std::move(pp));
+    return sets.back().get();
+}
+
+}  // namespace
+
+void keyset_release_ctx(const ckks_ctx* ctx) {
+    std::lock_guard<std::mutex> lock(g_sets_mu);
+    auto it = g_sets.find(ctx);
+    if (it == g_sets.end()) return;
+    for (auto& p : it->second) cudaFree(p->d);
+    g_sets.erase(it);
+}
+
+void keyset_forget_key(const ckks_ksk* key) {
+    std::lock_guard<std::mutex> lock(g_sets_mu);
+    auto it = g_sets.find(key->ctx);
+    if (it == g_sets.end()) return;
+    auto& sets = it->second;
+    bool synced = false;
+    for (size_t i = 0; i < sets.size();) {
+        if (std::find(sets[i]->keys.begin(), sets[i]->keys.end(), key) != sets[i]->keys.end()) {
+            if (!synced) {
+                cudaDeviceSynchronize();  // no launch may still read the set
+                synced = true;
+            }
+            cudaFree(sets[i]->d);
+            sets.erase(sets.begin() + i);
+        } else {
+            ++i;
+        }
+    }
+}
+
+namespace {
 
 // CUDA-event phase timer (the analogue of the reference's HybridRotationTiming,
 // ckks/hybrid_rns_galois_key.rs:323-336). Phases accumulate over groups.
@@ -382,17 +503,20 @@ struct PhaseTimer {
 // order. Both use the no-swizzle canonical layout (8 x 16-byte core matrices).
 //
 // Warp roles of a persistent CTA (one per SM, all 512 TMEM columns):
-//   warps 4-11 producers: cp.async of the key words and digit transforms of
-//              item t + 6 into an 8-deep ring, then the B operand of item t;
+//   warps 4-11 producers in two groups of four: group p owns the items t with
+//              t % 2 == p (B stage p); for item t it issues the bulk copy of
+//              the packed key block and the cp.async of the digit transforms
+//              of item t + 6 into an 8-deep ring, then builds the B operand of
+//              item t;
 //   warp 12    issues the MMAs of item t once its operands are ready;
 //   warps 0-3  epilogue: TMEM -> exact combine of the 8 planes, reduction mod
-//              q, base term and sparse carry corrections, stores.
+//              q and sparse carry corrections, stores.
 // An item is (tile of 4 slots of one limb, key chunk, 4-digit chunk); the
-// accumulators of consecutive (tile, key chunk) units alternate between TMEM
-// lanes 0-15 and 16-31 of every subpartition (the two M = 64 halves), so the
-// epilogue of one unit overlaps the MMAs of the next. Stages are handed over
-// with mbarriers (ready, empty, full, free); every wait is bounded and on a
-// timeout the kernel records an error, drains and frees its TMEM.
+// accumulators of consecutive (tile, key chunk) units alternate between two
+// TMEM column halves, so the epilogue of one unit overlaps the MMAs of the
+// next. Stages are handed over with mbarriers (ready, empty, full, free);
+// every wait is bounded and on a timeout the kernel records an error, drains
+// and frees its TMEM.
 namespace tc {
 
 constexpr int kTS = 4;            // slots per tile
@@ -401,29 +525,28 @@ constexpr int kKeys = 32;         // keys per pass (M = 2 kKeys = 64)
 constexpr int kJc = 4;            // digits per chunk (K = 32 bytes)
 constexpr int kRing = 8;          // A / Y prefetch ring depth
 constexpr int kAhead = 6;         // items fetched ahead
-constexpr int kBStages = 2;       // B operand stages (kRing - kAhead)
+constexpr int kBStages = 2;       // B operand stages (kRing - kAhead), one per producer group
 constexpr int kProdWarp0 = 4, kMmaWarp = 12;
 constexpr int kThreads = 416;     // 13 warps: 4 epilogue, 8 producer, 1 MMA
-constexpr int kProd = 256, kEpi = 128;
-// Strides are padded (slot and digit strides off multiples of 128 B) so the
-// shared-memory stores of a warp spread over the banks.
-constexpr u32 kSboA = 256, kLboA = 128;        // A: row groups of 8 x 32 B, 16-byte K chunks
+constexpr int kGrp = 128, kEpi = 128;          // threads per producer group, epilogue threads
+constexpr int kBarGrp0 = 1, kBarEpi = 3;  // named barriers: producer groups 1, 2; epilogue 3
+// A (packed key block, bulk-copied): row groups of 1 KB, slot i at 256 i, K
+// chunks 128 B apart. B strides are padded (slot and digit strides off
+// multiples of 128 B) so the producers' shared-memory stores spread over the banks.
+constexpr u32 kSboA = 1024, kLboA = 128, kASlot = 256;
 constexpr u32 kSboB = 128, kLboB = 1088;       // B: ciphertext pairs, digits
-constexpr u32 kASlot = 2080;                   // 64 rows x 32 B (+32)
 constexpr u32 kBSlot = 4368;                   // 4 digits x 8 weights x 128 B (+padding)
-constexpr u32 kAStage = kTS * kASlot;          // 8320
+constexpr u32 kAStage = 8192;                  // 8 row groups
 constexpr u32 kYStage = kCt * kJc * kTS * 8;   // 2048: Y words [c][jj][i]
 constexpr u32 kBStage = kTS * kBSlot;          // 17472
-constexpr u32 kOffY = kRing * kAStage;                     // 66560
-constexpr u32 kOffB = kOffY + kRing * kYStage;             // 82944
-constexpr u32 kOffE = kOffB + kBStages * kBStage;          // 117888: epilogue staging ring
-constexpr u32 kEStage = (kCt * kTS + 4) * 8;               // base terms [c][i] + pf, pf_q
-constexpr int kERing = 12;                                 // tiles whose staging may be live
-constexpr u32 kOffCnt = kOffE + kERing * kEStage;          // correction counts [c][g], g < kCntKeys
+constexpr u32 kOffY = kRing * kAStage;                     // 65536
+constexpr u32 kOffB = kOffY + kRing * kYStage;             // 81920
+constexpr u32 kOffCnt = kOffB + kBStages * kBStage;        // 116864: correction counts [c][g], g < kCntKeys
 constexpr int kCntKeys = 256;
-constexpr u32 kSmemBytes = kOffCnt + kCt * kCntKeys * 4;   // 140,800 B: one CTA per SM
+constexpr u32 kSmemBytes = kOffCnt + kCt * kCntKeys * 4;   // 133,248 B: one CTA per SM
 constexpr u32 kTmemCols = 512;
-static_assert(kBStages == kRing - kAhead, "B stages follow the ring");
+static_assert(kBStages == kRing - kAhead && kBStages == 2, "B stages follow the ring, one per producer group");
+static_assert(kAhead % 2 == 0, "a group prefetches its own items");
 constexpr long long kSpin = 1ll << 22;         // bounded waits (iterations)
 
 __device__ __forceinline__ u32 smem_u32(const void* p) { return (u32)__cvta_generic_to_shared(p); }
@@ -493,13 +616,14 @@ __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_grou
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
-
 // 32 TMEM lanes x 32 columns: lane L of the warp gets columns 0 .. 31 of lane L.
+// The wait is part of the same statement, so no use of r can be scheduled
+// before the load has completed.
 __device__ __forceinline__ void tmem_ld32(u32 taddr, u32 (&r)[32]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
           "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
           "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
@@ -525,20 +649,22 @@ struct Item {
 }  // namespace tc
 
 // Same arguments and results as k_mac_tiled for bounded keys (up to 16
-// ciphertexts per call, any number of keys, D <= 4096, N >= 4).
+// ciphertexts per call, any number of keys, D <= 4096, N >= 4); the A operand
+// comes from the packed set of the keys (rg row groups per block).
 __global__ void __launch_bounds__(tc::kThreads, 1)
-    k_mac_tc(const u64* __restrict__ Yhat, size_t y_stride, const u64* __restrict__ Bhat, size_t b_stride,
-             const u64* const* __restrict__ keys, const u64* __restrict__ exps_inv, const u64* __restrict__ pf,
-             const u64* __restrict__ pf_q, u64* __restrict__ acc, const NttTab* __restrict__ tabs, LimbMap lm,
-             int n_ct, int n_keys, int Lq, int LK, int D, int log_n, const Exc* __restrict__ exc,
+    k_mac_tc(const u64* __restrict__ Yhat, size_t y_stride, const u64* __restrict__ packed, int rg,
+             const u64* const* __restrict__ keys,
+             const u64* __restrict__ exps_inv, u64* __restrict__ acc, const NttTab* __restrict__ tabs, LimbMap lm,
+             int n_ct, int n_keys, int LK, int D, int log_n, const Exc* __restrict__ exc,
              const u32* __restrict__ exc_count, int cap, const u64* __restrict__ psi, int* __restrict__ err) {
     using namespace tc;
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ u32 s_tmem;
     __shared__ int s_abort;
-    // ready / empty: B stages (producers -> MMA, MMA -> producers);
-    // full / free: TMEM accumulator halves (MMA -> epilogue, epilogue -> MMA)
-    __shared__ __align__(8) uint64_t s_ready[kBStages], s_empty[kBStages], s_full[2], s_free[2];
+    // ready / empty: B stages (producer group -> MMA, MMA -> producer group);
+    // full / free: TMEM accumulator halves (MMA -> epilogue, epilogue -> MMA);
+    // afull: A ring slots (bulk copy -> MMA)
+    __shared__ __align__(8) uint64_t s_ready[kBStages], s_empty[kBStages], s_full[2], s_free[2], s_afull[kRing];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const u32 n = 1u << log_n;
     const int n_tiles_s = (int)(n / kTS), lts = log_n - 2;  // tiles per limb (a power of two)
@@ -560,6 +686,8 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_full[i])), "r"(1));
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_free[i])), "r"(1));
         }
+        for (int i = 0; i < kRing; ++i)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_afull[i])), "r"(1));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == kMmaWarp) {
@@ -569,11 +697,12 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     }
     // zero the operand rings once: A rows of absent keys and B columns of
     // absent ciphertexts stay zero; stage the correction counts
-    for (u32 i = tid; i < kOffE / 16; i += kThreads) ((uint4*)smem)[i] = make_uint4(0, 0, 0, 0);
+    for (u32 i = tid; i < kOffCnt / 16; i += kThreads) ((uint4*)smem)[i] = make_uint4(0, 0, 0, 0);
     u32* s_cnt = (u32*)(smem + kOffCnt);
     if (cnt_staged)
         for (int w = tid; w < kCt * n_keys; w += kThreads)
             s_cnt[w] = w / n_keys < n_ct ? exc_count[(size_t)(w / n_keys) * n_keys + w % n_keys] : 0u;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // zeros before the bulk copies
     fence_before();
     __syncthreads();
     fence_after();
@@ -583,76 +712,60 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     if (warp >= kProdWarp0 && warp < kMmaWarp) {
         // ------------------------------------------------------------ producers
         const int ptid = tid - kProdWarp0 * 32;
-        // A copies: producer thread ptid owns slot pi, digit pjj and component pcomp of the
-        // keys pg0 + 8 r (r < 4); Y copies: slot pi, digit pjj of ciphertext ptid / 16.
-        static_assert(kProd == 256 && kKeys == 32 && kTS * kJc * 2 * 8 == kProd, "producer work split");
-        const int pi = ptid & 3, pjj = (ptid >> 2) & 3, pcomp = (ptid >> 4) & 1, pg0 = ptid >> 5;
-        u32 a_dst[4];
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            const int m = 2 * (pg0 + 8 * r) + pcomp;
-            a_dst[r] = pi * kASlot + (m >> 3) * kSboA + (pjj >> 1) * kLboA + (m & 7) * 16 + (pjj & 1) * 8;
-        }
-        const int yc = ptid >> 4;  // ciphertext of this thread's Y copy (kCt * kJc * kTS == kProd)
-        const u64* kp[4] = {nullptr, nullptr, nullptr, nullptr};
-        int kp_kc = -1;
+        const int grp = ptid / kGrp, gtid = ptid % kGrp, bar = kBarGrp0 + grp;
+        // A: one bulk copy of the item's packed key block (thread 0 of the group);
+        // Y copies: slot pi, digit pjj of the ciphertexts gtid / 16 and
+        // gtid / 16 + 8 (Y word gtid and gtid + 128 of the stage).
+        static_assert(kGrp == 128 && kTS * kJc * 8 == kGrp, "producer work split");
+        const int pi = gtid & 3, pjj = (gtid >> 2) & 3;
+        const int yc = gtid >> 4;
+        const u32 a_bytes = (u32)rg * 1024u;
+        int last_issued = -1;  // last item whose block this thread's group copied
         auto prefetch = [&](int t, const Item& it) {
             if (t < n_items) {
                 const int tile = (int)blockIdx.x + it.tl * (int)gridDim.x;
                 const int l = tile >> lts;
                 const u32 s0 = (u32)(tile & (n_tiles_s - 1)) * kTS;
-                const int g0 = it.kc * kKeys;
-                const int gn = n_keys - g0 < kKeys ? n_keys - g0 : kKeys;
-                if (it.kc != kp_kc) {
-#pragma unroll
-                    for (int r = 0; r < 4; ++r) kp[r] = pg0 + 8 * r < gn ? keys[g0 + pg0 + 8 * r] : keys[0];
-                    kp_kc = it.kc;
+                if (gtid == 0) {
+                    const u64* src = packed + ((((size_t)tile * n_kc + it.kc) * n_chunks + it.ch) * (size_t)rg << 7);
+                    const u32 bar = smem_u32(&s_afull[t & (kRing - 1)]);
+                    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}\n"
+                                 ::"r"(bar), "r"(a_bytes) : "memory");
+                    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                                 ::"r"(sbase + (u32)(t & (kRing - 1)) * kAStage), "l"(src), "r"(a_bytes), "r"(bar)
+                                 : "memory");
+                    last_issued = t;
                 }
                 const int j = it.ch * kJc + pjj;
                 const bool jok = j < D;
-                const size_t koff = ((((size_t)(jok ? j : 0) * LK + l) * 2 + pcomp) << log_n) + s0 + pi;
-                const u32 a_st = sbase + (u32)(t & (kRing - 1)) * kAStage;
+                const size_t yoff = (((size_t)(jok ? j : 0) * LK + l) << log_n) + s0 + pi;
+                const u32 y_st = sbase + kOffY + (u32)(t & (kRing - 1)) * kYStage;
 #pragma unroll
-                for (int r = 0; r < 4; ++r)
-                    if (pg0 + 8 * r < gn) cp8(a_st + a_dst[r], kp[r] + koff, jok ? 8u : 0u);
-                if (yc < n_ct) {
-                    const u32 y_st = sbase + kOffY + (u32)(t & (kRing - 1)) * kYStage;
-                    cp8(y_st + (u32)ptid * 8, Yhat + yc * y_stride + (((size_t)(jok ? j : 0) * LK + l) << log_n) + s0 + pi,
-                        jok ? 8u : 0u);
-                }
-                if (it.kc == 0 && it.ch == 0) {  // epilogue inputs of this tile: base terms, pf, pf_q
-                    const u32 e_st = sbase + kOffE + (u32)(it.tl % kERing) * kEStage;
-                    const bool ok = l < Lq;
-                    if (ptid < n_ct * kTS)
-                        cp8(e_st + (u32)ptid * 8,
-                            Bhat + (ptid / kTS) * b_stride + ((size_t)(ok ? l : 0) << log_n) + s0 + (ptid % kTS),
-                            ok ? 8u : 0u);
-                    if (ptid == 0) {
-                        cp8(e_st + kCt * kTS * 8, pf + (ok ? l : 0), ok ? 8u : 0u);
-                        cp8(e_st + kCt * kTS * 8 + 8, pf_q + (ok ? l : 0), ok ? 8u : 0u);
-                    }
-                }
+                for (int h = 0; h < 2; ++h)
+                    if (yc + 8 * h < n_ct)
+                        cp8(y_st + (u32)(gtid + kGrp * h) * 8, Yhat + (yc + 8 * h) * y_stride + yoff, jok ? 8u : 0u);
             }
             cp_commit();
         };
-        Item ahead{0, 0, 0};
-        for (int t = 0; t < kAhead; ++t) {
-            prefetch(t, ahead);
+        Item it{0, 0, 0};
+        if (grp) it.next(n_kc, n_chunks);
+        Item ahead = it;
+        for (int k = 0; k < kAhead / 2; ++k) {
+            prefetch(grp + 2 * k, ahead);
+            ahead.next(n_kc, n_chunks);
             ahead.next(n_kc, n_chunks);
         }
         int f_limb = -1, q_bits = 0;
         bool near_pow2 = false;
-        u64 f256[1], f256q[1];  // 2^8 mod q_l with its Shoup companion
-        Item it{0, 0, 0};
-        for (int t = 0; t < n_items; ++t, it.next(n_kc, n_chunks)) {
+        u64 q = 0, f256 = 0, f256q = 0;  // q_l, 2^8 mod q_l and its Shoup companion
+        for (int t = grp; t < n_items; t += 2) {
             const int tile = (int)blockIdx.x + it.tl * (int)gridDim.x;
             const int l = tile >> lts;
-            const int bst = t & (kBStages - 1);
             bool bad = false;
-            if (t >= kBStages)  // the MMAs of item t - 2 released B stage bst and ring slot (t + kAhead) % kRing
-                bad = !wait_parity(smem_u32(&s_empty[bst]), (u32)(((t / kBStages) - 1) & 1));
-            if (group_any(1, kProd, bad || s_abort)) {  // one decision for all producers
-                if (ptid == 0) {
+            if (t >= kBStages)  // the MMAs of item t - 2 released B stage grp and ring slot (t + kAhead) % kRing
+                bad = !wait_parity(smem_u32(&s_empty[grp]), (u32)(((t >> 1) - 1) & 1));
+            if (group_any(bar, kGrp, bad || s_abort)) {  // one decision for the group
+                if (gtid == 0) {
                     atomicExch(err, 1);
                     s_abort = 1;
                 }
@@ -660,49 +773,62 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
             }
             prefetch(t + kAhead, ahead);
             ahead.next(n_kc, n_chunks);
-            cp_wait<kAhead>();   // this thread's copies of item t have landed
-            named_sync(1, kProd);
-            const NttTab& T = tabs[lm(l)];
-            const u64 q = T.q;
+            ahead.next(n_kc, n_chunks);
+            cp_wait<kAhead / 2>();  // this thread's copies of item t have landed
+            named_sync(bar, kGrp);
             if (l != f_limb) {
-                f256[0] = 256 % q;
-                f256q[0] = shoup_quotient_dev(f256[0], q);
+                q = tabs[lm(l)].q;
+                f256 = 256 % q;
+                f256q = shoup_quotient_dev(f256, q);
                 q_bits = 64 - __clzll(q);
                 near_pow2 = q_bits <= 55 && ((1ull << q_bits) - q) < (1ull << (q_bits - 9));
                 f_limb = l;
             }
-            // B: w_b(Y[c][j]) == 2^(8b) Y (mod q), lazily reduced below 2^64. A unit is one
-            // (ciphertext, slot, digit); the thread mapping (c & 1, slot, digit & 1 in the low
-            // bits) puts a half-warp's 8-byte stores on distinct banks.
+            // B: w_b(Y[c][j]) == 2^(8b) Y (mod q), lazily reduced below 2^64, for the
+            // units (c, slot, digit) and (c + 8, slot, digit): two independent chains.
+            // The thread mapping (c & 1, slot, digit & 1 in the low bits) puts a
+            // half-warp's 8-byte stores on distinct banks.
             {
                 const u64* ys = (const u64*)(smem + kOffY + (t & (kRing - 1)) * kYStage);
-                uint8_t* Bs = smem + kOffB + bst * kBStage;
-                const int c = ((ptid >> 5) << 1) | (ptid & 1), i = (ptid >> 1) & 3, jj = (ptid >> 3) & 3;
-                if (c < n_ct) {
-                    uint8_t* dst = Bs + i * kBSlot + jj * kLboB + (c >> 1) * kSboB + (c & 1) * 8;
-                    u64 w = ys[(c * kJc + jj) * kTS + i];
-                    if (near_pow2) {
-                        // q in (2^e - 2^(e-9), 2^e), e <= 55: w < 2^(e+1) stays below 2^(e+1)
+                const int c = ((gtid >> 5) << 1) | (gtid & 1), i = (gtid >> 1) & 3, jj = (gtid >> 3) & 3;
+                uint8_t* d0 = smem + kOffB + grp * kBStage + i * kBSlot + jj * kLboB + (c >> 1) * kSboB + (c & 1) * 8;
+                uint8_t* d1 = d0 + 4 * kSboB;  // ciphertext c + 8
+                const bool ok0 = c < n_ct, ok1 = c + 8 < n_ct;
+                u64 w0 = ys[(c * kJc + jj) * kTS + i], w1 = ys[((c + 8) * kJc + jj) * kTS + i];
+                if (near_pow2) {
+                    // q in (2^e - 2^(e-9), 2^e), e <= 55: w < 2^(e+1) stays below 2^(e+1)
 #pragma unroll
-                        for (int b = 0; b < 8; ++b) {
-                            *(u64*)(dst + b * 16) = w;
-                            const u64 x = w << 8;
-                            w = x - (x >> q_bits) * q;
-                        }
-                    } else {
+                    for (int b = 0; b < 8; ++b) {
+                        if (ok0) *(u64*)(d0 + b * 16) = w0;
+                        if (ok1) *(u64*)(d1 + b * 16) = w1;
+                        const u64 x0 = w0 << 8, x1 = w1 << 8;
+                        w0 = x0 - (x0 >> q_bits) * q;
+                        w1 = x1 - (x1 >> q_bits) * q;
+                    }
+                } else {
 #pragma unroll
-                        for (int b = 0; b < 8; ++b) {
-                            *(u64*)(dst + b * 16) = w;
-                            w = mul_shoup_lazy(w, f256[0], f256q[0], q);
-                        }
+                    for (int b = 0; b < 8; ++b) {
+                        if (ok0) *(u64*)(d0 + b * 16) = w0;
+                        if (ok1) *(u64*)(d1 + b * 16) = w1;
+                        w0 = mul_shoup_lazy(w0, f256, f256q, q);
+                        w1 = mul_shoup_lazy(w1, f256, f256q, q);
                     }
                 }
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            named_sync(1, kProd);
-            if (ptid == 0) arrive(smem_u32(&s_ready[bst]));
+            named_sync(bar, kGrp);
+            if (gtid == 0) arrive(smem_u32(&s_ready[grp]));
+            it.next(n_kc, n_chunks);
+            it.next(n_kc, n_chunks);
         }
         cp_wait<0>();
+        // bulk copies still in flight (after an abort) land before the CTA exits:
+        // only the group's last kAhead / 2 blocks can be outstanding
+        if (gtid == 0)
+            for (int k = 0; k < kAhead / 2; ++k) {
+                const int u = last_issued - 2 * k;
+                if (u >= 0) wait_parity(smem_u32(&s_afull[u & (kRing - 1)]), (u32)((u >> 3) & 1));
+            }
     } else if (warp == kMmaWarp) {
         // ------------------------------------------------------------- MMA issue
         if (lane == 0) {
@@ -720,6 +846,10 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                         atomicExch(err, 3);
                         s_abort = 1;
                     }
+                }
+                if (!s_abort && !wait_parity(smem_u32(&s_afull[t & (kRing - 1)]), (u32)((t >> 3) & 1))) {
+                    atomicExch(err, 5);
+                    s_abort = 1;
                 }
                 if (s_abort) break;
                 fence_after();
@@ -744,7 +874,8 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
         // -------------------------------------------------------------- epilogue
         const int qd = warp;  // TMEM subpartition (lanes 32 qd ..)
         int r_limb = -1;
-        u64 one_q = 0, r64 = 0, r64q = 0;  // floor(2^64 / q_l), 2^64 mod q_l, Shoup companion
+        u64 q = 0, one_q = 0, r64 = 0, r64q = 0;  // q_l, floor(2^64 / q_l), 2^64 mod q_l, Shoup companion
+        Barrett bm{0, 0, 0};
         for (int u = 0; u < n_units; ++u) {
             const int tl = u / n_kc, kc = u - tl * n_kc;
             const int tile = (int)blockIdx.x + tl * (int)gridDim.x;
@@ -753,7 +884,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
             const int g0 = kc * kKeys;
             const int gn = n_keys - g0 < kKeys ? n_keys - g0 : kKeys;
             const bool bad = !wait_parity(smem_u32(&s_full[u & 1]), (u32)((u >> 1) & 1));
-            if (group_any(2, kEpi, bad || s_abort)) {  // one decision for all epilogue threads
+            if (group_any(kBarEpi, kEpi, bad || s_abort)) {  // one decision for all epilogue threads
                 if (tid == 0) {
                     atomicExch(err, 4);
                     s_abort = 1;
@@ -761,17 +892,15 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                 break;
             }
             fence_after();
-            const NttTab& T = tabs[lm(l)];
-            const u64 q = T.q;
-            const Barrett bm{q, T.mu_hi, T.mu_lo};
             if (l != r_limb) {
+                const NttTab& T = tabs[lm(l)];
+                q = T.q;
+                bm = Barrett{q, T.mu_hi, T.mu_lo};
                 one_q = (~0ull) / q;                 // floor(2^64 / q), q odd
                 r64 = (u64)(-(q * one_q));           // 2^64 mod q
                 r64q = shoup_quotient_dev(r64, q);
                 r_limb = l;
             }
-            const u64* es = (const u64*)(smem + kOffE + (tl % kERing) * kEStage);
-            const u64 pfl = es[kCt * kTS], pfql = es[kCt * kTS + 1];
             // lane L of warp qd: row m = 16 qd + (L % 16); slot 2 p + (L / 16) of slot pair p
             const u32 taddr = tmem + ((u32)(32 * qd) << 16) + (u32)(256 * (u & 1));
             const int m = 16 * qd + (lane & 15);
@@ -784,7 +913,6 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                     u32 r[32];
                     __syncwarp();
                     tmem_ld32(taddr + (u32)(pp * 128 + 8 * cb), r);
-                    tmem_wait_ld();
 #pragma unroll
                     for (int cc = 0; cc < 4; ++cc) {
                         const int c = cb + cc;
@@ -797,7 +925,6 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                         const u64 lo = lo4 + (hi4 << 32);
                         const u64 hi = (hi4 >> 32) + (lo < lo4);                    // < 2^20
                         u64 v = add_mod(reduce_2q(mul_shoup_lazy(lo, 1, one_q, q), q), mul_shoup(hi, r64, r64q, q), q);
-                        if (comp == 0 && l < Lq) v = add_mod(v, mul_shoup(es[c * kTS + i], pfl, pfql, q), q);
                         // pairs whose list overflowed are recomputed by the exact fallback: skip them here
                         u32 cnt = cnt_staged ? s_cnt[c * n_keys + g] : exc_count[(size_t)c * n_keys + g];
                         if (cnt > (u32)cap) cnt = 0;
@@ -821,7 +948,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                 }
             }
             fence_before();
-            named_sync(2, kEpi);
+            named_sync(kBarEpi, kEpi);
             if (tid == 0) arrive(smem_u32(&s_free[u & 1]));
         }
     }
@@ -849,20 +976,22 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
     // Bounded keys use the tensor-core MAC with up to 16 ciphertexts per group
     // (each key word read once per group), as far as device memory allows;
     // otherwise groups of 4 on the CUDA-core tiled MAC.
-    const bool use_tc = bounded && n >= (u32)tc::kTS && D <= 4096 && tc_enabled();
+    bool use_tc = bounded && n >= (u32)tc::kTS && D <= 4096 && ctx->tensor_cores && tc_enabled();
+    // the tensor-core MAC reads the keys' packed set (made on first use)
+    const PackedSet* pset = use_tc ? packed_set_get(ctx, keys, n_keys, st) : nullptr;
+    use_tc = pset != nullptr;
     u32 G = n_ct >= 4 ? 4 : n_ct;
     if (use_tc) {
-        const size_t per_ct = ((size_t)D * LK * n + (size_t)Lq * n + 4 * (size_t)n_keys * LK * n) * sizeof(u64);
+        const size_t per_ct = ((size_t)D * LK * n + 4 * (size_t)n_keys * LK * n) * sizeof(u64);
         size_t free_b = 0, total_b = 0;
         cudaMemGetInfo(&free_b, &total_b);
         G = n_ct < (u32)tc::kCt ? n_ct : (u32)tc::kCt;
         while (G > 4 && (size_t)G * per_ct > free_b / 2) G -= 4;
     }
     const int cap = 1024;
-    const LimbMap lq = LimbMap::range(0, Lq), lqp = LimbMap::qp(ctx, Lq);
-    const size_t y_stride = (size_t)D * LK * n, b_stride = (size_t)Lq * n, d_stride = (size_t)D * n,
-                 f_stride = (size_t)n + 1;
-    Workspace<u64> Y, Bh, acc, Z, karr;
+    const LimbMap lqp = LimbMap::qp(ctx, Lq);
+    const size_t y_stride = (size_t)D * LK * n, d_stride = (size_t)D * n, f_stride = (size_t)n + 1;
+    Workspace<u64> Y, acc, Z, karr;
     Workspace<i64> dig;
     Workspace<u32> flags, cnt;
     Workspace<Exc> exc;
@@ -870,8 +999,7 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
     int32_t rc;
     if ((rc = terr.alloc(1, st))) return rc;
     CKKS_CUDA_TRY(cudaMemsetAsync(terr.p, 0, sizeof(int), st));
-    if ((rc = Y.alloc(G * y_stride, st)) || (rc = Bh.alloc(G * b_stride, st)) ||
-        (rc = acc.alloc((size_t)G * n_keys * 2 * LK * n, st)) || (rc = Z.alloc((size_t)G * n_keys * 2 * LK * n, st)) ||
+    if ((rc = Y.alloc(G * y_stride, st)) || (rc = acc.alloc((size_t)G * n_keys * 2 * LK * n, st)) || (rc = Z.alloc((size_t)G * n_keys * 2 * LK * n, st)) ||
         (rc = karr.alloc(3 * (size_t)n_keys + ctx->moduli.size(), st)) || (rc = dig.alloc(G * d_stride, st)) ||
         (rc = flags.alloc(G * f_stride, st)) || (rc = cnt.alloc((size_t)G * n_keys, st)) ||
         (rc = exc.alloc((size_t)G * n_keys * cap, st)))
@@ -908,7 +1036,6 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
                 if ((rc = rnsblock_modup_launch(ctx, k0, in + (size_t)Lq * n, Y.p + c * y_stride, st))) return rc;
                 if ((rc = ntt_forward_launch_map(ctx, Y.p + c * y_stride, Y.p + c * y_stride, D, lqp, LK, st))) return rc;
             }
-            if ((rc = ntt_forward_launch_map(ctx, in, Bh.p + c * b_stride, 1, lq, Lq, st))) return rc;
         }
         pt.end();
         pt.begin(2);
@@ -926,9 +1053,8 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
             CKKS_CUDA_TRY(cudaFuncSetAttribute(k_mac_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                (int)tc::kSmemBytes));
             k_mac_tc<<<n_tiles < n_sm ? n_tiles : n_sm, tc::kThreads, tc::kSmemBytes, st>>>(
-                Y.p, y_stride, Bh.p, b_stride, d_keys, d_exps_inv, ctx->d_pmodq, ctx->d_pmodq + ctx->L, acc.p,
-                ctx->d_tabs, lqp, (int)gn, (int)n_keys, (int)Lq, (int)LK, (int)D, (int)ctx->log_n, exc.p, cnt.p, cap,
-                d_psi, terr.p);
+                Y.p, y_stride, pset->d, (int)pset->rg, d_keys, d_exps_inv, acc.p, ctx->d_tabs, lqp, (int)gn,
+                (int)n_keys, (int)LK, (int)D, (int)ctx->log_n, exc.p, cnt.p, cap, d_psi, terr.p);
         } else {
             const size_t smem = (size_t)(G >= 3 ? 4 : G) * D * kS * sizeof(u64);
             if (n >= (u32)kS && smem <= 200 * 1024) {
@@ -937,8 +1063,8 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
     do {                                                                                                           \
         cudaFuncSetAttribute(k_mac_tiled<GG>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);            \
         k_mac_tiled<GG><<<g, kS * kLanes, (size_t)GG * D * kS * sizeof(u64), st>>>(                              \
-            Y.p, y_stride, Bh.p, b_stride, d_keys, d_exps_inv, ctx->d_pmodq, ctx->d_pmodq + ctx->L, acc.p,        \
-            ctx->d_tabs, lqp, gn, n_keys, Lq, LK, D, ctx->log_n, exc.p, cnt.p, cap, d_psi);                        \
+            Y.p, y_stride, d_keys, d_exps_inv, acc.p, ctx->d_tabs, lqp, gn, n_keys, Lq, LK, D, ctx->log_n, exc.p,  \
+            cnt.p, cap, d_psi);                                                                                    \
     } while (0)
                 if (G >= 3) CKKS_MACT(4);
                 else if (G == 2) CKKS_MACT(2);
@@ -947,9 +1073,8 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
             } else {
                 dim3 g((n + kT - 1) / kT, n_keys, LK);
 #define CKKS_MAC(GG)                                                                                               \
-    k_mac_hoisted<GG><<<g, kT, 0, st>>>(Y.p, y_stride, Bh.p, b_stride, d_keys, d_exps_inv, ctx->d_pmodq,            \
-                                        ctx->d_pmodq + ctx->L, acc.p, ctx->d_tabs, lqp, gn, n_keys, Lq, LK, D,      \
-                                        ctx->log_n, exc.p, cnt.p, cap, d_psi)
+    k_mac_hoisted<GG><<<g, kT, 0, st>>>(Y.p, y_stride, d_keys, d_exps_inv, acc.p, ctx->d_tabs, lqp, gn, n_keys, Lq, \
+                                        LK, D, ctx->log_n, exc.p, cnt.p, cap, d_psi)
                 if (G >= 3) CKKS_MAC(4);
                 else if (G == 2) CKKS_MAC(2);
                 else CKKS_MAC(1);
@@ -959,7 +1084,16 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
         CKKS_CUDA_TRY(cudaGetLastError());
         pt.end();
         pt.begin(4);
-        if ((rc = ntt_inverse_launch_map(ctx, acc.p, Z.p, gn * n_keys * 2, lqp, LK, st))) return rc;
+        // inverse transform; the b components get P b of their ciphertext added on the
+        // Q limbs (ModDown(x + P b) = ModDown(x) + b: the base term of the rotation)
+        InvBase ib;
+        ib.b = ct_in + (size_t)c0 * ct_words;
+        ib.b_stride = ct_words;
+        ib.n_keys = n_keys;
+        ib.q_limbs = Lq;
+        ib.pf = ctx->d_pmodq;
+        ib.pf_q = ctx->d_pmodq + ctx->L;
+        if ((rc = ntt_inverse_base_launch(ctx, acc.p, Z.p, gn * n_keys * 2, lqp, LK, ib, st))) return rc;
         pt.end();
         pt.begin(5);
         // ModDown of every (ciphertext, key) pair, then sigma_g, straight into the output

@@ -46,3 +46,10 @@ int32_t decode_launch(ckks_ctx* ctx, const u64* poly, double* slots, u32 n_msg, 
 // Per-context caches of gadget.cu and embed.cu, released by ckks_ctx_destroy.
 void gadget_release_ctx(const ckks_ctx* ctx);
 void embed_release_ctx(const ckks_ctx* ctx);
+// Packed Galois-key sets of the tensor-core MAC (hoisted.cu): all of a context,
+// or every set that contains a key (called when the key is destroyed).
+struct ckks_ksk;
+void keyset_release_ctx(const ckks_ctx* ctx);
+void keyset_forget_key(const ckks_ksk* key);
+// true on compute capability 10.0 devices (the tcgen05 INT8 key-switch MAC)
+bool tc_enabled();

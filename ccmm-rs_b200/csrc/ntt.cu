@@ -191,7 +191,8 @@ __global__ void __launch_bounds__(kMaxThreads) k_inv1(const u64* __restrict__ in
         u64 x[S::R2];
 #pragma unroll
         for (int e = 0; e < S::R2; ++e) x[e] = in[base + ((size_t)brev(S::R2 * g + e, LOG_M) << log_a) + b0 + c];
-        nttc::gs_stages<S::LR2>(x, 0, g, tw, q);
+        if (q < nttc::kLazyGsBound) nttc::gs_stages<S::LR2, true>(x, 0, g, tw, q);
+        else nttc::gs_stages<S::LR2, false>(x, 0, g, tw, q);
 #pragma unroll
         for (int e = 0; e < S::R2; ++e) {
             const int r = S::R2 * g + e;
@@ -207,7 +208,8 @@ __global__ void __launch_bounds__(kMaxThreads) k_inv1(const u64* __restrict__ in
             const int r = i0 + S::R2 * e;
             y[e] = sm[(r << log_c) + (c ^ (r & (C - 1)))];
         }
-        nttc::gs_stages<S::LR1>(y, S::LR2, 0, tw, q);
+        if (q < nttc::kLazyGsBound) nttc::gs_stages<S::LR1, true>(y, S::LR2, 0, tw, q);
+        else nttc::gs_stages<S::LR1, false>(y, S::LR2, 0, tw, q);
         const size_t row = (size_t)(b0 + c) << LOG_M;
 #pragma unroll
         for (int e = 0; e < S::R1; ++e) {
@@ -220,9 +222,10 @@ __global__ void __launch_bounds__(kMaxThreads) k_inv1(const u64* __restrict__ in
 // Inverse pass 2 over columns j_lo: negacyclic A-point merged GS with
 // psi_A^-1 on {j_lo + B brev(r)}; natural output j_lo + B i, canonical.
 // src may equal dst.
+// With ib.b, the b components of key-switch accumulators get P b added (InvBase).
 template <int LOG_M>
 __global__ void __launch_bounds__(kMaxThreads) k_inv2(const u64* src, u64* dst, const NttTab* __restrict__ tabs,
-                                                      LimbMap lm, int limb_count, int log_b, int log_c) {
+                                                      LimbMap lm, int limb_count, int log_b, int log_c, InvBase ib) {
     using S = Split<LOG_M>;
     extern __shared__ u64 sm[];
     const int C = 1 << log_c, tid = threadIdx.x;
@@ -245,7 +248,8 @@ __global__ void __launch_bounds__(kMaxThreads) k_inv2(const u64* src, u64* dst, 
         u64 x[S::R2];
 #pragma unroll
         for (int e = 0; e < S::R2; ++e) x[e] = src[base + c0 + c + ((size_t)brev(S::R2 * g + e, LOG_M) << log_b)];
-        nttc::gs_stages<S::LR2>(x, 0, g, tw, q);
+        if (q < nttc::kLazyGsBound) nttc::gs_stages<S::LR2, true>(x, 0, g, tw, q);
+        else nttc::gs_stages<S::LR2, false>(x, 0, g, tw, q);
 #pragma unroll
         for (int e = 0; e < S::R2; ++e) sm[((S::R2 * g + e) << log_c) + c] = x[e];
     }
@@ -255,9 +259,26 @@ __global__ void __launch_bounds__(kMaxThreads) k_inv2(const u64* src, u64* dst, 
         u64 y[S::R1];
 #pragma unroll
         for (int e = 0; e < S::R1; ++e) y[e] = sm[((i0 + S::R2 * e) << log_c) + c];
-        nttc::gs_stages<S::LR1>(y, S::LR2, 0, tw, q);
+        if (q < nttc::kLazyGsBound) {
+            nttc::gs_stages<S::LR1, true>(y, S::LR2, 0, tw, q);
+            const u64 one_q = (~0ull) / q;  // floor(2^64 / q) for odd q
 #pragma unroll
-        for (int e = 0; e < S::R1; ++e) dst[base + c0 + c + ((size_t)(i0 + S::R2 * e) << log_b)] = reduce_2q(y[e], q);
+            for (int e = 0; e < S::R1; ++e) y[e] = reduce_2q(mul_shoup_lazy(y[e], 1, one_q, q), q);
+        } else {
+            nttc::gs_stages<S::LR1, false>(y, S::LR2, 0, tw, q);
+#pragma unroll
+            for (int e = 0; e < S::R1; ++e) y[e] = reduce_2q(y[e], q);
+        }
+        const u32 poly = blockIdx.z;
+        if (ib.b && !(poly & 1) && (u32)limb < ib.q_limbs) {
+            const u64* bb = ib.b + (size_t)(poly / (2 * ib.n_keys)) * ib.b_stride + ((size_t)limb << (LOG_M + log_b));
+            const u64 pf = ib.pf[limb], pfq = ib.pf_q[limb];
+#pragma unroll
+            for (int e = 0; e < S::R1; ++e)
+                y[e] = add_mod(y[e], mul_shoup(__ldg(bb + c0 + c + ((size_t)(i0 + S::R2 * e) << log_b)), pf, pfq, q), q);
+        }
+#pragma unroll
+        for (int e = 0; e < S::R1; ++e) dst[base + c0 + c + ((size_t)(i0 + S::R2 * e) << log_b)] = y[e];
     }
 }
 
@@ -271,7 +292,7 @@ int pick_log_c(int log_avail) {
 
 template <int LOG_M>
 int32_t launch_pass(int which, const void* in, u64* out, const NttTab* tabs, LimbMap lm, u32 limbs, u32 polys,
-                    int log_other, cudaStream_t st) {
+                    int log_other, cudaStream_t st, const InvBase& ib) {
     const int lc = pick_log_c<LOG_M>(log_other);
     const int threads = Split<LOG_M>::RMAX << lc;
     const size_t smem = (sizeof(u64) << (LOG_M + lc)) + 2 * sizeof(u64) * (1u << LOG_M);
@@ -281,27 +302,27 @@ int32_t launch_pass(int which, const void* in, u64* out, const NttTab* tabs, Lim
         case 1: k_fwd1<LOG_M, true><<<grid, threads, smem, st>>>(in, out, tabs, lm, limbs, log_other, lc); break;
         case 2: k_fwd2<LOG_M><<<grid, threads, smem, st>>>((const u64*)in, out, tabs, lm, limbs, log_other, lc); break;
         case 3: k_inv1<LOG_M><<<grid, threads, smem, st>>>((const u64*)in, out, tabs, lm, limbs, log_other, lc); break;
-        default: k_inv2<LOG_M><<<grid, threads, smem, st>>>((const u64*)in, out, tabs, lm, limbs, log_other, lc); break;
+        default: k_inv2<LOG_M><<<grid, threads, smem, st>>>((const u64*)in, out, tabs, lm, limbs, log_other, lc, ib); break;
     }
     return CKKS_OK;
 }
 
 int32_t pass(int which, int log_m, const void* in, u64* out, const NttTab* tabs, LimbMap lm, u32 limbs, u32 polys,
-             int log_other, cudaStream_t st) {
+             int log_other, cudaStream_t st, const InvBase& ib = InvBase{}) {
     if (polys > 65535 || limbs > 65535) {  // grid y / z limits
         ckks_set_error("NTT: more than 65535 polynomials or limbs in one launch");
         return CKKS_ERR_BAD_ARG;
     }
     switch (log_m) {
-        case 1: return launch_pass<1>(which, in, out, tabs, lm, limbs, polys, log_other, st);
-        case 2: return launch_pass<2>(which, in, out, tabs, lm, limbs, polys, log_other, st);
-        case 3: return launch_pass<3>(which, in, out, tabs, lm, limbs, polys, log_other, st);
-        case 4: return launch_pass<4>(which, in, out, tabs, lm, limbs, polys, log_other, st);
-        case 5: return launch_pass<5>(which, in, out, tabs, lm, limbs, polys, log_other, st);
-        case 6: return launch_pass<6>(which, in, out, tabs, lm, limbs, polys, log_other, st);
-        case 7: return launch_pass<7>(which, in, out, tabs, lm, limbs, polys, log_other, st);
-        case 8: return launch_pass<8>(which, in, out, tabs, lm, limbs, polys, log_other, st);
-        case 9: return launch_pass<9>(which, in, out, tabs, lm, limbs, polys, log_other, st);
+        case 1: return launch_pass<1>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib);
+        case 2: return launch_pass<2>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib);
+        case 3: return launch_pass<3>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib);
+        case 4: return launch_pass<4>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib);
+        case 5: return launch_pass<5>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib);
+        case 6: return launch_pass<6>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib);
+        case 7: return launch_pass<7>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib);
+        case 8: return launch_pass<8>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib);
+        case 9: return launch_pass<9>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib);
         default: ckks_set_error("NTT: unsupported transform size"); return CKKS_ERR_BAD_ARG;
     }
 }
@@ -338,6 +359,11 @@ int32_t ntt_forward_launch_map(ckks_ctx* ctx, const u64* in, u64* out, u32 n_pol
 
 int32_t ntt_inverse_launch_map(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, LimbMap lm, u32 limb_count,
                                cudaStream_t st) {
+    return ntt_inverse_base_launch(ctx, in, out, n_polys, lm, limb_count, InvBase{}, st);
+}
+
+int32_t ntt_inverse_base_launch(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, LimbMap lm, u32 limb_count,
+                                const InvBase& ib, cudaStream_t st) {
     if (n_polys == 0 || limb_count == 0) return CKKS_OK;
     const int la = ctx->log_n1, lb = ctx->log_n2;
     u64* mid = out;
@@ -347,7 +373,7 @@ int32_t ntt_inverse_launch_map(ckks_ctx* ctx, const u64* in, u64* out, u32 n_pol
         mid = tmp.p;
     }
     if (int32_t rc = pass(3, lb, in, mid, ctx->d_tabs, lm, limb_count, n_polys, la, st)) return rc;
-    if (int32_t rc = pass(4, la, mid, out, ctx->d_tabs, lm, limb_count, n_polys, lb, st)) return rc;
+    if (int32_t rc = pass(4, la, mid, out, ctx->d_tabs, lm, limb_count, n_polys, lb, st, ib)) return rc;
     CKKS_CUDA_TRY(cudaGetLastError());
     return CKKS_OK;
 }

@@ -28,13 +28,25 @@ __device__ __forceinline__ void ct_bfly(u64& X, u64& Y, u64 W, u64 Wq, u64 q, u6
     Y = x - t + q2;
 }
 constexpr u64 kLazyCtBound = 1ull << 59;  // primes below this take the !kRed network
-// GS: X, Y in [0, 2q) -> X' = X + Y, Y' = (X - Y) W, both in [0, 2q).
+// GS (kLazy false): X, Y in [0, 2q) -> X' = X + Y, Y' = (X - Y) W, both in [0, 2q).
+// GS (kLazy): X, Y in [0, c) with c a multiple of q (passed as q2) -> X' = X + Y
+// in [0, 2c), Y' = (X + c - Y) W in [0, 2q); no conditional subtraction. Global
+// stage s of a network whose inputs are below 2q uses c = 2^(s+1) q, so a pass
+// of m stages stays below 2^(m+1) q < 2^64 for m <= 9 (N <= 2^18) and q < 2^54.
+template <bool kLazy = false>
 __device__ __forceinline__ void gs_bfly(u64& X, u64& Y, u64 W, u64 Wq, u64 q, u64 q2) {
-    u64 s = X + Y;
-    u64 d = X - Y + q2;
-    X = s >= q2 ? s - q2 : s;
-    Y = mul_shoup_lazy(d, W, Wq, q);
+    if (kLazy) {
+        const u64 d = X + q2 - Y;
+        X = X + Y;
+        Y = mul_shoup_lazy(d, W, Wq, q);
+    } else {
+        u64 s = X + Y;
+        u64 d = X - Y + q2;
+        X = s >= q2 ? s - q2 : s;
+        Y = mul_shoup_lazy(d, W, Wq, q);
+    }
 }
+constexpr u64 kLazyGsBound = 1ull << 54;  // primes below this take the lazy GS network
 
 // Merged CT stages s0 .. s0 + LR - 1 on R = 2^LR register values with pair
 // distance R/2, R/4, .., 1; the twiddle block of register e at stage ls is
@@ -61,28 +73,29 @@ __device__ __forceinline__ void ct_stages(u64 (&x)[1 << LR], int s0, u32 base, T
     ct_stage<LR, 0, kRed>(x, s0, base, tw, q, q << 1);
 }
 
-template <int LR, int LS, typename TW>
+template <int LR, int LS, bool kLazy, typename TW>
 __device__ __forceinline__ void gs_stage(u64 (&x)[1 << LR], int s0, u32 blk0, TW& tw, u64 q, u64 q2) {
     if constexpr (LS < LR) {
         constexpr int t = 1 << LS;
         constexpr int nblk = (1 << LR) >> (LS + 1);
+        const u64 c = kLazy ? q << (s0 + LS + 1) : q2;  // lazy: 2^(s+1) q at global stage s
 #pragma unroll
         for (int b = 0; b < nblk; ++b) {
             u64 W, Wq;
             tw(s0 + LS, (blk0 << (LR - LS - 1)) + b, W, Wq);
 #pragma unroll
-            for (int o = 0; o < t; ++o) gs_bfly(x[b * 2 * t + o], x[b * 2 * t + o + t], W, Wq, q, q2);
+            for (int o = 0; o < t; ++o) gs_bfly<kLazy>(x[b * 2 * t + o], x[b * 2 * t + o + t], W, Wq, q, c);
         }
-        gs_stage<LR, LS + 1>(x, s0, blk0, tw, q, q2);
+        gs_stage<LR, LS + 1, kLazy>(x, s0, blk0, tw, q, q2);
     }
 }
 
 // Merged GS stages with register distance t = 1, 2, .., 2^(LR-1) (local stages
 // s0 .. s0 + LR - 1 of the network whose t = 2^s); block of register e at
 // stage ls is (blk0 << (LR - ls - 1)) + (e >> (ls + 1)).
-template <int LR, typename TW>
+template <int LR, bool kLazy = false, typename TW>
 __device__ __forceinline__ void gs_stages(u64 (&x)[1 << LR], int s0, u32 blk0, TW tw, u64 q) {
-    gs_stage<LR, 0>(x, s0, blk0, tw, q, q << 1);
+    gs_stage<LR, 0, kLazy>(x, s0, blk0, tw, q, q << 1);
 }
 
 }  // namespace nttc

@@ -72,6 +72,14 @@ int32_t ckks_is_prime(uint64_t value);
 int32_t ckks_ctx_create(uint32_t log_n, const uint64_t* q, uint32_t L, const uint64_t* p, uint32_t K,
                         ckks_ctx** out);
 int32_t ckks_ctx_destroy(ckks_ctx* ctx);
+/* Selects the key-switch MAC of bounded hoisted rotations: enable != 0 (the
+ * default) runs it on the tcgen05 INT8 tensor cores when the device has them,
+ * 0 on CUDA cores (split-operand 64-bit accumulators). Both are bit-exact; the
+ * switch exists to compare them. No counterpart in the reference (its MAC is
+ * the serial loop of ring/ntt_polynomial.rs:211-236). */
+int32_t ckks_ctx_set_tensor_cores(ckks_ctx* ctx, int32_t enable);
+/* 1 when bounded hoisted rotations of this context use the tensor cores. */
+int32_t ckks_ctx_tensor_cores(const ckks_ctx* ctx);
 /* Writes the L+K roots psi (host array). */
 int32_t ckks_ctx_psi(const ckks_ctx* ctx, uint64_t* psi_host);
 

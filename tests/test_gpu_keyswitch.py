@@ -244,3 +244,30 @@ def test_hoisted_ntt_domain_corrections(oracle, cuda, small, base_log):
     for i in range(len(cts)):
         want = oracle.hybrid_rotate_hoisted(q, p, keys_ref, ks, base_log, cts[i])
         assert np.array_equal(got[i], want), i
+
+
+@pytest.mark.parametrize("base_log", [8, 32])
+def test_tensor_core_mac_equals_cuda_core_mac(oracle, cuda, base_log):
+    """The INT8 tensor-core key-switch MAC and the CUDA-core MAC give the same
+    words: 16 ciphertexts x 40 Galois keys (two key chunks, the second partial)
+    at N=2^12, plus an oracle check of a few (ciphertext, key) pairs."""
+    log_n, n = 12, 1 << 12
+    q = [int(x) for x in oracle.primes_below_bits(50, n, 6)]
+    p = [int(x) for x in oracle.primes_below_bits(60, n, 2)]
+    ctx = cb.Context(log_n, q, p)
+    rng = np.random.default_rng(70 + base_log)
+    s = rng.integers(-1, 2, n).astype(np.int8)
+    ks = [ctx.rotation_exponent_left(r) for r in range(1, 41)]
+    keys = [cb.KeySwitchKey.hybrid_generate(ctx, len(q), base_log, k, s, seed=900 + i) for i, k in enumerate(ks)]
+    cts = np.stack([np.stack([np.stack([rng.integers(0, m, n, dtype=np.uint64) for m in q]) for _ in range(2)])
+                    for _ in range(16)])
+    assert ctx.tensor_cores
+    tc = host(cb.rotate_hoisted(ctx, keys, dev(cts)))
+    ctx.tensor_cores = False
+    assert not ctx.tensor_cores
+    cc = host(cb.rotate_hoisted(ctx, keys, dev(cts)))
+    ctx.tensor_cores = True
+    assert np.array_equal(tc, cc)
+    for c, g in ((0, 0), (15, 39), (7, 33)):
+        want = oracle.hybrid_rotate(q, p, keys[g].download(), ks[g], base_log, cts[c])
+        assert np.array_equal(tc[c, g], want), (c, g)
