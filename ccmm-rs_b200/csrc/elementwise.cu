@@ -80,15 +80,36 @@ __global__ void k_rescale(const u64* __restrict__ in, u64* __restrict__ out, con
 // KT > 0 fixes the number of auxiliary limbs at compile time (KT == 0: md.K at
 // run time). The Q-limb gathers are issued kBatch at a time so each thread keeps
 // several independent loads in flight (the reads are scattered under sigma).
-template <int KT>
-__global__ void k_mod_down(const u64* __restrict__ in, u64* __restrict__ out, ModDownConst md, int q_limbs,
-                           int log_n, const u64* __restrict__ exps_inv, int n_keys) {
+// Per-limb constants are staged in shared memory: q, (P^-1 mod q, Shoup),
+// -P mod q, (2K+1) q, then (p_0..p_{j-1} mod q, Shoup) for j < K. kLazy (every Q
+// prime below 2^59): the K products are summed lazily in [0, 2q) each and the
+// difference x - r is formed as x + (2K+1) q - r < (2K+2) q < 2^64, with one
+// reduction at the end; the result is the same canonical residue.
+template <int KT, bool kLazy>
+__global__ void __launch_bounds__(kT) k_mod_down(const u64* __restrict__ in, u64* __restrict__ out, ModDownConst md,
+                                                 int q_limbs, int log_n, const u64* __restrict__ exps_inv, int n_keys) {
     constexpr int kBatch = 8;
+    extern __shared__ u64 cs[];
+    const int K = KT > 0 ? KT : md.K;
+    constexpr int KM = KT > 0 ? KT : kMaxAux;
+    const int W = 5 + 2 * K;
+    for (int idx = threadIdx.x; idx < q_limbs * W; idx += blockDim.x) {
+        const int i = idx / W, f = idx - i * W;
+        const u64 qi = md.q[i];
+        u64 v;
+        if (f == 0) v = qi;
+        else if (f == 1) v = md.pinv_mod_q[i];
+        else if (f == 2) v = md.pinv_mod_q_q[i];
+        else if (f == 3) v = qi - md.p_mod_q[i];  // P mod q is in [1, q): distinct primes
+        else if (f == 4) v = (u64)(2 * K + 1) * qi;
+        else if (f < 5 + K) v = md.pre[(size_t)i * kMaxAux + (f - 5)];
+        else v = md.pre_q[(size_t)i * kMaxAux + (f - 5 - K)];
+        cs[idx] = v;
+    }
+    __syncthreads();
     const u32 n = 1u << log_n;
     const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
-    const int K = KT > 0 ? KT : md.K;
-    constexpr int KM = KT > 0 ? KT : kMaxAux;
     const size_t src = (size_t)blockIdx.y * (q_limbs + K) << log_n;
     const size_t dst = (size_t)blockIdx.y * q_limbs << log_n;
     u32 c = t;
@@ -132,15 +153,21 @@ __global__ void k_mod_down(const u64* __restrict__ in, u64* __restrict__ out, Mo
         for (int u = 0; u < kBatch; ++u) {
             const int i = i0 + u;
             if (i < q_limbs) {
-                const u64 qi = md.q[i];
-                const u64* pre = md.pre + (size_t)i * kMaxAux;
-                const u64* pre_q = md.pre_q + (size_t)i * kMaxAux;
-                u64 r = 0;
+                const u64* ci = cs + i * W;
+                const u64 qi = ci[0];
+                u64 r = neg ? ci[3] : 0;  // r == centred CRT_P(x_P) mod q, lazily
+                u64 w;
+                if (kLazy) {
 #pragma unroll
-                for (int j = 0; j < KM; ++j)
-                    if (j < K) r = add_mod(r, mul_shoup(v[j], pre[j], pre_q[j], qi), qi);
-                if (neg) r = sub_mod(r, md.p_mod_q[i], qi);
-                const u64 w = mul_shoup(sub_mod(xin[u], r, qi), md.pinv_mod_q[i], md.pinv_mod_q_q[i], qi);
+                    for (int j = 0; j < KM; ++j)
+                        if (j < K) r += mul_shoup_lazy(v[j], ci[5 + j], ci[5 + K + j], qi);
+                    w = reduce_2q(mul_shoup_lazy(xin[u] + ci[4] - r, ci[1], ci[2], qi), qi);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < KM; ++j)
+                        if (j < K) r = add_mod(r, mul_shoup(v[j], ci[5 + j], ci[5 + K + j], qi), qi);
+                    w = mul_shoup(sub_mod(xin[u], r, qi), ci[1], ci[2], qi);
+                }
                 o[(size_t)i << log_n] = flip ? neg_mod(w, qi) : w;
             }
         }
@@ -204,6 +231,9 @@ int32_t mod_down_launch(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, u32
 int32_t mod_down_sigma_multi(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, u32 q_limbs,
                              const u64* d_exps_inv, u32 n_keys, cudaStream_t st) {
     if (!n_polys) return CKKS_OK;
+    // lazy differences need (2K + 2) q < 2^64: every Q prime below 2^59 (K <= 8)
+    bool lazy = true;
+    for (u32 i = 0; i < q_limbs; ++i) lazy = lazy && ctx->moduli[i] < (1ull << 59);
     // grid.y limit: chunks are multiples of 2 * n_keys so (poly / 2) % n_keys pairs stay aligned
     const u32 unit = 2 * (n_keys ? n_keys : 1);
     const u32 chunk = (65535 / unit) * unit;
@@ -213,12 +243,24 @@ int32_t mod_down_sigma_multi(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys
         const u64* pin = in + ((size_t)p0 * (q_limbs + ctx->K) << ctx->log_n);
         u64* pout = out + ((size_t)p0 * q_limbs << ctx->log_n);
         const int nk = n_keys ? (int)n_keys : 1;
-        switch (ctx->K) {
-            case 1: k_mod_down<1><<<g, kT, 0, st>>>(pin, pout, ctx->mod_down, q_limbs, ctx->log_n, d_exps_inv, nk); break;
-            case 2: k_mod_down<2><<<g, kT, 0, st>>>(pin, pout, ctx->mod_down, q_limbs, ctx->log_n, d_exps_inv, nk); break;
-            case 3: k_mod_down<3><<<g, kT, 0, st>>>(pin, pout, ctx->mod_down, q_limbs, ctx->log_n, d_exps_inv, nk); break;
-            default: k_mod_down<0><<<g, kT, 0, st>>>(pin, pout, ctx->mod_down, q_limbs, ctx->log_n, d_exps_inv, nk);
+        const size_t smem = (size_t)q_limbs * (5 + 2 * ctx->K) * sizeof(u64);
+#define CKKS_MD(KK, LZ) k_mod_down<KK, LZ><<<g, kT, smem, st>>>(pin, pout, ctx->mod_down, q_limbs, ctx->log_n, d_exps_inv, nk)
+        if (lazy) {
+            switch (ctx->K) {
+                case 1: CKKS_MD(1, true); break;
+                case 2: CKKS_MD(2, true); break;
+                case 3: CKKS_MD(3, true); break;
+                default: CKKS_MD(0, true);
+            }
+        } else {
+            switch (ctx->K) {
+                case 1: CKKS_MD(1, false); break;
+                case 2: CKKS_MD(2, false); break;
+                case 3: CKKS_MD(3, false); break;
+                default: CKKS_MD(0, false);
+            }
         }
+#undef CKKS_MD
     }
     CKKS_CUDA_TRY(cudaGetLastError());
     return CKKS_OK;

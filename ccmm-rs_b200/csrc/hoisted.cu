@@ -332,9 +332,12 @@ namespace {
 // shared memory by a single bulk copy. Blocks are in the MAC's shared-memory
 // image (K-major, no swizzle): row group rg (8 rows = 4 keys x 2 components) of
 // 1 KB, then slot i (256 B), K chunk kk (128 B: digits 2 kk, 2 kk + 1), row
-// (16 B), digit (8 B). Only the row groups of present keys are stored. A set is
-// packed once per ordered list of Galois keys and cached per context until a
-// key of the set or the context is destroyed.
+// (16 B), digit (8 B). Only the row groups of present keys are stored. Digit D
+// (one past the gadget digits) holds P mod q_l in the b rows of the Q limbs and
+// 0 elsewhere: paired with the NTT of the ciphertext's b it adds the base term
+// P b of the rotation inside the same contraction. A set is packed once per
+// ordered list of Galois keys and cached per context until a key of the set or
+// the context is destroyed.
 struct PackedSet {
     std::vector<const ckks_ksk*> keys;
     u64* d = nullptr;
@@ -344,7 +347,8 @@ std::mutex g_sets_mu;
 std::map<const ckks_ctx*, std::vector<std::unique_ptr<PackedSet>>> g_sets;
 
 __global__ void k_pack_keys(const u64* const* __restrict__ keys, int n_keys, int LK, int D, int log_n, u32 rg,
-                            u32 n_kc, u32 n_chunks, u64* __restrict__ out, size_t total) {
+                            u32 n_kc, u32 n_chunks, const u64* __restrict__ pf, int Lq, u64* __restrict__ out,
+                            size_t total) {
     const u32 block_words = rg * 128;
     const u32 tiles_s = (1u << log_n) >> 2;
     for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < total; w += (size_t)gridDim.x * blockDim.x) {
@@ -359,9 +363,12 @@ __global__ void k_pack_keys(const u64* const* __restrict__ keys, int n_keys, int
         const size_t tile = rest / n_kc;
         const u32 l = (u32)(tile / tiles_s), s = (u32)(tile % tiles_s) * 4 + i;
         const u32 g = kc * 32 + (m >> 1), comp = m & 1, j = ch * 4 + jj;
-        out[w] = (g < (u32)n_keys && j < (u32)D)
-                     ? __ldg(keys[g] + (((((size_t)j * LK + l) * 2 + comp) << log_n) + s))
-                     : 0;
+        u64 v = 0;
+        if (g < (u32)n_keys) {
+            if (j < (u32)D) v = __ldg(keys[g] + (((((size_t)j * LK + l) * 2 + comp) << log_n) + s));
+            else if (j == (u32)D && comp == 0 && l < (u32)Lq) v = pf[l];
+        }
+        out[w] = v;
     }
 }
 
@@ -378,7 +385,7 @@ const PackedSet* packed_set_get(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 
     PackedSet& p = *pp;
     p.keys.assign(keys, keys + n_keys);
     p.n_kc = (n_keys + 31) / 32;
-    p.n_chunks = (k0->D + 3) / 4;
+    p.n_chunks = (k0->D + 1 + 3) / 4;  // gadget digits and the base digit
     p.rg = n_keys >= 32 ? 8 : (n_keys + 3) / 4;
     const size_t total = (size_t)LK * (n / 4) * p.n_kc * p.n_chunks * p.rg * 128;
     // unused stream-ordered workspace memory goes back to the device first
@@ -403,7 +410,7 @@ const PackedSet* packed_set_get(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 
         return nullptr;
     }
     k_pack_keys<<<148 * 16, 256, 0, st>>>(d_ptr, (int)n_keys, (int)LK, (int)k0->D, (int)ctx->log_n, p.rg, p.n_kc,
-                                          p.n_chunks, p.d, total);
+                                          p.n_chunks, ctx->d_pmodq, (int)k0->q_limbs, p.d, total);
     // ready for every stream of the context
     const bool ok = cudaGetLastError() == cudaSuccess && cudaStreamSynchronize(st) == cudaSuccess;
     cudaFree(d_ptr);
@@ -503,14 +510,15 @@ struct PhaseTimer {
 // order. Both use the no-swizzle canonical layout (8 x 16-byte core matrices).
 //
 // Warp roles of a persistent CTA (one per SM, all 512 TMEM columns):
-//   warps 4-11 producers in two groups of four: group p owns the items t with
-//              t % 2 == p (B stage p); for item t it issues the bulk copy of
-//              the packed key block and the cp.async of the digit transforms
-//              of item t + 6 into an 8-deep ring, then builds the B operand of
-//              item t;
+//   producers  (warps kEpiWarps..11, groups of four taking alternate items):
+//              for item t a group issues the bulk copy of the packed key block
+//              and the cp.async of the digit transforms of item t + kAhead into
+//              an 8-deep ring, then builds the B operand of item t (B stage
+//              t % kBStages);
 //   warp 12    issues the MMAs of item t once its operands are ready;
-//   warps 0-3  epilogue: TMEM -> exact combine of the 8 planes, reduction mod
-//              q and sparse carry corrections, stores.
+//   epilogue   (warps 0..kEpiWarps-1, warp w on TMEM lane quadrant w % 4; with
+//              8 warps, warp w takes slot pair w / 4): TMEM -> exact combine of
+//              the 8 planes, reduction mod q and sparse carry corrections, stores.
 // An item is (tile of 4 slots of one limb, key chunk, 4-digit chunk); the
 // accumulators of consecutive (tile, key chunk) units alternate between two
 // TMEM column halves, so the epilogue of one unit overlaps the MMAs of the
@@ -523,13 +531,26 @@ constexpr int kTS = 4;            // slots per tile
 constexpr int kCt = 16;           // ciphertexts per group (N = 8 kCt = 128)
 constexpr int kKeys = 32;         // keys per pass (M = 2 kKeys = 64)
 constexpr int kJc = 4;            // digits per chunk (K = 32 bytes)
-constexpr int kRing = 8;          // A / Y prefetch ring depth
-constexpr int kAhead = 6;         // items fetched ahead
-constexpr int kBStages = 2;       // B operand stages (kRing - kAhead), one per producer group
-constexpr int kProdWarp0 = 4, kMmaWarp = 12;
-constexpr int kThreads = 416;     // 13 warps: 4 epilogue, 8 producer, 1 MMA
-constexpr int kGrp = 128, kEpi = 128;          // threads per producer group, epilogue threads
-constexpr int kBarGrp0 = 1, kBarEpi = 3;  // named barriers: producer groups 1, 2; epilogue 3
+// Tuning (measured on B200, see the design notes): epilogue warps (4 or 8; the
+// other 12 - kEpiWarps warps produce, in groups of 4 that take alternate items)
+// and B stages (2 or 4; the prefetch distance is kRing - kBStages items).
+#ifndef CKKS_TC_EPI_WARPS
+#define CKKS_TC_EPI_WARPS 4
+#endif
+#ifndef CKKS_TC_BSTAGES
+#define CKKS_TC_BSTAGES 2
+#endif
+constexpr int kEpiWarps = CKKS_TC_EPI_WARPS;
+constexpr int kBStages = CKKS_TC_BSTAGES;      // B operand stages
+constexpr int kRing = 8;                       // A / Y prefetch ring depth
+constexpr int kAhead = kRing - kBStages;       // items fetched ahead
+constexpr int kGroups = (12 - kEpiWarps) / 4;  // producer groups of 4 warps
+constexpr int kProdWarp0 = kEpiWarps, kMmaWarp = 12;
+constexpr int kThreads = 416;                  // 13 warps: epilogue, producers, 1 MMA
+constexpr int kGrp = 128, kEpi = 32 * kEpiWarps;  // threads per producer group, epilogue threads
+constexpr int kBarGrp0 = 1, kBarEpi = 3;       // named barriers: producer groups 1, 2; epilogue 3
+static_assert((kEpiWarps == 4 || kEpiWarps == 8) && (kBStages == 2 || kBStages == 4), "tuning range");
+static_assert(kAhead % kGroups == 0 && kBStages % kGroups == 0, "a group prefetches and builds its own items");
 // A (packed key block, bulk-copied): row groups of 1 KB, slot i at 256 i, K
 // chunks 128 B apart. B strides are padded (slot and digit strides off
 // multiples of 128 B) so the producers' shared-memory stores spread over the banks.
@@ -539,14 +560,13 @@ constexpr u32 kBSlot = 4368;                   // 4 digits x 8 weights x 128 B (
 constexpr u32 kAStage = 8192;                  // 8 row groups
 constexpr u32 kYStage = kCt * kJc * kTS * 8;   // 2048: Y words [c][jj][i]
 constexpr u32 kBStage = kTS * kBSlot;          // 17472
-constexpr u32 kOffY = kRing * kAStage;                     // 65536
-constexpr u32 kOffB = kOffY + kRing * kYStage;             // 81920
-constexpr u32 kOffCnt = kOffB + kBStages * kBStage;        // 116864: correction counts [c][g], g < kCntKeys
+constexpr u32 kOffY = kRing * kAStage;                     // 64 KB of A
+constexpr u32 kOffB = kOffY + kRing * kYStage;             // 16 KB of Y
+constexpr u32 kOffCnt = kOffB + kBStages * kBStage;        // correction counts [c][g], g < kCntKeys
 constexpr int kCntKeys = 256;
-constexpr u32 kSmemBytes = kOffCnt + kCt * kCntKeys * 4;   // 133,248 B: one CTA per SM
+constexpr u32 kSmemBytes = kOffCnt + kCt * kCntKeys * 4;   // 133 KB (2 B stages) or 168 KB (4): one CTA per SM
+static_assert(kSmemBytes <= 227 * 1024, "shared memory per CTA");
 constexpr u32 kTmemCols = 512;
-static_assert(kBStages == kRing - kAhead && kBStages == 2, "B stages follow the ring, one per producer group");
-static_assert(kAhead % 2 == 0, "a group prefetches its own items");
 constexpr long long kSpin = 1ll << 22;         // bounded waits (iterations)
 
 __device__ __forceinline__ u32 smem_u32(const void* p) { return (u32)__cvta_generic_to_shared(p); }
@@ -649,11 +669,11 @@ struct Item {
 }  // namespace tc
 
 // Same arguments and results as k_mac_tiled for bounded keys (up to 16
-// ciphertexts per call, any number of keys, D <= 4096, N >= 4); the A operand
+// ciphertexts per call, any number of keys, D < 4096, N >= 4); the A operand
 // comes from the packed set of the keys (rg row groups per block).
 __global__ void __launch_bounds__(tc::kThreads, 1)
-    k_mac_tc(const u64* __restrict__ Yhat, size_t y_stride, const u64* __restrict__ packed, int rg,
-             const u64* const* __restrict__ keys,
+    k_mac_tc(const u64* __restrict__ Yhat, size_t y_stride, const u64* __restrict__ Bhat, size_t b_stride, int Lq,
+             const u64* __restrict__ packed, int rg, const u64* const* __restrict__ keys,
              const u64* __restrict__ exps_inv, u64* __restrict__ acc, const NttTab* __restrict__ tabs, LimbMap lm,
              int n_ct, int n_keys, int LK, int D, int log_n, const Exc* __restrict__ exc,
              const u32* __restrict__ exc_count, int cap, const u64* __restrict__ psi, int* __restrict__ err) {
@@ -669,7 +689,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     const u32 n = 1u << log_n;
     const int n_tiles_s = (int)(n / kTS), lts = log_n - 2;  // tiles per limb (a power of two)
     const int n_tiles = LK * n_tiles_s;
-    const int n_chunks = (D + kJc - 1) / kJc;
+    const int n_chunks = (D + 1 + kJc - 1) / kJc;  // gadget digits and the base digit (P b)
     const int n_kc = (n_keys + kKeys - 1) / kKeys;
     const int per_tile = n_kc * n_chunks;
     const int my_tiles = (int)blockIdx.x < n_tiles ? (n_tiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
@@ -720,7 +740,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
         const int pi = gtid & 3, pjj = (gtid >> 2) & 3;
         const int yc = gtid >> 4;
         const u32 a_bytes = (u32)rg * 1024u;
-        int last_issued = -1;  // last item whose block this thread's group copied
+        int last_issued = -1;  // last item whose block this thread copied (thread 0 of a group)
         auto prefetch = [&](int t, const Item& it) {
             if (t < n_items) {
                 const int tile = (int)blockIdx.x + it.tl * (int)gridDim.x;
@@ -736,34 +756,42 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                                  : "memory");
                     last_issued = t;
                 }
+                // digit j < D: the digit transform; j == D: NTT(b) on the Q limbs
                 const int j = it.ch * kJc + pjj;
-                const bool jok = j < D;
-                const size_t yoff = (((size_t)(jok ? j : 0) * LK + l) << log_n) + s0 + pi;
+                const bool jok = j < D, bok = j == D && l < Lq;
+                const u64* ysrc = jok ? Yhat + ((((size_t)j * LK + l) << log_n) + s0 + pi)
+                                      : bok ? Bhat + (((size_t)l << log_n) + s0 + pi) : Yhat;
+                const size_t ystep = jok ? y_stride : b_stride;
                 const u32 y_st = sbase + kOffY + (u32)(t & (kRing - 1)) * kYStage;
 #pragma unroll
                 for (int h = 0; h < 2; ++h)
                     if (yc + 8 * h < n_ct)
-                        cp8(y_st + (u32)(gtid + kGrp * h) * 8, Yhat + (yc + 8 * h) * y_stride + yoff, jok ? 8u : 0u);
+                        cp8(y_st + (u32)(gtid + kGrp * h) * 8, ysrc + (jok || bok ? (yc + 8 * h) * ystep : 0),
+                            jok || bok ? 8u : 0u);
             }
             cp_commit();
+        };
+        auto advance = [&](Item& x) {
+#pragma unroll
+            for (int k = 0; k < kGroups; ++k) x.next(n_kc, n_chunks);
         };
         Item it{0, 0, 0};
         if (grp) it.next(n_kc, n_chunks);
         Item ahead = it;
-        for (int k = 0; k < kAhead / 2; ++k) {
-            prefetch(grp + 2 * k, ahead);
-            ahead.next(n_kc, n_chunks);
-            ahead.next(n_kc, n_chunks);
+        for (int k = 0; k < kAhead / kGroups; ++k) {
+            prefetch(grp + kGroups * k, ahead);
+            advance(ahead);
         }
         int f_limb = -1, q_bits = 0;
         bool near_pow2 = false;
         u64 q = 0, f256 = 0, f256q = 0;  // q_l, 2^8 mod q_l and its Shoup companion
-        for (int t = grp; t < n_items; t += 2) {
+        for (int t = grp; t < n_items; t += kGroups) {
             const int tile = (int)blockIdx.x + it.tl * (int)gridDim.x;
             const int l = tile >> lts;
+            const int bst = t & (kBStages - 1);
             bool bad = false;
-            if (t >= kBStages)  // the MMAs of item t - 2 released B stage grp and ring slot (t + kAhead) % kRing
-                bad = !wait_parity(smem_u32(&s_empty[grp]), (u32)(((t >> 1) - 1) & 1));
+            // the MMAs of item t - kBStages released B stage bst and ring slot (t + kAhead) % kRing
+            if (t >= kBStages) bad = !wait_parity(smem_u32(&s_empty[bst]), (u32)(((t / kBStages) - 1) & 1));
             if (group_any(bar, kGrp, bad || s_abort)) {  // one decision for the group
                 if (gtid == 0) {
                     atomicExch(err, 1);
@@ -772,9 +800,8 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                 break;
             }
             prefetch(t + kAhead, ahead);
-            ahead.next(n_kc, n_chunks);
-            ahead.next(n_kc, n_chunks);
-            cp_wait<kAhead / 2>();  // this thread's copies of item t have landed
+            advance(ahead);
+            cp_wait<kAhead / kGroups>();  // this thread's copies of item t have landed
             named_sync(bar, kGrp);
             if (l != f_limb) {
                 q = tabs[lm(l)].q;
@@ -791,7 +818,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
             {
                 const u64* ys = (const u64*)(smem + kOffY + (t & (kRing - 1)) * kYStage);
                 const int c = ((gtid >> 5) << 1) | (gtid & 1), i = (gtid >> 1) & 3, jj = (gtid >> 3) & 3;
-                uint8_t* d0 = smem + kOffB + grp * kBStage + i * kBSlot + jj * kLboB + (c >> 1) * kSboB + (c & 1) * 8;
+                uint8_t* d0 = smem + kOffB + bst * kBStage + i * kBSlot + jj * kLboB + (c >> 1) * kSboB + (c & 1) * 8;
                 uint8_t* d1 = d0 + 4 * kSboB;  // ciphertext c + 8
                 const bool ok0 = c < n_ct, ok1 = c + 8 < n_ct;
                 u64 w0 = ys[(c * kJc + jj) * kTS + i], w1 = ys[((c + 8) * kJc + jj) * kTS + i];
@@ -817,16 +844,15 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             named_sync(bar, kGrp);
-            if (gtid == 0) arrive(smem_u32(&s_ready[grp]));
-            it.next(n_kc, n_chunks);
-            it.next(n_kc, n_chunks);
+            if (gtid == 0) arrive(smem_u32(&s_ready[bst]));
+            advance(it);
         }
         cp_wait<0>();
         // bulk copies still in flight (after an abort) land before the CTA exits:
-        // only the group's last kAhead / 2 blocks can be outstanding
+        // only the group's last kAhead / kGroups blocks can be outstanding
         if (gtid == 0)
-            for (int k = 0; k < kAhead / 2; ++k) {
-                const int u = last_issued - 2 * k;
+            for (int k = 0; k < kAhead / kGroups; ++k) {
+                const int u = last_issued - kGroups * k;
                 if (u >= 0) wait_parity(smem_u32(&s_afull[u & (kRing - 1)]), (u32)((u >> 3) & 1));
             }
     } else if (warp == kMmaWarp) {
@@ -872,7 +898,9 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
         __syncwarp();
     } else {
         // -------------------------------------------------------------- epilogue
-        const int qd = warp;  // TMEM subpartition (lanes 32 qd ..)
+        // TMEM lane quadrant (lanes 32 qd ..); slot pairs [pp0, pp1) of each unit
+        const int qd = warp & 3;
+        const int pp0 = kEpiWarps == 8 ? warp >> 2 : 0, pp1 = kEpiWarps == 8 ? pp0 + 1 : kTS / 2;
         int r_limb = -1;
         u64 q = 0, one_q = 0, r64 = 0, r64q = 0;  // q_l, floor(2^64 / q_l), 2^64 mod q_l, Shoup companion
         Barrett bm{0, 0, 0};
@@ -901,12 +929,12 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                 r64q = shoup_quotient_dev(r64, q);
                 r_limb = l;
             }
-            // lane L of warp qd: row m = 16 qd + (L % 16); slot 2 p + (L / 16) of slot pair p
+            // lane L of warp qd: row m = 16 qd + (L % 16); slot 2 pp + (L / 16) of slot pair pp
             const u32 taddr = tmem + ((u32)(32 * qd) << 16) + (u32)(256 * (u & 1));
             const int m = 16 * qd + (lane & 15);
             const int gl = m >> 1, comp = m & 1, g = g0 + gl;
             const bool row_ok = gl < gn;
-            for (int pp = 0; pp < kTS / 2; ++pp) {
+            for (int pp = pp0; pp < pp1; ++pp) {
                 const int i = 2 * pp + (lane >> 4);
                 const u32 s = s0 + i;
                 for (int cb = 0; cb < kCt; cb += 4) {
@@ -976,7 +1004,7 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
     // Bounded keys use the tensor-core MAC with up to 16 ciphertexts per group
     // (each key word read once per group), as far as device memory allows;
     // otherwise groups of 4 on the CUDA-core tiled MAC.
-    bool use_tc = bounded && n >= (u32)tc::kTS && D <= 4096 && ctx->tensor_cores && tc_enabled();
+    bool use_tc = bounded && n >= (u32)tc::kTS && D < 4096 && ctx->tensor_cores && tc_enabled();
     // the tensor-core MAC reads the keys' packed set (made on first use)
     const PackedSet* pset = use_tc ? packed_set_get(ctx, keys, n_keys, st) : nullptr;
     use_tc = pset != nullptr;
@@ -990,8 +1018,9 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
     }
     const int cap = 1024;
     const LimbMap lqp = LimbMap::qp(ctx, Lq);
-    const size_t y_stride = (size_t)D * LK * n, d_stride = (size_t)D * n, f_stride = (size_t)n + 1;
-    Workspace<u64> Y, acc, Z, karr;
+    const size_t y_stride = (size_t)D * LK * n, d_stride = (size_t)D * n, f_stride = (size_t)n + 1,
+                 b_stride = (size_t)Lq * n;
+    Workspace<u64> Y, Bh, acc, Z, karr;
     Workspace<i64> dig;
     Workspace<u32> flags, cnt;
     Workspace<Exc> exc;
@@ -999,7 +1028,7 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
     int32_t rc;
     if ((rc = terr.alloc(1, st))) return rc;
     CKKS_CUDA_TRY(cudaMemsetAsync(terr.p, 0, sizeof(int), st));
-    if ((rc = Y.alloc(G * y_stride, st)) || (rc = acc.alloc((size_t)G * n_keys * 2 * LK * n, st)) || (rc = Z.alloc((size_t)G * n_keys * 2 * LK * n, st)) ||
+    if ((rc = Y.alloc(G * y_stride, st)) || (use_tc && (rc = Bh.alloc(G * b_stride, st))) || (rc = acc.alloc((size_t)G * n_keys * 2 * LK * n, st)) || (rc = Z.alloc((size_t)G * n_keys * 2 * LK * n, st)) ||
         (rc = karr.alloc(3 * (size_t)n_keys + ctx->moduli.size(), st)) || (rc = dig.alloc(G * d_stride, st)) ||
         (rc = flags.alloc(G * f_stride, st)) || (rc = cnt.alloc((size_t)G * n_keys, st)) ||
         (rc = exc.alloc((size_t)G * n_keys * cap, st)))
@@ -1032,6 +1061,10 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
                     return rc;
                 if ((rc = ntt_forward_digits_launch(ctx, dig.p + c * d_stride, Y.p + c * y_stride, D, lqp, LK, st)))
                     return rc;
+                // the tensor-core MAC takes P b as one more digit: NTT(b) on the Q limbs
+                if (use_tc && (rc = ntt_forward_launch_map(ctx, in, Bh.p + c * b_stride, 1, LimbMap::range(0, Lq), Lq,
+                                                           st)))
+                    return rc;
             } else {  // RNS blocks: ModUp of a, then transform (the permutation is the whole automorphism)
                 if ((rc = rnsblock_modup_launch(ctx, k0, in + (size_t)Lq * n, Y.p + c * y_stride, st))) return rc;
                 if ((rc = ntt_forward_launch_map(ctx, Y.p + c * y_stride, Y.p + c * y_stride, D, lqp, LK, st))) return rc;
@@ -1053,7 +1086,8 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
             CKKS_CUDA_TRY(cudaFuncSetAttribute(k_mac_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                (int)tc::kSmemBytes));
             k_mac_tc<<<n_tiles < n_sm ? n_tiles : n_sm, tc::kThreads, tc::kSmemBytes, st>>>(
-                Y.p, y_stride, pset->d, (int)pset->rg, d_keys, d_exps_inv, acc.p, ctx->d_tabs, lqp, (int)gn,
+                Y.p, y_stride, Bh.p, b_stride, (int)Lq, pset->d, (int)pset->rg, d_keys, d_exps_inv, acc.p,
+                ctx->d_tabs, lqp, (int)gn,
                 (int)n_keys, (int)LK, (int)D, (int)ctx->log_n, exc.p, cnt.p, cap, d_psi, terr.p);
         } else {
             const size_t smem = (size_t)(G >= 3 ? 4 : G) * D * kS * sizeof(u64);
@@ -1086,8 +1120,8 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
         pt.begin(4);
         // inverse transform; the b components get P b of their ciphertext added on the
         // Q limbs (ModDown(x + P b) = ModDown(x) + b: the base term of the rotation)
-        InvBase ib;
-        ib.b = ct_in + (size_t)c0 * ct_words;
+        InvBase ib;  // the tensor-core MAC already added P NTT(b) (base digit)
+        ib.b = use_tc ? nullptr : ct_in + (size_t)c0 * ct_words;
         ib.b_stride = ct_words;
         ib.n_keys = n_keys;
         ib.q_limbs = Lq;
