@@ -542,15 +542,22 @@ constexpr int kJc = 4;            // digits per chunk (K = 32 bytes)
 #endif
 constexpr int kEpiWarps = CKKS_TC_EPI_WARPS;
 constexpr int kBStages = CKKS_TC_BSTAGES;      // B operand stages
-constexpr int kRing = 8;                       // A / Y prefetch ring depth
-constexpr int kAhead = kRing - kBStages;       // items fetched ahead
+constexpr int kRing = 8;                       // Y prefetch ring depth
+constexpr int kAhead = kRing - kBStages;       // items whose Y is fetched ahead
+#ifndef CKKS_TC_ARING
+#define CKKS_TC_ARING 16
+#endif
+constexpr int kARing = CKKS_TC_ARING;          // A (packed key block) ring depth
+constexpr int kAAhead = kARing - 2 * kBStages;  // items whose A block is fetched ahead
 constexpr int kGroups = (12 - kEpiWarps) / 4;  // producer groups of 4 warps
 constexpr int kProdWarp0 = kEpiWarps, kMmaWarp = 12;
 constexpr int kThreads = 416;                  // 13 warps: epilogue, producers, 1 MMA
 constexpr int kGrp = 128, kEpi = 32 * kEpiWarps;  // threads per producer group, epilogue threads
 constexpr int kBarGrp0 = 1, kBarEpi = 3;       // named barriers: producer groups 1, 2; epilogue 3
 static_assert((kEpiWarps == 4 || kEpiWarps == 8) && (kBStages == 2 || kBStages == 4), "tuning range");
-static_assert(kAhead % kGroups == 0 && kBStages % kGroups == 0, "a group prefetches and builds its own items");
+static_assert(kAhead % kGroups == 0 && kAAhead % kGroups == 0 && kBStages % kGroups == 0,
+              "a group prefetches and builds its own items");
+static_assert((kARing & (kARing - 1)) == 0 && kAAhead >= kAhead, "A ring");
 // A (packed key block, bulk-copied): row groups of 1 KB, slot i at 256 i, K
 // chunks 128 B apart. B strides are padded (slot and digit strides off
 // multiples of 128 B) so the producers' shared-memory stores spread over the banks.
@@ -560,14 +567,18 @@ constexpr u32 kBSlot = 4368;                   // 4 digits x 8 weights x 128 B (
 constexpr u32 kAStage = 8192;                  // 8 row groups
 constexpr u32 kYStage = kCt * kJc * kTS * 8;   // 2048: Y words [c][jj][i]
 constexpr u32 kBStage = kTS * kBSlot;          // 17472
-constexpr u32 kOffY = kRing * kAStage;                     // 64 KB of A
+constexpr u32 kOffY = kARing * kAStage;                    // A ring
 constexpr u32 kOffB = kOffY + kRing * kYStage;             // 16 KB of Y
 constexpr u32 kOffCnt = kOffB + kBStages * kBStage;        // correction counts [c][g], g < kCntKeys
 constexpr int kCntKeys = 256;
-constexpr u32 kSmemBytes = kOffCnt + kCt * kCntKeys * 4;   // 133 KB (2 B stages) or 168 KB (4): one CTA per SM
+constexpr u32 kSmemBytes = kOffCnt + kCt * kCntKeys * 4;   // 197 KB (16 A slots, 2 B stages): one CTA per SM
 static_assert(kSmemBytes <= 227 * 1024, "shared memory per CTA");
 constexpr u32 kTmemCols = 512;
-constexpr long long kSpin = 1ll << 22;         // bounded waits (iterations)
+// Bounded waits: a waiting thread sleeps in mbarrier.try_wait (woken when the
+// phase completes, at the latest after kSuspendNs) so spinning warps do not
+// take issue slots from the working ones; it gives up after kWaitCycles.
+constexpr u32 kSuspendNs = 20000;
+constexpr long long kWaitCycles = 1ll << 31;   // about a second
 
 __device__ __forceinline__ u32 smem_u32(const void* p) { return (u32)__cvta_generic_to_shared(p); }
 
@@ -601,16 +612,17 @@ __device__ __forceinline__ void arrive(u32 bar) {
 
 // true once the phase with the given parity has completed (bounded)
 __device__ __forceinline__ bool wait_parity(u32 bar, u32 parity) {
-    for (long long it = 0; it < kSpin; ++it) {
+    const long long t0 = clock64();
+    do {
         u32 done;
         asm volatile(
-            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
             "selp.u32 %0, 1, 0, p;\n\t}\n"
             : "=r"(done)
-            : "r"(bar), "r"(parity)
+            : "r"(bar), "r"(parity), "r"(kSuspendNs)
             : "memory");
         if (done) return true;
-    }
+    } while (clock64() - t0 < kWaitCycles);
     return false;
 }
 
@@ -684,7 +696,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     // ready / empty: B stages (producer group -> MMA, MMA -> producer group);
     // full / free: TMEM accumulator halves (MMA -> epilogue, epilogue -> MMA);
     // afull: A ring slots (bulk copy -> MMA)
-    __shared__ __align__(8) uint64_t s_ready[kBStages], s_empty[kBStages], s_full[2], s_free[2], s_afull[kRing];
+    __shared__ __align__(8) uint64_t s_ready[kBStages], s_empty[kBStages], s_full[2], s_free[2], s_afull[kARing];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const u32 n = 1u << log_n;
     const int n_tiles_s = (int)(n / kTS), lts = log_n - 2;  // tiles per limb (a power of two)
@@ -706,7 +718,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_full[i])), "r"(1));
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_free[i])), "r"(1));
         }
-        for (int i = 0; i < kRing; ++i)
+        for (int i = 0; i < kARing; ++i)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_afull[i])), "r"(1));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -741,21 +753,25 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
         const int yc = gtid >> 4;
         const u32 a_bytes = (u32)rg * 1024u;
         int last_issued = -1;  // last item whose block this thread copied (thread 0 of a group)
+        // A block of item t into A slot t % kARing (thread 0 of the group)
+        auto prefetch_a = [&](int t, const Item& it) {
+            if (t < n_items && gtid == 0) {
+                const int tile = (int)blockIdx.x + it.tl * (int)gridDim.x;
+                const u64* src = packed + ((((size_t)tile * n_kc + it.kc) * n_chunks + it.ch) * (size_t)rg << 7);
+                const u32 bar = smem_u32(&s_afull[t & (kARing - 1)]);
+                asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}\n"
+                             ::"r"(bar), "r"(a_bytes) : "memory");
+                asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                             ::"r"(sbase + (u32)(t & (kARing - 1)) * kAStage), "l"(src), "r"(a_bytes), "r"(bar)
+                             : "memory");
+                last_issued = t;
+            }
+        };
         auto prefetch = [&](int t, const Item& it) {
             if (t < n_items) {
                 const int tile = (int)blockIdx.x + it.tl * (int)gridDim.x;
                 const int l = tile >> lts;
                 const u32 s0 = (u32)(tile & (n_tiles_s - 1)) * kTS;
-                if (gtid == 0) {
-                    const u64* src = packed + ((((size_t)tile * n_kc + it.kc) * n_chunks + it.ch) * (size_t)rg << 7);
-                    const u32 bar = smem_u32(&s_afull[t & (kRing - 1)]);
-                    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}\n"
-                                 ::"r"(bar), "r"(a_bytes) : "memory");
-                    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                                 ::"r"(sbase + (u32)(t & (kRing - 1)) * kAStage), "l"(src), "r"(a_bytes), "r"(bar)
-                                 : "memory");
-                    last_issued = t;
-                }
                 // digit j < D: the digit transform; j == D: NTT(b) on the Q limbs
                 const int j = it.ch * kJc + pjj;
                 const bool jok = j < D, bok = j == D && l < Lq;
@@ -777,7 +793,11 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
         };
         Item it{0, 0, 0};
         if (grp) it.next(n_kc, n_chunks);
-        Item ahead = it;
+        Item ahead = it, ahead_a = it;
+        for (int k = 0; k < kAAhead / kGroups; ++k) {
+            prefetch_a(grp + kGroups * k, ahead_a);
+            advance(ahead_a);
+        }
         for (int k = 0; k < kAhead / kGroups; ++k) {
             prefetch(grp + kGroups * k, ahead);
             advance(ahead);
@@ -799,6 +819,10 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                 }
                 break;
             }
+            // the MMAs of item t - kBStages (and so of t + kAAhead - kARing) are done:
+            // A slot (t + kAAhead) % kARing and Y slot (t + kAhead) % kRing are free
+            prefetch_a(t + kAAhead, ahead_a);
+            advance(ahead_a);
             prefetch(t + kAhead, ahead);
             advance(ahead);
             cp_wait<kAhead / kGroups>();  // this thread's copies of item t have landed
@@ -849,11 +873,11 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
         }
         cp_wait<0>();
         // bulk copies still in flight (after an abort) land before the CTA exits:
-        // only the group's last kAhead / kGroups blocks can be outstanding
+        // only the group's last kAAhead / kGroups blocks can be outstanding
         if (gtid == 0)
-            for (int k = 0; k < kAhead / kGroups; ++k) {
+            for (int k = 0; k < kAAhead / kGroups; ++k) {
                 const int u = last_issued - kGroups * k;
-                if (u >= 0) wait_parity(smem_u32(&s_afull[u & (kRing - 1)]), (u32)((u >> 3) & 1));
+                if (u >= 0) wait_parity(smem_u32(&s_afull[u & (kARing - 1)]), (u32)((u / kARing) & 1));
             }
     } else if (warp == kMmaWarp) {
         // ------------------------------------------------------------- MMA issue
@@ -873,13 +897,13 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                         s_abort = 1;
                     }
                 }
-                if (!s_abort && !wait_parity(smem_u32(&s_afull[t & (kRing - 1)]), (u32)((t >> 3) & 1))) {
+                if (!s_abort && !wait_parity(smem_u32(&s_afull[t & (kARing - 1)]), (u32)((t / kARing) & 1))) {
                     atomicExch(err, 5);
                     s_abort = 1;
                 }
                 if (s_abort) break;
                 fence_after();
-                const u32 a0 = sbase + (u32)(t & (kRing - 1)) * kAStage, b0 = sbase + kOffB + (u32)bst * kBStage;
+                const u32 a0 = sbase + (u32)(t & (kARing - 1)) * kAStage, b0 = sbase + kOffB + (u32)bst * kBStage;
                 // accumulator of slot i: columns 256 buf + 128 (i / 2), TMEM lanes 16 (i % 2) + ..
                 const u32 dbase = tmem + (u32)(256 * (unit & 1));
 #pragma unroll
@@ -903,6 +927,8 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
         const int pp0 = kEpiWarps == 8 ? warp >> 2 : 0, pp1 = kEpiWarps == 8 ? pp0 + 1 : kTS / 2;
         int r_limb = -1;
         u64 q = 0, one_q = 0, r64 = 0, r64q = 0;  // q_l, floor(2^64 / q_l), 2^64 mod q_l, Shoup companion
+        u64 r32 = 0, r32q = 0;                    // 2^32 mod q_l, Shoup companion
+        bool wide_q = false;                      // q_l > 2^49.5: the two-half combine below applies
         Barrett bm{0, 0, 0};
         for (int u = 0; u < n_units; ++u) {
             const int tl = u / n_kc, kc = u - tl * n_kc;
@@ -927,6 +953,9 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                 one_q = (~0ull) / q;                 // floor(2^64 / q), q odd
                 r64 = (u64)(-(q * one_q));           // 2^64 mod q
                 r64q = shoup_quotient_dev(r64, q);
+                r32 = (1ull << 32) % q;
+                r32q = shoup_quotient_dev(r32, q);
+                wide_q = q > 0x2D413CCCFE779ull;  // floor(2^49.5)
                 r_limb = l;
             }
             // lane L of warp qd: row m = 16 qd + (L % 16); slot 2 pp + (L / 16) of slot pair pp
@@ -945,14 +974,20 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                     for (int cc = 0; cc < 4; ++cc) {
                         const int c = cb + cc;
                         if (!row_ok || c >= n_ct) continue;
-                        // sum_a 2^(8a) P_a with P_a < 2^25: pairwise in 64 bits, then 128
+                        // sum_a 2^(8a) P_a with P_a < 2^25 as L + 2^32 H, L and H < 2^49.01
                         const u32* P = r + 8 * cc;
-                        const u64 p01 = (u64)P[0] + ((u64)P[1] << 8), p23 = (u64)P[2] + ((u64)P[3] << 8);
-                        const u64 p45 = (u64)P[4] + ((u64)P[5] << 8), p67 = (u64)P[6] + ((u64)P[7] << 8);
-                        const u64 lo4 = p01 + (p23 << 16), hi4 = p45 + (p67 << 16);  // each < 2^51
-                        const u64 lo = lo4 + (hi4 << 32);
-                        const u64 hi = (hi4 >> 32) + (lo < lo4);                    // < 2^20
-                        u64 v = add_mod(reduce_2q(mul_shoup_lazy(lo, 1, one_q, q), q), mul_shoup(hi, r64, r64q, q), q);
+                        const u64 L = (u64)P[0] + ((u64)P[1] << 8) + ((u64)P[2] << 16) + ((u64)P[3] << 24);
+                        const u64 H = (u64)P[4] + ((u64)P[5] << 8) + ((u64)P[6] << 16) + ((u64)P[7] << 24);
+                        u64 v;
+                        if (wide_q) {
+                            // L < q: 2^32 H mod q lazily in [0, 2q), plus L, below 3q
+                            v = mul_shoup_lazy(H, r32, r32q, q) + L;
+                            v = v >= 2 * q ? v - 2 * q : v;
+                            v = v >= q ? v - q : v;
+                        } else {
+                            const u64 lo = L + (H << 32), hi = (H >> 32) + (lo < L);  // exact 128-bit sum
+                            v = add_mod(reduce_2q(mul_shoup_lazy(lo, 1, one_q, q), q), mul_shoup(hi, r64, r64q, q), q);
+                        }
                         // pairs whose list overflowed are recomputed by the exact fallback: skip them here
                         u32 cnt = cnt_staged ? s_cnt[c * n_keys + g] : exc_count[(size_t)c * n_keys + g];
                         if (cnt > (u32)cap) cnt = 0;

@@ -246,16 +246,18 @@ def test_hoisted_ntt_domain_corrections(oracle, cuda, small, base_log):
         assert np.array_equal(got[i], want), i
 
 
-@pytest.mark.parametrize("base_log", [8, 32])
-def test_tensor_core_mac_equals_cuda_core_mac(oracle, cuda, base_log):
+@pytest.mark.parametrize("base_log,q_bits", [(8, 50), (32, 50), (20, 40)])
+def test_tensor_core_mac_equals_cuda_core_mac(oracle, cuda, base_log, q_bits):
     """The INT8 tensor-core key-switch MAC and the CUDA-core MAC give the same
     words: 16 ciphertexts x 40 Galois keys (two key chunks, the second partial)
-    at N=2^12, plus an oracle check of a few (ciphertext, key) pairs."""
+    at N=2^12, plus an oracle check of a few (ciphertext, key) pairs. 40-bit
+    primes take the epilogue's general 128-bit reduction, 50/60-bit ones the
+    two-half form."""
     log_n, n = 12, 1 << 12
-    q = [int(x) for x in oracle.primes_below_bits(50, n, 6)]
+    q = [int(x) for x in oracle.primes_below_bits(q_bits, n, 6)]
     p = [int(x) for x in oracle.primes_below_bits(60, n, 2)]
     ctx = cb.Context(log_n, q, p)
-    rng = np.random.default_rng(70 + base_log)
+    rng = np.random.default_rng(70 + base_log + q_bits)
     s = rng.integers(-1, 2, n).astype(np.int8)
     ks = [ctx.rotation_exponent_left(r) for r in range(1, 41)]
     keys = [cb.KeySwitchKey.hybrid_generate(ctx, len(q), base_log, k, s, seed=900 + i) for i, k in enumerate(ks)]
