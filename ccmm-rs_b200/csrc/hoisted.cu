@@ -963,6 +963,17 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
             const int m = 16 * qd + (lane & 15);
             const int gl = m >> 1, comp = m & 1, g = g0 + gl;
             const bool row_ok = gl < gn;
+            // ciphertexts of this row whose (ciphertext, key) pair has carry corrections
+            // (lists that overflowed are recomputed by the exact fallback: skipped here)
+            u32 corr = 0;
+            if (row_ok)
+                for (int c = 0; c < n_ct; ++c) {
+                    const u32 cnt = cnt_staged ? s_cnt[c * n_keys + g] : exc_count[(size_t)c * n_keys + g];
+                    if (cnt && cnt <= (u32)cap) corr |= 1u << c;
+                }
+            // output word (c, s) at acc_row + c * c_stride + s
+            u64* acc_row = acc + (((((size_t)g * 2 + comp) * LK + l) << log_n) + s0);
+            const size_t c_stride = ((size_t)n_keys * 2 * LK) << log_n;
             for (int pp = pp0; pp < pp1; ++pp) {
                 const int i = 2 * pp + (lane >> 4);
                 const u32 s = s0 + i;
@@ -970,32 +981,39 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                     u32 r[32];
                     __syncwarp();
                     tmem_ld32(taddr + (u32)(pp * 128 + 8 * cb), r);
+                    // sum_a 2^(8a) P_a with P_a < 2^25 as L + 2^32 H (L, H < 2^49.01) for the
+                    // 4 ciphertexts at once: independent chains, no branches
+                    u64 v[4];
+                    if (wide_q) {
 #pragma unroll
-                    for (int cc = 0; cc < 4; ++cc) {
-                        const int c = cb + cc;
-                        if (!row_ok || c >= n_ct) continue;
-                        // sum_a 2^(8a) P_a with P_a < 2^25 as L + 2^32 H, L and H < 2^49.01
-                        const u32* P = r + 8 * cc;
-                        const u64 L = (u64)P[0] + ((u64)P[1] << 8) + ((u64)P[2] << 16) + ((u64)P[3] << 24);
-                        const u64 H = (u64)P[4] + ((u64)P[5] << 8) + ((u64)P[6] << 16) + ((u64)P[7] << 24);
-                        u64 v;
-                        if (wide_q) {
+                        for (int cc = 0; cc < 4; ++cc) {
+                            const u32* P = r + 8 * cc;
+                            const u64 L = (u64)P[0] + ((u64)P[1] << 8) + ((u64)P[2] << 16) + ((u64)P[3] << 24);
+                            const u64 H = (u64)P[4] + ((u64)P[5] << 8) + ((u64)P[6] << 16) + ((u64)P[7] << 24);
                             // L < q: 2^32 H mod q lazily in [0, 2q), plus L, below 3q
-                            v = mul_shoup_lazy(H, r32, r32q, q) + L;
-                            v = v >= 2 * q ? v - 2 * q : v;
-                            v = v >= q ? v - q : v;
-                        } else {
-                            const u64 lo = L + (H << 32), hi = (H >> 32) + (lo < L);  // exact 128-bit sum
-                            v = add_mod(reduce_2q(mul_shoup_lazy(lo, 1, one_q, q), q), mul_shoup(hi, r64, r64q, q), q);
+                            u64 x = mul_shoup_lazy(H, r32, r32q, q) + L;
+                            x = x >= 2 * q ? x - 2 * q : x;
+                            v[cc] = x >= q ? x - q : x;
                         }
-                        // pairs whose list overflowed are recomputed by the exact fallback: skip them here
-                        u32 cnt = cnt_staged ? s_cnt[c * n_keys + g] : exc_count[(size_t)c * n_keys + g];
-                        if (cnt > (u32)cap) cnt = 0;
-                        if (cnt) {
+                    } else {
+#pragma unroll
+                        for (int cc = 0; cc < 4; ++cc) {
+                            const u32* P = r + 8 * cc;
+                            const u64 L = (u64)P[0] + ((u64)P[1] << 8) + ((u64)P[2] << 16) + ((u64)P[3] << 24);
+                            const u64 H = (u64)P[4] + ((u64)P[5] << 8) + ((u64)P[6] << 16) + ((u64)P[7] << 24);
+                            const u64 lo = L + (H << 32), hi = (H >> 32) + (lo < L);  // exact 128-bit sum
+                            v[cc] = add_mod(reduce_2q(mul_shoup_lazy(lo, 1, one_q, q), q), mul_shoup(hi, r64, r64q, q), q);
+                        }
+                    }
+                    if ((corr >> cb) & 15) {  // rare: sparse carry corrections of the hoisted digits
+                        const u64 ps = psi[lm(l)];
+                        const u32 k = galois_src(s, exps_inv[g], log_n);
+                        const u64* key = keys[g];
+                        for (int cc = 0; cc < 4; ++cc) {
+                            const int c = cb + cc;
+                            if (!((corr >> c) & 1)) continue;
+                            const u32 cnt = cnt_staged ? s_cnt[c * n_keys + g] : exc_count[(size_t)c * n_keys + g];
                             const Exc* list = exc + ((size_t)c * n_keys + g) * cap;
-                            const u64 ps = psi[lm(l)];
-                            const u32 k = galois_src(s, exps_inv[g], log_n);
-                            const u64* key = keys[g];
                             for (u32 e = 0; e < cnt; ++e) {
                                 const Exc xe = list[e];
                                 u64 wv = pow_mod_dev(ps, ((2ull * k + 1) * xe.t) & (2ull * n - 1), bm);
@@ -1003,10 +1021,14 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                                 if (xe.delta < 0 && dm) dm = q - dm;
                                 const u64 tv = mul_barrett(wv, dm, bm);
                                 const size_t kofs = (((size_t)xe.j * LK + l) * 2 + comp) << log_n;
-                                v = add_mod(v, mul_barrett(tv, key[kofs + s], bm), q);
+                                v[cc] = add_mod(v[cc], mul_barrett(tv, key[kofs + s], bm), q);
                             }
                         }
-                        acc[(((((size_t)c * n_keys + g) * 2 + comp) * LK + l) << log_n) + s] = v;
+                    }
+                    if (row_ok) {
+#pragma unroll
+                        for (int cc = 0; cc < 4; ++cc)
+                            if (cb + cc < n_ct) acc_row[(size_t)(cb + cc) * c_stride + i] = v[cc];
                     }
                 }
             }
