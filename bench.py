@@ -83,6 +83,11 @@ class Clocks:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # let nvidia-smi start up (and take its first sample) before the timed
+            # region, so its start-up does not overlap the timed launches
+            t = time.time()
+            while not self.lines and time.time() - t < 5.0 and self.proc.poll() is None:
+                time.sleep(0.05)
         except Exception:
             self.proc = None
 

@@ -540,6 +540,9 @@ constexpr int kJc = 4;            // digits per chunk (K = 32 bytes)
 #ifndef CKKS_TC_BSTAGES
 #define CKKS_TC_BSTAGES 2
 #endif
+#ifndef CKKS_TC_PROD_WARPS
+#define CKKS_TC_PROD_WARPS 8
+#endif
 constexpr int kEpiWarps = CKKS_TC_EPI_WARPS;
 constexpr int kBStages = CKKS_TC_BSTAGES;      // B operand stages
 constexpr int kRing = 8;                       // Y prefetch ring depth
@@ -549,12 +552,13 @@ constexpr int kAhead = kRing - kBStages;       // items whose Y is fetched ahead
 #endif
 constexpr int kARing = CKKS_TC_ARING;          // A (packed key block) ring depth
 constexpr int kAAhead = kARing - 2 * kBStages;  // items whose A block is fetched ahead
-constexpr int kGroups = (12 - kEpiWarps) / 4;  // producer groups of 4 warps
-constexpr int kProdWarp0 = kEpiWarps, kMmaWarp = 12;
-constexpr int kThreads = 416;                  // 13 warps: epilogue, producers, 1 MMA
+constexpr int kGroups = CKKS_TC_PROD_WARPS / 4;  // producer groups of 4 warps
+constexpr int kProdWarp0 = kEpiWarps, kMmaWarp = kEpiWarps + CKKS_TC_PROD_WARPS;
+constexpr int kThreads = 32 * (kMmaWarp + 1);  // epilogue, producers, 1 MMA warp
 constexpr int kGrp = 128, kEpi = 32 * kEpiWarps;  // threads per producer group, epilogue threads
 constexpr int kBarGrp0 = 1, kBarEpi = 3;       // named barriers: producer groups 1, 2; epilogue 3
-static_assert((kEpiWarps == 4 || kEpiWarps == 8) && (kBStages == 2 || kBStages == 4), "tuning range");
+static_assert((kEpiWarps == 4 || kEpiWarps == 8) && (kBStages == 2 || kBStages == 4) &&
+                  (CKKS_TC_PROD_WARPS == 4 || CKKS_TC_PROD_WARPS == 8), "tuning range");
 static_assert(kAhead % kGroups == 0 && kAAhead % kGroups == 0 && kBStages % kGroups == 0,
               "a group prefetches and builds its own items");
 static_assert((kARing & (kARing - 1)) == 0 && kAAhead >= kAhead, "A ring");
@@ -868,7 +872,14 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             named_sync(bar, kGrp);
-            if (gtid == 0) arrive(smem_u32(&s_ready[bst]));
+            if (gtid == 0) {
+                // the item's key block has landed before its B operand is announced
+                if (!wait_parity(smem_u32(&s_afull[t & (kARing - 1)]), (u32)((t / kARing) & 1))) {
+                    atomicExch(err, 5);
+                    s_abort = 1;  // ready is still announced; the MMA warp stops on the flag
+                }
+                arrive(smem_u32(&s_ready[bst]));
+            }
             advance(it);
         }
         cp_wait<0>();
@@ -884,25 +895,27 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
         if (lane == 0) {
             Item it{0, 0, 0};
             int unit = -1, last_t = -1;
+            // Every mbarrier wait costs the issuing thread a few hundred cycles even when the
+            // phase is complete, and the MMAs of one item issue back to back: per item this
+            // thread waits on `ready` only (the producers have already seen the key block
+            // land), and on `free` (plus the tcgen05 fence for the TMEM reuse) once per unit.
             for (int t = 0; t < n_items; ++t, it.next(n_kc, n_chunks)) {
                 const int bst = t & (kBStages - 1);
                 if (!wait_parity(smem_u32(&s_ready[bst]), (u32)((t / kBStages) & 1))) {
                     atomicExch(err, 2);
                     s_abort = 1;
+                    break;
                 }
                 if (it.ch == 0) {
                     ++unit;
-                    if (unit >= 2 && !wait_parity(smem_u32(&s_free[unit & 1]), (u32)(((unit >> 1) - 1) & 1))) {
+                    if ((unit >= 2 && !wait_parity(smem_u32(&s_free[unit & 1]), (u32)(((unit >> 1) - 1) & 1))) ||
+                        s_abort) {
                         atomicExch(err, 3);
                         s_abort = 1;
+                        break;
                     }
+                    fence_after();
                 }
-                if (!s_abort && !wait_parity(smem_u32(&s_afull[t & (kARing - 1)]), (u32)((t / kARing) & 1))) {
-                    atomicExch(err, 5);
-                    s_abort = 1;
-                }
-                if (s_abort) break;
-                fence_after();
                 const u32 a0 = sbase + (u32)(t & (kARing - 1)) * kAStage, b0 = sbase + kOffB + (u32)bst * kBStage;
                 // accumulator of slot i: columns 256 buf + 128 (i / 2), TMEM lanes 16 (i % 2) + ..
                 const u32 dbase = tmem + (u32)(256 * (unit & 1));
