@@ -38,6 +38,8 @@ _SIGS = {
     "ckks_ctx_destroy": (I32, [VP]),
     "ckks_ctx_set_tensor_cores": (I32, [VP, I32]),
     "ckks_ctx_tensor_cores": (I32, [VP]),
+    "ckks_ctx_autotune": (I32, [VP, U32, U32, VP]),
+    "ckks_ctx_tuning_report": (I32, [VP, ctypes.c_char_p, ctypes.c_uint64]),
     "ckks_ctx_psi": (I32, [VP, u64p]),
     "ckks_ntt_forward": (I32, [VP, VP, VP, U32, U32, U32, VP]),
     "ckks_ntt_inverse": (I32, [VP, VP, VP, U32, U32, U32, VP]),
@@ -183,6 +185,18 @@ class Context:
     @tensor_cores.setter
     def tensor_cores(self, enable):
         check(lib().ckks_ctx_set_tensor_cores(self.handle, 1 if enable else 0))
+
+    def autotune(self, limbs, polys, stream=None):
+        """Times the NTT passes' tile choices on a limbs x polys batch, keeps the
+        fastest, and returns the record."""
+        check(lib().ckks_ctx_autotune(self.handle, int(limbs), int(polys), _stream(stream)))
+        return self.tuning_report
+
+    @property
+    def tuning_report(self):
+        buf = ctypes.create_string_buffer(8192)
+        check(lib().ckks_ctx_tuning_report(self.handle, buf, len(buf)))
+        return buf.value.decode()
 
     def close(self):
         if getattr(self, "handle", None):

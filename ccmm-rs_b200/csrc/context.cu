@@ -379,6 +379,24 @@ int32_t ckks_ctx_set_tensor_cores(ckks_ctx* ctx, int32_t enable) {
     return CKKS_OK;
 }
 
+int32_t ckks_ctx_autotune(ckks_ctx* ctx, uint32_t limbs, uint32_t polys, void* stream) {
+    CKKS_CHECK_ARG(ctx != nullptr, "ckks_ctx_autotune: ctx is null");
+    cudaStream_t st = ckks_stream(ctx, stream);
+    const int32_t rc = ntt_autotune(ctx, limbs, polys, st);
+    if (rc == CKKS_OK) CKKS_CUDA_TRY(cudaStreamSynchronize(st));
+    return rc;
+}
+
+int32_t ckks_ctx_tuning_report(const ckks_ctx* ctx, char* buf, uint64_t len) {
+    CKKS_CHECK_ARG(ctx != nullptr && buf != nullptr && len > 0, "ckks_ctx_tuning_report: bad arguments");
+    const std::string& r = ctx->tuning_report.empty() ? std::string("NTT: built-in tile choices (not tuned)\n")
+                                                      : ctx->tuning_report;
+    const size_t n = r.size() < len - 1 ? r.size() : (size_t)(len - 1);
+    memcpy(buf, r.data(), n);
+    buf[n] = 0;
+    return CKKS_OK;
+}
+
 int32_t ckks_ctx_tensor_cores(const ckks_ctx* ctx) {
     if (!ctx) return 0;
     return ctx->tensor_cores && tc_enabled() ? 1 : 0;

@@ -68,6 +68,10 @@ struct ckks_ctx {
     // key-switch MAC of bounded hoisted rotations: tcgen05 INT8 tensor cores
     // (when the device has them) or the CUDA-core split-accumulator form
     bool tensor_cores = true;
+    // NTT columns per CTA (log2) per pass: forward 1, forward 1 of digits,
+    // forward 2, inverse 1, inverse 2; -1 = built-in choice; set by the autotuner
+    int ntt_log_c[5] = {-1, -1, -1, -1, -1};
+    std::string tuning_report;
 };
 
 // ---------------------------------------------------------------- errors
@@ -130,6 +134,9 @@ struct InvBase {
 };
 int32_t ntt_inverse_base_launch(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, LimbMap lm, u32 limb_count,
                                 const InvBase& ib, cudaStream_t st);
+// Times every admissible columns-per-CTA choice of the five NTT passes on a
+// scratch batch (limbs x polys) and keeps the fastest in ctx (ntt.cu).
+int32_t ntt_autotune(ckks_ctx* ctx, u32 limbs, u32 polys, cudaStream_t st);
 inline LimbMap LimbMap::qp(const ckks_ctx* c, u32 q_limbs) { return LimbMap{0, (int)q_limbs, (int)c->L}; }
 // Stream-ordered workspace (cudaMallocAsync / cudaFreeAsync on `st`).
 template <typename T>

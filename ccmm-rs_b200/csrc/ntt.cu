@@ -19,6 +19,8 @@
 // shared-memory exchange, and every global access is a 128-byte segment.
 // Butterflies are Harvey-lazy in [0, 4q) with Shoup multiplication
 // (__umul64hi); outputs are canonical.
+#include <cstdio>
+
 #include "ntt_core.cuh"
 
 namespace {
@@ -282,18 +284,24 @@ __global__ void __launch_bounds__(kMaxThreads) k_inv2(const u64* src, u64* dst, 
     }
 }
 
-// columns per CTA: min(16, available, 256 / RMAX)
+// columns per CTA: min(16, available, 256 / RMAX), or the tuned choice `pref`
+// when it is within those limits
 template <int LOG_M>
-int pick_log_c(int log_avail) {
+int max_log_c(int log_avail) {
     int lc = 4;
     while ((Split<LOG_M>::RMAX << lc) > kMaxThreads) --lc;
     return lc < log_avail ? lc : log_avail;
 }
+template <int LOG_M>
+int pick_log_c(int log_avail, int pref) {
+    const int mx = max_log_c<LOG_M>(log_avail);
+    return pref >= 0 && pref <= mx ? pref : mx;
+}
 
 template <int LOG_M>
 int32_t launch_pass(int which, const void* in, u64* out, const NttTab* tabs, LimbMap lm, u32 limbs, u32 polys,
-                    int log_other, cudaStream_t st, const InvBase& ib) {
-    const int lc = pick_log_c<LOG_M>(log_other);
+                    int log_other, cudaStream_t st, const InvBase& ib, int lc_pref) {
+    const int lc = pick_log_c<LOG_M>(log_other, lc_pref);
     const int threads = Split<LOG_M>::RMAX << lc;
     const size_t smem = (sizeof(u64) << (LOG_M + lc)) + 2 * sizeof(u64) * (1u << LOG_M);
     dim3 grid(1u << (log_other - lc), limbs, polys);
@@ -308,21 +316,21 @@ int32_t launch_pass(int which, const void* in, u64* out, const NttTab* tabs, Lim
 }
 
 int32_t pass(int which, int log_m, const void* in, u64* out, const NttTab* tabs, LimbMap lm, u32 limbs, u32 polys,
-             int log_other, cudaStream_t st, const InvBase& ib = InvBase{}) {
+             int log_other, cudaStream_t st, const InvBase& ib = InvBase{}, int lc_pref = -1) {
     if (polys > 65535 || limbs > 65535) {  // grid y / z limits
         ckks_set_error("NTT: more than 65535 polynomials or limbs in one launch");
         return CKKS_ERR_BAD_ARG;
     }
     switch (log_m) {
-        case 1: return launch_pass<1>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib);
-        case 2: return launch_pass<2>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib);
-        case 3: return launch_pass<3>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib);
-        case 4: return launch_pass<4>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib);
-        case 5: return launch_pass<5>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib);
-        case 6: return launch_pass<6>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib);
-        case 7: return launch_pass<7>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib);
-        case 8: return launch_pass<8>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib);
-        case 9: return launch_pass<9>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib);
+        case 1: return launch_pass<1>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib, lc_pref);
+        case 2: return launch_pass<2>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib, lc_pref);
+        case 3: return launch_pass<3>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib, lc_pref);
+        case 4: return launch_pass<4>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib, lc_pref);
+        case 5: return launch_pass<5>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib, lc_pref);
+        case 6: return launch_pass<6>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib, lc_pref);
+        case 7: return launch_pass<7>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib, lc_pref);
+        case 8: return launch_pass<8>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib, lc_pref);
+        case 9: return launch_pass<9>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib, lc_pref);
         default: ckks_set_error("NTT: unsupported transform size"); return CKKS_ERR_BAD_ARG;
     }
 }
@@ -351,8 +359,8 @@ int32_t ntt_forward_launch_map(ckks_ctx* ctx, const u64* in, u64* out, u32 n_pol
         if (int32_t rc = tmp.alloc((size_t)n_polys * limb_count * ctx->n, st)) return rc;
         mid = tmp.p;
     }
-    if (int32_t rc = pass(0, la, in, mid, ctx->d_tabs, lm, limb_count, n_polys, lb, st)) return rc;
-    if (int32_t rc = pass(2, lb, mid, out, ctx->d_tabs, lm, limb_count, n_polys, la, st)) return rc;
+    if (int32_t rc = pass(0, la, in, mid, ctx->d_tabs, lm, limb_count, n_polys, lb, st, InvBase{}, ctx->ntt_log_c[0])) return rc;
+    if (int32_t rc = pass(2, lb, mid, out, ctx->d_tabs, lm, limb_count, n_polys, la, st, InvBase{}, ctx->ntt_log_c[2])) return rc;
     CKKS_CUDA_TRY(cudaGetLastError());
     return CKKS_OK;
 }
@@ -372,8 +380,8 @@ int32_t ntt_inverse_base_launch(ckks_ctx* ctx, const u64* in, u64* out, u32 n_po
         if (int32_t rc = tmp.alloc((size_t)n_polys * limb_count * ctx->n, st)) return rc;
         mid = tmp.p;
     }
-    if (int32_t rc = pass(3, lb, in, mid, ctx->d_tabs, lm, limb_count, n_polys, la, st)) return rc;
-    if (int32_t rc = pass(4, la, mid, out, ctx->d_tabs, lm, limb_count, n_polys, lb, st, ib)) return rc;
+    if (int32_t rc = pass(3, lb, in, mid, ctx->d_tabs, lm, limb_count, n_polys, la, st, InvBase{}, ctx->ntt_log_c[3])) return rc;
+    if (int32_t rc = pass(4, la, mid, out, ctx->d_tabs, lm, limb_count, n_polys, lb, st, ib, ctx->ntt_log_c[4])) return rc;
     CKKS_CUDA_TRY(cudaGetLastError());
     return CKKS_OK;
 }
@@ -382,8 +390,8 @@ int32_t ntt_forward_digits_launch(ckks_ctx* ctx, const i64* digits, u64* out, u3
                                   cudaStream_t st) {
     if (D == 0 || limbs == 0) return CKKS_OK;
     const int la = ctx->log_n1, lb = ctx->log_n2;
-    if (int32_t rc = pass(1, la, digits, out, ctx->d_tabs, lm, limbs, D, lb, st)) return rc;
-    if (int32_t rc = pass(2, lb, out, out, ctx->d_tabs, lm, limbs, D, la, st)) return rc;
+    if (int32_t rc = pass(1, la, digits, out, ctx->d_tabs, lm, limbs, D, lb, st, InvBase{}, ctx->ntt_log_c[1])) return rc;
+    if (int32_t rc = pass(2, lb, out, out, ctx->d_tabs, lm, limbs, D, la, st, InvBase{}, ctx->ntt_log_c[2])) return rc;
     CKKS_CUDA_TRY(cudaGetLastError());
     return CKKS_OK;
 }
@@ -459,8 +467,105 @@ extern "C" int32_t ckks_ntt_forward_inplace_static(ckks_ctx* ctx, uint64_t* data
     cudaStream_t st = (cudaStream_t)stream;
     const LimbMap lm = LimbMap::range(limb_begin, limb_count);
     const int la = ctx->log_n1, lb = ctx->log_n2;
-    if (int32_t rc = pass(0, la, data, scratch, ctx->d_tabs, lm, limb_count, n_polys, lb, st)) return rc;
-    if (int32_t rc = pass(2, lb, scratch, data, ctx->d_tabs, lm, limb_count, n_polys, la, st)) return rc;
+    if (int32_t rc = pass(0, la, data, scratch, ctx->d_tabs, lm, limb_count, n_polys, lb, st, InvBase{}, ctx->ntt_log_c[0])) return rc;
+    if (int32_t rc = pass(2, lb, scratch, data, ctx->d_tabs, lm, limb_count, n_polys, la, st, InvBase{}, ctx->ntt_log_c[2])) return rc;
     CKKS_CUDA_TRY(cudaGetLastError());
     return CKKS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner: columns per CTA of every NTT pass.
+//
+// For each of the five passes (forward pass 1, forward pass 1 of signed digits,
+// forward pass 2, inverse pass 1, inverse pass 2) every admissible number of
+// columns per CTA (2^lc, lc = 1 .. the register/thread limit) is timed with CUDA
+// events on a scratch batch of polys x limbs zero polynomials (the passes'
+// running time does not depend on the data) and the fastest is kept in the
+// context; every later transform of that context uses it. The report lists
+// each pass's candidates and times (microseconds per launch) and the choice.
+namespace {
+
+template <int LOG_M>
+int max_lc_for(int log_other) { return max_log_c<LOG_M>(log_other); }
+
+int max_lc(int log_m, int log_other) {
+    switch (log_m) {
+        case 1: return max_lc_for<1>(log_other);
+        case 2: return max_lc_for<2>(log_other);
+        case 3: return max_lc_for<3>(log_other);
+        case 4: return max_lc_for<4>(log_other);
+        case 5: return max_lc_for<5>(log_other);
+        case 6: return max_lc_for<6>(log_other);
+        case 7: return max_lc_for<7>(log_other);
+        case 8: return max_lc_for<8>(log_other);
+        default: return max_lc_for<9>(log_other);
+    }
+}
+
+}  // namespace
+
+int32_t ntt_autotune(ckks_ctx* ctx, u32 limbs, u32 polys, cudaStream_t st) {
+    if (limbs == 0 || polys == 0 || limbs > ctx->L + ctx->K) {
+        ckks_set_error("ckks_ctx_autotune: limbs must be in [1, L + K] and polys >= 1");
+        return CKKS_ERR_BAD_ARG;
+    }
+    const int la = ctx->log_n1, lb = ctx->log_n2;
+    const LimbMap lm = LimbMap::range(0, limbs);
+    const size_t words = (size_t)polys * limbs * ctx->n;
+    Workspace<u64> a, b;
+    int32_t rc;
+    if ((rc = a.alloc(words, st)) || (rc = b.alloc(words, st))) return rc;
+    CKKS_CUDA_TRY(cudaMemsetAsync(a.p, 0, words * sizeof(u64), st));
+    cudaEvent_t e0, e1;
+    CKKS_CUDA_TRY(cudaEventCreate(&e0));
+    CKKS_CUDA_TRY(cudaEventCreate(&e1));
+    static const char* names[5] = {"forward pass 1", "forward pass 1 (digits)", "forward pass 2", "inverse pass 1",
+                                   "inverse pass 2"};
+    // pass: log_m, log_other, polys (digit pass: polys digits of one polynomial)
+    const int log_m[5] = {la, la, lb, lb, la}, log_o[5] = {lb, lb, la, la, lb};
+    std::string rep;
+    rc = CKKS_OK;
+    for (int w = 0; w < 5 && rc == CKKS_OK; ++w) {
+        const int mx = max_lc(log_m[w], log_o[w]);
+        int best = -1;
+        float best_ms = 0;
+        rep += names[w];
+        rep += ":";
+        for (int lc = mx < 1 ? mx : 1; lc <= mx && rc == CKKS_OK; ++lc) {
+            float ms = 0;
+            for (int it = 0; it < 4 && rc == CKKS_OK; ++it) {  // first launch untimed
+                if (it == 1) cudaEventRecord(e0, st);
+                rc = pass(w, log_m[w], a.p, b.p, ctx->d_tabs, lm, limbs, polys, log_o[w], st, InvBase{}, lc);
+            }
+            if (rc != CKKS_OK) break;
+            cudaEventRecord(e1, st);
+            if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+                rc = CKKS_ERR_CUDA;
+                ckks_set_error("ckks_ctx_autotune: event timing failed");
+                break;
+            }
+            ms /= 3;
+            char buf[64];
+            snprintf(buf, sizeof buf, " C=%d %.1f us", 1 << lc, 1000.0 * ms);
+            rep += buf;
+            if (best < 0 || ms < best_ms) {
+                best = lc;
+                best_ms = ms;
+            }
+        }
+        if (rc == CKKS_OK) {
+            ctx->ntt_log_c[w] = best;
+            char buf[64];
+            snprintf(buf, sizeof buf, " -> C=%d\n", 1 << best);
+            rep += buf;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc == CKKS_OK) {
+        char head[96];
+        snprintf(head, sizeof head, "NTT autotune N=2^%u, %u limbs x %u polys per launch\n", ctx->log_n, limbs, polys);
+        ctx->tuning_report = head + rep;
+    }
+    return rc;
 }

@@ -80,6 +80,15 @@ int32_t ckks_ctx_destroy(ckks_ctx* ctx);
 int32_t ckks_ctx_set_tensor_cores(ckks_ctx* ctx, int32_t enable);
 /* 1 when bounded hoisted rotations of this context use the tensor cores. */
 int32_t ckks_ctx_tensor_cores(const ckks_ctx* ctx);
+/* Autotuner (no counterpart in the reference, whose NTT has no launch shape):
+ * times every admissible columns-per-CTA choice of the five NTT passes
+ * (forward 1, forward 1 of signed digits, forward 2, inverse 1, inverse 2) on
+ * a scratch batch of `polys` polynomials x `limbs` limbs and keeps the fastest
+ * for every later transform of the context. Synchronous. */
+int32_t ckks_ctx_autotune(ckks_ctx* ctx, uint32_t limbs, uint32_t polys, void* stream);
+/* The autotuner's record (candidates, times, choices) as text, NUL-terminated,
+ * truncated to len - 1 characters. */
+int32_t ckks_ctx_tuning_report(const ckks_ctx* ctx, char* buf, uint64_t len);
 /* Writes the L+K roots psi (host array). */
 int32_t ckks_ctx_psi(const ckks_ctx* ctx, uint64_t* psi_host);
 

@@ -273,3 +273,34 @@ def test_tensor_core_mac_equals_cuda_core_mac(oracle, cuda, base_log, q_bits):
     for c, g in ((0, 0), (15, 39), (7, 33)):
         want = oracle.hybrid_rotate(q, p, keys[g].download(), ks[g], base_log, cts[c])
         assert np.array_equal(tc[c, g], want), (c, g)
+
+
+def test_tensor_core_mac_corrections_bit_exact(oracle, cuda):
+    """Tensor-core path (17 keys or more) with planted -B/2 digits: the carry
+    corrections of the NTT-domain hoisting are applied in the tensor-core
+    epilogue and the words equal the oracle's and the CUDA-core MAC's."""
+    log_n, n, base_log = 12, 1 << 12, 32
+    q = [int(x) for x in oracle.primes_below_bits(50, n, 4)]
+    p = [int(x) for x in oracle.primes_below_bits(60, n, 1)]
+    ctx = cb.Context(log_n, q, p)
+    rng = np.random.default_rng(91)
+    s = rng.integers(-1, 2, n).astype(np.int8)
+    cts = np.stack([np.stack([np.stack([rng.integers(0, m, n, dtype=np.uint64) for m in q]) for _ in range(2)])
+                    for _ in range(3)])
+    Q = 1
+    for m in q:
+        Q *= m
+    for c in range(0, n, 5):  # a-part values whose balanced digits contain -B/2
+        v = (Q - (1 << (base_log - 1)) * (1 + (c % 3) * (1 << base_log))) % Q
+        cts[0, 1, :, c] = [v % m for m in q]
+    ks = [ctx.rotation_exponent_left(r) for r in range(1, 18)] + [2 * n - 1]
+    keys = [cb.KeySwitchKey.hybrid_generate(ctx, len(q), base_log, k, s, seed=700 + i) for i, k in enumerate(ks)]
+    assert ctx.tensor_cores
+    tc = host(cb.rotate_hoisted(ctx, keys, dev(cts)))
+    ctx.tensor_cores = False
+    cc = host(cb.rotate_hoisted(ctx, keys, dev(cts)))
+    ctx.tensor_cores = True
+    assert np.array_equal(tc, cc)
+    for c, g in ((0, 0), (0, 17), (0, 9), (2, 3)):
+        want = oracle.hybrid_rotate(q, p, keys[g].download(), ks[g], base_log, cts[c])
+        assert np.array_equal(tc[c, g], want), (c, g)

@@ -110,3 +110,22 @@ def test_ntt_rejects_bad_arguments(cuda):
     with pytest.raises(cb.CkksError) as e:
         ctx.ntt_forward(d)  # 2 limbs requested, context has 1
     assert e.value.status == -2
+
+
+@pytest.mark.parametrize("log_n", [12, 16])
+def test_autotuned_ntt_stays_bit_exact(oracle, cuda, log_n):
+    """The autotuner records a choice for each of the five passes, and every
+    tile choice it can make gives the oracle's words (forward, inverse, digits)."""
+    n = 1 << log_n
+    moduli = [int(x) for x in oracle.primes_below_bits(50, n, 3)]
+    ctx = cb.Context(log_n, moduli)
+    assert "not tuned" in ctx.tuning_report
+    rep = ctx.autotune(limbs=3, polys=4)
+    assert rep.count("->") == 5, rep
+    rng = np.random.default_rng(log_n)
+    x = rand_polys(rng, moduli, n, 2)
+    d = cb.as_u64_tensor(x)
+    out = ctx.ntt_forward(d.clone())
+    assert np.array_equal(cb.to_numpy_u64(out), oracle.ntt_forward(moduli, x))
+    back = ctx.ntt_inverse(out)
+    assert np.array_equal(cb.to_numpy_u64(back), x)
