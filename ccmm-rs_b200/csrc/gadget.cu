@@ -107,11 +107,11 @@ __global__ void __launch_bounds__(kT) k_bounded_decompose(const u64* __restrict_
                                                           u32* __restrict__ flags, const NttTab* __restrict__ tabs,
                                                           GarnerQ g, const u64* __restrict__ half_mr,
                                                           const u64* __restrict__ q_words, int q_limbs, int L,
-                                                          int log_n, int base_log, int D) {
+                                                          int log_n, int base_log, int D, size_t poly_stride) {
     const u32 n = 1u << log_n;
     const u32 c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n) return;
-    const size_t pbase = (size_t)blockIdx.y * q_limbs << log_n;
+    const size_t pbase = (size_t)blockIdx.y * poly_stride;
     // mixed radix (Garner), v kept in registers/local memory
     u64 v[kMaxQ];
     bool neg = false;
@@ -290,7 +290,8 @@ int32_t bounded_digit_count(ckks_ctx* ctx, u32 q_limbs, u32 base_log, u32* out) 
 }
 
 int32_t bounded_decompose_launch(ckks_ctx* ctx, const u64* poly, u32 n_polys, u32 q_limbs, u32 base_log, i64* digits,
-                                 u32* flags, cudaStream_t st) {
+                                 u32* flags, cudaStream_t st, size_t poly_stride) {
+    if (!poly_stride) poly_stride = (size_t)q_limbs << ctx->log_n;
     u32 D;
     if (int32_t rc = bounded_digit_count(ctx, q_limbs, base_log, &D)) return rc;
     PrefixConst pc;
@@ -299,7 +300,7 @@ int32_t bounded_decompose_launch(ckks_ctx* ctx, const u64* poly, u32 n_polys, u3
     dim3 grid((ctx->n + kT - 1) / kT, n_polys);
 #define CKKS_DECOMP(WW)                                                                                          \
     k_bounded_decompose<WW><<<grid, kT, 0, st>>>(poly, digits, flags, ctx->d_tabs, ctx->garner, pc.d_half_mr,     \
-                                                 pc.d_q_words, q_limbs, ctx->L, ctx->log_n, base_log, D)
+                                                 pc.d_q_words, q_limbs, ctx->L, ctx->log_n, base_log, D, poly_stride)
     if (pc.W <= 4) CKKS_DECOMP(4);
     else if (pc.W <= 8) CKKS_DECOMP(8);
     else if (pc.W <= 16) CKKS_DECOMP(16);

@@ -25,8 +25,9 @@ int32_t mod_down_sigma_multi(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys
 
 // Bounded (balanced base-2^base_log) gadget, grafting/bounded_gadget.rs.
 int32_t bounded_digit_count(ckks_ctx* ctx, u32 q_limbs, u32 base_log, u32* out);
+// poly_stride: words between consecutive input polynomials (0: q_limbs N, contiguous)
 int32_t bounded_decompose_launch(ckks_ctx* ctx, const u64* poly, u32 n_polys, u32 q_limbs, u32 base_log, i64* digits,
-                                 u32* flags, cudaStream_t st);
+                                 u32* flags, cudaStream_t st, size_t poly_stride = 0);
 int32_t digits_automorphism_launch(ckks_ctx* ctx, const i64* in, i64* out, u32 n_polys, u32 D, u32 base_log, u64 k,
                                    cudaStream_t st);
 // Forward NTT of signed digits lifted to every limb of `lm` ([D][limbs][N] out).

@@ -11,6 +11,7 @@
 // The MAC accumulates exact 128-bit sums of products and reduces once per
 // 15 terms, so the result is the canonical residue of the same sum the
 // reference forms with pointwise_mul_add_assign (ring/ntt_polynomial.rs:222-236).
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -22,16 +23,21 @@ constexpr int kT = 256;
 
 // acc[0][l][k] = (l < Lq ? pf_l * base[l][pb(k)] : 0) + sum_j Y[j][l][py(k)] * key[j][l][0][k]
 // acc[1][l][k] =                                         sum_j Y[j][l][py(k)] * key[j][l][1][k]
-// py / pb: NTT-domain Galois source maps (k = 0: identity).
+// py / pb: NTT-domain Galois source maps (k = 0: identity). blockIdx.z batches
+// ciphertexts: Y, base and acc advance by y_stride, b_stride, a_stride words.
 __global__ void __launch_bounds__(kT) k_ks_mac(const u64* __restrict__ Y, const u64* __restrict__ key,
                                                const u64* __restrict__ base, const u64* __restrict__ pf,
                                                const u64* __restrict__ pf_q, u64* __restrict__ acc,
                                                const NttTab* __restrict__ tabs, LimbMap lm, int Lq, int LK, int D,
-                                               int log_n, u64 perm_y, u64 perm_b, u64 perm_key) {
+                                               int log_n, u64 perm_y, u64 perm_b, u64 perm_key, size_t y_stride,
+                                               size_t b_stride, size_t a_stride) {
     const u32 n = 1u << log_n;
     const u32 k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const int l = blockIdx.y;
+    Y += blockIdx.z * y_stride;
+    if (base) base += blockIdx.z * b_stride;
+    acc += blockIdx.z * a_stride;
     const NttTab& T = tabs[lm(l)];
     const u64 q = T.q, mu_hi = T.mu_hi, mu_lo = T.mu_lo;
     const u32 ky = perm_y ? galois_src(k, perm_y, log_n) : k;
@@ -295,12 +301,17 @@ std::vector<int8_t> host_secret_automorphism(const int8_t* s, u32 n, u64 k) { re
 
 // --------------------------------------------------------------- pipelines
 int32_t ks_mac_launch(ckks_ctx* ctx, const u64* Y, const u64* key, const u64* base, u64* acc, u32 q_limbs, u32 D,
-                      bool with_p, u64 perm_y, u64 perm_b, cudaStream_t st, u64 perm_key) {
+                      bool with_p, u64 perm_y, u64 perm_b, cudaStream_t st, u64 perm_key, u32 n_ct, size_t b_stride) {
     const u32 LK = with_p ? q_limbs + ctx->K : q_limbs;
     const LimbMap lm = with_p ? LimbMap::qp(ctx, q_limbs) : LimbMap::range(0, q_limbs);
-    dim3 g((ctx->n + kT - 1) / kT, LK, 1);
+    if (n_ct > 65535) {
+        ckks_set_error("key-switch MAC: more than 65535 ciphertexts in one launch");
+        return CKKS_ERR_BAD_ARG;
+    }
+    dim3 g((ctx->n + kT - 1) / kT, LK, n_ct);
     k_ks_mac<<<g, kT, 0, st>>>(Y, key, base, ctx->d_pmodq, ctx->d_pmodq + ctx->L, acc, ctx->d_tabs, lm, q_limbs, LK,
-                               D, ctx->log_n, perm_y, perm_b, perm_key);
+                               D, ctx->log_n, perm_y, perm_b, perm_key, ((size_t)D * LK) << ctx->log_n, b_stride,
+                               ((size_t)2 * LK) << ctx->log_n);
     CKKS_CUDA_TRY(cudaGetLastError());
     return CKKS_OK;
 }
@@ -320,28 +331,36 @@ int32_t rotate_hybrid(ckks_ctx* ctx, const ckks_ksk* key, const u64* ct_in, u64*
     }
     const u32 Lq = key->q_limbs, LK = ksk_limbs(key), D = key->D, n = ctx->n;
     const size_t ct_words = (size_t)2 * Lq * n;
+    // ciphertexts are batched through every launch, as many per batch as a few GB allow
+    const size_t per_ct = ct_words * 2 + (size_t)D * LK * n + 4 * (size_t)LK * n + (size_t)D * n;  // words
+    const u32 m_max = (u32)std::max<size_t>(1, std::min<size_t>({(size_t)n_ct, (size_t)65535,
+                                                                   ((size_t)4 << 30) / (per_ct * 8)}));
     Workspace<u64> ws;
     Workspace<i64> dg;
     int32_t rc;
-    if ((rc = ws.alloc(ct_words + (size_t)D * LK * n + 4 * (size_t)LK * n, st)) || (rc = dg.alloc((size_t)D * n, st)))
+    if ((rc = ws.alloc((size_t)m_max * (per_ct - (size_t)D * n), st)) || (rc = dg.alloc((size_t)m_max * D * n, st)))
         return rc;
-    u64* sct = ws.p;                    // sigma(ct) [2][Lq][N]
-    u64* b_hat = sct + (size_t)Lq * n;  // NTT(sigma b), written over sigma(a) once it is decomposed
-    u64* Y = sct + ct_words;            // [D][LK][N]
-    u64* acc = Y + (size_t)D * LK * n;  // [2][LK][N]
-    u64* Z = acc + (size_t)2 * LK * n;  // [2][LK][N]
+    u64* sct = ws.p;                               // sigma(ct) [m][2][Lq][N]
+    u64* s_hat = sct + (size_t)m_max * ct_words;   // NTT(sigma(ct)) [m][2][Lq][N]; the b parts are the base
+    u64* Y = s_hat + (size_t)m_max * ct_words;     // [m][D][LK][N]
+    u64* acc = Y + (size_t)m_max * D * LK * n;     // [m][2][LK][N]
+    u64* Z = acc + (size_t)m_max * 2 * LK * n;     // [m][2][LK][N]
     const LimbMap lq = LimbMap::range(0, Lq), lqp = LimbMap::qp(ctx, Lq);
-    for (u32 i = 0; i < n_ct; ++i) {
-        const u64* in = ct_in + (size_t)i * ct_words;
-        u64* out = ct_out + (size_t)i * ct_words;
-        if ((rc = automorphism_coef_launch(ctx, in, sct, 2, lq, Lq, key->exponent, st))) return rc;
-        if ((rc = bounded_decompose_launch(ctx, sct + (size_t)Lq * n, 1, Lq, key->base_log, dg.p, nullptr, st)))
+    for (u32 c0 = 0; c0 < n_ct; c0 += m_max) {
+        const u32 m = n_ct - c0 < m_max ? n_ct - c0 : m_max;
+        const u64* in = ct_in + (size_t)c0 * ct_words;
+        u64* out = ct_out + (size_t)c0 * ct_words;
+        if ((rc = automorphism_coef_launch(ctx, in, sct, 2 * m, lq, Lq, key->exponent, st))) return rc;
+        if ((rc = bounded_decompose_launch(ctx, sct + (size_t)Lq * n, m, Lq, key->base_log, dg.p, nullptr, st,
+                                           ct_words)))
             return rc;
-        if ((rc = ntt_forward_digits_launch(ctx, dg.p, Y, D, lqp, LK, st))) return rc;
-        if ((rc = ntt_forward_launch_map(ctx, sct, b_hat, 1, lq, Lq, st))) return rc;
-        if ((rc = ks_mac_launch(ctx, Y, key->d_entries, b_hat, acc, Lq, D, true, 0, 0, st, key->exponent))) return rc;
-        if ((rc = ntt_inverse_launch_map(ctx, acc, Z, 2, lqp, LK, st))) return rc;
-        if ((rc = mod_down_launch(ctx, Z, out, 2, Lq, st))) return rc;
+        if ((rc = ntt_forward_digits_launch(ctx, dg.p, Y, D * m, lqp, LK, st))) return rc;
+        if ((rc = ntt_forward_launch_map(ctx, sct, s_hat, 2 * m, lq, Lq, st))) return rc;
+        if ((rc = ks_mac_launch(ctx, Y, key->d_entries, s_hat, acc, Lq, D, true, 0, 0, st, key->exponent, m,
+                                ct_words)))
+            return rc;
+        if ((rc = ntt_inverse_launch_map(ctx, acc, Z, 2 * m, lqp, LK, st))) return rc;
+        if ((rc = mod_down_launch(ctx, Z, out, 2 * m, Lq, st))) return rc;
     }
     return CKKS_OK;
 }

@@ -40,8 +40,10 @@ std::vector<int8_t> host_secret_automorphism(const int8_t* s, u32 n, u64 k);
 int32_t rnsblock_prepare(ckks_ctx* ctx, ckks_ksk* key);
 int32_t rnsblock_modup_launch(ckks_ctx* ctx, const ckks_ksk* key, const u64* a, u64* Y, cudaStream_t st);
 
+// n_ct ciphertexts: Y [n_ct][D][LK][N], base b_stride words apart, acc [n_ct][2][LK][N]
 int32_t ks_mac_launch(ckks_ctx* ctx, const u64* Y, const u64* key, const u64* base, u64* acc, u32 q_limbs, u32 D,
-                      bool with_p, u64 perm_y, u64 perm_b, cudaStream_t st, u64 perm_key = 0);
+                      bool with_p, u64 perm_y, u64 perm_b, cudaStream_t st, u64 perm_key = 0, u32 n_ct = 1,
+                      size_t b_stride = 0);
 // Galois key entries [D][LK][2][N]: reference layout <-> permuted storage.
 int32_t ksk_permute_entries(ckks_ctx* ctx, const u64* src, u64* dst, size_t polys, u64 exponent, bool to_storage,
                             cudaStream_t st);
