@@ -483,10 +483,10 @@ def bench_rot_gpu(args, world, rank, local):
                  + rots * 2 * LK * n * 8)
     peak, kind = peaks()
     # DRAM traffic per launch: an ncu capture of k_mac_tc on the same limbs,
-    # digits, keys and ciphertexts at N=2^11 read 1.424 GB and wrote 0.488 GB for
+    # digits, keys and ciphertexts at N=2^11 read 1.430 GB and wrote 0.447 GB for
     # 1.804 GB of algorithmic bytes; every term scales with N, so the full launch
     # moves the same multiple of its algorithmic bytes
-    mac_traffic = mac_bytes * (1.424 + 0.488) / 1.804
+    mac_traffic = mac_bytes * (1.430 + 0.447) / 1.804
     mac_ms = phases["key-switch MAC"]
     achieved = mac_bytes / (mac_ms / 1000.0) / 1e9
     ct_bytes = 2 * ROT_L * n * 8
