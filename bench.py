@@ -616,6 +616,7 @@ def bench_mul_gpu(args, world, rank, local):
     dev = torch.device("cuda", local)
     n = 1 << MUL_LOG_N
     ctx = cb.Context(MUL_LOG_N, MUL_Q, MUL_P)
+    tuning = ctx.autotune(limbs=len(MUL_Q) + len(MUL_P), polys=64)  # NTT tile choices, outside the timed region
     rng = np.random.default_rng(99 + rank)
     secret = rng.integers(-1, 2, n).astype(np.int8)
     rk = cb.KeySwitchKey.relin_generate(ctx, 3, MUL_BASE_LOG, secret, seed=5)
@@ -684,7 +685,8 @@ def bench_mul_gpu(args, world, rank, local):
         "metric": "HMult+relinearize+rescale+rotate chains/s (N=2^12, 3 limbs, bit-exact)", "value": value,
         "unit": "chains/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "u64", "data": "synthetic (seeded uniform ciphertexts, GPU-generated keys)", "config": mul_config(),
+        "dtype": "u64", "data": "synthetic (seeded uniform ciphertexts, GPU-generated keys)",
+        "config": dict(mul_config(), autotune=tuning.strip().splitlines()),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "peak_kind": kind,
                      "kernel": "whole chain (working set fits L2: launch/latency-bound)",
@@ -750,6 +752,7 @@ def bench_ccmm_gpu(args, world, rank, local):
     n, d, L = 1 << CCMM_LOG_N, CCMM_D, CCMM_L
     q = ccmm_primes()
     ctx = cb.Context(CCMM_LOG_N, q)
+    tuning = ctx.autotune(limbs=len(q), polys=64)  # NTT tile choices, outside the timed region
     rng = np.random.default_rng(31 + rank)
     secret = rng.integers(-1, 2, n).astype(np.int8)
     rk = cb.KeySwitchKey.relin_generate(ctx, L, CCMM_BASE_LOG, secret, seed=9)
@@ -812,7 +815,7 @@ def bench_ccmm_gpu(args, world, rank, local):
         "unit": "CCMM/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u64", "data": "synthetic (seeded uniform ciphertext residues, GPU-generated key)",
-        "config": ccmm_config(),
+        "config": dict(ccmm_config(), autotune=tuning.strip().splitlines()),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "peak_kind": kind, "kernel": "whole CCMM (operands, product, key stream)",
                      "algorithmic_bytes_per_step": bytes_step},
@@ -877,6 +880,7 @@ def bench_fft2_gpu(args, world, rank, local):
     q = params.primes_below_bits(50, n, FFT2_L)
     p = params.primes_below_bits(60, n, FFT2_K)
     ctx = cb.Context(FFT2_LOG_N, q, p)
+    tuning = ctx.autotune(limbs=len(q) + len(p), polys=64)  # NTT tile choices, outside the timed region
     rng = np.random.default_rng(55 + rank)
     secret = rng.integers(-1, 2, n).astype(np.int8)
     plan = fft2.Fft2Plan(ctx, FFT2_S, FFT2_L, secret, base_log=FFT2_BASE_LOG)
@@ -931,7 +935,7 @@ def bench_fft2_gpu(args, world, rank, local):
         "value": value, "unit": "images/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u64", "data": "synthetic (seeded uniform ciphertexts, GPU-generated keys, GPU-encoded diagonals)",
-        "config": fft2_config(),
+        "config": dict(fft2_config(), autotune=tuning.strip().splitlines()),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "peak_kind": kind,
                      "kernel": "whole FFT2 (key streams and stage ciphertexts; rotations per step: %d)" % rotations,

@@ -98,9 +98,12 @@ __device__ __forceinline__ u64 split_fold(const Split3& a, u64 q, u64 one_q, u64
 
 // One CTA per (slot s, limb l): for the output block [m] x [nc] (columns
 // c_begin ..), C0/C1/C2 = sums over k of the products of At (m x k, entry
-// r + kk m) and Bt (k x n, entry kk + c k). Each thread owns 2 x 2 outputs.
-// Partial sums are folded into the canonical residue every `fold_k` terms.
-__global__ void __launch_bounds__(kT) k_ccmm_slot(const u64* __restrict__ At, const u64* __restrict__ Bt,
+// r + kk m) and Bt (k x n, entry kk + c k). Each thread owns one row and two
+// adjacent columns (8 independent split products per k); consecutive threads
+// take consecutive rows, so the A reads of a warp are contiguous and its B
+// reads broadcast. Partial sums are folded into the canonical residue every
+// `fold_k` terms.
+__global__ void __launch_bounds__(kT, 2) k_ccmm_slot(const u64* __restrict__ At, const u64* __restrict__ Bt,
                                                   u64* __restrict__ Ct, const NttTab* __restrict__ tabs, int m,
                                                   int kd, int nd, int c_begin, int nc, int log_n) {
     extern __shared__ u64 sm[];
@@ -126,72 +129,52 @@ __global__ void __launch_bounds__(kT) k_ccmm_slot(const u64* __restrict__ At, co
         b_s[i] = bsrc[(size_t)comp * kd * nd + (size_t)c_begin * kd + j];
     }
     __syncthreads();
-    const int mh = (m + 1) / 2, nh = (nc + 1) / 2;
+    const int pairs = (nc + 1) / 2;
     u64* cdst = Ct + slot * 3 * (size_t)(m * nc);
-    for (int blk = threadIdx.x; blk < mh * nh; blk += blockDim.x) {
-        const int r0 = 2 * (blk % mh), cc0 = 2 * (blk / mh);
-        Split3 acc[3][2][2];
+    for (int item = threadIdx.x; item < m * pairs; item += blockDim.x) {
+        const int r = item % m, c0 = 2 * (item / m);
+        const bool c1ok = c0 + 1 < nc;
+        const int cb0 = c0 * kd, cb1 = (c1ok ? c0 + 1 : c0) * kd;
+        Split3 acc[3][2];
+        u64 res[3][2];
 #pragma unroll
         for (int t = 0; t < 3; ++t)
-#pragma unroll
-            for (int i = 0; i < 2; ++i)
-#pragma unroll
-                for (int j = 0; j < 2; ++j) acc[t][i][j] = Split3{0, 0, 0};
-        u64 res[3][2][2];
-#pragma unroll
-        for (int t = 0; t < 3; ++t)
-#pragma unroll
-            for (int i = 0; i < 2; ++i)
-#pragma unroll
-                for (int j = 0; j < 2; ++j) res[t][i][j] = 0;
-        const bool r1ok = r0 + 1 < m, c1ok = cc0 + 1 < nc;
-        int since = 0;
-        for (int kk = 0; kk < kd; ++kk) {
-            u64 ab[2], aa[2], bb[2], ba[2];
-#pragma unroll
-            for (int i = 0; i < 2; ++i) {
-                const int r = (i && !r1ok) ? r0 : r0 + i;
-                ab[i] = a_s[kk * m + r];
-                aa[i] = a_s[m * kd + kk * m + r];
-            }
 #pragma unroll
             for (int j = 0; j < 2; ++j) {
-                const int c = (j && !c1ok) ? cc0 : cc0 + j;
-                bb[j] = b_s[c * kd + kk];
-                ba[j] = b_s[kd * nc + c * kd + kk];
+                acc[t][j] = Split3{0, 0, 0};
+                res[t][j] = 0;
             }
+        int since = 0;
+        for (int kk = 0; kk < kd; ++kk) {
+            const u64 ab = a_s[kk * m + r], aa = a_s[m * kd + kk * m + r];
+            const u64 bb[2] = {b_s[cb0 + kk], b_s[cb1 + kk]};
+            const u64 ba[2] = {b_s[kd * nc + cb0 + kk], b_s[kd * nc + cb1 + kk]};
 #pragma unroll
-            for (int i = 0; i < 2; ++i)
-#pragma unroll
-                for (int j = 0; j < 2; ++j) {
-                    acc[0][i][j].mac(ab[i], bb[j]);
-                    acc[1][i][j].mac(ab[i], ba[j]);
-                    acc[1][i][j].mac(aa[i], bb[j]);
-                    acc[2][i][j].mac(aa[i], ba[j]);
-                }
+            for (int j = 0; j < 2; ++j) {
+                acc[0][j].mac(ab, bb[j]);
+                acc[1][j].mac(ab, ba[j]);
+                acc[1][j].mac(aa, bb[j]);
+                acc[2][j].mac(aa, ba[j]);
+            }
             if (++since == fold_k) {
 #pragma unroll
                 for (int t = 0; t < 3; ++t)
 #pragma unroll
-                    for (int i = 0; i < 2; ++i)
-#pragma unroll
-                        for (int j = 0; j < 2; ++j) {
-                            res[t][i][j] = add_mod(res[t][i][j], split_fold(acc[t][i][j], q, one_q, r1, r1q, r2, r2q), q);
-                            acc[t][i][j] = Split3{0, 0, 0};
-                        }
+                    for (int j = 0; j < 2; ++j) {
+                        res[t][j] = add_mod(res[t][j], split_fold(acc[t][j], q, one_q, r1, r1q, r2, r2q), q);
+                        acc[t][j] = Split3{0, 0, 0};
+                    }
                 since = 0;
             }
         }
 #pragma unroll
         for (int t = 0; t < 3; ++t)
 #pragma unroll
-            for (int i = 0; i < 2; ++i)
-#pragma unroll
-                for (int j = 0; j < 2; ++j) {
-                    if ((i && !r1ok) || (j && !c1ok)) continue;
-                    const u64 v = add_mod(res[t][i][j], split_fold(acc[t][i][j], q, one_q, r1, r1q, r2, r2q), q);
-                    cdst[(size_t)t * m * nc + (size_t)(cc0 + j) * m + r0 + i] = v;
-                }
+            for (int j = 0; j < 2; ++j) {
+                if (j && !c1ok) continue;
+                const u64 v = add_mod(res[t][j], split_fold(acc[t][j], q, one_q, r1, r1q, r2, r2q), q);
+                cdst[(size_t)t * m * nc + (size_t)(c0 + j) * m + r] = v;
+            }
     }
 }
 
@@ -236,8 +219,9 @@ int32_t ccmm_structured_launch(ckks_ctx* ctx, const ckks_ksk* key, const u64* A,
     if ((rc = At.alloc(slots * 2 * m * kd, st)) || (rc = Bt.alloc(slots * 2 * kd * nd, st))) return rc;
     if ((rc = build_slot_major(ctx, A, At.p, m * kd, L, st))) return rc;
     if ((rc = build_slot_major(ctx, B, Bt.p, kd * nd, L, st))) return rc;
-    // output columns per chunk: slot-major products plus entry-major quadratic parts within about 2^30 words
-    u32 cc = (u32)((size_t(1) << 30) / (slots * 3 * m * 2));
+    // output columns per chunk: slot-major products plus entry-major quadratic parts within about 1.5 x 2^30 words
+    u32 cc = (u32)((size_t(3) << 29) / (slots * 3 * m * 2));
+    if (cc > 2) cc &= ~1u;  // whole column pairs per thread
     if (cc > 32767 / m) cc = 32767 / m;  // grid limits of the per-chunk transforms and rescale
     if (cc < 1) cc = 1;
     if (cc > nd) cc = nd;
