@@ -103,7 +103,7 @@ __device__ __forceinline__ u64 split_fold(const Split3& a, u64 q, u64 one_q, u64
 // take consecutive rows, so the A reads of a warp are contiguous and its B
 // reads broadcast. Partial sums are folded into the canonical residue every
 // `fold_k` terms.
-__global__ void __launch_bounds__(kT, 2) k_ccmm_slot(const u64* __restrict__ At, const u64* __restrict__ Bt,
+__global__ void __launch_bounds__(kT, 3) k_ccmm_slot(const u64* __restrict__ At, const u64* __restrict__ Bt,
                                                   u64* __restrict__ Ct, const NttTab* __restrict__ tabs, int m,
                                                   int kd, int nd, int c_begin, int nc, int log_n) {
     extern __shared__ u64 sm[];
@@ -219,8 +219,8 @@ int32_t ccmm_structured_launch(ckks_ctx* ctx, const ckks_ksk* key, const u64* A,
     if ((rc = At.alloc(slots * 2 * m * kd, st)) || (rc = Bt.alloc(slots * 2 * kd * nd, st))) return rc;
     if ((rc = build_slot_major(ctx, A, At.p, m * kd, L, st))) return rc;
     if ((rc = build_slot_major(ctx, B, Bt.p, kd * nd, L, st))) return rc;
-    // output columns per chunk: slot-major products plus entry-major quadratic parts within about 1.5 x 2^30 words
-    u32 cc = (u32)((size_t(3) << 29) / (slots * 3 * m * 2));
+    // output columns per chunk: slot-major products plus entry-major quadratic parts within about 2^31 words
+    u32 cc = (u32)((size_t(1) << 31) / (slots * 3 * m * 2));
     if (cc > 2) cc &= ~1u;  // whole column pairs per thread
     if (cc > 32767 / m) cc = 32767 / m;  // grid limits of the per-chunk transforms and rescale
     if (cc < 1) cc = 1;
