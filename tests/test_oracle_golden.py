@@ -39,7 +39,8 @@ def test_psi_constants(oracle):
         assert oracle.root(case["q"], case["n"]) == case["psi"]
         if case["q"] < (1 << 62):
             assert params.negacyclic_root(case["q"], case["n"]) == case["psi"]
-    # SURVEY Appendix A values (same rule): C1 q0 and the first N=2^16 50-bit prime
+    # roots of the reference's prime search (same smallest-generator rule): the 60-bit
+    # prime of the N=2^12 chain and the first 50-bit prime for N=2^16
     assert oracle.root(0xfffffffffffc001, 4096) == 431606828070683274
     assert oracle.root(0x3ffffffd20001, 65536) == 1077102403560341
     assert params.negacyclic_root(0x3ffffffd20001, 65536) == 1077102403560341
