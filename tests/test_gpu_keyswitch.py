@@ -304,3 +304,26 @@ def test_tensor_core_mac_corrections_bit_exact(oracle, cuda):
     for c, g in ((0, 0), (0, 17), (0, 9), (2, 3)):
         want = oracle.hybrid_rotate(q, p, keys[g].download(), ks[g], base_log, cts[c])
         assert np.array_equal(tc[c, g], want), (c, g)
+
+
+def test_packed_key_sets_follow_key_lifetimes(oracle, cuda):
+    """The tensor-core MAC's packed key set is rebuilt when a key of the list is
+    destroyed and a new one takes its place (the cache never serves a stale set)."""
+    log_n, n, base_log = 12, 1 << 12, 32
+    q = [int(x) for x in oracle.primes_below_bits(50, n, 3)]
+    p = [int(x) for x in oracle.primes_below_bits(60, n, 1)]
+    ctx = cb.Context(log_n, q, p)
+    rng = np.random.default_rng(123)
+    s = rng.integers(-1, 2, n).astype(np.int8)
+    cts = np.stack([np.stack([np.stack([rng.integers(0, m, n, dtype=np.uint64) for m in q]) for _ in range(2)])
+                    for _ in range(2)])
+    ks = [ctx.rotation_exponent_left(r) for r in range(1, 19)]
+    keys = [cb.KeySwitchKey.hybrid_generate(ctx, len(q), base_log, k, s, seed=40 + i) for i, k in enumerate(ks)]
+    first = host(cb.rotate_hoisted(ctx, keys, dev(cts)))
+    for trial in range(2):
+        keys[5].close()  # frees the key and every packed set that holds it
+        keys[5] = cb.KeySwitchKey.hybrid_generate(ctx, len(q), base_log, ks[5], s, seed=1000 + trial)
+        got = host(cb.rotate_hoisted(ctx, keys, dev(cts)))
+        want5 = oracle.hybrid_rotate(q, p, keys[5].download(), ks[5], base_log, cts[1])
+        assert np.array_equal(got[1, 5], want5)
+        assert np.array_equal(got[:, :5], first[:, :5]) and np.array_equal(got[:, 6:], first[:, 6:])
