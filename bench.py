@@ -536,6 +536,7 @@ def bench_rot_gpu(args, world, rank, local):
     }
     # kernels of one step, counted after every timed region (the tracing hooks stay out of the timing)
     counted = count_launches(step)
+    decoded = rot_decoded_error(cb, ctx, keys, ROT_STEPS, secret, q, n)
     line = {
         "metric": "key-switched rotations/s (N=2^16, 24 limbs, hoisted, bit-exact)", "value": value,
         "unit": "rotations/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -551,6 +552,7 @@ def bench_rot_gpu(args, world, rank, local):
         "whole_rotation_roofline": {"bytes_per_rotation": key_bytes + 2 * ct_bytes,
                                     "frac_no_key_reuse": (key_bytes + 2 * ct_bytes) * value / 1e9 / peak},
         "phases_ms_per_step": phases,
+        "decoded_error": decoded,
         "tensor_cores": ctx.tensor_cores,
         "plain_gpu": plain_gpu,
         "e2e": {"value": rots * e2e_steps * world / e2e_s, "unit": "rotations/s",
@@ -561,6 +563,36 @@ def bench_rot_gpu(args, world, rank, local):
         "clocks": clk,
     }
     return line
+
+
+def rot_decoded_error(cb, ctx, keys, steps, secret, q, n, seed=77):
+    """Decoded error of the rotations against FP64 (numpy) rotations of the
+    cleartext, outside every timed region and through the library alone: one
+    fresh encryption under the bench's secret (b = m + e - a s, sigma 3.2, scale
+    2^50) is rotated by every key, decrypted (b + a s) and decoded on the GPU.
+    Returns the largest relative L2 error over the keys and its log2."""
+    import torch
+    rng = np.random.default_rng(seed)
+    L, K = len(q), len(keys)
+    x = rng.uniform(-1, 1, n // 2) + 1j * rng.uniform(-1, 1, n // 2)
+    scale = 2.0 ** 50
+    m = cb.encode(ctx, x, L, scale)
+    a = cb.as_u64_tensor(np.stack([rng.integers(0, qi, n, dtype=np.uint64) for qi in q]))
+    e_int = np.rint(rng.normal(0.0, 3.2, n)).astype(np.int64)
+    e = cb.as_u64_tensor(np.stack([(e_int % qi).astype(np.uint64) for qi in q]))
+    s_res = cb.as_u64_tensor(np.stack([(secret.astype(np.int64) % qi).astype(np.uint64) for qi in q]))
+    s_hat = ctx.ntt_forward(s_res.clone())
+    a_s = ctx.ntt_inverse(ctx.pointwise(ctx.ntt_forward(a.clone()), s_hat, "mul"))
+    b = ctx.pointwise(ctx.pointwise(m, e, "add"), a_s, "sub")
+    ct = torch.stack([b, a])[None].contiguous()
+    out = cb.rotate_hoisted(ctx, keys, ct)[0]                   # [K][2][L][N]
+    s_hat_k = s_hat[None].expand(K, L, n).contiguous()
+    a2s = ctx.ntt_inverse(ctx.pointwise(ctx.ntt_forward(out[:, 1].contiguous()), s_hat_k, "mul"))
+    dec = cb.decode(ctx, ctx.pointwise(out[:, 0].contiguous(), a2s, "add"), scale).cpu().numpy()
+    errs = [float(np.linalg.norm(dec[g] - np.roll(x, -steps[g])) / np.linalg.norm(x)) for g in range(K)]
+    worst = max(errs)
+    return {"rel_l2_max": worst, "log2": float(np.log2(worst)) if worst > 0 else None,
+            "check": "fresh encryption rotated by every key, decoded vs numpy.roll of the FP64 slots"}
 
 
 def rot_cpu_sample(threads, n_keys=2):
