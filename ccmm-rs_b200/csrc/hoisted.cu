@@ -1123,14 +1123,16 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
         CKKS_CUDA_TRY(cudaMemsetAsync(flags.p, 0, G * f_stride * sizeof(u32), st));
         CKKS_CUDA_TRY(cudaMemsetAsync(cnt.p, 0, (size_t)G * n_keys * sizeof(u32), st));
         pt.begin(0);
+        if (bounded) {  // the group's decompositions and digit transforms in one launch each
+            const u64* in0 = ct_in + (size_t)c0 * ct_words;
+            if ((rc = bounded_decompose_launch(ctx, in0 + (size_t)Lq * n, gn, Lq, k0->base_log, dig.p, flags.p, st,
+                                               ct_words)))
+                return rc;
+            if ((rc = ntt_forward_digits_launch(ctx, dig.p, Y.p, D * gn, lqp, LK, st))) return rc;
+        }
         for (u32 c = 0; c < gn; ++c) {
             const u64* in = ct_in + (size_t)(c0 + c) * ct_words;
             if (bounded) {
-                if ((rc = bounded_decompose_launch(ctx, in + (size_t)Lq * n, 1, Lq, k0->base_log, dig.p + c * d_stride,
-                                                   flags.p + c * f_stride, st)))
-                    return rc;
-                if ((rc = ntt_forward_digits_launch(ctx, dig.p + c * d_stride, Y.p + c * y_stride, D, lqp, LK, st)))
-                    return rc;
                 // the tensor-core MAC takes P b as one more digit: NTT(b) on the Q limbs
                 if (use_tc && (rc = ntt_forward_launch_map(ctx, in, Bh.p + c * b_stride, 1, LimbMap::range(0, Lq), Lq,
                                                            st)))
