@@ -1129,15 +1129,15 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
                                                ct_words)))
                 return rc;
             if ((rc = ntt_forward_digits_launch(ctx, dig.p, Y.p, D * gn, lqp, LK, st))) return rc;
+            if (use_tc) {  // the tensor-core MAC takes P b as one more digit: NTT(b) on the Q limbs
+                CKKS_CUDA_TRY(cudaMemcpy2DAsync(Bh.p, b_stride * sizeof(u64), in0, ct_words * sizeof(u64),
+                                                b_stride * sizeof(u64), gn, cudaMemcpyDeviceToDevice, st));
+                if ((rc = ntt_forward_launch_map(ctx, Bh.p, Bh.p, gn, LimbMap::range(0, Lq), Lq, st))) return rc;
+            }
         }
-        for (u32 c = 0; c < gn; ++c) {
+        for (u32 c = 0; c < gn && !bounded; ++c) {
             const u64* in = ct_in + (size_t)(c0 + c) * ct_words;
-            if (bounded) {
-                // the tensor-core MAC takes P b as one more digit: NTT(b) on the Q limbs
-                if (use_tc && (rc = ntt_forward_launch_map(ctx, in, Bh.p + c * b_stride, 1, LimbMap::range(0, Lq), Lq,
-                                                           st)))
-                    return rc;
-            } else {  // RNS blocks: ModUp of a, then transform (the permutation is the whole automorphism)
+            {  // RNS blocks: ModUp of a, then transform (the permutation is the whole automorphism)
                 if ((rc = rnsblock_modup_launch(ctx, k0, in + (size_t)Lq * n, Y.p + c * y_stride, st))) return rc;
                 if ((rc = ntt_forward_launch_map(ctx, Y.p + c * y_stride, Y.p + c * y_stride, D, lqp, LK, st))) return rc;
             }
