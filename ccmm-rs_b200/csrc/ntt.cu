@@ -29,6 +29,18 @@ using nttc::brev;
 
 constexpr int kMaxThreads = 256;
 
+// Resident CTAs of kMaxThreads per SM asked of the register allocator: 3 caps a
+// thread at 80 registers, 4 at 64. Tiles of up to 2^8 points fit those caps with
+// at most a few words of spill, and the extra resident warps hide the global
+// loads (forward pass 1 over digits: 1157 -> 953 us for 27 limbs x 64 polys of
+// N = 2^16 at 64 registers; the inverse passes gain about 3 % at 80). 2^9-point
+// tiles spill hundreds of bytes at either cap and keep the compiler's own
+// allocation (a minimum of 0 leaves the count unspecified).
+template <int LOG_M>
+constexpr int min_ctas(int want) {
+    return LOG_M <= 8 ? want : 0;
+}
+
 template <int LOG_M>
 struct Split {
     static constexpr int M = 1 << LOG_M;
@@ -57,9 +69,10 @@ __device__ __forceinline__ void stage_table(u64* st, const u64* __restrict__ v, 
 // kDigits: the input is a signed digit polynomial [D][N] shared by every limb
 // (blockIdx.z = digit), lifted on load (signed_mod, hybrid_rns_galois_key.rs:55-57).
 template <int LOG_M, bool kDigits>
-__global__ void __launch_bounds__(kMaxThreads) k_fwd1(const void* __restrict__ in_, u64* __restrict__ out,
-                                                      const NttTab* __restrict__ tabs, LimbMap lm, int limb_count,
-                                                      int log_b, int log_c) {
+__global__ void __launch_bounds__(kMaxThreads, min_ctas<LOG_M>(4))
+k_fwd1(const void* __restrict__ in_, u64* __restrict__ out,
+       const NttTab* __restrict__ tabs, LimbMap lm, int limb_count,
+       int log_b, int log_c) {
     using S = Split<LOG_M>;
     extern __shared__ u64 sm[];
     const int C = 1 << log_c, tid = threadIdx.x;
@@ -114,8 +127,9 @@ __global__ void __launch_bounds__(kMaxThreads) k_fwd1(const void* __restrict__ i
 // psi_2B = psi^A on {k_a + A j_lo}; output k_b = brev(r) stored at k_a + A k_b
 // (natural order). src may equal dst; values < 4q in, canonical out.
 template <int LOG_M>
-__global__ void __launch_bounds__(kMaxThreads) k_fwd2(const u64* src, u64* dst, const NttTab* __restrict__ tabs,
-                                                      LimbMap lm, int limb_count, int log_a, int log_c) {
+__global__ void __launch_bounds__(kMaxThreads, min_ctas<LOG_M>(4))
+k_fwd2(const u64* src, u64* dst, const NttTab* __restrict__ tabs,
+       LimbMap lm, int limb_count, int log_a, int log_c) {
     using S = Split<LOG_M>;
     extern __shared__ u64 sm[];
     const int C = 1 << log_c, tid = threadIdx.x;
@@ -169,9 +183,10 @@ __global__ void __launch_bounds__(kMaxThreads) k_fwd2(const u64* src, u64* dst, 
 // on the bit-reversed input {k_a + A brev(r)}, times the inverse twist
 // N^-1 psi^-((2k_a+1-A) j_lo), stored as row k_a (lazy, [0, 2q)). in != out.
 template <int LOG_M>
-__global__ void __launch_bounds__(kMaxThreads) k_inv1(const u64* __restrict__ in, u64* __restrict__ out,
-                                                      const NttTab* __restrict__ tabs, LimbMap lm, int limb_count,
-                                                      int log_a, int log_c) {
+__global__ void __launch_bounds__(kMaxThreads, min_ctas<LOG_M>(3))
+k_inv1(const u64* __restrict__ in, u64* __restrict__ out,
+       const NttTab* __restrict__ tabs, LimbMap lm, int limb_count,
+       int log_a, int log_c) {
     using S = Split<LOG_M>;
     extern __shared__ u64 sm[];
     const int C = 1 << log_c, tid = threadIdx.x;
@@ -226,8 +241,9 @@ __global__ void __launch_bounds__(kMaxThreads) k_inv1(const u64* __restrict__ in
 // src may equal dst.
 // With ib.b, the b components of key-switch accumulators get P b added (InvBase).
 template <int LOG_M>
-__global__ void __launch_bounds__(kMaxThreads) k_inv2(const u64* src, u64* dst, const NttTab* __restrict__ tabs,
-                                                      LimbMap lm, int limb_count, int log_b, int log_c, InvBase ib) {
+__global__ void __launch_bounds__(kMaxThreads, min_ctas<LOG_M>(3))
+k_inv2(const u64* src, u64* dst, const NttTab* __restrict__ tabs,
+       LimbMap lm, int limb_count, int log_b, int log_c, InvBase ib) {
     using S = Split<LOG_M>;
     extern __shared__ u64 sm[];
     const int C = 1 << log_c, tid = threadIdx.x;
