@@ -17,8 +17,9 @@
 // table. Each CTA handles C columns (or units); a thread holds R1 points in
 // registers for the first half of the stages and R2 for the second, with one
 // shared-memory exchange, and every global access is a 128-byte segment.
-// Butterflies are Harvey-lazy in [0, 4q) with Shoup multiplication
-// (__umul64hi); outputs are canonical.
+// Butterflies are Harvey-lazy with Shoup multiplication (primes below 2^58 /
+// 2^54 skip the conditional subtractions and estimate the Shoup quotient from
+// three 32-bit partial products); outputs are canonical.
 #include <cstdio>
 
 #include "ntt_core.cuh"
@@ -49,10 +50,15 @@ struct Split {
     static constexpr int RMAX = R1 > R2 ? R1 : R2;
 };
 
-__device__ __forceinline__ u64 lift_digit(i64 d, u64 q) {
-    u64 a = d < 0 ? (u64)(-d) : (u64)d;
-    a = a >= q ? a % q : a;
-    return (d < 0 && a) ? q - a : a;
+// Signed digit -> residue mod q without a division: m = floor(2^64 / q) (the
+// high word of the Barrett constant floor(2^128 / q)) makes umulhi(|d|, m)
+// floor(|d| / q) or one less, so one conditional subtraction finishes |d| mod q
+// for every 64-bit |d|.
+__device__ __forceinline__ u64 lift_digit(i64 d, u64 q, u64 m) {
+    const u64 a = d < 0 ? 0 - (u64)d : (u64)d;
+    u64 r = a - __umul64hi(a, m) * q;
+    r = r >= q ? r - q : r;
+    return (d < 0 && r) ? q - r : r;
 }
 
 // Stage a small twiddle table (M values then M Shoup companions) in shared memory.
@@ -95,7 +101,7 @@ k_fwd1(const void* __restrict__ in_, u64* __restrict__ out,
         if (kDigits) {
             const i64* in = (const i64*)in_ + ((size_t)blockIdx.z << (LOG_M + log_b));
 #pragma unroll
-            for (int e = 0; e < S::R1; ++e) x[e] = lift_digit(in[c0 + c + ((size_t)(i0 + S::R2 * e) << log_b)], q);
+            for (int e = 0; e < S::R1; ++e) x[e] = lift_digit(in[c0 + c + ((size_t)(i0 + S::R2 * e) << log_b)], q, T.mu_hi);
         } else {
             const u64* in = (const u64*)in_ + base;
 #pragma unroll
