@@ -402,6 +402,37 @@ int32_t ckks_ctx_tensor_cores(const ckks_ctx* ctx) {
     return ctx->tensor_cores && tc_enabled() ? 1 : 0;
 }
 
+}  // extern "C"
+
+void* pinned_take(ckks_ctx* ctx, size_t bytes, size_t* got) {
+    {
+        std::lock_guard<std::mutex> lock(ctx->pinned_mu);
+        for (size_t i = 0; i < ctx->pinned_free.size(); ++i)
+            if (ctx->pinned_free[i].second >= bytes) {
+                auto b = ctx->pinned_free[i];
+                ctx->pinned_free.erase(ctx->pinned_free.begin() + (long)i);
+                *got = b.second;
+                return b.first;
+            }
+    }
+    const size_t sz = bytes < 4096 ? 4096 : (bytes + 4095) / 4096 * 4096;
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, sz, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    *got = sz;
+    return p;
+}
+
+void pinned_give(ckks_ctx* ctx, void* p, size_t bytes) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(ctx->pinned_mu);
+    ctx->pinned_free.emplace_back(p, bytes);
+}
+
+extern "C" {
+
 int32_t ckks_ctx_destroy(ckks_ctx* ctx) {
     if (!ctx) return CKKS_OK;
     cudaDeviceSynchronize();
@@ -412,6 +443,7 @@ int32_t ckks_ctx_destroy(ckks_ctx* ctx) {
     if (ctx->d_table_mem) cudaFree(ctx->d_table_mem);
     if (ctx->d_const_mem) cudaFree(ctx->d_const_mem);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    for (auto& b : ctx->pinned_free) cudaFreeHost(b.first);
     delete ctx;
     return CKKS_OK;
 }

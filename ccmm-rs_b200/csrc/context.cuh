@@ -72,7 +72,16 @@ struct ckks_ctx {
     // forward 2, inverse 1, inverse 2; -1 = built-in choice; set by the autotuner
     int ntt_log_c[5] = {-1, -1, -1, -1, -1};
     std::string tuning_report;
+    // pinned host buffers for asynchronous status read-backs (counts, error
+    // flags), reused across calls; a call takes one and gives it back
+    std::mutex pinned_mu;
+    std::vector<std::pair<void*, size_t>> pinned_free;
 };
+
+// A pinned host buffer of at least `bytes` from the context's free list (null
+// if pinned memory cannot be had), and its return.
+void* pinned_take(ckks_ctx* ctx, size_t bytes, size_t* got);
+void pinned_give(ckks_ctx* ctx, void* p, size_t bytes);
 
 // ---------------------------------------------------------------- errors
 void ckks_set_error(const std::string& msg);

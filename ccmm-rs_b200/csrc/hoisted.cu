@@ -21,6 +21,7 @@
 #include "keyswitch.cuh"
 
 #include <algorithm>
+#include <cstring>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -1057,6 +1058,32 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     if (warp == kMmaWarp) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
 }
 
+// A pinned status buffer from the context and an event marking when the
+// device's copies into it are done. The buffer goes back to the context only
+// after those copies have landed (also on early error returns).
+struct StatusReadback {
+    ckks_ctx* ctx;
+    void* p = nullptr;
+    size_t bytes = 0;
+    cudaEvent_t ev = nullptr;
+    StatusReadback(ckks_ctx* c, size_t want) : ctx(c) {
+        p = pinned_take(ctx, want, &bytes);
+        if (p && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            ev = nullptr;
+            pinned_give(ctx, p, bytes);
+            p = nullptr;
+        }
+    }
+    bool ok() const { return p && ev; }
+    ~StatusReadback() {
+        if (!ev) return;
+        cudaEventSynchronize(ev);
+        cudaEventDestroy(ev);
+        pinned_give(ctx, p, bytes);
+    }
+};
+
 }  // namespace
 
 // Hoisted hybrid rotations of n_ct ciphertexts by n_keys Galois keys (bounded
@@ -1118,6 +1145,11 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
     const u64* d_exps_inv = karr.p + 2 * n_keys + ctx->moduli.size();
     std::vector<u32> overflow;
     std::vector<u32> h_cnt((size_t)G * n_keys);
+    // the correction-list counts and the MAC's error flag come back through pinned
+    // memory behind the MAC, and the host waits for that event only: the call
+    // returns while the inverse transforms and ModDown of the last group still
+    // run, so back-to-back calls keep the device busy
+    StatusReadback rb(ctx, ((size_t)G * n_keys + 1) * sizeof(u32));
     for (u32 c0 = 0; c0 < n_ct; c0 += G) {
         const u32 gn = (n_ct - c0) < G ? (n_ct - c0) : G;
         CKKS_CUDA_TRY(cudaMemsetAsync(flags.p, 0, G * f_stride * sizeof(u32), st));
@@ -1189,6 +1221,12 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
         }
         CKKS_CUDA_TRY(cudaGetLastError());
         pt.end();
+        if (rb.ok()) {
+            u32* hc = (u32*)rb.p;
+            CKKS_CUDA_TRY(cudaMemcpyAsync(hc, cnt.p, (size_t)gn * n_keys * sizeof(u32), cudaMemcpyDeviceToHost, st));
+            CKKS_CUDA_TRY(cudaMemcpyAsync(hc + (size_t)G * n_keys, terr.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+            CKKS_CUDA_TRY(cudaEventRecord(rb.ev, st));
+        }
         pt.begin(4);
         // inverse transform; the b components get P b of their ciphertext added on the
         // Q limbs (ModDown(x + P b) = ModDown(x) + b: the base term of the rotation)
@@ -1209,9 +1247,17 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
         pt.end();
         // pairs whose correction lists overflowed are recomputed exactly
         int h_err = 0;
-        CKKS_CUDA_TRY(cudaMemcpyAsync(h_cnt.data(), cnt.p, (size_t)G * n_keys * sizeof(u32), cudaMemcpyDeviceToHost, st));
-        CKKS_CUDA_TRY(cudaMemcpyAsync(&h_err, terr.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-        CKKS_CUDA_TRY(cudaStreamSynchronize(st));
+        if (rb.ok()) {
+            CKKS_CUDA_TRY(cudaEventSynchronize(rb.ev));
+            const u32* hc = (const u32*)rb.p;
+            std::memcpy(h_cnt.data(), hc, (size_t)gn * n_keys * sizeof(u32));
+            std::memcpy(&h_err, hc + (size_t)G * n_keys, sizeof(int));
+        } else {  // no pinned memory: pageable copies and a stream synchronisation
+            CKKS_CUDA_TRY(cudaMemcpyAsync(h_cnt.data(), cnt.p, (size_t)G * n_keys * sizeof(u32),
+                                          cudaMemcpyDeviceToHost, st));
+            CKKS_CUDA_TRY(cudaMemcpyAsync(&h_err, terr.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+            CKKS_CUDA_TRY(cudaStreamSynchronize(st));
+        }
         if (h_err) {
             ckks_set_error("key-switch MAC: a tensor-core pipeline wait timed out");
             return CKKS_ERR_TIMEOUT;

@@ -218,7 +218,11 @@ int32_t ckks_rotate(ckks_ctx* ctx, const ckks_ksk* key, const uint64_t* ct_in, u
  * keys (all of one kind, level and gadget). out [n_ct][n_keys][2][q_limbs][N].
  * Bounded keys: digits re-normalised per key exactly as
  * BoundedGadgetDecomposition::automorphism_hoisted (bounded_gadget.rs:273-312),
- * so every word equals the non-hoisted rotation. */
+ * so every word equals the non-hoisted rotation. The host waits inside the call
+ * only for each group's carry-correction counts and MAC status (to schedule the
+ * exact recomputation of any pair whose correction list overflowed); the
+ * inverse transforms and ModDown of the last group are still in flight on
+ * `stream` when it returns. */
 int32_t ckks_rotate_hoisted(ckks_ctx* ctx, const ckks_ksk* const* keys, uint32_t n_keys, const uint64_t* ct_in,
                             uint64_t* ct_out, uint32_t n_ct, void* stream);
 /* ckks_rotate_hoisted with per-phase device time in milliseconds (CUDA
