@@ -367,24 +367,7 @@ def reference_arm(args, world, rank):
             "e2e": {"value": value, "unit": "chains/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }
     if args.workload == "rotation":
-        threads = os.cpu_count() or 1
-        vals, sample = [], None
-        for i in range(args.warmup + args.steps):
-            if i < args.warmup and i > 0:
-                continue  # one untimed warm-up pass: the key generation dominates and is not timed
-            v, sample = rot_cpu_sample(threads, n_keys=1 if i < args.warmup else 2)
-            if i >= args.warmup:
-                vals.append(v)
-        value = float(np.median(vals))
-        return {
-            "metric": "key-switched rotations/s (N=2^16, 24 limbs, hoisted, bit-exact)", "value": value,
-            "unit": "rotations/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1000.0 * ROT_NCT * len(ROT_STEPS) / value, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded uniform ciphertexts)",
-            "config": rot_config(), "impl": "reference",
-            "cpu_baseline": {"value": value, "unit": "rotations/s", "cores": threads, "kind": "port", "sample": sample},
-            "e2e": {"value": value, "unit": "rotations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        }
+        return reference_rotation(args, world)
     threads = os.cpu_count() or 1
     per_step = []
     sample = None
@@ -402,6 +385,69 @@ def reference_arm(args, world, rank):
         "cpu_baseline": {"value": value, "unit": "limb-NTT/s", "cores": threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": "limb-NTT/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def reference_rotation(args, world):
+    """Reference arm of the rotation workload: the oracle's restatement of the
+    reference's hoisted rotation on every host core. Keys are made once; each
+    timed step is a real sample of one ciphertext per thread x 2 Galois keys
+    (the decomposition is shared by the keys of a ciphertext, as in the
+    reference's automorphism_hoisted; per key the reference re-transforms every
+    digit, so the rate hardly depends on the key count: the line records the
+    measured per-key and per-decomposition cost). A 1-thread figure follows."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import Oracle, arr
+    import concurrent.futures as cf
+    o = Oracle()
+    threads = os.cpu_count() or 1
+    n = 1 << ROT_LOG_N
+    q = arr(o.primes_below_bits(ROT_QBITS, n, ROT_L))
+    p = arr(o.primes_below_bits(ROT_PBITS, n, ROT_K))
+    rng = np.random.default_rng(77)
+    secret = rng.integers(-1, 2, n).astype(np.int8)
+    exps = [int(o.L.oracle_rotation_exponent_left(n, r)) for r in ROT_STEPS[:2]]
+    with cf.ThreadPoolExecutor(2) as ex:
+        keys = list(ex.map(lambda ik: o.hybrid_key(q, p, secret, ik[1], ROT_BASE_LOG, seed=500 + ik[0]),
+                           enumerate(exps)))
+    cts = np.stack([np.stack([rng.integers(0, m, (2, n), dtype=np.uint64) for m in q], axis=1)
+                    for _ in range(threads)])
+    # warm-up: one key per ciphertext (also gives the 1-key cost for the split below)
+    v1, _, _ = rot_cpu_sample(threads, 1, keys=keys, exps=exps, cts=cts)
+    for _ in range(max(0, args.warmup - 1)):
+        rot_cpu_sample(threads, 1, keys=keys, exps=exps, cts=cts)
+    vals, samples = [], []
+    for _ in range(args.steps):
+        v, sample, _ = rot_cpu_sample(threads, 2, keys=keys, exps=exps, cts=cts)
+        vals.append(v)
+        samples.append(2 * threads / v)
+    value = float(np.median(vals))
+    # per-thread cost split: t(k keys) = decomposition + k x per-key
+    t1, t2 = 1.0 / (v1 / threads), 1.0 / (value / (2 * threads))
+    per_key, decomp = t2 - t1, 2 * t1 - t2
+    v_1t, sample_1t, _ = rot_cpu_sample(1, 2, keys=keys, exps=exps, cts=cts[:1])
+    rots = ROT_NCT * len(ROT_STEPS)
+    ccmm = None
+    if not args.no_ccmm:
+        cv, csample = ccmm_cpu_sample(threads)
+        ccmm = {"metric": "64x64 structured CCMM/s (N=2^15, 14 limbs, both operands encrypted, bit-exact)",
+                "value": cv, "unit": "CCMM/s", "higher_is_better": True, "config": ccmm_config(),
+                "cpu_baseline": {"value": cv, "unit": "CCMM/s", "cores": threads, "kind": "port", "sample": csample}}
+    return {
+        "metric": "key-switched rotations/s (N=2^16, 24 limbs, hoisted, bit-exact)", "value": value,
+        "unit": "rotations/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * rots / value, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded uniform ciphertexts)",
+        "config": rot_config(), "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "rotations/s", "cores": threads, "kind": "port", "sample": sample},
+        "timed_samples": {"rotations_per_sample": 2 * threads, "seconds": samples,
+                          "note": "ms_per_step is the time the measured rate needs for one step of %d rotations "
+                                  "(16 ct x 32 keys); each timed sample ran %d rotations" % (rots, 2 * threads)},
+        "cost_split_s_per_thread": {"decomposition": decomp, "per_key": per_key,
+                                    "rate_at_32_keys": threads * 32 / (decomp + 32 * per_key)},
+        "cpu_1thread": {"value": v_1t, "unit": "rotations/s", "cores": 1, "sample": sample_1t},
+        "e2e": {"value": value, "unit": "rotations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "ccmm": ccmm,
     }
 
 
@@ -536,7 +582,27 @@ def bench_rot_gpu(args, world, rank, local):
     }
     # kernels of one step, counted after every timed region (the tracing hooks stay out of the timing)
     counted = count_launches(step)
-    decoded = rot_decoded_error(cb, ctx, keys, ROT_STEPS, secret, q, n)
+    assert ctx.last_mac_path == "tensor_cores", "the headline run must take the tensor-core MAC"
+    mac_path = ctx.last_mac_path
+    decoded, fresh = rot_decoded_error(cb, ctx, keys, ROT_STEPS, secret, q, n)
+    parity, cpu_base = None, None
+    if rank == 0 and world == 1:
+        # CPU baseline on the GPU arm's own ciphertexts and (downloaded) keys: the
+        # oracle's outputs are compared word for word with the GPU's
+        threads = os.cpu_count() or 1
+        n_cpu = min(threads, ROT_NCT)
+        keys_h = [keys[g].download() for g in range(2)]
+        v, sample, cpu_out = rot_cpu_sample(n_cpu, 2, keys=keys_h, exps=exps[:2], cts=host)
+        gpu_out = cb.to_numpy_u64(out[:n_cpu, :2])
+        cpu_base = {"value": v, "unit": "rotations/s", "cores": n_cpu, "kind": "port", "sample": sample}
+        od = rot_oracle_decoded(fresh, keys_h[0], exps[0], ROT_STEPS[0], secret, q, p)
+        parity = {"words_compared": int(gpu_out.size) + od["words_compared"],
+                  "mismatches": int(np.count_nonzero(gpu_out != cpu_out)) + od["mismatches"],
+                  "what": "%d ct x 2 keys of the timed batch (tensor-core MAC) and the fresh encryption's key-0 "
+                          "rotation, against the oracle's restatement of the reference rotation" % n_cpu}
+        decoded["oracle_key0_rel_l2"] = od["key0_rel_l2"]
+        decoded["oracle_key0_log2"] = od["key0_log2"]
+        decoded["gpu_key0_log2"] = float(np.log2(decoded["key0_rel_l2"])) if decoded["key0_rel_l2"] > 0 else None
     line = {
         "metric": "key-switched rotations/s (N=2^16, 24 limbs, hoisted, bit-exact)", "value": value,
         "unit": "rotations/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -553,7 +619,7 @@ def bench_rot_gpu(args, world, rank, local):
                                     "frac_no_key_reuse": (key_bytes + 2 * ct_bytes) * value / 1e9 / peak},
         "phases_ms_per_step": phases,
         "decoded_error": decoded,
-        "tensor_cores": ctx.tensor_cores,
+        "mac_path": mac_path,
         "plain_gpu": plain_gpu,
         "e2e": {"value": rots * e2e_steps * world / e2e_s, "unit": "rotations/s",
                 "h2d_bytes_per_step": int(host.nbytes), "d2h_bytes_per_step": int(hout.nbytes),
@@ -562,6 +628,9 @@ def bench_rot_gpu(args, world, rank, local):
         "gpu_launches": args.steps * (counted if counted else groups * (5 * min(group, ROT_NCT) + 5)),
         "clocks": clk,
     }
+    if cpu_base:
+        line["cpu_baseline"] = cpu_base
+        line["parity"] = parity
     return line
 
 
@@ -591,41 +660,68 @@ def rot_decoded_error(cb, ctx, keys, steps, secret, q, n, seed=77):
     dec = cb.decode(ctx, ctx.pointwise(out[:, 0].contiguous(), a2s, "add"), scale).cpu().numpy()
     errs = [float(np.linalg.norm(dec[g] - np.roll(x, -steps[g])) / np.linalg.norm(x)) for g in range(K)]
     worst = max(errs)
-    return {"rel_l2_max": worst, "log2": float(np.log2(worst)) if worst > 0 else None,
-            "check": "fresh encryption rotated by every key, decoded vs numpy.roll of the FP64 slots"}
+    res = {"rel_l2_max": worst, "log2": float(np.log2(worst)) if worst > 0 else None,
+           "key0_rel_l2": errs[0],
+           "check": "fresh encryption rotated by every key, decoded vs numpy.roll of the FP64 slots"}
+    fresh = {"ct": cb.to_numpy_u64(ct[0]), "out0": cb.to_numpy_u64(out[0]), "slots": x, "scale": scale}
+    return res, fresh
 
 
-def rot_cpu_sample(threads, n_keys=2):
+def rot_oracle_decoded(fresh, key0, exp0, step0, secret, q, p):
+    """The oracle's side of the decoded-error check: the same fresh encryption
+    rotated by key 0 with the oracle's restatement of the reference rotation,
+    compared word for word with the GPU's output and decoded with the oracle's
+    FP64 decode (the reference's CkksCanonicalEmbedding order of operations)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import Oracle
+    o = Oracle()
+    want = o.hybrid_rotate(q, p, key0, exp0, ROT_BASE_LOG, fresh["ct"])
+    dec = o.decode(q, o.decrypt(q, secret, want), fresh["scale"])
+    x = fresh["slots"]
+    err = float(np.linalg.norm(dec - np.roll(x, -step0)) / np.linalg.norm(x))
+    return {"key0_rel_l2": err, "key0_log2": float(np.log2(err)) if err > 0 else None,
+            "words_compared": int(want.size), "mismatches": int(np.count_nonzero(want != fresh["out0"]))}
+
+
+def rot_cpu_sample(threads, n_keys=2, keys=None, exps=None, cts=None, n_ct=None):
     """Times the oracle's restatement of the reference's hoisted hybrid-QP
     rotation (hybrid_rns_galois_key.rs:550-780 with bounded_gadget.rs:273-312
     hoisting) on the host: one ciphertext per thread, n_keys Galois keys each,
-    each rotation single-threaded (the reference's rayon granularity)."""
+    each rotation single-threaded (the reference's rayon granularity).
+    keys/exps/cts: the GPU arm's own keys (downloaded, reference layout),
+    exponents and ciphertexts; generated with the oracle when absent.
+    Returns (rotations/s, sample description, outputs [n_ct][n_keys][2][L][N])."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import ctypes
     from oracle_lib import Oracle, P, arr, u64p
     o = Oracle()
     n = 1 << ROT_LOG_N
+    n_ct = threads if n_ct is None else n_ct
     q = arr(o.primes_below_bits(ROT_QBITS, n, ROT_L))
     p = arr(o.primes_below_bits(ROT_PBITS, n, ROT_K))
     rng = np.random.default_rng(77)
-    secret = rng.integers(-1, 2, n).astype(np.int8)
-    exps = [int(o.L.oracle_rotation_exponent_left(n, r)) for r in ROT_STEPS[:n_keys]]
-    import concurrent.futures as cf
-    with cf.ThreadPoolExecutor(n_keys) as ex:
-        keys = list(ex.map(lambda ik: o.hybrid_key(q, p, secret, ik[1], ROT_BASE_LOG, seed=500 + ik[0]),
-                           enumerate(exps)))
-    cts = np.stack([np.stack([rng.integers(0, m, (2, n), dtype=np.uint64) for m in q], axis=1)
-                    for _ in range(threads)])
-    out = np.zeros((threads, n_keys, 2, ROT_L, n), np.uint64)
+    if keys is None:
+        secret = rng.integers(-1, 2, n).astype(np.int8)
+        exps = [int(o.L.oracle_rotation_exponent_left(n, r)) for r in ROT_STEPS[:n_keys]]
+        import concurrent.futures as cf
+        with cf.ThreadPoolExecutor(n_keys) as ex:
+            keys = list(ex.map(lambda ik: o.hybrid_key(q, p, secret, ik[1], ROT_BASE_LOG, seed=500 + ik[0]),
+                               enumerate(exps)))
+    if cts is None:
+        cts = np.stack([np.stack([rng.integers(0, m, (2, n), dtype=np.uint64) for m in q], axis=1)
+                        for _ in range(n_ct)])
+    cts = np.ascontiguousarray(cts[:n_ct])
+    keys = [np.ascontiguousarray(k) for k in keys[:n_keys]]
+    out = np.zeros((n_ct, n_keys, 2, ROT_L, n), np.uint64)
     kp = (u64p * n_keys)(*[P(k) for k in keys])
-    ex_arr = arr(exps)
+    ex_arr = arr(exps[:n_keys])
     t = time.perf_counter()
     o.L.oracle_hybrid_rotate_hoisted_batch(P(q), ROT_L, P(p), ROT_K, n, ROT_BASE_LOG, n_keys, P(ex_arr), kp,
-                                           threads, P(cts), P(out), threads)
+                                           n_ct, P(cts), P(out), threads)
     dt = time.perf_counter() - t
-    rots = threads * n_keys
-    return rots / dt, ("%d ciphertexts x %d Galois keys (one ciphertext per thread), N=2^%d, %d+%d limbs, "
-                       "base 2^%d, %.1f s" % (threads, n_keys, ROT_LOG_N, ROT_L, ROT_K, ROT_BASE_LOG, dt))
+    rots = n_ct * n_keys
+    return rots / dt, ("%d ciphertexts x %d Galois keys on %d thread(s) (one ciphertext per thread), N=2^%d, "
+                       "%d+%d limbs, base 2^%d: %d rotations in %.2f s"
+                       % (n_ct, n_keys, threads, ROT_LOG_N, ROT_L, ROT_K, ROT_BASE_LOG, rots, dt)), out
 
 
 # ------------------------------------------------- multiply chain (N=2^12)
@@ -843,6 +939,7 @@ def bench_ccmm_gpu(args, world, rank, local):
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(world, time.perf_counter() - t)
     launches_per_step = count_launches(step)  # after every timed region
+    parity = ccmm_parity(cb, ctx, rk, A, B, C, q) if (rank == 0 and world == 1) else None
     return {
         "metric": "64x64 structured CCMM/s (N=2^15, 14 limbs, both operands encrypted, bit-exact)", "value": value,
         "unit": "CCMM/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -855,7 +952,49 @@ def bench_ccmm_gpu(args, world, rank, local):
         "e2e": {"value": world / e2e_s, "unit": "CCMM/s", "h2d_bytes_per_step": int(2 * A.numel() * 8),
                 "d2h_bytes_per_step": int(C.numel() * 8), "path": "torch pinned copies + ckks_ccmm_structured"},
         "gpu_launches": None if launches_per_step is None else args.steps * launches_per_step, "clocks": clk,
+        "parity": parity,
     }
+
+
+def ccmm_parity(cb, ctx, rk, A, B, C, q):
+    """Output entry (0, 0) of the timed product recomputed by the oracle from
+    the same operands and key: 64 tensors summed, bounded relinearization,
+    rescale (matrix/rns_ckks_ciphertext.rs:220-318), compared word for word."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import Oracle
+    o = Oracle()
+    n, d, L = 1 << CCMM_LOG_N, CCMM_D, CCMM_L
+    row = cb.to_numpy_u64(A[0::d])             # A[0 + k d], k = 0..d-1 (column-major)
+    col = cb.to_numpy_u64(B[0:d])              # B[k + 0 d]
+    key_ntt = rk.download().reshape(-1, L, n)
+    key = o.ntt_inverse(q, key_ntt).reshape(-1, 2, L, n)  # the reference's coefficient-domain layout
+    acc = None
+    for kk in range(d):
+        t = o.tensor(q, row[kk], col[kk]).astype(object)
+        acc = t if acc is None else acc + t
+    quad = np.stack([acc[:, l] % q[l] for l in range(L)], axis=1).astype(np.uint64)
+    want = o.rescale(q, o.relinearize(q, quad, key, CCMM_BASE_LOG).reshape(2, L, n))
+    got = cb.to_numpy_u64(C[0])
+    return {"words_compared": int(want.size), "mismatches": int(np.count_nonzero(got != want)),
+            "what": "output entry (0, 0): 64 tensors + relinearization + rescale, against the oracle's "
+                    "restatement of the reference"}
+
+
+def ccmm_object(args, world, rank, local):
+    """The 64x64 CCMM measured beside the headline rotations (same run): 3
+    timed products after 3 warm-up ones, with its own roofline, e2e, parity
+    and, at N=1, the CPU baseline."""
+    import copy
+    a = copy.copy(args)
+    a.steps, a.warmup = 3, 3
+    line = bench_ccmm_gpu(a, world, rank, local)
+    if rank == 0 and world == 1:
+        threads = os.cpu_count() or 1
+        v, sample = ccmm_cpu_sample(threads)
+        line["cpu_baseline"] = {"value": v, "unit": "CCMM/s", "cores": threads, "kind": "port", "sample": sample}
+    keep = ["metric", "value", "unit", "steps", "warmup", "ms_per_step", "higher_is_better", "config", "roofline",
+            "e2e", "gpu_launches", "clocks", "parity", "cpu_baseline"]
+    return {k: line[k] for k in keep if k in line}
 
 
 def ccmm_cpu_sample(threads):
@@ -1024,6 +1163,29 @@ def fft2_cpu_sample(threads):
                                  "per image" % (threads, dt))
 
 
+def free_port():
+    import socket
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as sk:
+        sk.bind(("127.0.0.1", 0))
+        return sk.getsockname()[1]
+
+
+def launch_replicas(args):
+    """`--gpus N` without a torchrun environment: re-executes this command as
+    N ranks (one process per GPU) under torch.distributed.run on 127.0.0.1.
+    The b200 arm needs N visible GPUs and stops with an error otherwise; the
+    reference arm runs on the host cores (rank 0 measures, the others exit)."""
+    if args.impl == "b200":
+        import torch
+        have = torch.cuda.device_count()
+        if have < args.gpus:
+            raise SystemExit("bench.py: --gpus %d but only %d CUDA device(s) are visible" % (args.gpus, have))
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=%d" % args.gpus,
+           "--master-addr=127.0.0.1", "--master-port=%d" % free_port(), os.path.abspath(__file__)] + sys.argv[1:]
+    sys.stdout.flush()
+    os.execv(sys.executable, cmd)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1038,7 +1200,15 @@ def main():
     ap.add_argument("--rot-keys", type=int, default=32)
     ap.add_argument("--rot-base-log", type=int, default=32)
     ap.add_argument("--rot-log-n", type=int, default=16)
+    ap.add_argument("--no-ccmm", action="store_true",
+                    help="rotation workload: leave out the 64x64 CCMM measured beside it")
     args = ap.parse_args()
+    if args.gpus < 1:
+        ap.error("--gpus must be at least 1")
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        launch_replicas(args)  # does not return
+    if int(os.environ.get("WORLD_SIZE", "1")) != args.gpus:
+        raise SystemExit("bench.py: --gpus %d but WORLD_SIZE=%s" % (args.gpus, os.environ.get("WORLD_SIZE")))
     global ROT_L, ROT_NCT, ROT_STEPS, ROT_BASE_LOG, ROT_LOG_N
     ROT_L, ROT_NCT, ROT_BASE_LOG, ROT_LOG_N = args.rot_limbs, args.rot_ct, args.rot_base_log, args.rot_log_n
     ROT_STEPS = ROT_STEPS[:args.rot_keys]
@@ -1052,11 +1222,12 @@ def main():
         return
     if args.workload == "fft2":
         line = bench_fft2_gpu(args, world, rank, local)
-        if rank == 0:
+        if rank == 0 and world == 1:
             threads = os.cpu_count() or 1
             v, sample = fft2_cpu_sample(threads)
             line["cpu_baseline"] = {"value": v, "unit": "images/s", "cores": threads, "kind": "port",
                                     "sample": sample}
+        if rank == 0:
             print(json.dumps(line), flush=True)
         if world > 1:
             import torch.distributed as dist
@@ -1064,10 +1235,11 @@ def main():
         return
     if args.workload == "ccmm":
         line = bench_ccmm_gpu(args, world, rank, local)
-        if rank == 0:
+        if rank == 0 and world == 1:
             threads = os.cpu_count() or 1
             v, sample = ccmm_cpu_sample(threads)
             line["cpu_baseline"] = {"value": v, "unit": "CCMM/s", "cores": threads, "kind": "port", "sample": sample}
+        if rank == 0:
             print(json.dumps(line), flush=True)
         if world > 1:
             import torch.distributed as dist
@@ -1075,11 +1247,12 @@ def main():
         return
     if args.workload == "multiply":
         line = bench_mul_gpu(args, world, rank, local)
-        if rank == 0:
+        if rank == 0 and world == 1:
             threads = os.cpu_count() or 1
             v, sample = mul_cpu_sample(threads, pairs=4 * threads)
             line["cpu_baseline"] = {"value": v, "unit": "chains/s", "cores": threads, "kind": "port",
                                     "sample": sample}
+        if rank == 0:
             print(json.dumps(line), flush=True)
         if world > 1:
             import torch.distributed as dist
@@ -1089,21 +1262,27 @@ def main():
         line = bench_ntt_gpu(args, world, rank, local)
     else:
         line = bench_rot_gpu(args, world, rank, local)
+        if not args.no_ccmm:
+            # the metric's second half: one 64x64 CCMM at the CCMM configuration,
+            # measured in the same run after the rotation's memory is released
+            import gc
+            import torch
+            gc.collect()
+            torch.cuda.synchronize()
+            torch.cuda.empty_cache()
+            line["ccmm"] = ccmm_object(args, world, rank, local)
         if rank == 0:
-            threads = os.cpu_count() or 1
-            v, sample = rot_cpu_sample(threads)
-            line["cpu_baseline"] = {"value": v, "unit": "rotations/s", "cores": threads, "kind": "port",
-                                    "sample": sample}
             print(json.dumps(line), flush=True)
         if world > 1:
             import torch.distributed as dist
             dist.destroy_process_group()
         return
-    if rank == 0:
+    if rank == 0 and world == 1:
         threads = os.cpu_count() or 1
         v, sample = ntt_cpu_sample(threads, seconds_target=10.0)
         line["cpu_baseline"] = {"value": v, "unit": "limb-NTT/s", "cores": threads, "kind": "port",
                                 "sample": sample}
+    if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

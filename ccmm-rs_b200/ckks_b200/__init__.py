@@ -38,6 +38,7 @@ _SIGS = {
     "ckks_ctx_destroy": (I32, [VP]),
     "ckks_ctx_set_tensor_cores": (I32, [VP, I32]),
     "ckks_ctx_tensor_cores": (I32, [VP]),
+    "ckks_ctx_last_mac_path": (I32, [VP]),
     "ckks_ctx_autotune": (I32, [VP, U32, U32, VP]),
     "ckks_ctx_tuning_report": (I32, [VP, ctypes.c_char_p, ctypes.c_uint64]),
     "ckks_ctx_psi": (I32, [VP, u64p]),
@@ -185,6 +186,12 @@ class Context:
     @tensor_cores.setter
     def tensor_cores(self, enable):
         check(lib().ckks_ctx_set_tensor_cores(self.handle, 1 if enable else 0))
+
+    @property
+    def last_mac_path(self):
+        """MAC of the most recent hoisted rotation on this context:
+        "tensor_cores", "cuda_cores" or None (no hoisted rotation yet)."""
+        return {1: "tensor_cores", 0: "cuda_cores"}.get(int(lib().ckks_ctx_last_mac_path(self.handle)))
 
     def autotune(self, limbs, polys, stream=None):
         """Times the NTT passes' tile choices on a limbs x polys batch, keeps the

@@ -5,13 +5,7 @@
 
 namespace {
 
-int32_t need_ctx(ckks_ctx* ctx, const char* who) {
-    if (!ctx) {
-        ckks_set_error(std::string(who) + ": null context");
-        return CKKS_ERR_BAD_ARG;
-    }
-    return CKKS_OK;
-}
+int32_t need_ctx(ckks_ctx* ctx, const char* who) { return ckks_require_device(ctx, who); }
 
 int32_t limb_range(ckks_ctx* ctx, u32 begin, u32 count, const char* who) {
     if (int32_t rc = need_ctx(ctx, who)) return rc;

@@ -7,7 +7,8 @@
 namespace {
 
 int32_t check_relin_key(ckks_ctx* ctx, const ckks_ksk* key, const char* who) {
-    CKKS_CHECK_ARG(ctx != nullptr && key != nullptr, std::string(who) + ": null context or key");
+    if (int32_t rc = ckks_require_device(ctx, who)) return rc;
+    CKKS_CHECK_ARG(key != nullptr, std::string(who) + ": null key");
     if (key->ctx != ctx || key->kind != CKKS_KSK_RELIN_BOUNDED) {
         ckks_set_error(std::string(who) + ": key is not a bounded relinearization key of this context");
         return CKKS_ERR_BASIS_MISMATCH;
@@ -26,7 +27,7 @@ extern "C" {
 
 int32_t ckks_tensor(ckks_ctx* ctx, const uint64_t* lhs, const uint64_t* rhs, uint64_t* out, uint32_t n_ct,
                     uint32_t q_limbs, void* stream) {
-    CKKS_CHECK_ARG(ctx != nullptr, "ckks_tensor: null context");
+    if (int32_t rc = ckks_require_device(ctx, "ckks_tensor")) return rc;
     CKKS_CHECK_ARG(lhs && rhs && out, "ckks_tensor: null buffer");
     if (q_limbs < 1 || q_limbs > ctx->L) {
         ckks_set_error("ckks_tensor: q_limbs outside the context Q basis");
@@ -87,7 +88,7 @@ int32_t ckks_multiply_relin_rescale_host(ckks_ctx* ctx, const ckks_ksk* key, con
 
 int32_t ckks_mul_plain(ckks_ctx* ctx, const uint64_t* ct, const uint64_t* plain_ntt, uint64_t* out, uint32_t n_ct,
                        uint32_t q_limbs, uint32_t n_plain, void* stream) {
-    CKKS_CHECK_ARG(ctx != nullptr, "ckks_mul_plain: null context");
+    if (int32_t rc = ckks_require_device(ctx, "ckks_mul_plain")) return rc;
     CKKS_CHECK_ARG(ct && plain_ntt && out, "ckks_mul_plain: null buffer");
     if (q_limbs < 1 || q_limbs > ctx->L) {
         ckks_set_error("ckks_mul_plain: q_limbs outside the context Q basis");
@@ -101,7 +102,7 @@ int32_t ckks_mul_plain(ckks_ctx* ctx, const uint64_t* ct, const uint64_t* plain_
 int32_t ckks_fft_stage(ckks_ctx* ctx, const ckks_ksk* const* keys, uint32_t n_rot, int32_t identity,
                        const uint64_t* diag_ntt, const uint64_t* ct_in, uint64_t* ct_out, uint32_t n_ct,
                        uint32_t q_limbs, void* stream) {
-    CKKS_CHECK_ARG(ctx != nullptr, "ckks_fft_stage: null context");
+    if (int32_t rc = ckks_require_device(ctx, "ckks_fft_stage")) return rc;
     CKKS_CHECK_ARG(diag_ntt && ct_in && ct_out && (n_rot == 0 || keys) && (n_rot || identity),
                    "ckks_fft_stage: bad arguments");
     CKKS_CHECK_ARG(q_limbs >= 2 && q_limbs <= ctx->L, "ckks_fft_stage: need 2..L limbs (the stage rescales)");
@@ -139,7 +140,7 @@ int32_t ckks_ccmm_structured(ckks_ctx* ctx, const ckks_ksk* key, const uint64_t*
 int32_t ckks_fft_stage_multi(ckks_ctx* ctx, const ckks_ksk* const* keys, uint32_t n_rot, const uint32_t* terms_host,
                              uint32_t n_terms, const uint64_t* diag_ntt, const uint64_t* ct_in, uint32_t n_in,
                              uint64_t* ct_out, uint32_t n_out, uint32_t q_limbs, void* stream) {
-    CKKS_CHECK_ARG(ctx != nullptr, "ckks_fft_stage_multi: null context");
+    if (int32_t rc = ckks_require_device(ctx, "ckks_fft_stage_multi")) return rc;
     CKKS_CHECK_ARG(terms_host && diag_ntt && ct_in && ct_out && n_terms && n_in && n_out && (n_rot == 0 || keys),
                    "ckks_fft_stage_multi: bad arguments");
     CKKS_CHECK_ARG(q_limbs >= 2 && q_limbs <= ctx->L, "ckks_fft_stage_multi: need 2..L limbs (the stage rescales)");
@@ -164,7 +165,7 @@ int32_t ckks_fft_stage_multi(ckks_ctx* ctx, const ckks_ksk* const* keys, uint32_
 
 int32_t ckks_encode(ckks_ctx* ctx, const double* slots, uint64_t* out, uint32_t n_msg, uint32_t q_limbs, double scale,
                     void* stream) {
-    CKKS_CHECK_ARG(ctx != nullptr, "ckks_encode: null context");
+    if (int32_t rc = ckks_require_device(ctx, "ckks_encode")) return rc;
     CKKS_CHECK_ARG(slots && out, "ckks_encode: null buffer");
     CKKS_CHECK_ARG(q_limbs >= 1 && q_limbs <= ctx->L, "ckks_encode: q_limbs outside the context Q basis");
     CKKS_CHECK_ARG(std::isfinite(scale) && scale > 0, "ckks_encode: scale must be finite and positive");
@@ -175,7 +176,7 @@ int32_t ckks_encode(ckks_ctx* ctx, const double* slots, uint64_t* out, uint32_t 
 
 int32_t ckks_decode(ckks_ctx* ctx, const uint64_t* poly, double* slots, uint32_t n_msg, uint32_t q_limbs,
                     double scale, void* stream) {
-    CKKS_CHECK_ARG(ctx != nullptr, "ckks_decode: null context");
+    if (int32_t rc = ckks_require_device(ctx, "ckks_decode")) return rc;
     CKKS_CHECK_ARG(poly && slots, "ckks_decode: null buffer");
     CKKS_CHECK_ARG(q_limbs >= 1 && q_limbs <= ctx->L, "ckks_decode: q_limbs outside the context Q basis");
     CKKS_CHECK_ARG(std::isfinite(scale) && scale > 0, "ckks_decode: scale must be finite and positive");

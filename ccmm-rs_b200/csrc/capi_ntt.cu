@@ -4,10 +4,7 @@
 namespace {
 
 int32_t check_range(ckks_ctx* ctx, uint32_t limb_begin, uint32_t limb_count, const char* who) {
-    if (!ctx) {
-        ckks_set_error(std::string(who) + ": null context");
-        return CKKS_ERR_BAD_ARG;
-    }
+    if (int32_t rc = ckks_require_device(ctx, who)) return rc;
     if ((size_t)limb_begin + limb_count > ctx->moduli.size()) {
         ckks_set_error(std::string(who) + ": limb range outside the context basis");
         return CKKS_ERR_BASIS_MISMATCH;

@@ -295,10 +295,40 @@ int32_t ckks_ctx_create(uint32_t log_n, const uint64_t* q, uint32_t L, const uin
         ckks_set_error("ckks_ctx_create: out of device memory for NTT tables");
         return CKKS_ERR_OOM;
     }
+    // FP64 networks: primes below 2^50 when both transform halves have at most
+    // 2^8 points (four register stages on each side of the exchange)
+    const bool f64_shape = ctx->log_n1 <= 8 && ctx->log_n2 <= 8;
+    const size_t fper = 2 * ((size_t)(1u << ctx->log_n1) + (1u << ctx->log_n2) + n);
+    size_t n_f64 = 0;
+    for (size_t i = 0; i < M; ++i) n_f64 += f64_shape && mod[i] < (1ull << 50);
+    std::vector<double2> fhost(fper * n_f64);
+    if (n_f64 && cudaMalloc(&ctx->d_ftable_mem, fhost.size() * sizeof(double2)) != cudaSuccess) {
+        cudaGetLastError();
+        ckks_ctx_destroy(ctx);
+        ckks_set_error("ckks_ctx_create: out of device memory for NTT tables");
+        return CKKS_ERR_OOM;
+    }
+    size_t foff = 0;
     for (size_t i = 0; i < M; ++i) {
         u64 m = mod[i];
         size_t off = per * i;
         NttTab& T = ctx->h_tabs[i];
+        T.f64 = f64_shape && m < (1ull << 50);
+        T.qd = (double)m;
+        T.qinv = 1.0 / (double)m;
+        if (T.f64) {
+            auto fput = [&](const std::vector<u64>& v, const double2** dst) {
+                for (size_t k = 0; k < v.size(); ++k) fhost[foff + k] = make_double2((double)v[k], (double)v[k] / (double)m);
+                *dst = ctx->d_ftable_mem + foff;
+                foff += v.size();
+            };
+            fput(ht[i].psiA, &T.fA);
+            fput(ht[i].psiA_inv, &T.fA_inv);
+            fput(ht[i].psiB, &T.fB);
+            fput(ht[i].psiB_inv, &T.fB_inv);
+            fput(ht[i].mid, &T.fmid);
+            fput(ht[i].midi, &T.fmidi);
+        }
         T.q = m;
         barrett_host(m, &T.mu_hi, &T.mu_lo);
         auto put = [&](const std::vector<u64>& v, const u64** val, const u64** quo) {
@@ -318,6 +348,8 @@ int32_t ckks_ctx_create(uint32_t log_n, const uint64_t* q, uint32_t L, const uin
         put(ht[i].midi, &T.midi, &T.midi_q);
     }
     if (cudaMemcpy(ctx->d_table_mem, host.data(), host.size() * sizeof(u64), cudaMemcpyHostToDevice) != cudaSuccess ||
+        (n_f64 && cudaMemcpy(ctx->d_ftable_mem, fhost.data(), fhost.size() * sizeof(double2),
+                             cudaMemcpyHostToDevice) != cudaSuccess) ||
         cudaMemcpy(ctx->d_tabs, ctx->h_tabs.data(), M * sizeof(NttTab), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
         std::string e = cudaGetErrorString(cudaGetLastError());
@@ -380,7 +412,7 @@ int32_t ckks_ctx_set_tensor_cores(ckks_ctx* ctx, int32_t enable) {
 }
 
 int32_t ckks_ctx_autotune(ckks_ctx* ctx, uint32_t limbs, uint32_t polys, void* stream) {
-    CKKS_CHECK_ARG(ctx != nullptr, "ckks_ctx_autotune: ctx is null");
+    if (int32_t rc = ckks_require_device(ctx, "ckks_ctx_autotune")) return rc;
     cudaStream_t st = ckks_stream(ctx, stream);
     const int32_t rc = ntt_autotune(ctx, limbs, polys, st);
     if (rc == CKKS_OK) CKKS_CUDA_TRY(cudaStreamSynchronize(st));
@@ -402,7 +434,27 @@ int32_t ckks_ctx_tensor_cores(const ckks_ctx* ctx) {
     return ctx->tensor_cores && tc_enabled() ? 1 : 0;
 }
 
+int32_t ckks_ctx_last_mac_path(const ckks_ctx* ctx) {
+    if (!ctx) return -1;
+    return ctx->last_mac_path;
+}
+
 }  // extern "C"
+
+int32_t ckks_require_device(const ckks_ctx* ctx, const char* who) {
+    if (!ctx) {
+        ckks_set_error(std::string(who) + ": null context");
+        return CKKS_ERR_BAD_ARG;
+    }
+    int dev = -1;
+    CKKS_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev != ctx->device) {
+        ckks_set_error(std::string(who) + ": the current CUDA device (" + std::to_string(dev) +
+                       ") is not the context's device (" + std::to_string(ctx->device) + ")");
+        return CKKS_ERR_BAD_ARG;
+    }
+    return CKKS_OK;
+}
 
 void* pinned_take(ckks_ctx* ctx, size_t bytes, size_t* got) {
     {
@@ -441,6 +493,7 @@ int32_t ckks_ctx_destroy(ckks_ctx* ctx) {
     keyset_release_ctx(ctx);
     if (ctx->d_tabs) cudaFree(ctx->d_tabs);
     if (ctx->d_table_mem) cudaFree(ctx->d_table_mem);
+    if (ctx->d_ftable_mem) cudaFree(ctx->d_ftable_mem);
     if (ctx->d_const_mem) cudaFree(ctx->d_const_mem);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     for (auto& b : ctx->pinned_free) cudaFreeHost(b.first);

@@ -23,6 +23,11 @@ struct NttTab {
     const u64 *psiA, *psiA_q, *psiA_inv, *psiA_inv_q;
     const u64 *psiB, *psiB_q, *psiB_inv, *psiB_inv_q;
     const u64 *mid, *mid_q, *midi, *midi_q;
+    // FP64 networks (primes below 2^50 and transform halves of up to 2^8
+    // points): the same tables as (W, fl(W / q)) pairs, q and fl(1 / q)
+    int f64;
+    double qd, qinv;
+    const double2 *fA, *fA_inv, *fB, *fB_inv, *fmid, *fmidi;
 };
 
 constexpr int kMaxAux = 8;  // auxiliary (P) limbs
@@ -54,6 +59,7 @@ struct ckks_ctx {
     std::vector<u64> moduli;  // Q limbs then P limbs
     std::vector<u64> psi;     // primitive 2N-th roots (reference search rule)
     u64* d_table_mem = nullptr;
+    double2* d_ftable_mem = nullptr;  // (W, W/q) tables of the FP64 moduli
     NttTab* d_tabs = nullptr;  // [L+K]
     std::vector<NttTab> h_tabs;
     cudaStream_t own_stream = nullptr;
@@ -68,6 +74,9 @@ struct ckks_ctx {
     // key-switch MAC of bounded hoisted rotations: tcgen05 INT8 tensor cores
     // (when the device has them) or the CUDA-core split-accumulator form
     bool tensor_cores = true;
+    // MAC of the most recent hoisted rotation on this context: 1 tensor cores,
+    // 0 CUDA cores, -1 none yet (diagnostic; read by ckks_ctx_last_mac_path)
+    int last_mac_path = -1;
     // NTT columns per CTA (log2) per pass: forward 1, forward 1 of digits,
     // forward 2, inverse 1, inverse 2; -1 = built-in choice; set by the autotuner
     int ntt_log_c[5] = {-1, -1, -1, -1, -1};
@@ -85,6 +94,12 @@ void pinned_give(ckks_ctx* ctx, void* p, size_t bytes);
 
 // ---------------------------------------------------------------- errors
 void ckks_set_error(const std::string& msg);
+
+// Entry points that touch device memory require the calling thread's current
+// CUDA device to be the context's device (its tables, keys and constants live
+// there): a mismatch returns CKKS_ERR_BAD_ARG instead of mixing two GPUs'
+// memory in one launch.
+int32_t ckks_require_device(const ckks_ctx* ctx, const char* who);
 
 #define CKKS_CUDA_TRY(expr)                                                       \
     do {                                                                          \

@@ -1105,6 +1105,7 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
     // the tensor-core MAC reads the keys' packed set (made on first use)
     const PackedSet* pset = use_tc ? packed_set_get(ctx, keys, n_keys, st) : nullptr;
     use_tc = pset != nullptr;
+    ctx->last_mac_path = use_tc ? 1 : 0;
     u32 G = n_ct >= 4 ? 4 : n_ct;
     if (use_tc) {
         const size_t per_ct = ((size_t)D * LK * n + 4 * (size_t)n_keys * LK * n) * sizeof(u64);
@@ -1184,8 +1185,8 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
         pt.end();
         pt.begin(3);
         if (use_tc) {
-            static int n_sm = 0;
-            if (!n_sm) cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, ctx->device);
+            int n_sm = 0;
+            CKKS_CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, ctx->device));
             const int n_tiles = (int)(LK * (n / tc::kTS));
             CKKS_CUDA_TRY(cudaFuncSetAttribute(k_mac_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                (int)tc::kSmemBytes));

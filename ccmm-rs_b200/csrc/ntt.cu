@@ -61,6 +61,14 @@ __device__ __forceinline__ u64 lift_digit(i64 d, u64 q, u64 m) {
     return (d < 0 && r) ? q - r : r;
 }
 
+// Stage a small (W, W/q) table of the FP64 networks in shared memory (16-byte
+// entries: one 128-bit shared load per twiddle).
+__device__ __forceinline__ const double2* stage_table_f64(u64* at, const double2* __restrict__ v, int M) {
+    double2* st = reinterpret_cast<double2*>(at);
+    for (int i = threadIdx.x; i < M; i += blockDim.x) st[i] = __ldg(v + i);
+    return st;
+}
+
 // Stage a small twiddle table (M values then M Shoup companions) in shared memory.
 __device__ __forceinline__ void stage_table(u64* st, const u64* __restrict__ v, const u64* __restrict__ vq, int M) {
     for (int i = threadIdx.x; i < M; i += blockDim.x) {
@@ -85,10 +93,51 @@ k_fwd1(const void* __restrict__ in_, u64* __restrict__ out,
     const int limb = blockIdx.y;
     const NttTab& T = tabs[lm(limb)];
     const u64 q = T.q;
-    u64* st = sm + (S::M << log_c);
-    stage_table(st, T.psiA, T.psiA_q, S::M);
     const size_t base = ((size_t)blockIdx.z * limb_count + limb) << (LOG_M + log_b);
     const int c0 = blockIdx.x << log_c;
+    if (LOG_M <= 8 && T.f64) {  // FP64 network: inputs in [0, q), twist output below q in magnitude
+        const double2* tab = stage_table_f64(sm + (S::M << log_c), T.fA, S::M);
+        const double qd = T.qd, qinv = T.qinv;
+        double* smd = reinterpret_cast<double*>(sm);
+        auto twf = [&](int s, u32 blk) { return tab[(1u << s) + blk]; };
+        __syncthreads();
+        if (tid < (C << S::LR2)) {
+            const int c = tid & (C - 1), i0 = tid >> log_c;
+            double x[S::R1];
+            if (kDigits) {
+                const i64* in = (const i64*)in_ + ((size_t)blockIdx.z << (LOG_M + log_b));
+#pragma unroll
+                for (int e = 0; e < S::R1; ++e)
+                    x[e] = nttf::from_u52(lift_digit(in[c0 + c + ((size_t)(i0 + S::R2 * e) << log_b)], q, T.mu_hi));
+            } else {
+                const u64* in = (const u64*)in_ + base;
+#pragma unroll
+                for (int e = 0; e < S::R1; ++e) x[e] = nttf::from_u52(in[c0 + c + ((size_t)(i0 + S::R2 * e) << log_b)]);
+            }
+            nttf::ct_stages<S::LR1>(x, 0, 0, twf, qd);
+#pragma unroll
+            for (int e = 0; e < S::R1; ++e)
+                smd[((i0 + S::R2 * e) << log_c) + (c ^ (e & (C - 1)))] = nttf::center(x[e], qd, qinv);
+        }
+        __syncthreads();
+        if (tid < (C << S::LR1)) {
+            const int g = tid & (S::R1 - 1), c = tid >> S::LR1;
+            double y[S::R2];
+#pragma unroll
+            for (int e = 0; e < S::R2; ++e) y[e] = smd[((S::R2 * g + e) << log_c) + (c ^ (g & (C - 1)))];
+            nttf::ct_stages<S::LR2>(y, S::LR1, g, twf, qd);
+            const size_t row = (size_t)(c0 + c) << LOG_M;
+#pragma unroll
+            for (int e = 0; e < S::R2; ++e) {
+                const size_t p = row + brev(S::R2 * g + e, LOG_M);
+                const double2 w = __ldg(T.fmid + p);
+                out[base + p] = (u64)__double_as_longlong(nttf::mulmod(y[e], w.x, w.y, qd));
+            }
+        }
+        return;
+    }
+    u64* st = sm + (S::M << log_c);
+    stage_table(st, T.psiA, T.psiA_q, S::M);
     auto tw = [&](int s, u32 blk, u64& W, u64& Wq) {
         u32 idx = (1u << s) + blk;
         W = st[idx];
@@ -142,11 +191,40 @@ k_fwd2(const u64* src, u64* dst, const NttTab* __restrict__ tabs,
     const int limb = blockIdx.y;
     const NttTab& T = tabs[lm(limb)];
     const u64 q = T.q;
-    u64* st = sm + (S::M << log_c);
-    stage_table(st, T.psiB, T.psiB_q, S::M);
     const size_t base = ((size_t)blockIdx.z * limb_count + limb) << (LOG_M + log_a);
     const int b0 = blockIdx.x << log_c;
     const int c = tid & (C - 1);
+    if (LOG_M <= 8 && T.f64) {  // FP64 network: pass-1 doubles (below q in magnitude) in, canonical out
+        const double2* tab = stage_table_f64(sm + (S::M << log_c), T.fB, S::M);
+        const double qd = T.qd, qinv = T.qinv;
+        double* smd = reinterpret_cast<double*>(sm);
+        auto twf = [&](int s, u32 blk) { return tab[(1u << s) + blk]; };
+        __syncthreads();
+        if (tid < (C << S::LR2)) {
+            const int i0 = tid >> log_c;
+            double x[S::R1];
+#pragma unroll
+            for (int e = 0; e < S::R1; ++e)
+                x[e] = __longlong_as_double((long long)src[base + ((size_t)(i0 + S::R2 * e) << log_a) + b0 + c]);
+            nttf::ct_stages<S::LR1>(x, 0, 0, twf, qd);
+#pragma unroll
+            for (int e = 0; e < S::R1; ++e) smd[((i0 + S::R2 * e) << log_c) + c] = nttf::center(x[e], qd, qinv);
+        }
+        __syncthreads();
+        if (tid < (C << S::LR1)) {
+            const int g = tid >> log_c;
+            double y[S::R2];
+#pragma unroll
+            for (int e = 0; e < S::R2; ++e) y[e] = smd[((S::R2 * g + e) << log_c) + c];
+            nttf::ct_stages<S::LR2>(y, S::LR1, g, twf, qd);
+#pragma unroll
+            for (int e = 0; e < S::R2; ++e)
+                dst[base + ((size_t)brev(S::R2 * g + e, LOG_M) << log_a) + b0 + c] = nttf::to_canonical(y[e], qd, qinv);
+        }
+        return;
+    }
+    u64* st = sm + (S::M << log_c);
+    stage_table(st, T.psiB, T.psiB_q, S::M);
     auto tw = [&](int s, u32 blk, u64& W, u64& Wq) {
         u32 idx = (1u << s) + blk;
         W = st[idx];
@@ -199,10 +277,50 @@ k_inv1(const u64* __restrict__ in, u64* __restrict__ out,
     const int limb = blockIdx.y;
     const NttTab& T = tabs[lm(limb)];
     const u64 q = T.q;
-    u64* st = sm + (S::M << log_c);
-    stage_table(st, T.psiB_inv, T.psiB_inv_q, S::M);
     const size_t base = ((size_t)blockIdx.z * limb_count + limb) << (LOG_M + log_a);
     const int b0 = blockIdx.x << log_c;
+    if (LOG_M <= 8 && T.f64) {  // FP64 network: inputs below 2^52, inverse-twist output below 1.5 q
+        const double2* tab = stage_table_f64(sm + (S::M << log_c), T.fB_inv, S::M);
+        const double qd = T.qd, qinv = T.qinv;
+        double* smd = reinterpret_cast<double*>(sm);
+        auto twf = [&](int s, u32 blk) { return tab[(S::M >> (s + 1)) + blk]; };
+        __syncthreads();
+        if (tid < (C << S::LR1)) {
+            const int c = tid & (C - 1), g = tid >> log_c;
+            double x[S::R2];
+#pragma unroll
+            for (int e = 0; e < S::R2; ++e)
+                x[e] = nttf::center(nttf::from_u52(in[base + ((size_t)brev(S::R2 * g + e, LOG_M) << log_a) + b0 + c]),
+                                    qd, qinv);
+            nttf::gs_stages<S::LR2>(x, 0, g, twf, qd);
+#pragma unroll
+            for (int e = 0; e < S::R2; ++e) {
+                const int r = S::R2 * g + e;
+                smd[(r << log_c) + (c ^ (r & (C - 1)))] = nttf::center(x[e], qd, qinv);
+            }
+        }
+        __syncthreads();
+        if (tid < (C << S::LR2)) {
+            const int i0 = tid & (S::R2 - 1), c = tid >> S::LR2;
+            double y[S::R1];
+#pragma unroll
+            for (int e = 0; e < S::R1; ++e) {
+                const int r = i0 + S::R2 * e;
+                y[e] = smd[(r << log_c) + (c ^ (r & (C - 1)))];
+            }
+            nttf::gs_stages<S::LR1>(y, S::LR2, 0, twf, qd);
+            const size_t row = (size_t)(b0 + c) << LOG_M;
+#pragma unroll
+            for (int e = 0; e < S::R1; ++e) {
+                const size_t p = row + i0 + S::R2 * e;
+                const double2 w = __ldg(T.fmidi + p);
+                out[base + p] = (u64)__double_as_longlong(nttf::mulmod(y[e], w.x, w.y, qd));
+            }
+        }
+        return;
+    }
+    u64* st = sm + (S::M << log_c);
+    stage_table(st, T.psiB_inv, T.psiB_inv_q, S::M);
     auto tw = [&](int s, u32 blk, u64& W, u64& Wq) {
         u32 idx = (S::M >> (s + 1)) + blk;
         W = st[idx];
@@ -256,11 +374,53 @@ k_inv2(const u64* src, u64* dst, const NttTab* __restrict__ tabs,
     const int limb = blockIdx.y;
     const NttTab& T = tabs[lm(limb)];
     const u64 q = T.q;
-    u64* st = sm + (S::M << log_c);
-    stage_table(st, T.psiA_inv, T.psiA_inv_q, S::M);
     const size_t base = ((size_t)blockIdx.z * limb_count + limb) << (LOG_M + log_b);
     const int c0 = blockIdx.x << log_c;
     const int c = tid & (C - 1);
+    if (LOG_M <= 8 && T.f64) {  // FP64 network: pass-1 doubles (below 1.5 q in magnitude) in, canonical out
+        const double2* tab = stage_table_f64(sm + (S::M << log_c), T.fA_inv, S::M);
+        const double qd = T.qd, qinv = T.qinv;
+        double* smd = reinterpret_cast<double*>(sm);
+        auto twf = [&](int s, u32 blk) { return tab[(S::M >> (s + 1)) + blk]; };
+        __syncthreads();
+        if (tid < (C << S::LR1)) {
+            const int g = tid >> log_c;
+            double x[S::R2];
+#pragma unroll
+            for (int e = 0; e < S::R2; ++e)
+                x[e] = nttf::center(
+                    __longlong_as_double((long long)src[base + c0 + c + ((size_t)brev(S::R2 * g + e, LOG_M) << log_b)]),
+                    qd, qinv);
+            nttf::gs_stages<S::LR2>(x, 0, g, twf, qd);
+#pragma unroll
+            for (int e = 0; e < S::R2; ++e) smd[((S::R2 * g + e) << log_c) + c] = nttf::center(x[e], qd, qinv);
+        }
+        __syncthreads();
+        if (tid < (C << S::LR2)) {
+            const int i0 = tid >> log_c;
+            double y[S::R1];
+#pragma unroll
+            for (int e = 0; e < S::R1; ++e) y[e] = smd[((i0 + S::R2 * e) << log_c) + c];
+            nttf::gs_stages<S::LR1>(y, S::LR2, 0, twf, qd);
+            const u32 poly = blockIdx.z;
+            if (ib.b && !(poly & 1) && (u32)limb < ib.q_limbs) {
+                const u64* bb = ib.b + (size_t)(poly / (2 * ib.n_keys)) * ib.b_stride + ((size_t)limb << (LOG_M + log_b));
+                const u64 pf = ib.pf[limb], pfq = ib.pf_q[limb];
+#pragma unroll
+                for (int e = 0; e < S::R1; ++e) {
+                    const size_t o = c0 + c + ((size_t)(i0 + S::R2 * e) << log_b);
+                    dst[base + o] = add_mod(nttf::to_canonical(y[e], qd, qinv), mul_shoup(__ldg(bb + o), pf, pfq, q), q);
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < S::R1; ++e)
+                    dst[base + c0 + c + ((size_t)(i0 + S::R2 * e) << log_b)] = nttf::to_canonical(y[e], qd, qinv);
+            }
+        }
+        return;
+    }
+    u64* st = sm + (S::M << log_c);
+    stage_table(st, T.psiA_inv, T.psiA_inv_q, S::M);
     auto tw = [&](int s, u32 blk, u64& W, u64& Wq) {
         u32 idx = (S::M >> (s + 1)) + blk;
         W = st[idx];
@@ -468,7 +628,8 @@ int32_t static_scratch_address(u64** out) {
 
 extern "C" int32_t ckks_ntt_forward_inplace_static(ckks_ctx* ctx, uint64_t* data, uint32_t n_polys,
                                                    uint32_t limb_begin, uint32_t limb_count, void* stream) {
-    if (!ctx || !data) {
+    if (int32_t rc = ckks_require_device(ctx, "ckks_ntt_forward_inplace_static")) return rc;
+    if (!data) {
         ckks_set_error("ckks_ntt_forward_inplace_static: null argument");
         return CKKS_ERR_BAD_ARG;
     }

@@ -121,3 +121,104 @@ __device__ __forceinline__ void gs_stages(u64 (&x)[1 << LR], int s0, u32 blk0, T
 }
 
 }  // namespace nttc
+
+// ---------------------------------------------------------------------------
+// Exact modular butterflies on the FP64 pipe, for primes q < 2^50.
+//
+// Values are integers held in doubles, signed, of magnitude below 2^53 (so
+// every one is exact). The product Y W (up to 2^103) is split error-free into
+// h = fl(Y W) and l = Y W - h (one FMA, exact: Dekker/Ogita TwoProduct); the
+// quotient estimate t = rint(fl(Y Wp)) with Wp = fl(W / q) differs from
+// Y W / q by at most 1/2 + |Y| 2^-54 + ulp(Y Wp)/2; then h - t q (one FMA)
+// is an integer below 2^53 in magnitude and exact, and r = (h - t q) + l =
+// Y W - t q exactly. Hence r = Y W (mod q) with
+//   |r| <= 0.75 q for |Y| < 2^51, <= q for |Y| < 2^52, <= 1.5 q for |Y| < 2^53.
+// No result depends on a rounding: the residues are the same integers the
+// Shoup network produces, up to a multiple of q, and every pass ends in an
+// exact reduction to [0, q).
+//
+// Cooley-Tukey (X, Y) -> (X + r, X - r): a stage adds at most |r| to the
+// bound. From inputs below q (or the centred reduction's q/2 + tiny), four
+// stages stay below 4.5 q. Gentleman-Sande (X, Y) -> (X + Y, (X - Y) W) doubles
+// the sum path: four stages from centred inputs stay below 8 q <= 2^53 - 8.
+// The passes therefore reduce once at their shared-memory exchange (every
+// four stages) and once at the end; the tests of lazy_bounds_cpu restate
+// these bounds.
+namespace nttf {
+
+constexpr u64 kF64Bound = 1ull << 50;  // primes below this take the FP64 networks
+constexpr double kTwo52 = 4503599627370496.0;
+
+// Y W mod q as a signed integer (bounds above).
+__device__ __forceinline__ double mulmod(double y, double w, double wp, double q) {
+    const double h = __dmul_rn(y, w);
+    const double l = __fma_rn(y, w, -h);
+    const double t = rint(__dmul_rn(y, wp));
+    return __dadd_rn(__fma_rn(-t, q, h), l);
+}
+// v - rint(v / q) q: |result| <= q/2 + |v| 2^-52 for |v| < 2^53 (exact).
+__device__ __forceinline__ double center(double v, double q, double qinv) {
+    return __fma_rn(-rint(__dmul_rn(v, qinv)), q, v);
+}
+// u64 below 2^52 -> double (exact): bits 0x433 | v is 2^52 + v.
+__device__ __forceinline__ double from_u52(u64 v) {
+    return __dsub_rn(__longlong_as_double((long long)(v | 0x4330000000000000ull)), kTwo52);
+}
+// |v| < 2^53 -> its residue in [0, q) as u64.
+__device__ __forceinline__ u64 to_canonical(double v, double q, double qinv) {
+    double r = center(v, q, qinv);
+    r = r < 0.0 ? __dadd_rn(r, q) : r;
+    return (u64)__double_as_longlong(__dadd_rn(r, kTwo52)) & 0xFFFFFFFFFFFFFull;
+}
+
+__device__ __forceinline__ void ct_bfly(double& X, double& Y, double W, double Wp, double q) {
+    const double r = mulmod(Y, W, Wp, q);
+    const double x = X;
+    X = __dadd_rn(x, r);
+    Y = __dsub_rn(x, r);
+}
+__device__ __forceinline__ void gs_bfly(double& X, double& Y, double W, double Wp, double q) {
+    const double d = __dsub_rn(X, Y);
+    X = __dadd_rn(X, Y);
+    Y = mulmod(d, W, Wp, q);
+}
+
+// Merged CT / GS stages with the register and twiddle indexing of
+// nttc::ct_stages / nttc::gs_stages; tw(stage, block) returns (W, Wp).
+template <int LR, int LS, typename TW>
+__device__ __forceinline__ void ct_stage(double (&x)[1 << LR], int s0, u32 base, TW& tw, double q) {
+    if constexpr (LS < LR) {
+        constexpr int half = (1 << LR) >> (LS + 1);
+#pragma unroll
+        for (int b = 0; b < (1 << LS); ++b) {
+            const double2 w = tw(s0 + LS, (base << LS) + b);
+#pragma unroll
+            for (int o = 0; o < half; ++o) ct_bfly(x[b * 2 * half + o], x[b * 2 * half + o + half], w.x, w.y, q);
+        }
+        ct_stage<LR, LS + 1>(x, s0, base, tw, q);
+    }
+}
+template <int LR, typename TW>
+__device__ __forceinline__ void ct_stages(double (&x)[1 << LR], int s0, u32 base, TW tw, double q) {
+    ct_stage<LR, 0>(x, s0, base, tw, q);
+}
+template <int LR, int LS, typename TW>
+__device__ __forceinline__ void gs_stage(double (&x)[1 << LR], int s0, u32 blk0, TW& tw, double q) {
+    if constexpr (LS < LR) {
+        constexpr int t = 1 << LS;
+        constexpr int nblk = (1 << LR) >> (LS + 1);
+#pragma unroll
+        for (int b = 0; b < nblk; ++b) {
+            const double2 w = tw(s0 + LS, (blk0 << (LR - LS - 1)) + b);
+#pragma unroll
+            for (int o = 0; o < t; ++o) gs_bfly(x[b * 2 * t + o], x[b * 2 * t + o + t], w.x, w.y, q);
+        }
+        gs_stage<LR, LS + 1>(x, s0, blk0, tw, q);
+    }
+}
+template <int LR, typename TW>
+__device__ __forceinline__ void gs_stages(double (&x)[1 << LR], int s0, u32 blk0, TW tw, double q) {
+    gs_stage<LR, 0>(x, s0, blk0, tw, q);
+}
+
+}  // namespace nttf

@@ -24,6 +24,9 @@
  *     stream. Work is stream-ordered; workspaces come from the stream-ordered
  *     allocator (cudaMallocAsync). Calls on one context are thread-safe when
  *     given distinct streams.
+ *   - device: a context belongs to the CUDA device that was current when it
+ *     was created; every call that touches device memory must be made with
+ *     that device current and returns CKKS_ERR_BAD_ARG otherwise.
  */
 #ifndef CKKS_B200_H
 #define CKKS_B200_H
@@ -80,6 +83,13 @@ int32_t ckks_ctx_destroy(ckks_ctx* ctx);
 int32_t ckks_ctx_set_tensor_cores(ckks_ctx* ctx, int32_t enable);
 /* 1 when bounded hoisted rotations of this context use the tensor cores. */
 int32_t ckks_ctx_tensor_cores(const ckks_ctx* ctx);
+/* Which key-switch MAC the most recent hoisted rotation on this context ran
+ * (ckks_rotate_hoisted and the calls built on it): 1 the tcgen05 INT8
+ * tensor-core MAC, 0 the CUDA-core MAC (tensor cores switched off, RNS-block
+ * keys, rings below the tensor-core tile, or too little free device memory
+ * for the packed key set), -1 no hoisted rotation yet. Diagnostic only; no
+ * counterpart in the reference. */
+int32_t ckks_ctx_last_mac_path(const ckks_ctx* ctx);
 /* Autotuner (no counterpart in the reference, whose NTT has no launch shape):
  * times every admissible columns-per-CTA choice of the five NTT passes
  * (forward 1, forward 1 of signed digits, forward 2, inverse 1, inverse 2) on
@@ -111,9 +121,12 @@ int32_t ckks_ntt_inverse(ckks_ctx* ctx, const uint64_t* in, uint64_t* out, uint3
  * compiled into the library (resident on every device that loads it until the
  * process exits); batches with n_polys * limb_count * N > 2^21 words are
  * rejected with CKKS_ERR_BAD_ARG. The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress); make that first call before
- * any stream capture. All calls share the array: calls whose work overlaps on
- * the GPU race. Output equals ckks_ntt_forward word for word. */
+ * array's device address (cudaGetSymbolAddress) and keeps it for the process;
+ * make that first call before any stream capture, and do not use this entry
+ * point on a device after a cudaDeviceReset (the reset reloads the module, so
+ * the kept address no longer names the array). All calls share the array:
+ * calls whose work overlaps on the GPU race. Output equals ckks_ntt_forward
+ * word for word. */
 int32_t ckks_ntt_forward_inplace_static(ckks_ctx* ctx, uint64_t* data, uint32_t n_polys, uint32_t limb_begin,
                                         uint32_t limb_count, void* stream);
 /* Host-buffer forms: copy in, transform, copy out (synchronous). */

@@ -2,6 +2,9 @@
 
 Runs only where the reference checkout is present (its Python oracles are
 imported from there); the GPU box and the tests read the committed JSON.
+
+Usage: python tests/golden/make_golden.py <reference checkout>
+(or set CCMM_REFERENCE to the checkout's root).
 Sources:
   security/p6a/generate_candidates.py  -- the reference's prime search
   tools/ckks_embedding_oracle.py       -- O(N^2) canonical embedding
@@ -16,8 +19,10 @@ import random
 import re
 import sys
 
-REF = os.environ.get("CCMM_REFERENCE", "/root/reference")
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CCMM_REFERENCE")
 HERE = os.path.dirname(os.path.abspath(__file__))
+if not REF or not os.path.isdir(REF):
+    sys.exit("usage: make_golden.py <reference checkout>  (or CCMM_REFERENCE=<checkout>)")
 
 
 def load(path, name):

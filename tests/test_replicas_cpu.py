@@ -46,3 +46,30 @@ def test_two_gloo_ranks_take_the_max_time():
     res = [json.loads(o.strip().splitlines()[-1]) for o, _ in outs]
     assert all(r["max"] == 2.5 for r in res)
     assert all(abs(r["rate"] - 1024 / 2.5) < 1e-9 for r in res)
+
+
+def test_bench_gpus_flag_launches_ranks():
+    """`bench.py --gpus 2` launches two ranks itself (torch.distributed.run on
+    127.0.0.1) and the printed line carries n_gpus = 2. The reference arm runs
+    on the host cores, so this runs on CPU: rank 0 measures and prints, rank 1
+    exits without work."""
+    import json
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    for k in ("WORLD_SIZE", "RANK", "LOCAL_RANK", "MASTER_ADDR", "MASTER_PORT"):
+        env.pop(k, None)
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2",
+                        "--workload", "multiply", "--steps", "1", "--warmup", "3"],
+                       env=env, capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-3000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1, r.stdout[-3000:]
+    line = json.loads(lines[0])
+    assert line["n_gpus"] == 2 and line["impl"] == "reference"
+
+
+def test_bench_rejects_mismatched_world_size():
+    env = dict(os.environ, WORLD_SIZE="3", RANK="0", CUDA_VISIBLE_DEVICES="")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2",
+                        "--workload", "multiply", "--steps", "1"], env=env, capture_output=True, text=True,
+                       timeout=300, cwd=ROOT)
+    assert r.returncode != 0 and "WORLD_SIZE=3" in (r.stderr + r.stdout)
