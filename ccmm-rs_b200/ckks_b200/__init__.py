@@ -55,6 +55,7 @@ _SIGS = {
     "ckks_pointwise": (I32, [VP, VP, VP, VP, U32, U32, U32, I32, VP]),
     "ckks_rescale": (I32, [VP, VP, VP, U32, U32, VP]),
     "ckks_mod_down": (I32, [VP, VP, VP, U32, U32, VP]),
+    "ckks_mod_switch": (I32, [VP, VP, VP, U32, U32, U32, VP]),
     "ckks_bounded_digit_count": (I32, [VP, U32, U32, ctypes.POINTER(U32)]),
     "ckks_bounded_decompose": (I32, [VP, VP, U32, U32, U32, VP, VP]),
     "ckks_bounded_digits_automorphism": (I32, [VP, VP, VP, U32, U32, U32, U64, VP]),
@@ -62,6 +63,10 @@ _SIGS = {
     "ckks_hybrid_key_upload": (I32, [VP, U32, U32, U64, u64p, ctypes.POINTER(VP)]),
     "ckks_rnsblock_key_generate": (I32, [VP, U32, u32p, U32, U64, i8p, U64, ctypes.c_double, ctypes.POINTER(VP)]),
     "ckks_rnsblock_key_upload": (I32, [VP, U32, u32p, U32, U64, u64p, ctypes.POINTER(VP)]),
+    "ckks_rns_key_generate": (I32, [VP, U32, u32p, U32, U64, i8p, U64, ctypes.c_double, ctypes.POINTER(VP)]),
+    "ckks_rns_key_upload": (I32, [VP, U32, u32p, U32, U64, u64p, ctypes.POINTER(VP)]),
+    "ckks_rns_relin_key_generate": (I32, [VP, U32, u32p, U32, i8p, U64, ctypes.c_double, ctypes.POINTER(VP)]),
+    "ckks_rns_relin_key_upload": (I32, [VP, U32, u32p, U32, u64p, ctypes.POINTER(VP)]),
     "ckks_relin_key_generate": (I32, [VP, U32, U32, i8p, U64, ctypes.c_double, ctypes.POINTER(VP)]),
     "ckks_relin_key_upload": (I32, [VP, U32, U32, u64p, ctypes.POINTER(VP)]),
     "ckks_ksk_info": (I32, [VP, ctypes.POINTER(U32), ctypes.POINTER(U64)]),
@@ -77,6 +82,7 @@ _SIGS = {
     "ckks_multiply_relin_rescale_host": (I32, [VP, VP, u64p, u64p, u64p, U32]),
     "ckks_mul_plain": (I32, [VP, VP, VP, VP, U32, U32, U32, VP]),
     "ckks_fft_stage": (I32, [VP, ctypes.POINTER(VP), U32, I32, VP, VP, VP, U32, U32, VP]),
+    "ckks_diag_stage": (I32, [VP, ctypes.POINTER(VP), U32, I32, VP, VP, VP, U32, U32, I32, VP]),
     "ckks_ccmm_structured": (I32, [VP, VP, VP, VP, VP, U32, U32, U32, VP]),
     "ckks_fft_stage_multi": (I32, [VP, ctypes.POINTER(VP), U32, u32p, U32, VP, VP, U32, VP, U32, U32, VP]),
     "ckks_encode": (I32, [VP, VP, VP, U32, U32, ctypes.c_double, VP]),
@@ -284,6 +290,17 @@ class Context:
                                  _stream(stream)))
         return out
 
+    def mod_switch(self, ct, limbs_out=None, stream=None):
+        """ckks/rns_mod_switch.rs:14-58: [..., 2, limbs, N] -> [..., 2, limbs_out, N]
+        keeping the leading limbs (default: one level down), scale unchanged."""
+        import torch
+        limbs = ct.shape[-2]
+        limbs_out = limbs - 1 if limbs_out is None else int(limbs_out)
+        out = torch.empty(ct.shape[:-2] + (limbs_out, self.n), dtype=torch.int64, device=ct.device)
+        check(lib().ckks_mod_switch(self.handle, _dptr(ct), _dptr(out), ct.numel() // (2 * limbs * self.n), limbs,
+                                    limbs_out, _stream(stream)))
+        return out
+
     def mod_down(self, data, stream=None):
         """ring/auxiliary_modulus.rs:89-171: [..., q_limbs+K, N] -> [..., q_limbs, N]."""
         import torch
@@ -328,7 +345,7 @@ class Context:
 class KeySwitchKey:
     """A key-switching key resident in HBM (ckks_ksk)."""
 
-    HYBRID_BOUNDED, HYBRID_RNS_BLOCK, RELIN_BOUNDED = 0, 1, 2
+    HYBRID_BOUNDED, HYBRID_RNS_BLOCK, RELIN_BOUNDED, RNS_BLOCK, RELIN_RNS_BLOCK = 0, 1, 2, 3, 4
 
     def __init__(self, ctx, handle, kind, q_limbs, exponent=1, base_log=0, blocks=()):
         self.ctx, self.handle, self.kind = ctx, handle, kind
@@ -372,6 +389,47 @@ class KeySwitchKey:
         check(lib().ckks_rnsblock_key_upload(ctx.handle, q_limbs, b.ctypes.data_as(u32p), len(b), int(exponent), ep,
                                              ctypes.byref(h)))
         return cls(ctx, h, cls.HYBRID_RNS_BLOCK, q_limbs, exponent, 0, blocks)
+
+    @classmethod
+    def rns_generate(cls, ctx, q_limbs, blocks, exponent, secret, seed, sigma=3.2):
+        """Ordinary RNS Galois key without auxiliary limbs: PreparedRnsGaloisKey
+        (ckks/rns_galois_key.rs, grafting/rns_key_switch.rs:1155-1258)."""
+        s, sp = cls._secret(secret)
+        b = np.ascontiguousarray(np.asarray(blocks, np.uint32))
+        h = ctypes.c_void_p()
+        check(lib().ckks_rns_key_generate(ctx.handle, q_limbs, b.ctypes.data_as(u32p), len(b), int(exponent), sp,
+                                          seed, sigma, ctypes.byref(h)))
+        return cls(ctx, h, cls.RNS_BLOCK, q_limbs, exponent, 0, blocks)
+
+    @classmethod
+    def rns_upload(cls, ctx, q_limbs, blocks, exponent, entries):
+        """NTT-domain entries [dnum][q_limbs][2][N] (the reference's PreparedRnsKeySwitchKey)."""
+        e, ep = _u64(entries)
+        b = np.ascontiguousarray(np.asarray(blocks, np.uint32))
+        h = ctypes.c_void_p()
+        check(lib().ckks_rns_key_upload(ctx.handle, q_limbs, b.ctypes.data_as(u32p), len(b), int(exponent), ep,
+                                        ctypes.byref(h)))
+        return cls(ctx, h, cls.RNS_BLOCK, q_limbs, exponent, 0, blocks)
+
+    @classmethod
+    def rns_relin_generate(cls, ctx, q_limbs, blocks, secret, seed, sigma=3.2):
+        """RNS-block relinearization key (RnsMultiplicationKey, target s^2)."""
+        s, sp = cls._secret(secret)
+        b = np.ascontiguousarray(np.asarray(blocks, np.uint32))
+        h = ctypes.c_void_p()
+        check(lib().ckks_rns_relin_key_generate(ctx.handle, q_limbs, b.ctypes.data_as(u32p), len(b), sp, seed, sigma,
+                                                ctypes.byref(h)))
+        return cls(ctx, h, cls.RELIN_RNS_BLOCK, q_limbs, 1, 0, blocks)
+
+    @classmethod
+    def rns_relin_upload(cls, ctx, q_limbs, blocks, entries):
+        """Coefficient-domain entries [dnum][2][q_limbs][N]."""
+        e, ep = _u64(entries)
+        b = np.ascontiguousarray(np.asarray(blocks, np.uint32))
+        h = ctypes.c_void_p()
+        check(lib().ckks_rns_relin_key_upload(ctx.handle, q_limbs, b.ctypes.data_as(u32p), len(b), ep,
+                                              ctypes.byref(h)))
+        return cls(ctx, h, cls.RELIN_RNS_BLOCK, q_limbs, 1, 0, blocks)
 
     @classmethod
     def relin_generate(cls, ctx, q_limbs, base_log, secret, seed, sigma=3.2):
@@ -556,6 +614,22 @@ def fft_stage(ctx, keys, diag_ntt, ct, identity=True, out=None, stream=None):
     arr = (VP * max(1, len(keys)))(*[k.handle.value for k in keys])
     check(lib().ckks_fft_stage(ctx.handle, arr, len(keys), 1 if identity else 0, _dptr(diag_ntt), _dptr(ct),
                                _dptr(out), n_ct, L, _stream(stream)))
+    return out
+
+
+def diag_stage(ctx, keys, diag_ntt, ct, identity=True, rescale=True, out=None, stream=None):
+    """fft_stage with the rescale optional; with keys (rotate left by r, rotate
+    right by r) and the identity term it is the packed radix-2 DIF FFT2 stage
+    (eblas/fft.rs:3378-3470, fused-rescale form :3906-4000)."""
+    import torch
+    L = ct.shape[-2]
+    n_ct = _n_ct(ctx, ct, 2, L)
+    lo = L - 1 if rescale else L
+    if out is None:
+        out = torch.empty((n_ct, 2, lo, ctx.n), dtype=torch.int64, device=ct.device)
+    arr = (VP * max(1, len(keys)))(*[k.handle.value for k in keys])
+    check(lib().ckks_diag_stage(ctx.handle, arr, len(keys), 1 if identity else 0, _dptr(diag_ntt), _dptr(ct),
+                                _dptr(out), n_ct, L, 1 if rescale else 0, _stream(stream)))
     return out
 
 

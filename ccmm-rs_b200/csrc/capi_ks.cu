@@ -48,13 +48,13 @@ int32_t new_key(ckks_ctx* ctx, int kind, u32 q_limbs, u32 base_log, u64 exponent
     k->q_limbs = q_limbs;
     k->base_log = base_log;
     k->exponent = exponent % (2ull * ctx->n);
-    k->with_p = kind != CKKS_KSK_RELIN_BOUNDED;
+    k->with_p = kind == CKKS_KSK_HYBRID_BOUNDED || kind == CKKS_KSK_HYBRID_RNS_BLOCK;
     if (k->with_p && ctx->K == 0) {
         delete k;
         ckks_set_error(std::string(who) + ": hybrid keys need auxiliary limbs in the context");
         return CKKS_ERR_BASIS_MISMATCH;
     }
-    if (kind == CKKS_KSK_HYBRID_RNS_BLOCK) {
+    if (kind == CKKS_KSK_HYBRID_RNS_BLOCK || kind == CKKS_KSK_RNS_BLOCK || kind == CKKS_KSK_RELIN_RNS_BLOCK) {
         k->blocks = blocks;
         k->D = (u32)blocks.size();
         if (int32_t rc = rnsblock_prepare(ctx, k)) {
@@ -159,6 +159,20 @@ int32_t ckks_mod_down(ckks_ctx* ctx, const uint64_t* in, uint64_t* out, uint32_t
     return mod_down_launch(ctx, in, out, n_polys, q_limbs, ckks_stream(ctx, stream));
 }
 
+int32_t ckks_mod_switch(ckks_ctx* ctx, const uint64_t* in, uint64_t* out, uint32_t n_ct, uint32_t limbs_in,
+                        uint32_t limbs_out, void* stream) {
+    if (int32_t rc = need_ctx(ctx, "ckks_mod_switch")) return rc;
+    CKKS_CHECK_ARG(in && out, "ckks_mod_switch: null buffer");
+    CKKS_CHECK_ARG(limbs_out >= 1 && limbs_out <= limbs_in && limbs_in <= ctx->L,
+                   "ckks_mod_switch: need 1 <= limbs_out <= limbs_in <= L");
+    if (!n_ct) return CKKS_OK;
+    const size_t n = ctx->n;
+    // the limbs of the lower level are the leading ones (ring/modulus_chain.rs:19-27)
+    CKKS_CUDA_TRY(cudaMemcpy2DAsync(out, limbs_out * n * 8, in, limbs_in * n * 8, limbs_out * n * 8, 2 * (size_t)n_ct,
+                                    cudaMemcpyDeviceToDevice, ckks_stream(ctx, stream)));
+    return CKKS_OK;
+}
+
 int32_t ckks_bounded_digit_count(ckks_ctx* ctx, uint32_t q_limbs, uint32_t base_log, uint32_t* out) {
     if (int32_t rc = need_ctx(ctx, "ckks_bounded_digit_count")) return rc;
     CKKS_CHECK_ARG(out != nullptr, "ckks_bounded_digit_count: out is null");
@@ -234,6 +248,65 @@ int32_t ckks_rnsblock_key_upload(ckks_ctx* ctx, uint32_t q_limbs, const uint32_t
     return finish_key(k, upload_galois(ctx, k, entries_host), out);
 }
 
+int32_t ckks_rns_key_generate(ckks_ctx* ctx, uint32_t q_limbs, const uint32_t* block_sizes, uint32_t n_blocks,
+                              uint64_t exponent, const int8_t* secret_host, uint64_t seed, double sigma,
+                              ckks_ksk** out) {
+    if (int32_t rc = need_ctx(ctx, "ckks_rns_key_generate")) return rc;
+    CKKS_CHECK_ARG(out && block_sizes && n_blocks && secret_host && sigma > 0, "ckks_rns_key_generate: bad arguments");
+    if (int32_t rc = check_exponent(ctx, exponent, "ckks_rns_key_generate")) return rc;
+    ckks_ksk* k;
+    std::vector<u32> bs(block_sizes, block_sizes + n_blocks);
+    if (int32_t rc = new_key(ctx, CKKS_KSK_RNS_BLOCK, q_limbs, 0, exponent, bs, &k, "ckks_rns_key_generate")) return rc;
+    *out = k;
+    auto st_secret = host_secret_automorphism(secret_host, ctx->n, k->exponent);
+    int32_t rc = ksk_generate(ctx, k, secret_host, seed, sigma, rns_factors(ctx, k), st_secret, false, TAG_KEY_A,
+                              TAG_KEY_E, nullptr);
+    return finish_key(k, rc, out);
+}
+
+int32_t ckks_rns_key_upload(ckks_ctx* ctx, uint32_t q_limbs, const uint32_t* block_sizes, uint32_t n_blocks,
+                            uint64_t exponent, const uint64_t* entries_host, ckks_ksk** out) {
+    if (int32_t rc = need_ctx(ctx, "ckks_rns_key_upload")) return rc;
+    CKKS_CHECK_ARG(out && block_sizes && n_blocks && entries_host, "ckks_rns_key_upload: bad arguments");
+    if (int32_t rc = check_exponent(ctx, exponent, "ckks_rns_key_upload")) return rc;
+    ckks_ksk* k;
+    std::vector<u32> bs(block_sizes, block_sizes + n_blocks);
+    if (int32_t rc = new_key(ctx, CKKS_KSK_RNS_BLOCK, q_limbs, 0, exponent, bs, &k, "ckks_rns_key_upload")) return rc;
+    *out = k;
+    return finish_key(k, upload_galois(ctx, k, entries_host), out);
+}
+
+int32_t ckks_rns_relin_key_generate(ckks_ctx* ctx, uint32_t q_limbs, const uint32_t* block_sizes, uint32_t n_blocks,
+                                    const int8_t* secret_host, uint64_t seed, double sigma, ckks_ksk** out) {
+    if (int32_t rc = need_ctx(ctx, "ckks_rns_relin_key_generate")) return rc;
+    CKKS_CHECK_ARG(out && block_sizes && n_blocks && secret_host && sigma > 0,
+                   "ckks_rns_relin_key_generate: bad arguments");
+    ckks_ksk* k;
+    std::vector<u32> bs(block_sizes, block_sizes + n_blocks);
+    if (int32_t rc = new_key(ctx, CKKS_KSK_RELIN_RNS_BLOCK, q_limbs, 0, 1, bs, &k, "ckks_rns_relin_key_generate"))
+        return rc;
+    *out = k;
+    return finish_key(k, relin_generate(ctx, k, secret_host, seed, sigma, nullptr), out);
+}
+
+int32_t ckks_rns_relin_key_upload(ckks_ctx* ctx, uint32_t q_limbs, const uint32_t* block_sizes, uint32_t n_blocks,
+                                  const uint64_t* entries_host, ckks_ksk** out) {
+    if (int32_t rc = need_ctx(ctx, "ckks_rns_relin_key_upload")) return rc;
+    CKKS_CHECK_ARG(out && block_sizes && n_blocks && entries_host, "ckks_rns_relin_key_upload: bad arguments");
+    ckks_ksk* k;
+    std::vector<u32> bs(block_sizes, block_sizes + n_blocks);
+    if (int32_t rc = new_key(ctx, CKKS_KSK_RELIN_RNS_BLOCK, q_limbs, 0, 1, bs, &k, "ckks_rns_relin_key_upload"))
+        return rc;
+    *out = k;
+    cudaError_t e = cudaMemcpy(k->d_entries, entries_host, k->words * 8, cudaMemcpyHostToDevice);
+    int32_t rc = e == cudaSuccess ? CKKS_OK : CKKS_ERR_CUDA;
+    if (e != cudaSuccess) ckks_set_error(cudaGetErrorString(e));
+    // coefficient domain [dnum][2][q_limbs][N] in, NTT domain stored
+    if (rc == CKKS_OK) rc = ntt_forward_launch_map(ctx, k->d_entries, k->d_entries, 2 * k->D, LimbMap::range(0, q_limbs),
+                                                   q_limbs, nullptr);
+    return finish_key(k, rc, out);
+}
+
 int32_t ckks_relin_key_generate(ckks_ctx* ctx, uint32_t q_limbs, uint32_t base_log, const int8_t* secret_host,
                                 uint64_t seed, double sigma, ckks_ksk** out) {
     CKKS_CHECK_ARG(secret_host && sigma > 0, "ckks_relin_key_generate: bad secret or sigma");
@@ -270,7 +343,7 @@ int32_t ckks_ksk_info(const ckks_ksk* key, uint32_t* digits, uint64_t* words) {
 
 int32_t ckks_ksk_download(const ckks_ksk* key, uint64_t* entries_host) {
     CKKS_CHECK_ARG(key && entries_host, "ckks_ksk_download: null argument");
-    if (key->kind == CKKS_KSK_RELIN_BOUNDED) {
+    if (key->kind == CKKS_KSK_RELIN_BOUNDED || key->kind == CKKS_KSK_RELIN_RNS_BLOCK) {
         CKKS_CUDA_TRY(cudaMemcpy(entries_host, key->d_entries, key->words * 8, cudaMemcpyDeviceToHost));
         return CKKS_OK;
     }
@@ -300,7 +373,7 @@ int32_t ckks_rotate(ckks_ctx* ctx, const ckks_ksk* key, const uint64_t* ct_in, u
                     void* stream) {
     if (int32_t rc = need_ctx(ctx, "ckks_rotate")) return rc;
     CKKS_CHECK_ARG(key && ct_in && ct_out && ct_in != ct_out, "ckks_rotate: bad arguments");
-    if (key->ctx != ctx || key->kind == CKKS_KSK_RELIN_BOUNDED) {
+    if (key->ctx != ctx || key->kind == CKKS_KSK_RELIN_BOUNDED || key->kind == CKKS_KSK_RELIN_RNS_BLOCK) {
         ckks_set_error("ckks_rotate: key is not a Galois key of this context");
         return CKKS_ERR_BASIS_MISMATCH;
     }
@@ -315,6 +388,7 @@ int32_t ckks_rotate_hoisted(ckks_ctx* ctx, const ckks_ksk* const* keys, uint32_t
     for (u32 g = 0; g < n_keys; ++g) {
         const ckks_ksk* k = keys[g];
         if (!k || k->ctx != ctx || k->kind != k0->kind || k->kind == CKKS_KSK_RELIN_BOUNDED ||
+            k->kind == CKKS_KSK_RELIN_RNS_BLOCK ||
             k->q_limbs != k0->q_limbs || k->base_log != k0->base_log || k->D != k0->D || k->blocks != k0->blocks) {
             ckks_set_error("ckks_rotate_hoisted: keys must be Galois keys of one kind, level and gadget");
             return CKKS_ERR_BASIS_MISMATCH;
@@ -332,12 +406,17 @@ int32_t ckks_rotate_hoisted_timed(ckks_ctx* ctx, const ckks_ksk* const* keys, ui
     for (u32 g = 0; g < n_keys; ++g) {
         const ckks_ksk* k = keys[g];
         if (!k || k->ctx != ctx || k->kind != k0->kind || k->kind == CKKS_KSK_RELIN_BOUNDED ||
+            k->kind == CKKS_KSK_RELIN_RNS_BLOCK ||
             k->q_limbs != k0->q_limbs || k->base_log != k0->base_log || k->D != k0->D || k->blocks != k0->blocks) {
             ckks_set_error("ckks_rotate_hoisted_timed: keys must be Galois keys of one kind, level and gadget");
             return CKKS_ERR_BASIS_MISMATCH;
         }
     }
     for (int i = 0; i < 8; ++i) phase_ms[i] = 0;
+    if (k0->kind == CKKS_KSK_RNS_BLOCK) {
+        ckks_set_error("ckks_rotate_hoisted_timed: keys without auxiliary limbs have no hoisted phases");
+        return CKKS_ERR_BAD_ARG;
+    }
     return rotate_hoisted_ntt(ctx, keys, n_keys, ct_in, ct_out, n_ct, ckks_stream(ctx, stream), phase_ms);
 }
 

@@ -9,8 +9,8 @@ namespace {
 int32_t check_relin_key(ckks_ctx* ctx, const ckks_ksk* key, const char* who) {
     if (int32_t rc = ckks_require_device(ctx, who)) return rc;
     CKKS_CHECK_ARG(key != nullptr, std::string(who) + ": null key");
-    if (key->ctx != ctx || key->kind != CKKS_KSK_RELIN_BOUNDED) {
-        ckks_set_error(std::string(who) + ": key is not a bounded relinearization key of this context");
+    if (key->ctx != ctx || (key->kind != CKKS_KSK_RELIN_BOUNDED && key->kind != CKKS_KSK_RELIN_RNS_BLOCK)) {
+        ckks_set_error(std::string(who) + ": key is not a relinearization key of this context");
         return CKKS_ERR_BASIS_MISMATCH;
     }
     return CKKS_OK;
@@ -99,27 +99,44 @@ int32_t ckks_mul_plain(ckks_ctx* ctx, const uint64_t* ct, const uint64_t* plain_
     return mul_plain_launch(ctx, ct, plain_ntt, out, n_ct, q_limbs, n_plain > 1, ckks_stream(ctx, stream));
 }
 
-int32_t ckks_fft_stage(ckks_ctx* ctx, const ckks_ksk* const* keys, uint32_t n_rot, int32_t identity,
-                       const uint64_t* diag_ntt, const uint64_t* ct_in, uint64_t* ct_out, uint32_t n_ct,
-                       uint32_t q_limbs, void* stream) {
-    if (int32_t rc = ckks_require_device(ctx, "ckks_fft_stage")) return rc;
+namespace {
+int32_t diag_stage(ckks_ctx* ctx, const ckks_ksk* const* keys, uint32_t n_rot, int32_t identity,
+                   const uint64_t* diag_ntt, const uint64_t* ct_in, uint64_t* ct_out, uint32_t n_ct, uint32_t q_limbs,
+                   bool rescale, void* stream, const char* who) {
+    if (int32_t rc = ckks_require_device(ctx, who)) return rc;
     CKKS_CHECK_ARG(diag_ntt && ct_in && ct_out && (n_rot == 0 || keys) && (n_rot || identity),
-                   "ckks_fft_stage: bad arguments");
-    CKKS_CHECK_ARG(q_limbs >= 2 && q_limbs <= ctx->L, "ckks_fft_stage: need 2..L limbs (the stage rescales)");
+                   std::string(who) + ": bad arguments");
+    CKKS_CHECK_ARG(q_limbs >= (rescale ? 2u : 1u) && q_limbs <= ctx->L,
+                   std::string(who) + ": need 2..L limbs to rescale, 1..L otherwise");
     for (u32 g = 0; g < n_rot; ++g) {
         const ckks_ksk* k = keys[g];
-        if (!k || k->ctx != ctx || k->kind == CKKS_KSK_RELIN_BOUNDED || k->kind != keys[0]->kind ||
-            k->q_limbs != q_limbs || k->base_log != keys[0]->base_log || k->D != keys[0]->D ||
-            k->blocks != keys[0]->blocks) {
-            ckks_set_error("ckks_fft_stage: keys must be Galois keys of one kind and gadget at level q_limbs");
+        if (!k || k->ctx != ctx || !k->with_p || k->kind != keys[0]->kind || k->q_limbs != q_limbs ||
+            k->base_log != keys[0]->base_log || k->D != keys[0]->D || k->blocks != keys[0]->blocks) {
+            ckks_set_error(std::string(who) + ": keys must be hybrid Galois keys of one kind and gadget at level q_limbs");
             return CKKS_ERR_BASIS_MISMATCH;
         }
     }
-    const size_t in = (size_t)2 * q_limbs * ctx->n * 8 * n_ct, o = (size_t)2 * (q_limbs - 1) * ctx->n * 8 * n_ct;
-    CKKS_CHECK_ARG(!overlaps(ct_out, o, ct_in, in), "ckks_fft_stage: out overlaps the input");
+    const size_t in = (size_t)2 * q_limbs * ctx->n * 8 * n_ct,
+                 o = (size_t)2 * (rescale ? q_limbs - 1 : q_limbs) * ctx->n * 8 * n_ct;
+    CKKS_CHECK_ARG(!overlaps(ct_out, o, ct_in, in), std::string(who) + ": out overlaps the input");
     if (!n_ct) return CKKS_OK;
     return fft_stage_launch(ctx, keys, n_rot, identity != 0, diag_ntt, ct_in, ct_out, n_ct, q_limbs,
-                            ckks_stream(ctx, stream));
+                            ckks_stream(ctx, stream), rescale);
+}
+}  // namespace
+
+int32_t ckks_fft_stage(ckks_ctx* ctx, const ckks_ksk* const* keys, uint32_t n_rot, int32_t identity,
+                       const uint64_t* diag_ntt, const uint64_t* ct_in, uint64_t* ct_out, uint32_t n_ct,
+                       uint32_t q_limbs, void* stream) {
+    return diag_stage(ctx, keys, n_rot, identity, diag_ntt, ct_in, ct_out, n_ct, q_limbs, true, stream,
+                      "ckks_fft_stage");
+}
+
+int32_t ckks_diag_stage(ckks_ctx* ctx, const ckks_ksk* const* keys, uint32_t n_rot, int32_t identity,
+                        const uint64_t* diag_ntt, const uint64_t* ct_in, uint64_t* ct_out, uint32_t n_ct,
+                        uint32_t q_limbs, int32_t rescale, void* stream) {
+    return diag_stage(ctx, keys, n_rot, identity, diag_ntt, ct_in, ct_out, n_ct, q_limbs, rescale != 0, stream,
+                      "ckks_diag_stage");
 }
 
 int32_t ckks_ccmm_structured(ckks_ctx* ctx, const ckks_ksk* key, const uint64_t* A, const uint64_t* B, uint64_t* C,
@@ -150,10 +167,10 @@ int32_t ckks_fft_stage_multi(ckks_ctx* ctx, const ckks_ksk* const* keys, uint32_
                        "ckks_fft_stage_multi: term index out of range");
     for (u32 g = 0; g < n_rot; ++g) {
         const ckks_ksk* k = keys[g];
-        if (!k || k->ctx != ctx || k->kind == CKKS_KSK_RELIN_BOUNDED || k->kind != keys[0]->kind ||
+        if (!k || k->ctx != ctx || !k->with_p || k->kind != keys[0]->kind ||
             k->q_limbs != q_limbs || k->base_log != keys[0]->base_log || k->D != keys[0]->D ||
             k->blocks != keys[0]->blocks) {
-            ckks_set_error("ckks_fft_stage_multi: keys must be Galois keys of one kind and gadget at level q_limbs");
+            ckks_set_error("ckks_fft_stage_multi: keys must be hybrid Galois keys of one kind and gadget at level q_limbs");
             return CKKS_ERR_BASIS_MISMATCH;
         }
     }

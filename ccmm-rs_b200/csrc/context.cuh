@@ -156,8 +156,19 @@ struct InvBase {
     u32 n_keys = 1, q_limbs = 0;
     const u64 *pf = nullptr, *pf_q = nullptr;
 };
+// Optional Galois automorphism folded into the inverse transform of key-switch
+// accumulators [n_ct][n_keys][2][limbs][N]: polynomial p leaves as
+// sigma_k(INTT(p)) with k = exps[(p / 2) % n_keys] (X^j -> X^(j k), a sign
+// flip past N) and exps_inv[g] = k^-1 mod 2N. Pass 1 stores each row with its
+// columns permuted (j_lo -> j_lo k mod B); pass 2 reads consecutive permuted
+// columns and writes every element to its image row through shared memory.
+struct GaloisOut {
+    const u64* exps = nullptr;
+    const u64* exps_inv = nullptr;
+    u32 n_keys = 1;
+};
 int32_t ntt_inverse_base_launch(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, LimbMap lm, u32 limb_count,
-                                const InvBase& ib, cudaStream_t st);
+                                const InvBase& ib, cudaStream_t st, const GaloisOut& go = GaloisOut{});
 // Times every admissible columns-per-CTA choice of the five NTT passes on a
 // scratch batch (limbs x polys) and keeps the fastest in ctx (ntt.cu).
 int32_t ntt_autotune(ckks_ctx* ctx, u32 limbs, u32 polys, cudaStream_t st);

@@ -144,7 +144,7 @@ int32_t fft_stage_multi_launch(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n
 }
 
 int32_t fft_stage_launch(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_rot, bool identity, const u64* diag_ntt,
-                         const u64* ct_in, u64* ct_out, u32 n_ct, u32 L, cudaStream_t st) {
+                         const u64* ct_in, u64* ct_out, u32 n_ct, u32 L, cudaStream_t st, bool rescale) {
     const u32 N = ctx->n;
     const size_t poly = (size_t)L * N, ct = 2 * poly;
     // ciphertexts per chunk: rotated copies (n_rot + 1 per ciphertext) within about 2^29 words
@@ -172,8 +172,12 @@ int32_t fft_stage_launch(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_rot, 
         k_diag_mac<<<g, kT, 0, st>>>(R.p, identity ? X.p : nullptr, diag_ntt, acc, ctx->d_tabs, (int)n_rot, (int)L,
                                      (int)ctx->log_n);
         CKKS_CUDA_TRY(cudaGetLastError());
-        if ((rc = ntt_inverse_launch(ctx, acc, acc, 2 * m, 0, L, st))) return rc;
-        if ((rc = rescale_launch(ctx, acc, ct_out + (size_t)c0 * 2 * (L - 1) * N, 2 * m, L, st))) return rc;
+        if (rescale) {
+            if ((rc = ntt_inverse_launch(ctx, acc, acc, 2 * m, 0, L, st))) return rc;
+            if ((rc = rescale_launch(ctx, acc, ct_out + (size_t)c0 * 2 * (L - 1) * N, 2 * m, L, st))) return rc;
+        } else if ((rc = ntt_inverse_launch(ctx, acc, ct_out + (size_t)c0 * ct, 2 * m, 0, L, st))) {
+            return rc;
+        }
     }
     return CKKS_OK;
 }

@@ -1086,6 +1086,15 @@ struct StatusReadback {
 
 }  // namespace
 
+// sigma_g folded into the inverse transform (pass 1 permutes row columns, pass 2
+// rows through shared memory) instead of gathered by ModDown. Measured at the
+// 16 ct x 32 keys shape: inverse NTT +2.7 ms, ModDown -1.9 ms per step, so it
+// stays off; kept for the fused inverse-transform + ModDown layout.
+#ifndef CKKS_FOLD_SIGMA
+#define CKKS_FOLD_SIGMA 0
+#endif
+constexpr bool kFoldSigma = CKKS_FOLD_SIGMA != 0;
+
 // Hoisted hybrid rotations of n_ct ciphertexts by n_keys Galois keys (bounded
 // or RNS-block gadget), out [n_ct][n_keys][2][Lq][N]. Ciphertexts are
 // processed in groups of up to 4 sharing each streamed key slice.
@@ -1139,7 +1148,17 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
         hk[2 * n_keys + ctx->moduli.size() + g] = galois_inverse_host(keys[g]->exponent, n);
     }
     for (size_t i = 0; i < ctx->moduli.size(); ++i) hk[2 * n_keys + i] = ctx->psi[i];
-    CKKS_CUDA_TRY(cudaMemcpyAsync(karr.p, hk.data(), hk.size() * 8, cudaMemcpyHostToDevice, st));
+    // through a pinned buffer: a copy from pageable memory would first wait for
+    // the stream to drain (the previous call's inverse transforms and ModDown),
+    // leaving the device idle while this call is enqueued
+    StatusReadback up(ctx, hk.size() * 8);
+    if (up.ok()) {
+        std::memcpy(up.p, hk.data(), hk.size() * 8);
+        CKKS_CUDA_TRY(cudaMemcpyAsync(karr.p, up.p, hk.size() * 8, cudaMemcpyHostToDevice, st));
+        CKKS_CUDA_TRY(cudaEventRecord(up.ev, st));
+    } else {
+        CKKS_CUDA_TRY(cudaMemcpyAsync(karr.p, hk.data(), hk.size() * 8, cudaMemcpyHostToDevice, st));
+    }
     const u64* const* d_keys = (const u64* const*)karr.p;
     const u64* d_exps = karr.p + n_keys;
     const u64* d_psi = karr.p + 2 * n_keys;
@@ -1238,12 +1257,21 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
         ib.q_limbs = Lq;
         ib.pf = ctx->d_pmodq;
         ib.pf_q = ctx->d_pmodq + ctx->L;
-        if ((rc = ntt_inverse_base_launch(ctx, acc.p, Z.p, gn * n_keys * 2, lqp, LK, ib, st))) return rc;
+        // the tensor-core path folds sigma_g into the inverse transform (ModDown then
+        // streams without a gather); the CUDA-core path adds P b in the inverse
+        // transform and applies sigma_g in ModDown
+        GaloisOut go;
+        if (use_tc && kFoldSigma) {
+            go.exps = d_exps;
+            go.exps_inv = d_exps_inv;
+            go.n_keys = n_keys;
+        }
+        if ((rc = ntt_inverse_base_launch(ctx, acc.p, Z.p, gn * n_keys * 2, lqp, LK, ib, st, go))) return rc;
         pt.end();
         pt.begin(5);
-        // ModDown of every (ciphertext, key) pair, then sigma_g, straight into the output
+        // ModDown of every (ciphertext, key) pair (and sigma_g unless folded above), into the output
         if ((rc = mod_down_sigma_multi(ctx, Z.p, ct_out + (size_t)c0 * n_keys * ct_words, gn * n_keys * 2, Lq,
-                                       d_exps_inv, n_keys, st)))
+                                       go.exps ? nullptr : d_exps_inv, n_keys, st)))
             return rc;
         pt.end();
         // pairs whose correction lists overflowed are recomputed exactly

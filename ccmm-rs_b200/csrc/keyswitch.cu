@@ -58,9 +58,10 @@ __global__ void __launch_bounds__(kT) k_ks_mac(const u64* __restrict__ Y, const 
     ab.fold(q, mu_hi, mu_lo);
     aa.fold(q, mu_hi, mu_lo);
     u64 b = ab.lo;
-    if (base && l < Lq) {
+    if (base && l < Lq) {  // P b with auxiliary limbs, b without (ordinary RNS key switch)
         const u32 kb = perm_b ? galois_src(k, perm_b, log_n) : k;
-        b = add_mod(b, mul_shoup(base[((size_t)l << log_n) + kb], pf[l], pf_q[l], q), q);
+        const u64 bv = base[((size_t)l << log_n) + kb];
+        b = add_mod(b, pf ? mul_shoup(bv, pf[l], pf_q[l], q) : bv, q);
     }
     acc[((size_t)l << log_n) + k] = b;
     acc[(((size_t)LK + l) << log_n) + k] = aa.lo;
@@ -262,6 +263,19 @@ std::vector<u64> rnsblock_factors(ckks_ctx* ctx, const ckks_ksk* key) {
     return f;
 }
 
+// Block factors without P: E_i mod q_l = [l in block i] (rns_gadget.rs:77-135,
+// crt_idempotent_residue / crt_idempotent reduced per limb).
+std::vector<u64> rns_factors(ckks_ctx* ctx, const ckks_ksk* key) {
+    const u32 LK = ksk_limbs(key);
+    std::vector<u64> f((size_t)key->D * LK, 0);
+    u32 start = 0;
+    for (u32 i = 0; i < key->D; ++i) {
+        for (u32 l = start; l < start + key->blocks[i]; ++l) f[(size_t)i * LK + l] = 1;
+        start += key->blocks[i];
+    }
+    return f;
+}
+
 // Relinearization factors B^j mod q (bounded_key_switch.rs:63-79), target s^2.
 std::vector<u64> relin_factors(ckks_ctx* ctx, const ckks_ksk* key) {
     const u32 L = key->q_limbs;
@@ -293,8 +307,9 @@ int32_t relin_generate(ckks_ctx* ctx, ckks_ksk* key, const int8_t* secret, u64 s
     if ((rc = pointwise_launch(ctx, S2, S2, S2, 1, lm, L, 0, st))) return rc;
     if ((rc = ntt_inverse_launch_map(ctx, S2, S.p, 1, lm, L, st))) return rc;
     std::vector<int8_t> none;
-    return ksk_generate(ctx, key, secret, seed, sigma, relin_factors(ctx, key), none, true, TAG_RLK_A, TAG_RLK_E, st,
-                        S.p);
+    return ksk_generate(ctx, key, secret, seed, sigma,
+                        key->kind == CKKS_KSK_RELIN_RNS_BLOCK ? rns_factors(ctx, key) : relin_factors(ctx, key), none,
+                        true, TAG_RLK_A, TAG_RLK_E, st, S.p);
 }
 
 std::vector<int8_t> host_secret_automorphism(const int8_t* s, u32 n, u64 k) { return secret_automorphism(s, n, k); }
@@ -309,7 +324,8 @@ int32_t ks_mac_launch(ckks_ctx* ctx, const u64* Y, const u64* key, const u64* ba
         return CKKS_ERR_BAD_ARG;
     }
     dim3 g((ctx->n + kT - 1) / kT, LK, n_ct);
-    k_ks_mac<<<g, kT, 0, st>>>(Y, key, base, ctx->d_pmodq, ctx->d_pmodq + ctx->L, acc, ctx->d_tabs, lm, q_limbs, LK,
+    k_ks_mac<<<g, kT, 0, st>>>(Y, key, base, with_p ? ctx->d_pmodq : nullptr, with_p ? ctx->d_pmodq + ctx->L : nullptr,
+                               acc, ctx->d_tabs, lm, q_limbs, LK,
                                D, ctx->log_n, perm_y, perm_b, perm_key, ((size_t)D * LK) << ctx->log_n, b_stride,
                                ((size_t)2 * LK) << ctx->log_n);
     CKKS_CUDA_TRY(cudaGetLastError());
@@ -320,6 +336,8 @@ int32_t ks_mac_launch(ckks_ctx* ctx, const u64* Y, const u64* key, const u64* ba
 // decompose sigma(a), transform every digit): the exact fallback of the hoisted
 // path. The permuted key storage is read through the permutation.
 int32_t rotate_hybrid(ckks_ctx* ctx, const ckks_ksk* key, const u64* ct_in, u64* ct_out, u32 n_ct, cudaStream_t st) {
+    if (key->kind == CKKS_KSK_RNS_BLOCK)
+        return rotate_rns(ctx, key, ct_in, ct_out, n_ct, (size_t)2 * key->q_limbs * ctx->n, st);
     if (key->kind != CKKS_KSK_HYBRID_BOUNDED) {
         const ckks_ksk* keys[1] = {key};
         for (u32 i = 0; i < n_ct; ++i) {
@@ -367,7 +385,58 @@ int32_t rotate_hybrid(ckks_ctx* ctx, const ckks_ksk* key, const u64* ct_in, u64*
 
 int32_t rotate_hybrid_hoisted(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_keys, const u64* ct_in, u64* ct_out,
                               u32 n_ct, cudaStream_t st) {
+    if (keys[0]->kind == CKKS_KSK_RNS_BLOCK) {
+        // the reference decomposes sigma(a) for every Galois element
+        // (rns_galois_key.rs:439-469): one full key switch per key, outputs
+        // interleaved as [n_ct][n_keys][2][Lq][N]
+        const size_t ct_words = (size_t)2 * keys[0]->q_limbs * ctx->n;
+        for (u32 g = 0; g < n_keys; ++g)
+            if (int32_t rc = rotate_rns(ctx, keys[g], ct_in, ct_out + g * ct_words, n_ct, n_keys * ct_words, st))
+                return rc;
+        return CKKS_OK;
+    }
     return rotate_hoisted_ntt(ctx, keys, n_keys, ct_in, ct_out, n_ct, st);
+}
+
+int32_t rotate_rns(ckks_ctx* ctx, const ckks_ksk* key, const u64* ct_in, u64* ct_out, u32 n_ct, size_t out_stride,
+                   cudaStream_t st) {
+    const u32 Lq = key->q_limbs, D = key->D, n = ctx->n;
+    const size_t ct_words = (size_t)2 * Lq * n, y_words = (size_t)D * Lq * n;
+    const size_t per_ct = 3 * ct_words + y_words;  // sigma(ct), NTT(sigma(ct)), accumulators, digits
+    const u32 m_max = (u32)std::max<size_t>(1, std::min<size_t>({(size_t)n_ct, (size_t)(65535 / (D > 2 ? D : 2)),
+                                                                   ((size_t)4 << 30) / (per_ct * 8)}));
+    Workspace<u64> ws;
+    int32_t rc;
+    if ((rc = ws.alloc((size_t)m_max * per_ct, st))) return rc;
+    u64* sct = ws.p;                              // [m][2][Lq][N]
+    u64* s_hat = sct + (size_t)m_max * ct_words;  // [m][2][Lq][N]
+    u64* acc = s_hat + (size_t)m_max * ct_words;  // [m][2][Lq][N]
+    u64* Y = acc + (size_t)m_max * ct_words;      // [m][D][Lq][N]
+    const LimbMap lq = LimbMap::range(0, Lq);
+    for (u32 c0 = 0; c0 < n_ct; c0 += m_max) {
+        const u32 m = n_ct - c0 < m_max ? n_ct - c0 : m_max;
+        // sigma_k on (b, a) in the coefficient domain (apply_rns_automorphism)
+        if ((rc = automorphism_coef_launch(ctx, ct_in + (size_t)c0 * ct_words, sct, 2 * m, lq, Lq, key->exponent, st)))
+            return rc;
+        // block digits of sigma(a) (RnsGadgetLayout::decompose), lifted to every Q limb
+        for (u32 c = 0; c < m; ++c)
+            if ((rc = rnsblock_modup_launch(ctx, key, sct + c * ct_words + (size_t)Lq * n, Y + c * y_words, st)))
+                return rc;
+        if ((rc = ntt_forward_launch_map(ctx, Y, Y, D * m, lq, Lq, st))) return rc;
+        if ((rc = ntt_forward_launch_map(ctx, sct, s_hat, 2 * m, lq, Lq, st))) return rc;
+        // b' = NTT(sigma(b)) + sum_i NTT(d_i) k_b[i], a' = sum_i NTT(d_i) k_a[i]
+        if ((rc = ks_mac_launch(ctx, Y, key->d_entries, s_hat, acc, Lq, D, false, 0, 0, st, key->exponent, m, ct_words)))
+            return rc;
+        if (out_stride == ct_words) {
+            if ((rc = ntt_inverse_launch_map(ctx, acc, ct_out + (size_t)c0 * ct_words, 2 * m, lq, Lq, st))) return rc;
+        } else {
+            for (u32 c = 0; c < m; ++c)  // inverse transform into each (interleaved) output slot
+                if ((rc = ntt_inverse_launch_map(ctx, acc + c * ct_words, ct_out + (size_t)(c0 + c) * out_stride, 2, lq,
+                                                 Lq, st)))
+                    return rc;
+        }
+    }
+    return CKKS_OK;
 }
 
 // Galois key entries [polys][N] (each poly one (digit, limb, component)):

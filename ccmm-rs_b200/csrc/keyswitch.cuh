@@ -10,6 +10,11 @@
 //   HYBRID_RNS_BLOCK: entries [dnum][q_limbs+K][2][N], encrypting P * E_i * sigma(s)
 //   RELIN_BOUNDED  : entries [D][2][q_limbs][N], NTT domain, encrypting B^j * s^2
 //                    over Q (bounded_key_switch.rs:22-120)
+//   RNS_BLOCK      : entries [dnum][q_limbs][2][N], NTT domain, encrypting
+//                    E_i * sigma(s) over Q, no auxiliary limbs (the ordinary RNS
+//                    key switch, grafting/rns_key_switch.rs:1155-1258)
+//   RELIN_RNS_BLOCK: entries [dnum][2][q_limbs][N], NTT domain, encrypting
+//                    E_i * s^2 over Q (RnsMultiplicationKey)
 // Galois keys are stored permuted by their own automorphism: slot pi_g(k)
 // (ring/ntt_galois_permutation.rs:5-19 source index) holds the reference
 // entry of slot k, so the key-switch MAC runs contiguously in the permuted
@@ -33,6 +38,14 @@ int32_t ksk_generate(ckks_ctx* ctx, ckks_ksk* key, const int8_t* secret, u64 see
                      const std::vector<u64>& factors, const std::vector<int8_t>& s_target, bool comp_major, u64 tag_a,
                      u64 tag_e, cudaStream_t st, const u64* d_target_limbs = nullptr);
 int32_t relin_generate(ckks_ctx* ctx, ckks_ksk* key, const int8_t* secret, u64 seed, double sigma, cudaStream_t st);
+// Block factors E_i mod q_l = [l in block i] without the auxiliary P (RNS_BLOCK, RELIN_RNS_BLOCK).
+std::vector<u64> rns_factors(ckks_ctx* ctx, const ckks_ksk* key);
+// Ordinary RNS key-switched Galois automorphism with an RNS_BLOCK key in the
+// reference's order: sigma on (b, a), block digits of sigma(a) lifted to every
+// Q limb, NTT, MAC with the key plus NTT(sigma(b)), inverse NTT (no ModDown).
+// Output c goes to ct_out + c * out_stride words.
+int32_t rotate_rns(ckks_ctx* ctx, const ckks_ksk* key, const u64* ct_in, u64* ct_out, u32 n_ct, size_t out_stride,
+                   cudaStream_t st);
 std::vector<u64> hybrid_factors(ckks_ctx* ctx, const ckks_ksk* key);
 std::vector<u64> rnsblock_factors(ckks_ctx* ctx, const ckks_ksk* key);
 std::vector<u64> relin_factors(ckks_ctx* ctx, const ckks_ksk* key);
@@ -71,8 +84,9 @@ int32_t mul_plain_launch(ckks_ctx* ctx, const u64* ct_in, const u64* plain_ntt, 
                          bool plain_per_ct, cudaStream_t st);
 
 // One diagonal-rotation FFT stage (fft.cu): diag_ntt [n_rot + identity][L][N].
+// rescale false: the sum stays at level L (scale * plaintext scale).
 int32_t fft_stage_launch(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_rot, bool identity, const u64* diag_ntt,
-                         const u64* ct_in, u64* ct_out, u32 n_ct, u32 L, cudaStream_t st);
+                         const u64* ct_in, u64* ct_out, u32 n_ct, u32 L, cudaStream_t st, bool rescale = true);
 
 // Structured CCMM (ccmm.cu): A [k][m], B [n][k], C [n][m] column-major
 // ciphertexts [2][L][N] at the key's level L; C one level down.

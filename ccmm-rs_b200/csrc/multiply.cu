@@ -146,9 +146,18 @@ int32_t relin_core_launch(ckks_ctx* ctx, const ckks_ksk* key, const u64* c2, u64
     Workspace<i64> dg;
     Workspace<u64> Y;
     int32_t rc;
-    if ((rc = dg.alloc((size_t)n * D * N, st)) || (rc = Y.alloc((size_t)n * D * L * N, st))) return rc;
-    if ((rc = bounded_decompose_launch(ctx, c2, n, L, key->base_log, dg.p, nullptr, st))) return rc;
-    if ((rc = ntt_forward_digits_launch(ctx, dg.p, Y.p, n * D, LimbMap::range(0, L), L, st))) return rc;
+    if ((rc = Y.alloc((size_t)n * D * L * N, st))) return rc;
+    if (key->kind == CKKS_KSK_RELIN_RNS_BLOCK) {
+        // block digits of c2 (canonical mod Q_i, rns_key_switch.rs:1875) lifted to every Q limb
+        for (u32 c = 0; c < n; ++c)
+            if ((rc = rnsblock_modup_launch(ctx, key, c2 + (size_t)c * L * N, Y.p + (size_t)c * D * L * N, st)))
+                return rc;
+        if ((rc = ntt_forward_launch_map(ctx, Y.p, Y.p, n * D, LimbMap::range(0, L), L, st))) return rc;
+    } else {
+        if ((rc = dg.alloc((size_t)n * D * N, st))) return rc;
+        if ((rc = bounded_decompose_launch(ctx, c2, n, L, key->base_log, dg.p, nullptr, st))) return rc;
+        if ((rc = ntt_forward_digits_launch(ctx, dg.p, Y.p, n * D, LimbMap::range(0, L), L, st))) return rc;
+    }
     dim3 g((N + kT - 1) / kT, L, (n + kRelinGroup - 1) / kRelinGroup);
     k_relin_mac<kRelinGroup><<<g, kT, 0, st>>>(Y.p, key->d_entries, acc01, acc01, ctx->d_tabs, (int)n, (int)L, (int)D,
                                                (int)ctx->log_n);

@@ -265,12 +265,16 @@ k_fwd2(const u64* src, u64* dst, const NttTab* __restrict__ tabs,
 
 // Inverse pass 1 over units k_a: negacyclic B-point merged GS with psi_2B^-1
 // on the bit-reversed input {k_a + A brev(r)}, times the inverse twist
-// N^-1 psi^-((2k_a+1-A) j_lo), stored as row k_a (lazy, [0, 2q)). in != out.
+// N^-1 psi^-((2k_a+1-A) j_lo), stored as row k_a (lazy, [0, 2q); limbs on the
+// FP64 network: doubles below 1.5 q in magnitude). in != out.
+// With go.exps (sigma_k folded in), column j_lo of the row is stored at
+// position j_lo k mod B, so pass 2 reads the columns of each output column
+// together.
 template <int LOG_M>
 __global__ void __launch_bounds__(kMaxThreads, min_ctas<LOG_M>(3))
 k_inv1(const u64* __restrict__ in, u64* __restrict__ out,
        const NttTab* __restrict__ tabs, LimbMap lm, int limb_count,
-       int log_a, int log_c) {
+       int log_a, int log_c, GaloisOut go) {
     using S = Split<LOG_M>;
     extern __shared__ u64 sm[];
     const int C = 1 << log_c, tid = threadIdx.x;
@@ -279,14 +283,23 @@ k_inv1(const u64* __restrict__ in, u64* __restrict__ out,
     const u64 q = T.q;
     const size_t base = ((size_t)blockIdx.z * limb_count + limb) << (LOG_M + log_a);
     const int b0 = blockIdx.x << log_c;
-    if (LOG_M <= 8 && T.f64) {  // FP64 network: inputs below 2^52, inverse-twist output below 1.5 q
-        const double2* tab = stage_table_f64(sm + (S::M << log_c), T.fB_inv, S::M);
-        const double qd = T.qd, qinv = T.qinv;
-        double* smd = reinterpret_cast<double*>(sm);
-        auto twf = [&](int s, u32 blk) { return tab[(S::M >> (s + 1)) + blk]; };
-        __syncthreads();
-        if (tid < (C << S::LR1)) {
-            const int c = tid & (C - 1), g = tid >> log_c;
+    const bool f64 = LOG_M <= 8 && T.f64;
+    u64* st = sm + (S::M << log_c);
+    if (f64) stage_table_f64(st, T.fB_inv, S::M);
+    else stage_table(st, T.psiB_inv, T.psiB_inv_q, S::M);
+    const double2* tabf = reinterpret_cast<const double2*>(st);
+    const double qd = T.qd, qinv = T.qinv;
+    double* smd = reinterpret_cast<double*>(sm);
+    auto tw = [&](int s, u32 blk, u64& W, u64& Wq) {
+        u32 idx = (S::M >> (s + 1)) + blk;
+        W = st[idx];
+        Wq = st[S::M + idx];
+    };
+    auto twf = [&](int s, u32 blk) { return tabf[(S::M >> (s + 1)) + blk]; };
+    __syncthreads();
+    if (tid < (C << S::LR1)) {
+        const int c = tid & (C - 1), g = tid >> log_c;
+        if (f64) {  // centred inputs, four GS stages (below 8 q), centred at the exchange
             double x[S::R2];
 #pragma unroll
             for (int e = 0; e < S::R2; ++e)
@@ -298,10 +311,26 @@ k_inv1(const u64* __restrict__ in, u64* __restrict__ out,
                 const int r = S::R2 * g + e;
                 smd[(r << log_c) + (c ^ (r & (C - 1)))] = nttf::center(x[e], qd, qinv);
             }
+        } else {
+            u64 x[S::R2];
+#pragma unroll
+            for (int e = 0; e < S::R2; ++e) x[e] = in[base + ((size_t)brev(S::R2 * g + e, LOG_M) << log_a) + b0 + c];
+            if (q < nttc::kLazyGsBound) nttc::gs_stages<S::LR2, true>(x, 0, g, tw, q);
+            else nttc::gs_stages<S::LR2, false>(x, 0, g, tw, q);
+#pragma unroll
+            for (int e = 0; e < S::R2; ++e) {
+                const int r = S::R2 * g + e;
+                sm[(r << log_c) + (c ^ (r & (C - 1)))] = x[e];
+            }
         }
-        __syncthreads();
-        if (tid < (C << S::LR2)) {
-            const int i0 = tid & (S::R2 - 1), c = tid >> S::LR2;
+    }
+    __syncthreads();
+    const bool act = tid < (C << S::LR2);
+    const int i0 = tid & (S::R2 - 1), c = tid >> S::LR2;
+    const size_t row = (size_t)(b0 + c) << LOG_M;
+    u64 v[S::R1];
+    if (act) {
+        if (f64) {
             double y[S::R1];
 #pragma unroll
             for (int e = 0; e < S::R1; ++e) {
@@ -309,54 +338,43 @@ k_inv1(const u64* __restrict__ in, u64* __restrict__ out,
                 y[e] = smd[(r << log_c) + (c ^ (r & (C - 1)))];
             }
             nttf::gs_stages<S::LR1>(y, S::LR2, 0, twf, qd);
-            const size_t row = (size_t)(b0 + c) << LOG_M;
+#pragma unroll
+            for (int e = 0; e < S::R1; ++e) {
+                const double2 w = __ldg(T.fmidi + row + i0 + S::R2 * e);
+                v[e] = (u64)__double_as_longlong(nttf::mulmod(y[e], w.x, w.y, qd));
+            }
+        } else {
+            u64 y[S::R1];
+#pragma unroll
+            for (int e = 0; e < S::R1; ++e) {
+                const int r = i0 + S::R2 * e;
+                y[e] = sm[(r << log_c) + (c ^ (r & (C - 1)))];
+            }
+            if (q < nttc::kLazyGsBound) nttc::gs_stages<S::LR1, true>(y, S::LR2, 0, tw, q);
+            else nttc::gs_stages<S::LR1, false>(y, S::LR2, 0, tw, q);
 #pragma unroll
             for (int e = 0; e < S::R1; ++e) {
                 const size_t p = row + i0 + S::R2 * e;
-                const double2 w = __ldg(T.fmidi + p);
-                out[base + p] = (u64)__double_as_longlong(nttf::mulmod(y[e], w.x, w.y, qd));
+                v[e] = mul_shoup_lazy(y[e], __ldg(T.midi + p), __ldg(T.midi_q + p), q);
             }
         }
-        return;
     }
-    u64* st = sm + (S::M << log_c);
-    stage_table(st, T.psiB_inv, T.psiB_inv_q, S::M);
-    auto tw = [&](int s, u32 blk, u64& W, u64& Wq) {
-        u32 idx = (S::M >> (s + 1)) + blk;
-        W = st[idx];
-        Wq = st[S::M + idx];
-    };
-    __syncthreads();
-    if (tid < (C << S::LR1)) {
-        const int c = tid & (C - 1), g = tid >> log_c;
-        u64 x[S::R2];
+    if (go.exps) {  // columns of the row permuted: j_lo -> j_lo k mod B (B = M)
+        const u32 k = (u32)(go.exps[(blockIdx.z >> 1) % go.n_keys] & (S::M - 1));
+        __syncthreads();
+        if (act) {
 #pragma unroll
-        for (int e = 0; e < S::R2; ++e) x[e] = in[base + ((size_t)brev(S::R2 * g + e, LOG_M) << log_a) + b0 + c];
-        if (q < nttc::kLazyGsBound) nttc::gs_stages<S::LR2, true>(x, 0, g, tw, q);
-        else nttc::gs_stages<S::LR2, false>(x, 0, g, tw, q);
+            for (int e = 0; e < S::R1; ++e) sm[(c << LOG_M) + (((u32)(i0 + S::R2 * e) * k) & (S::M - 1))] = v[e];
+        }
+        __syncthreads();
+        if (act) {
 #pragma unroll
-        for (int e = 0; e < S::R2; ++e) {
-            const int r = S::R2 * g + e;
-            sm[(r << log_c) + (c ^ (r & (C - 1)))] = x[e];
+            for (int e = 0; e < S::R1; ++e) v[e] = sm[(c << LOG_M) + i0 + S::R2 * e];
         }
     }
-    __syncthreads();
-    if (tid < (C << S::LR2)) {
-        const int i0 = tid & (S::R2 - 1), c = tid >> S::LR2;
-        u64 y[S::R1];
+    if (act) {
 #pragma unroll
-        for (int e = 0; e < S::R1; ++e) {
-            const int r = i0 + S::R2 * e;
-            y[e] = sm[(r << log_c) + (c ^ (r & (C - 1)))];
-        }
-        if (q < nttc::kLazyGsBound) nttc::gs_stages<S::LR1, true>(y, S::LR2, 0, tw, q);
-        else nttc::gs_stages<S::LR1, false>(y, S::LR2, 0, tw, q);
-        const size_t row = (size_t)(b0 + c) << LOG_M;
-#pragma unroll
-        for (int e = 0; e < S::R1; ++e) {
-            const size_t p = row + i0 + S::R2 * e;
-            out[base + p] = mul_shoup_lazy(y[e], __ldg(T.midi + p), __ldg(T.midi_q + p), q);
-        }
+        for (int e = 0; e < S::R1; ++e) out[base + row + i0 + S::R2 * e] = v[e];
     }
 }
 
@@ -364,10 +382,14 @@ k_inv1(const u64* __restrict__ in, u64* __restrict__ out,
 // psi_A^-1 on {j_lo + B brev(r)}; natural output j_lo + B i, canonical.
 // src may equal dst.
 // With ib.b, the b components of key-switch accumulators get P b added (InvBase).
+// With go.exps (pass 1 stored permuted columns), position p holds column
+// j_lo = p k^-1 mod B, and element i of it goes to coefficient
+// sigma_k(j_lo + B i) = p + B ((m + i k) mod 2A), m = floor((j_lo k mod 2N) / B),
+// negated past A rows; ib.b must then be null.
 template <int LOG_M>
 __global__ void __launch_bounds__(kMaxThreads, min_ctas<LOG_M>(3))
 k_inv2(const u64* src, u64* dst, const NttTab* __restrict__ tabs,
-       LimbMap lm, int limb_count, int log_b, int log_c, InvBase ib) {
+       LimbMap lm, int limb_count, int log_b, int log_c, InvBase ib, GaloisOut go) {
     using S = Split<LOG_M>;
     extern __shared__ u64 sm[];
     const int C = 1 << log_c, tid = threadIdx.x;
@@ -377,14 +399,23 @@ k_inv2(const u64* src, u64* dst, const NttTab* __restrict__ tabs,
     const size_t base = ((size_t)blockIdx.z * limb_count + limb) << (LOG_M + log_b);
     const int c0 = blockIdx.x << log_c;
     const int c = tid & (C - 1);
-    if (LOG_M <= 8 && T.f64) {  // FP64 network: pass-1 doubles (below 1.5 q in magnitude) in, canonical out
-        const double2* tab = stage_table_f64(sm + (S::M << log_c), T.fA_inv, S::M);
-        const double qd = T.qd, qinv = T.qinv;
-        double* smd = reinterpret_cast<double*>(sm);
-        auto twf = [&](int s, u32 blk) { return tab[(S::M >> (s + 1)) + blk]; };
-        __syncthreads();
-        if (tid < (C << S::LR1)) {
-            const int g = tid >> log_c;
+    const bool f64 = LOG_M <= 8 && T.f64;
+    u64* st = sm + (S::M << log_c);
+    if (f64) stage_table_f64(st, T.fA_inv, S::M);
+    else stage_table(st, T.psiA_inv, T.psiA_inv_q, S::M);
+    const double2* tabf = reinterpret_cast<const double2*>(st);
+    const double qd = T.qd, qinv = T.qinv;
+    double* smd = reinterpret_cast<double*>(sm);
+    auto tw = [&](int s, u32 blk, u64& W, u64& Wq) {
+        u32 idx = (S::M >> (s + 1)) + blk;
+        W = st[idx];
+        Wq = st[S::M + idx];
+    };
+    auto twf = [&](int s, u32 blk) { return tabf[(S::M >> (s + 1)) + blk]; };
+    __syncthreads();
+    if (tid < (C << S::LR1)) {
+        const int g = tid >> log_c;
+        if (f64) {  // pass-1 doubles (below 1.5 q) centred, four GS stages, centred at the exchange
             double x[S::R2];
 #pragma unroll
             for (int e = 0; e < S::R2; ++e)
@@ -394,64 +425,41 @@ k_inv2(const u64* src, u64* dst, const NttTab* __restrict__ tabs,
             nttf::gs_stages<S::LR2>(x, 0, g, twf, qd);
 #pragma unroll
             for (int e = 0; e < S::R2; ++e) smd[((S::R2 * g + e) << log_c) + c] = nttf::center(x[e], qd, qinv);
+        } else {
+            u64 x[S::R2];
+#pragma unroll
+            for (int e = 0; e < S::R2; ++e) x[e] = src[base + c0 + c + ((size_t)brev(S::R2 * g + e, LOG_M) << log_b)];
+            if (q < nttc::kLazyGsBound) nttc::gs_stages<S::LR2, true>(x, 0, g, tw, q);
+            else nttc::gs_stages<S::LR2, false>(x, 0, g, tw, q);
+#pragma unroll
+            for (int e = 0; e < S::R2; ++e) sm[((S::R2 * g + e) << log_c) + c] = x[e];
         }
-        __syncthreads();
-        if (tid < (C << S::LR2)) {
-            const int i0 = tid >> log_c;
+    }
+    __syncthreads();
+    const bool act = tid < (C << S::LR2);
+    const int i0 = tid >> log_c;
+    u64 v[S::R1];
+    if (act) {
+        if (f64) {
             double y[S::R1];
 #pragma unroll
             for (int e = 0; e < S::R1; ++e) y[e] = smd[((i0 + S::R2 * e) << log_c) + c];
             nttf::gs_stages<S::LR1>(y, S::LR2, 0, twf, qd);
-            const u32 poly = blockIdx.z;
-            if (ib.b && !(poly & 1) && (u32)limb < ib.q_limbs) {
-                const u64* bb = ib.b + (size_t)(poly / (2 * ib.n_keys)) * ib.b_stride + ((size_t)limb << (LOG_M + log_b));
-                const u64 pf = ib.pf[limb], pfq = ib.pf_q[limb];
 #pragma unroll
-                for (int e = 0; e < S::R1; ++e) {
-                    const size_t o = c0 + c + ((size_t)(i0 + S::R2 * e) << log_b);
-                    dst[base + o] = add_mod(nttf::to_canonical(y[e], qd, qinv), mul_shoup(__ldg(bb + o), pf, pfq, q), q);
-                }
-            } else {
-#pragma unroll
-                for (int e = 0; e < S::R1; ++e)
-                    dst[base + c0 + c + ((size_t)(i0 + S::R2 * e) << log_b)] = nttf::to_canonical(y[e], qd, qinv);
-            }
-        }
-        return;
-    }
-    u64* st = sm + (S::M << log_c);
-    stage_table(st, T.psiA_inv, T.psiA_inv_q, S::M);
-    auto tw = [&](int s, u32 blk, u64& W, u64& Wq) {
-        u32 idx = (S::M >> (s + 1)) + blk;
-        W = st[idx];
-        Wq = st[S::M + idx];
-    };
-    __syncthreads();
-    if (tid < (C << S::LR1)) {
-        const int g = tid >> log_c;
-        u64 x[S::R2];
-#pragma unroll
-        for (int e = 0; e < S::R2; ++e) x[e] = src[base + c0 + c + ((size_t)brev(S::R2 * g + e, LOG_M) << log_b)];
-        if (q < nttc::kLazyGsBound) nttc::gs_stages<S::LR2, true>(x, 0, g, tw, q);
-        else nttc::gs_stages<S::LR2, false>(x, 0, g, tw, q);
-#pragma unroll
-        for (int e = 0; e < S::R2; ++e) sm[((S::R2 * g + e) << log_c) + c] = x[e];
-    }
-    __syncthreads();
-    if (tid < (C << S::LR2)) {
-        const int i0 = tid >> log_c;
-        u64 y[S::R1];
-#pragma unroll
-        for (int e = 0; e < S::R1; ++e) y[e] = sm[((i0 + S::R2 * e) << log_c) + c];
-        if (q < nttc::kLazyGsBound) {
-            nttc::gs_stages<S::LR1, true>(y, S::LR2, 0, tw, q);
-            const u64 one_q = (~0ull) / q;  // floor(2^64 / q) for odd q
-#pragma unroll
-            for (int e = 0; e < S::R1; ++e) y[e] = reduce_2q(mul_shoup_lazy(y[e], 1, one_q, q), q);
+            for (int e = 0; e < S::R1; ++e) v[e] = nttf::to_canonical(y[e], qd, qinv);
         } else {
-            nttc::gs_stages<S::LR1, false>(y, S::LR2, 0, tw, q);
 #pragma unroll
-            for (int e = 0; e < S::R1; ++e) y[e] = reduce_2q(y[e], q);
+            for (int e = 0; e < S::R1; ++e) v[e] = sm[((i0 + S::R2 * e) << log_c) + c];
+            if (q < nttc::kLazyGsBound) {
+                nttc::gs_stages<S::LR1, true>(v, S::LR2, 0, tw, q);
+                const u64 one_q = (~0ull) / q;  // floor(2^64 / q) for odd q
+#pragma unroll
+                for (int e = 0; e < S::R1; ++e) v[e] = reduce_2q(mul_shoup_lazy(v[e], 1, one_q, q), q);
+            } else {
+                nttc::gs_stages<S::LR1, false>(v, S::LR2, 0, tw, q);
+#pragma unroll
+                for (int e = 0; e < S::R1; ++e) v[e] = reduce_2q(v[e], q);
+            }
         }
         const u32 poly = blockIdx.z;
         if (ib.b && !(poly & 1) && (u32)limb < ib.q_limbs) {
@@ -459,10 +467,34 @@ k_inv2(const u64* src, u64* dst, const NttTab* __restrict__ tabs,
             const u64 pf = ib.pf[limb], pfq = ib.pf_q[limb];
 #pragma unroll
             for (int e = 0; e < S::R1; ++e)
-                y[e] = add_mod(y[e], mul_shoup(__ldg(bb + c0 + c + ((size_t)(i0 + S::R2 * e) << log_b)), pf, pfq, q), q);
+                v[e] = add_mod(v[e], mul_shoup(__ldg(bb + c0 + c + ((size_t)(i0 + S::R2 * e) << log_b)), pf, pfq, q), q);
         }
+    }
+    if (go.exps) {  // every element to its image row (through shared memory: stores stay row-coalesced)
+        const u32 gk = (blockIdx.z >> 1) % go.n_keys;
+        const u64 k = go.exps[gk], kinv = go.exps_inv[gk];
+        const u32 bmask = (1u << log_b) - 1, amask2 = (2u << LOG_M) - 1;
+        const u32 jl = (u32)(((u64)(c0 + c) * (kinv & bmask)) & bmask);
+        const u32 m = (u32)((((u64)jl * k) & ((2ull << (LOG_M + log_b)) - 1)) >> log_b);
+        const u32 k2a = (u32)(k & amask2);
+        __syncthreads();
+        if (act) {
 #pragma unroll
-        for (int e = 0; e < S::R1; ++e) dst[base + c0 + c + ((size_t)(i0 + S::R2 * e) << log_b)] = y[e];
+            for (int e = 0; e < S::R1; ++e) {
+                const u32 r = (m + (u32)(i0 + S::R2 * e) * k2a) & amask2;
+                const bool neg = r >= (u32)S::M;
+                sm[((r & (S::M - 1)) << log_c) + c] = neg ? neg_mod(v[e], q) : v[e];
+            }
+        }
+        __syncthreads();
+        if (act) {
+#pragma unroll
+            for (int e = 0; e < S::R1; ++e) v[e] = sm[((i0 + S::R2 * e) << log_c) + c];
+        }
+    }
+    if (act) {
+#pragma unroll
+        for (int e = 0; e < S::R1; ++e) dst[base + c0 + c + ((size_t)(i0 + S::R2 * e) << log_b)] = v[e];
     }
 }
 
@@ -482,7 +514,7 @@ int pick_log_c(int log_avail, int pref) {
 
 template <int LOG_M>
 int32_t launch_pass(int which, const void* in, u64* out, const NttTab* tabs, LimbMap lm, u32 limbs, u32 polys,
-                    int log_other, cudaStream_t st, const InvBase& ib, int lc_pref) {
+                    int log_other, cudaStream_t st, const InvBase& ib, int lc_pref, const GaloisOut& go) {
     const int lc = pick_log_c<LOG_M>(log_other, lc_pref);
     const int threads = Split<LOG_M>::RMAX << lc;
     const size_t smem = (sizeof(u64) << (LOG_M + lc)) + 2 * sizeof(u64) * (1u << LOG_M);
@@ -491,28 +523,29 @@ int32_t launch_pass(int which, const void* in, u64* out, const NttTab* tabs, Lim
         case 0: k_fwd1<LOG_M, false><<<grid, threads, smem, st>>>(in, out, tabs, lm, limbs, log_other, lc); break;
         case 1: k_fwd1<LOG_M, true><<<grid, threads, smem, st>>>(in, out, tabs, lm, limbs, log_other, lc); break;
         case 2: k_fwd2<LOG_M><<<grid, threads, smem, st>>>((const u64*)in, out, tabs, lm, limbs, log_other, lc); break;
-        case 3: k_inv1<LOG_M><<<grid, threads, smem, st>>>((const u64*)in, out, tabs, lm, limbs, log_other, lc); break;
-        default: k_inv2<LOG_M><<<grid, threads, smem, st>>>((const u64*)in, out, tabs, lm, limbs, log_other, lc, ib); break;
+        case 3: k_inv1<LOG_M><<<grid, threads, smem, st>>>((const u64*)in, out, tabs, lm, limbs, log_other, lc, go); break;
+        default: k_inv2<LOG_M><<<grid, threads, smem, st>>>((const u64*)in, out, tabs, lm, limbs, log_other, lc, ib, go); break;
     }
     return CKKS_OK;
 }
 
 int32_t pass(int which, int log_m, const void* in, u64* out, const NttTab* tabs, LimbMap lm, u32 limbs, u32 polys,
-             int log_other, cudaStream_t st, const InvBase& ib = InvBase{}, int lc_pref = -1) {
+             int log_other, cudaStream_t st, const InvBase& ib = InvBase{}, int lc_pref = -1,
+             const GaloisOut& go = GaloisOut{}) {
     if (polys > 65535 || limbs > 65535) {  // grid y / z limits
         ckks_set_error("NTT: more than 65535 polynomials or limbs in one launch");
         return CKKS_ERR_BAD_ARG;
     }
     switch (log_m) {
-        case 1: return launch_pass<1>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib, lc_pref);
-        case 2: return launch_pass<2>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib, lc_pref);
-        case 3: return launch_pass<3>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib, lc_pref);
-        case 4: return launch_pass<4>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib, lc_pref);
-        case 5: return launch_pass<5>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib, lc_pref);
-        case 6: return launch_pass<6>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib, lc_pref);
-        case 7: return launch_pass<7>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib, lc_pref);
-        case 8: return launch_pass<8>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib, lc_pref);
-        case 9: return launch_pass<9>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib, lc_pref);
+        case 1: return launch_pass<1>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib, lc_pref, go);
+        case 2: return launch_pass<2>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib, lc_pref, go);
+        case 3: return launch_pass<3>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib, lc_pref, go);
+        case 4: return launch_pass<4>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib, lc_pref, go);
+        case 5: return launch_pass<5>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib, lc_pref, go);
+        case 6: return launch_pass<6>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib, lc_pref, go);
+        case 7: return launch_pass<7>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib, lc_pref, go);
+        case 8: return launch_pass<8>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib, lc_pref, go);
+        case 9: return launch_pass<9>(which, in, out, tabs, lm, limbs, polys, log_other, st, ib, lc_pref, go);
         default: ckks_set_error("NTT: unsupported transform size"); return CKKS_ERR_BAD_ARG;
     }
 }
@@ -553,7 +586,11 @@ int32_t ntt_inverse_launch_map(ckks_ctx* ctx, const u64* in, u64* out, u32 n_pol
 }
 
 int32_t ntt_inverse_base_launch(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, LimbMap lm, u32 limb_count,
-                                const InvBase& ib, cudaStream_t st) {
+                                const InvBase& ib, cudaStream_t st, const GaloisOut& go) {
+    if (go.exps && ib.b) {
+        ckks_set_error("inverse NTT: a folded Galois automorphism cannot take a base term");
+        return CKKS_ERR_BAD_ARG;
+    }
     if (n_polys == 0 || limb_count == 0) return CKKS_OK;
     const int la = ctx->log_n1, lb = ctx->log_n2;
     u64* mid = out;
@@ -562,8 +599,8 @@ int32_t ntt_inverse_base_launch(ckks_ctx* ctx, const u64* in, u64* out, u32 n_po
         if (int32_t rc = tmp.alloc((size_t)n_polys * limb_count * ctx->n, st)) return rc;
         mid = tmp.p;
     }
-    if (int32_t rc = pass(3, lb, in, mid, ctx->d_tabs, lm, limb_count, n_polys, la, st, InvBase{}, ctx->ntt_log_c[3])) return rc;
-    if (int32_t rc = pass(4, la, mid, out, ctx->d_tabs, lm, limb_count, n_polys, lb, st, ib, ctx->ntt_log_c[4])) return rc;
+    if (int32_t rc = pass(3, lb, in, mid, ctx->d_tabs, lm, limb_count, n_polys, la, st, InvBase{}, ctx->ntt_log_c[3], go)) return rc;
+    if (int32_t rc = pass(4, la, mid, out, ctx->d_tabs, lm, limb_count, n_polys, lb, st, ib, ctx->ntt_log_c[4], go)) return rc;
     CKKS_CUDA_TRY(cudaGetLastError());
     return CKKS_OK;
 }

@@ -164,6 +164,14 @@ int32_t ckks_pointwise(ckks_ctx* ctx, const uint64_t* a, const uint64_t* b, uint
 int32_t ckks_rescale(ckks_ctx* ctx, const uint64_t* in, uint64_t* out, uint32_t n_polys, uint32_t limbs_in,
                      void* stream);
 
+/* Modulus switch without rescaling: ciphertexts [n_ct][2][limbs_in][N] ->
+ * [n_ct][2][limbs_out][N] keeping the leading limbs_out limbs (the lower
+ * chain level), scale unchanged. Replaces mod_switch_rns_ckks_to_next
+ * (ckks/rns_mod_switch.rs:14-58) for limbs_out = limbs_in - 1 and chains of
+ * such switches otherwise. out must not overlap in. */
+int32_t ckks_mod_switch(ckks_ctx* ctx, const uint64_t* in, uint64_t* out, uint32_t n_ct, uint32_t limbs_in,
+                        uint32_t limbs_out, void* stream);
+
 /* Exact ModDown by P: in [n][q_limbs + K][N] (Q prefix then all K auxiliary
  * limbs, coefficient domain) -> out [n][q_limbs][N]
  * (ring/auxiliary_modulus.rs:89-171 auxiliary_mod_down_rns_candidate). */
@@ -195,10 +203,24 @@ int32_t ckks_bounded_digits_automorphism(ckks_ctx* ctx, const int64_t* in, int64
  *     BoundedRnsMultiplicationKey (grafting/bounded_key_switch.rs:22-120);
  *     uploaded in the reference's coefficient-domain layout [D][2][q_limbs][N],
  *     stored NTT-domain.
+ *   CKKS_KSK_RNS_BLOCK : the ordinary RNS Galois key without auxiliary limbs,
+ *     PreparedRnsGaloisKey / PreparedRnsKeySwitchKey
+ *     (grafting/rns_key_switch.rs:1155-1258, ckks/rns_galois_key.rs): block i
+ *     of consecutive Q limbs, entries [dnum][q_limbs][2][N] (b_ntt, a_ntt)
+ *     encrypting E_i * sigma(s) over Q (E_i mod q_l = [l in block i]).
+ *   CKKS_KSK_RELIN_RNS_BLOCK : the RNS-block relinearization key without
+ *     auxiliary limbs, RnsMultiplicationKey (target s^2): uploaded
+ *     coefficient-domain [dnum][2][q_limbs][N], stored NTT-domain.
  * Generation samples a counter-based stream (seed) on the GPU: uniform a in
  * the NTT domain, discrete Gaussian e of width sigma shared across limbs;
  * secret_host is the ternary secret (int8 in {-1,0,1}, N entries). */
-enum { CKKS_KSK_HYBRID_BOUNDED = 0, CKKS_KSK_HYBRID_RNS_BLOCK = 1, CKKS_KSK_RELIN_BOUNDED = 2 };
+enum {
+    CKKS_KSK_HYBRID_BOUNDED = 0,
+    CKKS_KSK_HYBRID_RNS_BLOCK = 1,
+    CKKS_KSK_RELIN_BOUNDED = 2,
+    CKKS_KSK_RNS_BLOCK = 3,
+    CKKS_KSK_RELIN_RNS_BLOCK = 4
+};
 typedef struct ckks_ksk ckks_ksk;
 
 int32_t ckks_hybrid_key_generate(ckks_ctx* ctx, uint32_t q_limbs, uint32_t base_log, uint64_t exponent,
@@ -210,6 +232,22 @@ int32_t ckks_rnsblock_key_generate(ckks_ctx* ctx, uint32_t q_limbs, const uint32
                                    ckks_ksk** out);
 int32_t ckks_rnsblock_key_upload(ckks_ctx* ctx, uint32_t q_limbs, const uint32_t* block_sizes, uint32_t n_blocks,
                                  uint64_t exponent, const uint64_t* entries_host, ckks_ksk** out);
+/* Ordinary RNS Galois key (no auxiliary limbs) over the Q prefix of q_limbs
+ * limbs split into consecutive blocks of block_sizes (1..16 limbs each):
+ * replaces PreparedRnsGaloisKey generation (ckks/rns_galois_key.rs with
+ * grafting/rns_key_switch.rs:1155-1258); upload takes the reference's
+ * NTT-domain entries [dnum][q_limbs][2][N]. */
+int32_t ckks_rns_key_generate(ckks_ctx* ctx, uint32_t q_limbs, const uint32_t* block_sizes, uint32_t n_blocks,
+                              uint64_t exponent, const int8_t* secret_host, uint64_t seed, double sigma,
+                              ckks_ksk** out);
+int32_t ckks_rns_key_upload(ckks_ctx* ctx, uint32_t q_limbs, const uint32_t* block_sizes, uint32_t n_blocks,
+                            uint64_t exponent, const uint64_t* entries_host, ckks_ksk** out);
+/* RNS-block relinearization key without auxiliary limbs (RnsMultiplicationKey,
+ * target s^2); upload takes coefficient-domain entries [dnum][2][q_limbs][N]. */
+int32_t ckks_rns_relin_key_generate(ckks_ctx* ctx, uint32_t q_limbs, const uint32_t* block_sizes, uint32_t n_blocks,
+                                    const int8_t* secret_host, uint64_t seed, double sigma, ckks_ksk** out);
+int32_t ckks_rns_relin_key_upload(ckks_ctx* ctx, uint32_t q_limbs, const uint32_t* block_sizes, uint32_t n_blocks,
+                                  const uint64_t* entries_host, ckks_ksk** out);
 int32_t ckks_relin_key_generate(ckks_ctx* ctx, uint32_t q_limbs, uint32_t base_log, const int8_t* secret_host,
                                 uint64_t seed, double sigma, ckks_ksk** out);
 int32_t ckks_relin_key_upload(ckks_ctx* ctx, uint32_t q_limbs, uint32_t base_log, const uint64_t* entries_host,
@@ -224,7 +262,12 @@ int32_t ckks_ksk_destroy(ckks_ksk* key);
  * (coefficient domain) with one key; the output stays at the same level.
  * Replaces apply_hybrid_rns_galois_automorphism_{with_prepared_ntt,
  * prepared_qp} and rotate_{left,right}_hybrid_rns_ckks_with_prepared_ntt
- * (ckks/hybrid_rns_galois_key.rs:202-273, 293-521). in != out. */
+ * (ckks/hybrid_rns_galois_key.rs:202-273, 293-521). With a CKKS_KSK_RNS_BLOCK
+ * key it is the ordinary RNS key switch in the reference's order: sigma on
+ * (b, a), block digits of sigma(a), NTT-domain MAC plus NTT(sigma(b)), inverse
+ * NTT, no ModDown (apply_rns_galois_automorphism_with_prepared_ntt,
+ * ckks/rns_galois_key.rs:439-469, rns_key_switch_with_prepared_ntt,
+ * grafting/rns_key_switch.rs:2438-2524). in != out. */
 int32_t ckks_rotate(ckks_ctx* ctx, const ckks_ksk* key, const uint64_t* ct_in, uint64_t* ct_out, uint32_t n_ct,
                     void* stream);
 /* Hoisted rotations: one decomposition per ciphertext shared by n_keys Galois
@@ -266,6 +309,8 @@ int32_t ckks_tensor(ckks_ctx* ctx, const uint64_t* lhs, const uint64_t* rhs, uin
  * level: b = c0 + sum_j d_j k_b[j], a = c1 + sum_j d_j k_a[j] with d_j the
  * balanced base-2^base_log digits of c2. Replaces
  * bounded_rns_relinearize_with_ntt(_observed) (grafting/bounded_key_switch.rs:139-223).
+ * With a CKKS_KSK_RELIN_RNS_BLOCK key the digits are the block residues of c2
+ * (canonical mod Q_i): rns_relinearize_with_ntt (grafting/rns_key_switch.rs:1842-1905).
  * quad [n_ct][3][L][N] -> out [n_ct][2][L][N] (no overlap). */
 int32_t ckks_relinearize(ckks_ctx* ctx, const ckks_ksk* key, const uint64_t* quad, uint64_t* out, uint32_t n_ct,
                          void* stream);
@@ -301,6 +346,18 @@ int32_t ckks_mul_plain(ckks_ctx* ctx, const uint64_t* ct, const uint64_t* plain_
 int32_t ckks_fft_stage(ckks_ctx* ctx, const ckks_ksk* const* keys, uint32_t n_rot, int32_t identity,
                        const uint64_t* diag_ntt, const uint64_t* ct_in, uint64_t* ct_out, uint32_t n_ct,
                        uint32_t q_limbs, void* stream);
+
+
+/* ckks_fft_stage with the rescale optional: rescale == 0 leaves the sum at
+ * level q_limbs (ct_out [n_ct][2][q_limbs][N], scale * plaintext scale).
+ * With two keys rotating left and right by the same span and the identity
+ * term it is the packed radix-2 DIF FFT2 stage
+ * (execute_repeated_packed_fft2_dif_stage_cp_hybrid_prepared,
+ * eblas/fft.rs:3378-3470: direct, left and right complex-slot diagonals,
+ * summed) and, with rescale, its fused-rescale form (:3906-4000). */
+int32_t ckks_diag_stage(ckks_ctx* ctx, const ckks_ksk* const* keys, uint32_t n_rot, int32_t identity,
+                        const uint64_t* diag_ntt, const uint64_t* ct_in, uint64_t* ct_out, uint32_t n_ct,
+                        uint32_t q_limbs, int32_t rescale, void* stream);
 
 
 /* Structured encrypted matrix product (one ciphertext per entry):

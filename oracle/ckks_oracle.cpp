@@ -1133,6 +1133,105 @@ void oracle_rnsblock_rotate(const uint64_t* q, uint32_t L, const uint64_t* p, ui
     md.apply(acc_a.data(), ct_out + (size_t)L * n, n);
 }
 
+void oracle_rns_rotate(const uint64_t* q, uint32_t L, uint32_t n, const uint32_t* sizes, uint32_t nb,
+                       uint64_t exponent, const uint64_t* key, const uint64_t* ct_in, uint64_t* ct_out) {
+    // The ordinary RNS Galois path without auxiliary limbs, in the reference's
+    // order: apply_rns_automorphism on (b, a) (rns_galois_key.rs:439-469), then
+    // rns_key_switch_with_prepared_ntt (rns_key_switch.rs:2438-2524): block
+    // digits of sigma(a) (canonical mod Q_i, rns_gadget.rs:143-228) reduced
+    // into each limb, b' = NTT(sigma(b)) + sum_i NTT(d_i) k_b, a' = sum_i NTT(d_i) k_a,
+    // inverse NTT. key: [nb][L][2][N] NTT domain (reference layout).
+    exponent %= 2ull * n;
+    std::vector<u64> sct((size_t)2 * L * n);
+    oracle_automorphism_coef(q, L, n, exponent, ct_in, sct.data(), 2);
+    BlockLayout b = block_layout(q, sizes, nb);
+    std::vector<u64> words((size_t)nb * n * b.words);
+    oracle_rns_block_decompose(q, L, sizes, nb, n, sct.data() + (size_t)L * n, words.data());
+    std::vector<u64> dig(n);
+    for (uint32_t l = 0; l < L; ++l) {
+        const u64 mod = q[l];
+        u64* bb = ct_out + (size_t)l * n;
+        u64* aa = ct_out + (size_t)(L + l) * n;
+        std::copy(sct.begin() + (size_t)l * n, sct.begin() + (size_t)(l + 1) * n, bb);
+        ntt_forward_poly(mod, n, bb);
+        std::fill(aa, aa + n, 0);
+        for (uint32_t i = 0; i < nb; ++i) {
+            for (uint32_t c = 0; c < n; ++c) dig[c] = wide_mod_small(&words[((size_t)i * n + c) * b.words], b.words, mod);
+            ntt_forward_poly(mod, n, dig.data());
+            const u64* kb = key + (((size_t)i * L + l) * 2 + 0) * n;
+            const u64* ka = key + (((size_t)i * L + l) * 2 + 1) * n;
+            for (uint32_t c = 0; c < n; ++c) {
+                bb[c] = add_mod(bb[c], mul_mod(dig[c], kb[c], mod), mod);
+                aa[c] = add_mod(aa[c], mul_mod(dig[c], ka[c], mod), mod);
+            }
+        }
+        ntt_inverse_poly(mod, n, bb);
+        ntt_inverse_poly(mod, n, aa);
+    }
+}
+
+void oracle_rns_relin_key_generate(const uint64_t* q, uint32_t L, uint32_t n, const uint32_t* sizes, uint32_t nb,
+                                   const int8_t* secret, uint64_t seed, double sigma, uint64_t* key) {
+    // RnsMultiplicationKey (rns_key_switch.rs:1155-1258 with target s^2): block i
+    // encrypts E_i * s^2, E_i mod q_l = [l in block i]; coefficient domain [nb][2][L][N]
+    auto cdt = cdt_table(sigma);
+    auto s_ntt = secret_ntt(q, L, n, secret);
+    BlockLayout b = block_layout(q, sizes, nb);
+    std::vector<u64> s2((size_t)L * n), target((size_t)L * n);
+    for (uint32_t l = 0; l < L; ++l) {
+        for (uint32_t c = 0; c < n; ++c) s2[(size_t)l * n + c] = mul_mod(s_ntt[(size_t)l * n + c], s_ntt[(size_t)l * n + c], q[l]);
+        ntt_inverse_poly(q[l], n, &s2[(size_t)l * n]);
+    }
+    for (uint32_t i = 0; i < nb; ++i) {
+        for (uint32_t l = 0; l < L; ++l) {
+            const bool in_block = l >= b.start[i] && l < b.start[i] + b.size[i];
+            for (uint32_t c = 0; c < n; ++c) target[(size_t)l * n + c] = in_block ? s2[(size_t)l * n + c] : 0;
+        }
+        u64* e0 = key + (size_t)i * 2 * L * n;
+        rlwe_encrypt_ntt(q, L, n, s_ntt, target.data(), seed, TAG_RLK_A, TAG_RLK_E, i, cdt, e0, n, e0 + (size_t)L * n, n);
+        for (uint32_t l = 0; l < L; ++l) {
+            ntt_inverse_poly(q[l], n, e0 + (size_t)l * n);
+            ntt_inverse_poly(q[l], n, e0 + (size_t)(L + l) * n);
+        }
+    }
+}
+
+void oracle_rns_relinearize(const uint64_t* q, uint32_t L, uint32_t n, const uint32_t* sizes, uint32_t nb,
+                            const uint64_t* quad, const uint64_t* key, uint64_t* out) {
+    // rns_relinearize_with_ntt (rns_key_switch.rs:1842-1905): block digits of c2;
+    // per limb b = c0 + sum_i negacyclic_mul(d_i, k_b[i]), a = c1 + sum_i negacyclic_mul(d_i, k_a[i])
+    BlockLayout b = block_layout(q, sizes, nb);
+    std::vector<u64> words((size_t)nb * n * b.words);
+    oracle_rns_block_decompose(q, L, sizes, nb, n, quad + (size_t)2 * L * n, words.data());
+    std::vector<u64> d(n), kb(n), ka(n);
+    for (uint32_t l = 0; l < L; ++l) {
+        const u64 mod = q[l];
+        u64* ob = out + (size_t)l * n;
+        u64* oa = out + (size_t)(L + l) * n;
+        std::copy(quad + (size_t)l * n, quad + (size_t)(l + 1) * n, ob);
+        std::copy(quad + (size_t)(L + l) * n, quad + (size_t)(L + l + 1) * n, oa);
+        for (uint32_t i = 0; i < nb; ++i) {
+            for (uint32_t c = 0; c < n; ++c) d[c] = wide_mod_small(&words[((size_t)i * n + c) * b.words], b.words, mod);
+            ntt_forward_poly(mod, n, d.data());
+            const u64* e0 = key + (size_t)i * 2 * L * n;
+            std::copy(e0 + (size_t)l * n, e0 + (size_t)(l + 1) * n, kb.begin());
+            std::copy(e0 + (size_t)(L + l) * n, e0 + (size_t)(L + l + 1) * n, ka.begin());
+            ntt_forward_poly(mod, n, kb.data());
+            ntt_forward_poly(mod, n, ka.data());
+            for (uint32_t c = 0; c < n; ++c) {
+                kb[c] = mul_mod(d[c], kb[c], mod);
+                ka[c] = mul_mod(d[c], ka[c], mod);
+            }
+            ntt_inverse_poly(mod, n, kb.data());
+            ntt_inverse_poly(mod, n, ka.data());
+            for (uint32_t c = 0; c < n; ++c) {
+                ob[c] = add_mod(ob[c], kb[c], mod);
+                oa[c] = add_mod(oa[c], ka[c], mod);
+            }
+        }
+    }
+}
+
 void oracle_tensor(const uint64_t* q, uint32_t L, uint32_t n, const uint64_t* lhs, const uint64_t* rhs,
                    uint64_t* out) {  // quadratic.rs:99-140
     const u64 *b0 = lhs, *a0 = lhs + (size_t)L * n, *b1 = rhs, *a1 = rhs + (size_t)L * n;

@@ -119,6 +119,17 @@ void oracle_rnsblock_key_generate(const uint64_t* q, uint32_t L, const uint64_t*
 void oracle_rnsblock_rotate(const uint64_t* q, uint32_t L, const uint64_t* p, uint32_t K, uint32_t degree,
                             const uint32_t* block_sizes, uint32_t n_blocks, uint64_t exponent,
                             const uint64_t* key, const uint64_t* ct_in, uint64_t* ct_out);
+// Ordinary RNS key switch without auxiliary limbs (rns_galois_key.rs:439-469,
+// rns_key_switch.rs:2438-2524, 1842-1905); the Galois key is
+// oracle_rnsblock_key_generate with K = 0.
+void oracle_rns_rotate(const uint64_t* q, uint32_t L, uint32_t degree, const uint32_t* block_sizes,
+                       uint32_t n_blocks, uint64_t exponent, const uint64_t* key, const uint64_t* ct_in,
+                       uint64_t* ct_out);
+void oracle_rns_relin_key_generate(const uint64_t* q, uint32_t L, uint32_t degree, const uint32_t* block_sizes,
+                                   uint32_t n_blocks, const int8_t* secret, uint64_t seed, double sigma,
+                                   uint64_t* key);
+void oracle_rns_relinearize(const uint64_t* q, uint32_t L, uint32_t degree, const uint32_t* block_sizes,
+                            uint32_t n_blocks, const uint64_t* quad, const uint64_t* key, uint64_t* out);
 
 /* rlwe/quadratic.rs:99-140 -- out [3][L][N] */
 void oracle_tensor(const uint64_t* moduli, uint32_t limbs, uint32_t degree,

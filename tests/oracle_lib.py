@@ -60,6 +60,9 @@ _SIGS = {
                                                   ctypes.POINTER(u64p), U32, u64p, u64p, U32]),
     "oracle_rnsblock_key_generate": (None, [u64p, U32, u64p, U32, U32, u32p, U32, i8p, U64, U64, F64, u64p]),
     "oracle_rnsblock_rotate": (None, [u64p, U32, u64p, U32, U32, u32p, U32, U64, u64p, u64p, u64p]),
+    "oracle_rns_rotate": (None, [u64p, U32, U32, u32p, U32, U64, u64p, u64p, u64p]),
+    "oracle_rns_relin_key_generate": (None, [u64p, U32, U32, u32p, U32, i8p, U64, F64, u64p]),
+    "oracle_rns_relinearize": (None, [u64p, U32, U32, u32p, U32, u64p, u64p, u64p]),
     "oracle_tensor": (None, [u64p, U32, U32, u64p, u64p, u64p]),
     "oracle_bounded_relin_key_generate": (None, [u64p, U32, U32, U32, i8p, U64, F64, u64p]),
     "oracle_bounded_relinearize": (None, [u64p, U32, U32, U32, u64p, u64p, u64p]),
@@ -239,6 +242,33 @@ class Oracle:
         out = np.zeros((2, len(q), n), np.uint64)
         self.L.oracle_rnsblock_rotate(P(q), len(q), P(p), len(p), n, P(bs, u32p), len(bs), int(exponent),
                                       P(key), P(ct), P(out))
+        return out
+
+    def rns_key(self, q, block_sizes, secret, exponent, seed, sigma=3.2):
+        """Ordinary RNS Galois key (no P): the block key with K = 0, NTT domain [nb][L][2][N]."""
+        q = arr(q); s = arr(secret, np.int8); bs = arr(block_sizes, np.uint32); n = len(s)
+        key = np.zeros((len(bs), len(q), 2, n), np.uint64)
+        empty = np.zeros(1, np.uint64)
+        self.L.oracle_rnsblock_key_generate(P(q), len(q), P(empty), 0, n, P(bs, u32p), len(bs), P(s, i8p),
+                                            int(exponent), seed, sigma, P(key))
+        return key
+
+    def rns_rotate(self, q, block_sizes, key, exponent, ct):
+        q = arr(q); bs = arr(block_sizes, np.uint32); key = arr(key); ct = arr(ct); n = ct.shape[-1]
+        out = np.zeros((2, len(q), n), np.uint64)
+        self.L.oracle_rns_rotate(P(q), len(q), n, P(bs, u32p), len(bs), int(exponent), P(key), P(ct), P(out))
+        return out
+
+    def rns_relin_key(self, q, block_sizes, secret, seed, sigma=3.2):
+        q = arr(q); s = arr(secret, np.int8); bs = arr(block_sizes, np.uint32); n = len(s)
+        key = np.zeros((len(bs), 2, len(q), n), np.uint64)
+        self.L.oracle_rns_relin_key_generate(P(q), len(q), n, P(bs, u32p), len(bs), P(s, i8p), seed, sigma, P(key))
+        return key
+
+    def rns_relinearize(self, q, block_sizes, quad, key):
+        q = arr(q); bs = arr(block_sizes, np.uint32); quad = arr(quad); key = arr(key); n = quad.shape[-1]
+        out = np.zeros((2, len(q), n), np.uint64)
+        self.L.oracle_rns_relinearize(P(q), len(q), n, P(bs, u32p), len(bs), P(quad), P(key), P(out))
         return out
 
     def tensor(self, moduli, lhs, rhs):
