@@ -9,7 +9,16 @@ reference's prime search), the reference's bounded hybrid-QP gadget with base
 rotated by the same 32 Galois steps (powers of two 1..2^14 and odd steps
 3..35) sharing one decomposition per ciphertext. One step = all 512
 rotations; outputs are word-for-word the reference algorithm's. Metric:
-rotations per second.
+rotations per second. The line also carries, measured in the same run:
+  parity      the CPU baseline runs the oracle on the timed batch's own
+              ciphertexts and (downloaded) keys and its outputs are compared
+              word for word with the GPU's, plus one fresh encryption decoded
+              on both sides (decoded_error);
+  ccmm        the metric's second half: one 64 x 64 structured CCMM at N=2^15
+              (the "ccmm" workload below; 3 timed after 3 warm-up products)
+              with its own roofline, e2e, parity and CPU baseline
+              (--no-ccmm leaves it out);
+  plain_gpu   the plain GPU forms of the same rotations.
 
 Workload "ntt": batched forward + inverse negacyclic NTT at N=2^16 over 32
 limbs of 50-bit primes q = 1 mod 2N (the reference's prime search), 64
@@ -32,9 +41,11 @@ P = 60 bits, the reference's prime search): HMult -> bounded relinearization
 (base 2^20) -> rescale -> key-switched rotation by one slot, for 64
 ciphertext pairs. One step = 64 chains. Metric: chains per second.
 
-One JSON line on rank 0. Under torchrun each rank runs an independent replica
-(the path shards into independent polynomials/ciphertexts; no collective on
-the data path): value = units of all ranks / max-over-ranks time.
+One JSON line on rank 0. `--gpus N` runs N independent replicas, one process
+per GPU (launched through torch.distributed.run when no torchrun environment is
+set; the path shards into independent polynomials/ciphertexts, with no
+collective on the data path): value = units of all ranks / max-over-ranks
+time. CPU baselines and parity checks run at N=1.
 `--impl reference` times the CPU restatement of the reference algorithm
 (oracle/, the reference itself is Rust and cannot be built here) on the host
 cores with every thread, on the same workload and metric.

@@ -118,8 +118,8 @@ int32_t build_constants(ckks_ctx* ctx) {
     // layout: rescale [L][2][L] | pmodq [2][L] | md.q [L] | pre, pre_q [L][kMaxAux] x2 | p_mod_q [L] |
     //         pinv_mod_q [L] | pinv_mod_q_q [L] | gq, gq_q [L][L] x2 | ginv, ginv_q [L] x2
     const size_t n_res = (size_t)L * 2 * L, n_pm = 2 * (size_t)L, n_md = (size_t)L * (4 + 2 * kMaxAux),
-                 n_g = 2 * (size_t)L * L + 2 * (size_t)L;
-    std::vector<u64> h(n_res + n_pm + n_md + n_g, 0);
+                 n_g = 2 * (size_t)L * L + 2 * (size_t)L, n_f = (size_t)L * 12;
+    std::vector<u64> h(n_res + n_pm + n_md + n_g + n_f, 0);
     u64* res = h.data();
     for (u32 d = 1; d < L; ++d)
         for (u32 i = 0; i < d; ++i) {
@@ -204,6 +204,36 @@ int32_t build_constants(ckks_ctx* ctx) {
         ginv[i] = invmod(gq[(size_t)i * L + i], m[i]);
         ginv_q[i] = shoup_quotient_host(ginv[i], m[i]);
     }
+    {  // FP64 ModDown constants: P in three words and, per Q limb, (value, value / q) pairs
+        std::vector<u64> Pw(4, 0);
+        Pw[0] = 1;
+        for (u32 k = 0; k < K && K <= 3; ++k) {
+            unsigned __int128 c = 0;
+            for (auto& w : Pw) {
+                unsigned __int128 t = (unsigned __int128)w * m[L + k] + c;
+                w = (u64)t;
+                c = t >> 64;
+            }
+        }
+        for (int w = 0; w < 3; ++w) md.P3[w] = Pw[w];
+        double* fc = (double*)(h.data() + n_res + n_pm + n_md + n_g);
+        for (u32 i = 0; i < L; ++i) {
+            const u64 qi = m[i];
+            double* c = fc + (size_t)i * 12;
+            c[0] = (double)qi;
+            c[1] = 1.0 / (double)qi;
+            const u64 pinv = pinvq[i] % qi;
+            c[2] = (double)pinv;
+            c[3] = (double)pinv / (double)qi;
+            u64 r = 1 % qi;  // 2^(47 k) mod q
+            for (int k = 0; k < 4; ++k) {
+                const u64 v = mulmod(r, pinv, qi);
+                c[4 + 2 * k] = (double)v;
+                c[5 + 2 * k] = (double)v / (double)qi;
+                r = mulmod(r, (1ull << 47) % qi, qi);
+            }
+        }
+    }
     if (cudaMalloc(&ctx->d_const_mem, h.size() * sizeof(u64)) != cudaSuccess) {
         cudaGetLastError();
         return CKKS_ERR_OOM;
@@ -225,6 +255,7 @@ int32_t build_constants(ckks_ctx* ctx) {
     ctx->garner.gq_q = dg + (size_t)L * L;
     ctx->garner.ginv = dg + 2 * (size_t)L * L;
     ctx->garner.ginv_q = ctx->garner.ginv + L;
+    md.f64c = (const double*)(d + n_res + n_pm + n_md + n_g);
     return CKKS_OK;
 }
 

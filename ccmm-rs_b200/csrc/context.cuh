@@ -44,6 +44,11 @@ struct ModDownConst {
     const u64 *pre, *pre_q;                            // [L][kMaxAux]: (p_0..p_{j-1}) mod q_i
     const u64* p_mod_q;                                // [L]
     const u64 *pinv_mod_q, *pinv_mod_q_q;              // [L]: (P mod q_i)^-1
+    // FP64 ModDown (K <= 3, Q primes below 2^50): P as three words, and per Q
+    // limb [L][12] doubles: q, 1/q, then (c, c/q) for c = P^-1 and
+    // c = 2^(47 k) P^-1 mod q (k = 0..3)
+    u64 P3[3];
+    const double* f64c;
 };
 
 // Garner constants of the Q basis prefix (shared by every prefix length).
@@ -188,7 +193,9 @@ struct Workspace {
         }
         return CKKS_OK;
     }
-    ~Workspace() {
+    void release() {
         if (p) cudaFreeAsync(p, st);
+        p = nullptr;
     }
+    ~Workspace() { release(); }
 };

@@ -4,6 +4,7 @@
 // (N / 256, limbs, polys), coalesced on the contiguous coefficient axis.
 #include "context.cuh"
 #include "kernels.cuh"
+#include "ntt_core.cuh"
 
 namespace {
 
@@ -174,6 +175,99 @@ __global__ void __launch_bounds__(kT) k_mod_down(const u64* __restrict__ in, u64
     }
 }
 
+// ModDown on the FP64 pipe, for Q primes below 2^50 and K <= 3 auxiliary limbs
+// (the integer form above is instruction-bound on the ALU and FMA pipes while
+// the FP64 pipe idles). The centred CRT value y_c of the auxiliary residues is
+// rebuilt exactly from its mixed-radix digits as three 64-bit words
+// (|y_c| < P/2 < 2^187) and its magnitude split into four 47-bit words w_k;
+// then per Q limb, with s the sign of y_c,
+//   out = x P^-1 - s sum_k w_k (2^(47 k) P^-1 mod q)   (mod q):
+// five exact FP64 modular products (nttf::mulmod, multiplicands below 2^51, so
+// each result is below 0.75 q in magnitude and the sum below 3.75 q) and one
+// exact reduction. The words equal k_mod_down's. sigma as there.
+template <int KT>
+__global__ void __launch_bounds__(kT) k_mod_down_f64(const u64* __restrict__ in, u64* __restrict__ out,
+                                                     ModDownConst md, int q_limbs, int log_n,
+                                                     const u64* __restrict__ exps_inv, int n_keys) {
+    extern __shared__ double fcs[];  // [q_limbs][12]: q, 1/q, (P^-1, /q), (2^(47k) P^-1, /q) k = 0..3
+    for (int idx = threadIdx.x; idx < q_limbs * 12; idx += blockDim.x) fcs[idx] = md.f64c[idx];
+    __syncthreads();
+    const u32 n = 1u << log_n;
+    const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const size_t src = (size_t)blockIdx.y * (q_limbs + KT) << log_n;
+    const size_t dst = (size_t)blockIdx.y * q_limbs << log_n;
+    u32 c = t;
+    bool flip = false;
+    if (exps_inv) {
+        const u64 sg = ((u64)t * exps_inv[(blockIdx.y >> 1) % n_keys]) & (2ull * n - 1);
+        flip = sg >= n;
+        c = (u32)(sg & (n - 1));
+    }
+    const u64* x = in + src + c;
+    u64 v[KT];
+#pragma unroll
+    for (int i = 0; i < KT; ++i) v[i] = __ldg(x + ((size_t)(q_limbs + i) << log_n));
+#pragma unroll
+    for (int i = 0; i < KT; ++i) {  // mixed-radix digits (Garner), as k_mod_down
+        const u64 p = md.p[i];
+        u64 acc = 0;
+#pragma unroll
+        for (int j = 0; j < i; ++j) acc = add_mod(acc, mul_shoup(v[j], md.pp[i][j], md.pp_q[i][j], p), p);
+        v[i] = mul_shoup(sub_mod(v[i], acc, p), md.pinv[i], md.pinv_q[i], p);
+    }
+    bool neg = false, decided = false;  // value > floor(P/2) -> negative
+#pragma unroll
+    for (int i = KT - 1; i >= 0; --i) {
+        if (!decided && v[i] != md.half[i]) {
+            neg = v[i] > md.half[i];
+            decided = true;
+        }
+    }
+    // y = v0 + p0 (v1 + p1 v2) in three words
+    typedef unsigned __int128 u128;
+    u64 y0, y1 = 0, y2 = 0;
+    if (KT == 1) {
+        y0 = v[0];
+    } else if (KT == 2) {
+        const u128 a = (u128)v[1] * md.p[0] + v[0];
+        y0 = (u64)a;
+        y1 = (u64)(a >> 64);
+    } else {
+        const u128 tt = (u128)v[KT - 1] * md.p[1] + v[1];
+        const u128 a = (u128)(u64)tt * md.p[0] + v[0];
+        const u128 b = (u128)(u64)(tt >> 64) * md.p[0] + (u64)(a >> 64);
+        y0 = (u64)a;
+        y1 = (u64)b;
+        y2 = (u64)(b >> 64);
+    }
+    if (neg) {  // |y - P| = P - y
+        const u64 d0 = md.P3[0] - y0, b0 = md.P3[0] < y0;
+        const u64 t1 = md.P3[1] - y1, b1 = md.P3[1] < y1;
+        const u64 d1 = t1 - b0, b1b = t1 < b0;
+        const u64 d2 = md.P3[2] - y2 - (b1 | b1b);
+        y0 = d0;
+        y1 = d1;
+        y2 = d2;
+    }
+    const u64 m47 = (1ull << 47) - 1;
+    const double w0 = nttf::from_u52(y0 & m47), w1 = nttf::from_u52(((y0 >> 47) | (y1 << 17)) & m47),
+                 w2 = nttf::from_u52(((y1 >> 30) | (y2 << 34)) & m47), w3 = nttf::from_u52((y2 >> 13) & m47);
+    u64* o = out + dst + t;
+    for (int i = 0; i < q_limbs; ++i) {
+        const double* ci = fcs + i * 12;
+        const double q = ci[0], qinv = ci[1];
+        const double xd = nttf::from_u52(__ldg(x + ((size_t)i << log_n)));
+        const double r = nttf::mulmod(xd, ci[2], ci[3], q);
+        const double sm = __dadd_rn(__dadd_rn(nttf::mulmod(w0, ci[4], ci[5], q), nttf::mulmod(w1, ci[6], ci[7], q)),
+                                    __dadd_rn(nttf::mulmod(w2, ci[8], ci[9], q), nttf::mulmod(w3, ci[10], ci[11], q)));
+        double rr = nttf::center(neg ? __dadd_rn(r, sm) : __dsub_rn(r, sm), q, qinv);
+        if (flip) rr = -rr;
+        rr = rr < 0.0 ? __dadd_rn(rr, q) : rr;
+        o[(size_t)i << log_n] = (u64)__double_as_longlong(__dadd_rn(rr, nttf::kTwo52)) & 0xFFFFFFFFFFFFFull;
+    }
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ launchers
@@ -232,8 +326,12 @@ int32_t mod_down_sigma_multi(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys
                              const u64* d_exps_inv, u32 n_keys, cudaStream_t st) {
     if (!n_polys) return CKKS_OK;
     // lazy differences need (2K + 2) q < 2^64: every Q prime below 2^59 (K <= 8)
-    bool lazy = true;
-    for (u32 i = 0; i < q_limbs; ++i) lazy = lazy && ctx->moduli[i] < (1ull << 59);
+    bool lazy = true, f64 = ctx->K >= 1 && ctx->K <= 3;
+    for (u32 i = 0; i < q_limbs; ++i) {
+        lazy = lazy && ctx->moduli[i] < (1ull << 59);
+        f64 = f64 && ctx->moduli[i] < (1ull << 50);
+    }
+    for (u32 k = 0; k < ctx->K; ++k) f64 = f64 && ctx->moduli[ctx->L + k] < (1ull << 62);
     // grid.y limit: chunks are multiples of 2 * n_keys so (poly / 2) % n_keys pairs stay aligned
     const u32 unit = 2 * (n_keys ? n_keys : 1);
     const u32 chunk = (65535 / unit) * unit;
@@ -245,7 +343,15 @@ int32_t mod_down_sigma_multi(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys
         const int nk = n_keys ? (int)n_keys : 1;
         const size_t smem = (size_t)q_limbs * (5 + 2 * ctx->K) * sizeof(u64);
 #define CKKS_MD(KK, LZ) k_mod_down<KK, LZ><<<g, kT, smem, st>>>(pin, pout, ctx->mod_down, q_limbs, ctx->log_n, d_exps_inv, nk)
-        if (lazy) {
+#define CKKS_MDF(KK) k_mod_down_f64<KK><<<g, kT, (size_t)q_limbs * 12 * sizeof(double), st>>>(pin, pout, ctx->mod_down, \
+                                                                                          q_limbs, ctx->log_n, d_exps_inv, nk)
+        if (f64) {
+            switch (ctx->K) {
+                case 1: CKKS_MDF(1); break;
+                case 2: CKKS_MDF(2); break;
+                default: CKKS_MDF(3);
+            }
+        } else if (lazy) {
             switch (ctx->K) {
                 case 1: CKKS_MD(1, true); break;
                 case 2: CKKS_MD(2, true); break;
@@ -261,6 +367,7 @@ int32_t mod_down_sigma_multi(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys
             }
         }
 #undef CKKS_MD
+#undef CKKS_MDF
     }
     CKKS_CUDA_TRY(cudaGetLastError());
     return CKKS_OK;

@@ -343,7 +343,9 @@ struct PackedSet {
     std::vector<const ckks_ksk*> keys;
     u64* d = nullptr;
     u32 rg = 0, n_kc = 0, n_chunks = 0;
+    u32 g_max = 4;  // ciphertexts per group that fit the device next to the set (sized once, at packing)
 };
+constexpr u32 kGroupMax = 16;  // ciphertexts per tensor-core MAC group (tc::kCt)
 std::mutex g_sets_mu;
 std::map<const ckks_ctx*, std::vector<std::unique_ptr<PackedSet>>> g_sets;
 
@@ -409,6 +411,13 @@ const PackedSet* packed_set_get(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 
         if (p.d) cudaFree(p.d);
         if (d_ptr) cudaFree(d_ptr);
         return nullptr;
+    }
+    {  // group size: workspace per ciphertext (digit transforms, accumulators) within half the free memory
+        const size_t per_ct = ((size_t)k0->D * LK * n + 4 * (size_t)n_keys * LK * n) * sizeof(u64);
+        const size_t left = free_b - bytes;
+        u32 g = kGroupMax;
+        while (g > 4 && (size_t)g * per_ct > left / 2) g -= 4;
+        p.g_max = g;
     }
     k_pack_keys<<<148 * 16, 256, 0, st>>>(d_ptr, (int)n_keys, (int)LK, (int)k0->D, (int)ctx->log_n, p.rg, p.n_kc,
                                           p.n_chunks, ctx->d_pmodq, (int)k0->q_limbs, p.d, total);
@@ -683,6 +692,7 @@ struct Item {
     }
 };
 
+static_assert(kCt == (int)kGroupMax, "group size of the packed sets");
 }  // namespace tc
 
 // Same arguments and results as k_mac_tiled for bounded keys (up to 16
@@ -1116,13 +1126,7 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
     use_tc = pset != nullptr;
     ctx->last_mac_path = use_tc ? 1 : 0;
     u32 G = n_ct >= 4 ? 4 : n_ct;
-    if (use_tc) {
-        const size_t per_ct = ((size_t)D * LK * n + 4 * (size_t)n_keys * LK * n) * sizeof(u64);
-        size_t free_b = 0, total_b = 0;
-        cudaMemGetInfo(&free_b, &total_b);
-        G = n_ct < (u32)tc::kCt ? n_ct : (u32)tc::kCt;
-        while (G > 4 && (size_t)G * per_ct > free_b / 2) G -= 4;
-    }
+    if (use_tc) G = n_ct < pset->g_max ? n_ct : pset->g_max;
     const int cap = 1024;
     const LimbMap lqp = LimbMap::qp(ctx, Lq);
     const size_t y_stride = (size_t)D * LK * n, d_stride = (size_t)D * n, f_stride = (size_t)n + 1,
@@ -1135,11 +1139,21 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
     int32_t rc;
     if ((rc = terr.alloc(1, st))) return rc;
     CKKS_CUDA_TRY(cudaMemsetAsync(terr.p, 0, sizeof(int), st));
-    if ((rc = Y.alloc(G * y_stride, st)) || (use_tc && (rc = Bh.alloc(G * b_stride, st))) || (rc = acc.alloc((size_t)G * n_keys * 2 * LK * n, st)) || (rc = Z.alloc((size_t)G * n_keys * 2 * LK * n, st)) ||
-        (rc = karr.alloc(3 * (size_t)n_keys + ctx->moduli.size(), st)) || (rc = dig.alloc(G * d_stride, st)) ||
-        (rc = flags.alloc(G * f_stride, st)) || (rc = cnt.alloc((size_t)G * n_keys, st)) ||
-        (rc = exc.alloc((size_t)G * n_keys * cap, st)))
-        return rc;
+    // the group size was sized against the free memory when the key set was packed; if the
+    // workspaces do not fit now, smaller groups are taken (same words, keys read more often)
+    for (;;) {
+        if (!(rc = Y.alloc(G * y_stride, st)) && !(use_tc && (rc = Bh.alloc(G * b_stride, st))) &&
+            !(rc = acc.alloc((size_t)G * n_keys * 2 * LK * n, st)) &&
+            !(rc = Z.alloc((size_t)G * n_keys * 2 * LK * n, st)) &&
+            !(rc = karr.alloc(3 * (size_t)n_keys + ctx->moduli.size(), st)) && !(rc = dig.alloc(G * d_stride, st)) &&
+            !(rc = flags.alloc(G * f_stride, st)) && !(rc = cnt.alloc((size_t)G * n_keys, st)) &&
+            !(rc = exc.alloc((size_t)G * n_keys * cap, st)))
+            break;
+        if (rc != CKKS_ERR_OOM || G <= 1) return rc;
+        Y.release(), Bh.release(), acc.release(), Z.release(), karr.release(), dig.release(), flags.release();
+        cnt.release(), exc.release();
+        G = G > 4 ? G - 4 : G / 2;
+    }
     // key pointers, exponents and psi per modulus
     std::vector<u64> hk(3 * (size_t)n_keys + ctx->moduli.size());
     for (u32 g = 0; g < n_keys; ++g) {

@@ -96,10 +96,26 @@ k_fwd1(const void* __restrict__ in_, u64* __restrict__ out,
     const size_t base = ((size_t)blockIdx.z * limb_count + limb) << (LOG_M + log_b);
     const int c0 = blockIdx.x << log_c;
     if (LOG_M <= 8 && T.f64) {  // FP64 network: inputs in [0, q), twist output below q in magnitude
-        const double2* tab = stage_table_f64(sm + (S::M << log_c), T.fA, S::M);
+        // Phase 2 runs the row group g = tid % R1 in the low lanes, so a warp reads 16
+        // different blocks (g << ls) + b of a stage s = LR1 + ls: they are staged at
+        // (1 << s) + (b << LR1) + g (consecutive in g) instead of 2^ls entries apart,
+        // which cost up to 16-way shared-memory bank conflicts per twiddle load.
+        double2* tab = reinterpret_cast<double2*>(sm + (S::M << log_c));
+        for (int i = tid; i < S::M; i += blockDim.x) {
+            int pos = i;
+            if (i >= (1 << S::LR1)) {
+                const int s = 31 - __clz(i), ls = s - S::LR1, blk = i - (1 << s);
+                pos = (1 << s) + ((blk & ((1 << ls) - 1)) << S::LR1) + (blk >> ls);
+            }
+            tab[pos] = __ldg(T.fA + i);
+        }
         const double qd = T.qd, qinv = T.qinv;
         double* smd = reinterpret_cast<double*>(sm);
-        auto twf = [&](int s, u32 blk) { return tab[(1u << s) + blk]; };
+        auto twf = [&](int s, u32 blk) { return tab[(1u << s) + blk]; };  // stages below LR1: natural order
+        auto twf2 = [&](int s, u32 blk) {
+            const int ls = s - S::LR1;
+            return tab[(1u << s) + ((blk & ((1u << ls) - 1)) << S::LR1) + (blk >> ls)];
+        };
         __syncthreads();
         if (tid < (C << S::LR2)) {
             const int c = tid & (C - 1), i0 = tid >> log_c;
@@ -125,7 +141,7 @@ k_fwd1(const void* __restrict__ in_, u64* __restrict__ out,
             double y[S::R2];
 #pragma unroll
             for (int e = 0; e < S::R2; ++e) y[e] = smd[((S::R2 * g + e) << log_c) + (c ^ (g & (C - 1)))];
-            nttf::ct_stages<S::LR2>(y, S::LR1, g, twf, qd);
+            nttf::ct_stages<S::LR2>(y, S::LR1, g, twf2, qd);
             const size_t row = (size_t)(c0 + c) << LOG_M;
 #pragma unroll
             for (int e = 0; e < S::R2; ++e) {
