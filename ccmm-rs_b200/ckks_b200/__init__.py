@@ -185,8 +185,9 @@ class Context:
 
     @property
     def tensor_cores(self):
-        """True when bounded hoisted rotations run their key-switch MAC on the
-        INT8 tensor cores (enabled by default where the device has them)."""
+        """True when bounded hoisted rotations run their key-switch MAC, and the
+        structured CCMM its per-slot products (m, k <= 64), on the INT8 tensor
+        cores (enabled by default where the device has them)."""
         return bool(lib().ckks_ctx_tensor_cores(self.handle))
 
     @tensor_cores.setter
@@ -195,8 +196,8 @@ class Context:
 
     @property
     def last_mac_path(self):
-        """MAC of the most recent hoisted rotation on this context:
-        "tensor_cores", "cuda_cores" or None (no hoisted rotation yet)."""
+        """Path of the most recent hoisted rotation MAC or CCMM slot product on
+        this context: "tensor_cores", "cuda_cores" or None (neither ran yet)."""
         return {1: "tensor_cores", 0: "cuda_cores"}.get(int(lib().ckks_ctx_last_mac_path(self.handle)))
 
     def autotune(self, limbs, polys, stream=None):

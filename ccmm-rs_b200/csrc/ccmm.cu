@@ -9,10 +9,11 @@
 //   C0 = Ab Bb,  C1 = Ab Ba + Aa Bb,  C2 = Aa Ba      (m x k times k x n)
 // which equal the reference's per-product NTTs, inverse NTTs and additions word
 // for word (the NTT is linear mod q). The schedule:
-//   1. forward NTT of every entry, transposed to slot-major [l][s][comp][entry]
-//      with each residue pre-split into sb-bit halves (sb = ceil(bits(q-1)/2));
-//   2. one CTA per (l, s) forms the three products with split-operand
-//      accumulators (four 32x32->64-bit multiply-adds per product, exact);
+//   1. forward NTT of every entry, transposed to slot-major [l][s][comp][entry];
+//   2. the three products per (l, s): on the INT8 tensor cores (ccmm_tc.cu,
+//      byte planes, exact) when m, k <= 64, else one CTA per (l, s) with
+//      split-operand accumulators (residues pre-split into sb-bit halves,
+//      sb = ceil(bits(q-1)/2); four 32x32->64-bit multiply-adds per product);
 //   3. the results go back to entry-major [entry][comp][l][s] in chunks of
 //      output columns, c2 is transformed back, relinearized with the bounded
 //      key (digits, digit NTTs, key MAC with c0/c1 as base), transformed back
@@ -27,10 +28,11 @@ constexpr int kTile = 32;
 __device__ __forceinline__ int split_bits(u64 q) { return (65 - __clzll(q - 1)) / 2; }
 
 // X [n_ent][2][L][N] (NTT domain) -> Xt [L][N][2][ld] at entries e0.., each word
-// pre-split as (x >> sb) << 32 | (x & mask). Grid (N/32, n_ent/32 rounded up, 2 L).
+// pre-split as (x >> sb) << 32 | (x & mask) when `split`, else canonical.
+// Grid (N/32, n_ent/32 rounded up, 2 L).
 __global__ void __launch_bounds__(kTile * 8) k_to_slot_major(const u64* __restrict__ X, u64* __restrict__ Xt,
                                                              const NttTab* __restrict__ tabs, int n_ent, int e0,
-                                                             int ld, int L, int log_n) {
+                                                             int ld, int L, int log_n, int split) {
     __shared__ u64 tile[kTile][kTile + 1];
     const u32 n = 1u << log_n;
     const int l = blockIdx.z >> 1, comp = blockIdx.z & 1;
@@ -44,7 +46,7 @@ __global__ void __launch_bounds__(kTile * 8) k_to_slot_major(const u64* __restri
         const int e = c0 + r;
         if (e < n_ent) {
             const u64 x = X[((((size_t)e * 2 + comp) * L + l) << log_n) + s0 + tx];
-            tile[r][tx] = ((x >> sb) << 32) | (x & mask);
+            tile[r][tx] = split ? ((x >> sb) << 32) | (x & mask) : x;
         }
     }
     __syncthreads();
@@ -178,16 +180,17 @@ __global__ void __launch_bounds__(kT, 3) k_ccmm_slot(const u64* __restrict__ At,
     }
 }
 
-int32_t to_slot_major(ckks_ctx* ctx, const u64* X, u64* Xt, u32 n_ent, u32 e0, u32 ld, u32 L, cudaStream_t st) {
+int32_t to_slot_major(ckks_ctx* ctx, const u64* X, u64* Xt, u32 n_ent, u32 e0, u32 ld, u32 L, bool split,
+                      cudaStream_t st) {
     dim3 g(ctx->n / kTile, (n_ent + kTile - 1) / kTile, 2 * L);
     k_to_slot_major<<<g, kTile * 8, 0, st>>>(X, Xt, ctx->d_tabs, (int)n_ent, (int)e0, (int)ld, (int)L,
-                                             (int)ctx->log_n);
+                                             (int)ctx->log_n, split ? 1 : 0);
     CKKS_CUDA_TRY(cudaGetLastError());
     return CKKS_OK;
 }
 
 // entry-major transforms of n_ent entries (NTT) written slot-major into Xt
-int32_t build_slot_major(ckks_ctx* ctx, const u64* X, u64* Xt, u32 n_ent, u32 L, cudaStream_t st) {
+int32_t build_slot_major(ckks_ctx* ctx, const u64* X, u64* Xt, u32 n_ent, u32 L, bool split, cudaStream_t st) {
     const size_t ct = (size_t)2 * L * ctx->n;
     u32 chunk = (u32)((size_t(1) << 28) / ct);
     if (chunk < 1) chunk = 1;
@@ -199,7 +202,7 @@ int32_t build_slot_major(ckks_ctx* ctx, const u64* X, u64* Xt, u32 n_ent, u32 L,
     for (u32 e0 = 0; e0 < n_ent; e0 += chunk) {
         const u32 m = n_ent - e0 < chunk ? n_ent - e0 : chunk;
         if ((rc = ntt_forward_launch(ctx, X + (size_t)e0 * ct, buf.p, 2 * m, 0, L, st))) return rc;
-        if ((rc = to_slot_major(ctx, buf.p, Xt, m, e0, n_ent, L, st))) return rc;
+        if ((rc = to_slot_major(ctx, buf.p, Xt, m, e0, n_ent, L, split, st))) return rc;
     }
     return CKKS_OK;
 }
@@ -214,11 +217,17 @@ int32_t ccmm_structured_launch(ckks_ctx* ctx, const ckks_ksk* key, const u64* A,
         ckks_set_error("ckks_ccmm_structured: ring degree below 32 is not supported");
         return CKKS_ERR_BAD_ARG;
     }
+    const bool use_tc = ccmm_tc_supported(ctx, m, kd);
     Workspace<u64> At, Bt;
+    Workspace<int> terr;
     int32_t rc;
     if ((rc = At.alloc(slots * 2 * m * kd, st)) || (rc = Bt.alloc(slots * 2 * kd * nd, st))) return rc;
-    if ((rc = build_slot_major(ctx, A, At.p, m * kd, L, st))) return rc;
-    if ((rc = build_slot_major(ctx, B, Bt.p, kd * nd, L, st))) return rc;
+    if (use_tc) {
+        if ((rc = terr.alloc(1, st))) return rc;
+        CKKS_CUDA_TRY(cudaMemsetAsync(terr.p, 0, sizeof(int), st));
+    }
+    if ((rc = build_slot_major(ctx, A, At.p, m * kd, L, !use_tc, st))) return rc;
+    if ((rc = build_slot_major(ctx, B, Bt.p, kd * nd, L, !use_tc, st))) return rc;
     // output columns per chunk: slot-major products plus entry-major quadratic parts within about 2^31 words
     u32 cc = (u32)((size_t(1) << 31) / (slots * 3 * m * 2));
     if (cc > 2) cc &= ~1u;  // whole column pairs per thread
@@ -226,7 +235,7 @@ int32_t ccmm_structured_launch(ckks_ctx* ctx, const ckks_ksk* key, const u64* A,
     if (cc < 1) cc = 1;
     if (cc > nd) cc = nd;
     const size_t smem = (size_t)2 * (m * kd + kd * cc) * sizeof(u64);
-    if (smem > 200 * 1024) {
+    if (!use_tc && smem > 200 * 1024) {
         ckks_set_error("ckks_ccmm_structured: matrix blocks exceed shared memory (rows * inner too large)");
         return CKKS_ERR_BAD_ARG;
     }
@@ -238,10 +247,14 @@ int32_t ccmm_structured_launch(ckks_ctx* ctx, const ckks_ksk* key, const u64* A,
         if ((rc = Ct.alloc(slots * 3 * n_out, st)) || (rc = Q.alloc(3 * poly * n_out, st))) return rc;
         u64* Q01 = Q.p;                       // [n_out][2][L][N]
         u64* C2 = Q.p + 2 * poly * n_out;     // [n_out][L][N]
-        dim3 g(N, L);
-        k_ccmm_slot<<<g, kT, smem, st>>>(At.p, Bt.p, Ct.p, ctx->d_tabs, (int)m, (int)kd, (int)nd, (int)c0, (int)nc,
-                                         (int)ctx->log_n);
-        CKKS_CUDA_TRY(cudaGetLastError());
+        if (use_tc) {
+            if ((rc = ccmm_slot_tc_launch(ctx, At.p, Bt.p, Ct.p, L, m, kd, nd, c0, nc, terr.p, st))) return rc;
+        } else {
+            dim3 g(N, L);
+            k_ccmm_slot<<<g, kT, smem, st>>>(At.p, Bt.p, Ct.p, ctx->d_tabs, (int)m, (int)kd, (int)nd, (int)c0,
+                                             (int)nc, (int)ctx->log_n);
+            CKKS_CUDA_TRY(cudaGetLastError());
+        }
         dim3 gt(N / kTile, (n_out + kTile - 1) / kTile, 3 * L);
         k_from_slot_major<<<gt, kTile * 8, 0, st>>>(Ct.p, Q01, C2, (int)n_out, (int)n_out, (int)L, (int)ctx->log_n);
         CKKS_CUDA_TRY(cudaGetLastError());
@@ -260,5 +273,18 @@ int32_t ccmm_structured_launch(ckks_ctx* ctx, const ckks_ksk* key, const u64* A,
         if ((rc = rescale_launch(ctx, Q01, C + (size_t)c0 * m * 2 * (L - 1) * N, 2 * n_out, L, st))) return rc;
     }
     (void)ct;
+    if (use_tc) {
+        int h_err = 0;
+        CKKS_CUDA_TRY(cudaMemcpyAsync(&h_err, terr.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CKKS_CUDA_TRY(cudaStreamSynchronize(st));
+        ctx->last_mac_path = 1;
+        if (h_err) {
+            ckks_set_error("ckks_ccmm_structured: a tensor-core pipeline wait timed out (stage " +
+                           std::to_string(h_err) + ")");
+            return CKKS_ERR_TIMEOUT;
+        }
+    } else {
+        ctx->last_mac_path = 0;
+    }
     return CKKS_OK;
 }

@@ -92,6 +92,11 @@ int32_t fft_stage_launch(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_rot, 
 // ciphertexts [2][L][N] at the key's level L; C one level down.
 int32_t ccmm_structured_launch(ckks_ctx* ctx, const ckks_ksk* key, const u64* A, const u64* B, u64* C, u32 m, u32 kd,
                                u32 nd, cudaStream_t st);
+// Per-(limb, slot) products of the structured CCMM on the INT8 tensor cores
+// (ccmm_tc.cu): At, Bt slot-major canonical residues, m, kd <= 64.
+bool ccmm_tc_supported(const ckks_ctx* ctx, u32 m, u32 kd);
+int32_t ccmm_slot_tc_launch(ckks_ctx* ctx, const u64* At, const u64* Bt, u64* Ct, u32 L, u32 m, u32 kd, u32 nd,
+                            u32 c_begin, u32 nc, int* err, cudaStream_t st);
 
 // Multi-ciphertext diagonal stage: terms_host [n_terms][3] = (output, source, key or n_rot
 // for the unrotated source); diag_ntt [n_terms][L][N] in the caller's term order.

@@ -75,20 +75,23 @@ int32_t ckks_is_prime(uint64_t value);
 int32_t ckks_ctx_create(uint32_t log_n, const uint64_t* q, uint32_t L, const uint64_t* p, uint32_t K,
                         ckks_ctx** out);
 int32_t ckks_ctx_destroy(ckks_ctx* ctx);
-/* Selects the key-switch MAC of bounded hoisted rotations: enable != 0 (the
- * default) runs it on the tcgen05 INT8 tensor cores when the device has them,
- * 0 on CUDA cores (split-operand 64-bit accumulators). Both are bit-exact; the
- * switch exists to compare them. No counterpart in the reference (its MAC is
- * the serial loop of ring/ntt_polynomial.rs:211-236). */
+/* Selects the key-switch MAC of bounded hoisted rotations and the per-slot
+ * products of ckks_ccmm_structured (rows and inner dimension <= 64): enable != 0
+ * (the default) runs them on the tcgen05 INT8 tensor cores when the device has
+ * them, 0 on CUDA cores (split-operand 64-bit accumulators). Both are
+ * bit-exact; the switch exists to compare them. No counterpart in the reference
+ * (its MAC is the serial loop of ring/ntt_polynomial.rs:211-236, its CCMM the
+ * per-product loop of matrix/rns_ckks_ciphertext.rs:220-318). */
 int32_t ckks_ctx_set_tensor_cores(ckks_ctx* ctx, int32_t enable);
-/* 1 when bounded hoisted rotations of this context use the tensor cores. */
+/* 1 when bounded hoisted rotations and CCMM products of this context use the
+ * tensor cores. */
 int32_t ckks_ctx_tensor_cores(const ckks_ctx* ctx);
-/* Which key-switch MAC the most recent hoisted rotation on this context ran
- * (ckks_rotate_hoisted and the calls built on it): 1 the tcgen05 INT8
- * tensor-core MAC, 0 the CUDA-core MAC (tensor cores switched off, RNS-block
- * keys, rings below the tensor-core tile, or too little free device memory
- * for the packed key set), -1 no hoisted rotation yet. Diagnostic only; no
- * counterpart in the reference. */
+/* Which path the most recent hoisted rotation MAC (ckks_rotate_hoisted and the
+ * calls built on it) or structured CCMM slot product on this context ran: 1 the
+ * tcgen05 INT8 tensor cores, 0 the CUDA cores (tensor cores switched off,
+ * RNS-block keys, rings below the tensor-core tile, too little free device
+ * memory for the packed key set, or CCMM blocks beyond 64 rows or inner
+ * entries), -1 neither yet. Diagnostic only; no counterpart in the reference. */
 int32_t ckks_ctx_last_mac_path(const ckks_ctx* ctx);
 /* Autotuner (no counterpart in the reference, whose NTT has no launch shape):
  * times every admissible columns-per-CTA choice of the five NTT passes

@@ -68,6 +68,44 @@ def test_ccmm_bit_exact(oracle, cuda, setup, m, k, n_cols):
     assert np.array_equal(got.reshape(want.shape), want)
 
 
+def oracle_entry(oracle, q, key_ref, A, B, m, k, r, c):
+    L, N = len(q), A.shape[-1]
+    acc = sum(oracle.tensor(q, A[r + kk * m], B[kk + c * k]).astype(object) for kk in range(k))
+    quad = np.stack([acc[:, l] % q[l] for l in range(L)], axis=1).astype(np.uint64)
+    return oracle.rescale(q, oracle.relinearize(q, quad, key_ref, 20).reshape(2, L, N))
+
+
+@pytest.mark.parametrize("m,k,n_cols", [(1, 1, 1), (5, 7, 19), (64, 64, 3), (33, 5, 40), (64, 65, 2)])
+def test_ccmm_tensor_cores_equal_cuda_cores(oracle, cuda, setup, m, k, n_cols):
+    """The per-slot products on the INT8 tensor cores (m, k <= 64: byte planes,
+    one MMA per 16 columns x 4 inner indices) give the same words as the
+    CUDA-core products; ragged column blocks, one-item slots and the largest
+    tile are covered, and k = 65 falls back to the CUDA cores. Sampled entries
+    equal the oracle."""
+    import torch
+    n, q, ctx, s, key, key_ref = setup
+    rng = np.random.default_rng(m + 7 * k + 31 * n_cols)
+    A = np.stack([np.stack([rng.integers(0, mm, (2, n), dtype=np.uint64) for mm in q], axis=1) for _ in range(m * k)])
+    B = np.stack([np.stack([rng.integers(0, mm, (2, n), dtype=np.uint64) for mm in q], axis=1)
+                  for _ in range(k * n_cols)])
+    dA, dB = dev(A), dev(B)
+    assert ctx.tensor_cores
+    tc = cb.matmul_structured(ctx, key, dA, dB, m, k, n_cols)
+    torch.cuda.synchronize()
+    assert ctx.last_mac_path == ("tensor_cores" if k <= 64 else "cuda_cores")
+    ctx.tensor_cores = False
+    try:
+        cc = cb.matmul_structured(ctx, key, dA, dB, m, k, n_cols)
+        torch.cuda.synchronize()
+        assert ctx.last_mac_path == "cuda_cores"
+    finally:
+        ctx.tensor_cores = True
+    assert torch.equal(tc, cc)
+    got = host(tc)
+    for r, c in {(0, 0), (m - 1, n_cols - 1), (m // 2, n_cols // 2)}:
+        assert np.array_equal(got[c, r], oracle_entry(oracle, q, key_ref, A, B, m, k, r, c)), (r, c)
+
+
 def test_ccmm_decodes_to_cleartext_gemm(oracle, cuda, setup):
     n, q, ctx, s, key, key_ref = setup
     rng = np.random.default_rng(11)
