@@ -85,6 +85,19 @@ _SIGS = {
     "ckks_diag_stage": (I32, [VP, ctypes.POINTER(VP), U32, I32, VP, VP, VP, U32, U32, I32, VP]),
     "ckks_ccmm_structured": (I32, [VP, VP, VP, VP, VP, U32, U32, U32, VP]),
     "ckks_fft_stage_multi": (I32, [VP, ctypes.POINTER(VP), U32, u32p, U32, VP, VP, U32, VP, U32, U32, VP]),
+    "ckks_rng_create": (I32, [U64, ctypes.POINTER(VP)]),
+    "ckks_rng_create_from_seed": (I32, [ctypes.c_char_p, ctypes.POINTER(VP)]),
+    "ckks_rng_destroy": (I32, [VP]),
+    "ckks_rng_next_u32": (I32, [VP, u32p]),
+    "ckks_rng_next_u64": (I32, [VP, u64p]),
+    "ckks_rng_fill_u32": (I32, [VP, u32p, U64]),
+    "ckks_rng_word_position": (I32, [VP, u64p]),
+    "ckks_rng_ternary_secret": (I32, [VP, U32, i8p]),
+    "ckks_rng_error": (I32, [VP, U32, I32, ctypes.c_double, ctypes.POINTER(ctypes.c_int64)]),
+    "ckks_rng_uniform_residues": (I32, [VP, U32, U64, u64p]),
+    "ckks_hybrid_key_generate_rng": (I32, [VP, U32, U32, U64, i8p, I32, ctypes.c_double, VP, ctypes.POINTER(VP)]),
+    "ckks_relin_key_generate_rng": (I32, [VP, U32, U32, i8p, I32, ctypes.c_double, VP, ctypes.POINTER(VP)]),
+    "ckks_encrypt_rng_host": (I32, [VP, U32, u64p, i8p, I32, ctypes.c_double, VP, u64p]),
     "ckks_encode": (I32, [VP, VP, VP, U32, U32, ctypes.c_double, VP]),
     "ckks_decode": (I32, [VP, VP, VP, U32, U32, ctypes.c_double, VP]),
 }
@@ -343,6 +356,96 @@ class Context:
         return int(lib().ckks_rotation_exponent_right(self.n, int(steps)))
 
 
+class ChaCha20Rng:
+    """rand_chacha::ChaCha20Rng as the reference seeds and consumes it (host side).
+
+    seed_from_u64 / from_seed, next_u32 / next_u64, and the reference's
+    samplers: ternary secret (rlwe/secret_key.rs:25-40), errors
+    (rlwe/error.rs:33-156: ErrorDistribution BoundedUniform or
+    DiscreteGaussian) and uniform residues (rlwe/uniform.rs:12-30). Passing
+    one instance through several calls continues one stream, as `&mut rng`
+    does in the reference.
+    """
+
+    BOUNDED_UNIFORM, GAUSSIAN = 0, 1
+
+    def __init__(self, handle):
+        self.handle = handle
+
+    @classmethod
+    def seed_from_u64(cls, seed):
+        h = ctypes.c_void_p()
+        check(lib().ckks_rng_create(int(seed) & (2**64 - 1), ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_seed(cls, seed32):
+        b = bytes(seed32)
+        if len(b) != 32:
+            raise ValueError("ChaCha20Rng seed must be 32 bytes")
+        h = ctypes.c_void_p()
+        check(lib().ckks_rng_create_from_seed(b, ctypes.byref(h)))
+        return cls(h)
+
+    def next_u32(self):
+        v = U32()
+        check(lib().ckks_rng_next_u32(self.handle, ctypes.byref(v)))
+        return v.value
+
+    def next_u64(self):
+        v = U64()
+        check(lib().ckks_rng_next_u64(self.handle, ctypes.byref(v)))
+        return v.value
+
+    def words(self, n):
+        out = np.zeros(n, np.uint32)
+        check(lib().ckks_rng_fill_u32(self.handle, out.ctypes.data_as(u32p), n))
+        return out
+
+    def word_position(self):
+        v = U64()
+        check(lib().ckks_rng_word_position(self.handle, ctypes.byref(v)))
+        return v.value
+
+    def ternary_secret(self, n):
+        out = np.zeros(n, np.int8)
+        check(lib().ckks_rng_ternary_secret(self.handle, n, out.ctypes.data_as(i8p)))
+        return out
+
+    def error(self, n, kind, param):
+        out = np.zeros(n, np.int64)
+        check(lib().ckks_rng_error(self.handle, n, kind, float(param),
+                                   out.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
+        return out
+
+    def uniform_residues(self, n, modulus):
+        out = np.zeros(n, np.uint64)
+        check(lib().ckks_rng_uniform_residues(self.handle, n, int(modulus), out.ctypes.data_as(u64p)))
+        return out
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().ckks_rng_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def encrypt_rng(ctx, q_limbs, message, secret, rng, kind=ChaCha20Rng.GAUSSIAN, param=3.2):
+    """encrypt_rns_raw_with_distribution_ntt_rng (grafting/rns_key_switch.rs:245-387) on the
+    reference's stream: message [q_limbs][N] coefficients -> ciphertext [2][q_limbs][N]."""
+    m = np.ascontiguousarray(np.asarray(message, np.uint64))
+    s = np.ascontiguousarray(np.asarray(secret, np.int8))
+    out = np.zeros((2, q_limbs, ctx.n), np.uint64)
+    check(lib().ckks_encrypt_rng_host(ctx.handle, q_limbs, m.ctypes.data_as(u64p), s.ctypes.data_as(i8p), kind,
+                                      float(param), rng.handle, out.ctypes.data_as(u64p)))
+    return out
+
+
 class KeySwitchKey:
     """A key-switching key resident in HBM (ckks_ksk)."""
 
@@ -364,6 +467,16 @@ class KeySwitchKey:
         h = ctypes.c_void_p()
         check(lib().ckks_hybrid_key_generate(ctx.handle, q_limbs, base_log, int(exponent), sp, seed, sigma,
                                              ctypes.byref(h)))
+        return cls(ctx, h, cls.HYBRID_BOUNDED, q_limbs, exponent, base_log)
+
+    @classmethod
+    def hybrid_generate_rng(cls, ctx, q_limbs, base_log, exponent, secret, rng, kind=ChaCha20Rng.GAUSSIAN,
+                            param=3.2):
+        """generate_with_distribution_ntt_rng on the reference's ChaCha20 stream (rng continues)."""
+        s, sp = cls._secret(secret)
+        h = ctypes.c_void_p()
+        check(lib().ckks_hybrid_key_generate_rng(ctx.handle, q_limbs, base_log, int(exponent), sp, kind, float(param),
+                                                 rng.handle, ctypes.byref(h)))
         return cls(ctx, h, cls.HYBRID_BOUNDED, q_limbs, exponent, base_log)
 
     @classmethod
@@ -438,6 +551,15 @@ class KeySwitchKey:
         s, sp = cls._secret(secret)
         h = ctypes.c_void_p()
         check(lib().ckks_relin_key_generate(ctx.handle, q_limbs, base_log, sp, seed, sigma, ctypes.byref(h)))
+        return cls(ctx, h, cls.RELIN_BOUNDED, q_limbs, 1, base_log)
+
+    @classmethod
+    def relin_generate_rng(cls, ctx, q_limbs, base_log, secret, rng, kind=ChaCha20Rng.GAUSSIAN, param=3.2):
+        """BoundedRnsMultiplicationKey::generate_with_distribution_ntt_rng on the reference's stream."""
+        s, sp = cls._secret(secret)
+        h = ctypes.c_void_p()
+        check(lib().ckks_relin_key_generate_rng(ctx.handle, q_limbs, base_log, sp, kind, float(param), rng.handle,
+                                                ctypes.byref(h)))
         return cls(ctx, h, cls.RELIN_BOUNDED, q_limbs, 1, base_log)
 
     @classmethod

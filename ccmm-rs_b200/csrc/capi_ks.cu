@@ -76,6 +76,14 @@ int32_t new_key(ckks_ctx* ctx, int kind, u32 q_limbs, u32 base_log, u64 exponent
     return CKKS_OK;
 }
 
+}  // namespace
+
+int32_t ksk_new(ckks_ctx* ctx, int kind, u32 q_limbs, u32 base_log, u64 exponent, ckks_ksk** out, const char* who) {
+    return new_key(ctx, kind, q_limbs, base_log, exponent, {}, out, who);
+}
+
+namespace {
+
 int32_t finish_key(ckks_ksk* k, int32_t rc, ckks_ksk** out) {
     if (rc == CKKS_OK) {
         cudaError_t e = cudaDeviceSynchronize();

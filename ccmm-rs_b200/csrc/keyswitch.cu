@@ -93,13 +93,14 @@ __device__ __forceinline__ i64 gaussian(const u64* cdt, int len, u64 word) {
 __global__ void k_keygen_target(u64* __restrict__ T, const int8_t* __restrict__ s_t, const u64* __restrict__ t_limbs,
                                 const u64* __restrict__ fac, const u64* __restrict__ fac_q,
                                 const NttTab* __restrict__ tabs, LimbMap lm, int LK, int log_n, u64 seed, u64 tag_e,
-                                const u64* __restrict__ cdt, int cdt_len) {
+                                const u64* __restrict__ cdt, int cdt_len, const i64* __restrict__ e_arr) {
     const u32 n = 1u << log_n;
     const u32 c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n) return;
     const int l = blockIdx.y, j = blockIdx.z;
     const u64 m = tabs[lm(l)].q;
-    i64 e = gaussian(cdt, cdt_len, rng_word(seed, tag_e | (u64)j, c));
+    // e_arr: the caller's sampled errors [D][N] (one logical error polynomial per entry)
+    const i64 e = e_arr ? e_arr[((size_t)j << log_n) + c] : gaussian(cdt, cdt_len, rng_word(seed, tag_e | (u64)j, c));
     u64 su;
     if (t_limbs) {
         su = t_limbs[((size_t)l << log_n) + c];
@@ -108,21 +109,25 @@ __global__ void k_keygen_target(u64* __restrict__ T, const int8_t* __restrict__ 
         su = sv < 0 ? m - 1 : (u64)sv;
     }
     u64 t = mul_shoup(su, fac[(size_t)j * LK + l], fac_q[(size_t)j * LK + l], m);
-    u64 eu = e < 0 ? m - (u64)(-e) : (u64)e;
+    const u64 mag = e < 0 ? 0 - (u64)e : (u64)e;  // signed_mod (hybrid_rns_galois_key.rs:55-57)
+    u64 eu = mag >= m ? mag % m : mag;
+    eu = (e < 0 && eu) ? m - eu : eu;
     T[(((size_t)j * LK + l) << log_n) + c] = add_mod(t, eu, m);
 }
 
 // entries[j][l][0] = That - a * s_hat, entries[j][l][1] = a (a uniform, sampled in the NTT domain)
 __global__ void k_keygen_finish(const u64* __restrict__ That, const u64* __restrict__ s_hat, u64* __restrict__ entries,
                                 const NttTab* __restrict__ tabs, LimbMap lm, int LK, int log_n, u64 seed, u64 tag_a,
-                                int comp_major, u64 perm) {
+                                int comp_major, u64 perm, const u64* __restrict__ a_arr) {
     const u32 n = 1u << log_n;
     const u32 c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n) return;
     const int l = blockIdx.y, j = blockIdx.z;
     const NttTab& T = tabs[lm(l)];
     Barrett bm{T.q, T.mu_hi, T.mu_lo};
-    u64 a = uniform_mod(T.q, seed, tag_a | ((u64)j << 16) | (u64)l, c);
+    // a_arr: NTT of the caller's sampled uniform a [D][LK][N]
+    const u64 a = a_arr ? a_arr[(((size_t)j * LK + l) << log_n) + c]
+                        : uniform_mod(T.q, seed, tag_a | ((u64)j << 16) | (u64)l, c);
     u64 b = sub_mod(That[(((size_t)j * LK + l) << log_n) + c], mul_barrett(a, s_hat[((size_t)l << log_n) + c], bm), T.q);
     if (comp_major) {  // [j][2][LK][N] (relinearization key layout)
         entries[((((size_t)j * 2 + 0) * LK + l) << log_n) + c] = b;
@@ -186,7 +191,8 @@ u32 ksk_limbs(const ckks_ksk* k) { return k->with_p ? k->q_limbs + k->ctx->K : k
 
 int32_t ksk_generate(ckks_ctx* ctx, ckks_ksk* key, const int8_t* secret, u64 seed, double sigma,
                      const std::vector<u64>& factors /*[D][LK] host*/, const std::vector<int8_t>& s_target,
-                     bool comp_major, u64 tag_a, u64 tag_e, cudaStream_t st, const u64* d_target_limbs) {
+                     bool comp_major, u64 tag_a, u64 tag_e, cudaStream_t st, const u64* d_target_limbs,
+                     const KeySamples& smp) {
     const u32 LK = ksk_limbs(key), D = key->D, n = ctx->n;
     const LimbMap lm = key->with_p ? LimbMap::qp(ctx, key->q_limbs) : LimbMap::range(0, key->q_limbs);
     std::vector<u64> fq(factors.size());
@@ -205,15 +211,27 @@ int32_t ksk_generate(ckks_ctx* ctx, ckks_ksk* key, const int8_t* secret, u64 see
     CKKS_CUDA_TRY(cudaMemcpyAsync(d_cdt.p, cdt.data(), cdt.size() * 8, cudaMemcpyHostToDevice, st));
     if (!d_target_limbs) CKKS_CUDA_TRY(cudaMemcpyAsync(d_st.p, s_target.data(), n, cudaMemcpyHostToDevice, st));
     CKKS_CUDA_TRY(cudaMemcpyAsync(d_sec.p, secret, n, cudaMemcpyHostToDevice, st));
+    Workspace<i64> d_e;
+    Workspace<u64> d_a;
+    if (smp.e) {
+        if ((rc = d_e.alloc((size_t)D * n, st))) return rc;
+        CKKS_CUDA_TRY(cudaMemcpyAsync(d_e.p, smp.e, (size_t)D * n * 8, cudaMemcpyHostToDevice, st));
+    }
+    if (smp.a) {  // a_ntt = NTT(a) (grafting/rns_key_switch.rs:844-850)
+        if ((rc = d_a.alloc((size_t)D * LK * n, st))) return rc;
+        CKKS_CUDA_TRY(cudaMemcpyAsync(d_a.p, smp.a, (size_t)D * LK * n * 8, cudaMemcpyHostToDevice, st));
+        if ((rc = ntt_forward_launch_map(ctx, d_a.p, d_a.p, D, lm, LK, st))) return rc;
+    }
     dim3 g((n + kT - 1) / kT, LK, D);
     k_keygen_target<<<g, kT, 0, st>>>(d_T.p, d_st.p, d_target_limbs, d_fac.p, d_fac.p + factors.size(), ctx->d_tabs, lm, LK,
-                                      ctx->log_n, seed, tag_e, d_cdt.p, (int)cdt.size());
+                                      ctx->log_n, seed, tag_e, d_cdt.p, (int)cdt.size(), d_e.p);
     if ((rc = ntt_forward_launch_map(ctx, d_T.p, d_That.p, D, lm, LK, st))) return rc;
     dim3 gs((n + kT - 1) / kT, LK, 1);
     k_lift_ternary<<<gs, kT, 0, st>>>(d_sec.p, d_s.p, ctx->d_tabs, lm, ctx->log_n);
     if ((rc = ntt_forward_launch_map(ctx, d_s.p, d_s.p + (size_t)LK * n, 1, lm, LK, st))) return rc;
     k_keygen_finish<<<g, kT, 0, st>>>(d_That.p, d_s.p + (size_t)LK * n, key->d_entries, ctx->d_tabs, lm, LK,
-                                      ctx->log_n, seed, tag_a, comp_major ? 1 : 0, comp_major ? 0 : key->exponent);
+                                      ctx->log_n, seed, tag_a, comp_major ? 1 : 0, comp_major ? 0 : key->exponent,
+                                      d_a.p);
     CKKS_CUDA_TRY(cudaGetLastError());
     return CKKS_OK;
 }
@@ -292,7 +310,8 @@ std::vector<u64> relin_factors(ckks_ctx* ctx, const ckks_ksk* key) {
 
 // Bounded relinearization key: entry j encrypts B^j * s^2 over Q
 // (bounded_key_switch.rs:28-104); s^2 formed in the NTT domain.
-int32_t relin_generate(ckks_ctx* ctx, ckks_ksk* key, const int8_t* secret, u64 seed, double sigma, cudaStream_t st) {
+int32_t relin_generate(ckks_ctx* ctx, ckks_ksk* key, const int8_t* secret, u64 seed, double sigma, cudaStream_t st,
+                       const KeySamples& smp) {
     const u32 L = key->q_limbs, n = ctx->n;
     const LimbMap lm = LimbMap::range(0, L);
     Workspace<u64> S;
@@ -309,7 +328,7 @@ int32_t relin_generate(ckks_ctx* ctx, ckks_ksk* key, const int8_t* secret, u64 s
     std::vector<int8_t> none;
     return ksk_generate(ctx, key, secret, seed, sigma,
                         key->kind == CKKS_KSK_RELIN_RNS_BLOCK ? rns_factors(ctx, key) : relin_factors(ctx, key), none,
-                        true, TAG_RLK_A, TAG_RLK_E, st, S.p);
+                        true, TAG_RLK_A, TAG_RLK_E, st, S.p, smp);
 }
 
 std::vector<int8_t> host_secret_automorphism(const int8_t* s, u32 n, u64 k) { return secret_automorphism(s, n, k); }

@@ -33,11 +33,24 @@ struct ckks_ksk {
 };
 
 u32 ksk_limbs(const ckks_ksk* k);
+// A key of the given kind and shape with its entries allocated, not filled
+// (bounded kinds; capi_ks.cu).
+int32_t ksk_new(ckks_ctx* ctx, int kind, u32 q_limbs, u32 base_log, u64 exponent, ckks_ksk** out, const char* who);
 int32_t ksk_alloc(ckks_ctx* ctx, ckks_ksk* key);
+// Host-sampled randomness of a key (the reference's ChaCha20 stream, rng.cu):
+// e [D][N] one logical error polynomial per entry, a [D][LK][N] uniform
+// residues in the coefficient domain (transformed here). Null members: the
+// counter-based stream of (seed, tags) is sampled on the GPU instead.
+struct KeySamples {
+    const i64* e = nullptr;
+    const u64* a = nullptr;
+};
 int32_t ksk_generate(ckks_ctx* ctx, ckks_ksk* key, const int8_t* secret, u64 seed, double sigma,
                      const std::vector<u64>& factors, const std::vector<int8_t>& s_target, bool comp_major, u64 tag_a,
-                     u64 tag_e, cudaStream_t st, const u64* d_target_limbs = nullptr);
-int32_t relin_generate(ckks_ctx* ctx, ckks_ksk* key, const int8_t* secret, u64 seed, double sigma, cudaStream_t st);
+                     u64 tag_e, cudaStream_t st, const u64* d_target_limbs = nullptr,
+                     const KeySamples& smp = KeySamples{});
+int32_t relin_generate(ckks_ctx* ctx, ckks_ksk* key, const int8_t* secret, u64 seed, double sigma, cudaStream_t st,
+                       const KeySamples& smp = KeySamples{});
 // Block factors E_i mod q_l = [l in block i] without the auxiliary P (RNS_BLOCK, RELIN_RNS_BLOCK).
 std::vector<u64> rns_factors(ckks_ctx* ctx, const ckks_ksk* key);
 // Ordinary RNS key-switched Galois automorphism with an RNS_BLOCK key in the

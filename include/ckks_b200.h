@@ -260,6 +260,54 @@ int32_t ckks_ksk_info(const ckks_ksk* key, uint32_t* digits, uint64_t* words);
 int32_t ckks_ksk_download(const ckks_ksk* key, uint64_t* entries_host);
 int32_t ckks_ksk_destroy(ckks_ksk* key);
 
+/* --------------------------------------------- seeded sampling stream -----
+ * The reference draws every secret, error and uniform mask from
+ * rand_chacha 0.3.1's ChaCha20Rng (ChaCha20, 64-bit block counter, stream 0)
+ * seeded by rand_core 0.6.4's seed_from_u64, through rand 0.8's gen_range.
+ * A ckks_rng is that generator, restated on the host: the same seed gives the
+ * same keystream words, and the samplers and key generation / encryption
+ * below consume them in the reference's order, so keys and ciphertexts made
+ * from one seed are the reference's (the sampling is sequential and runs on
+ * the host; the arithmetic runs on the GPU). Handles are not thread-safe. */
+typedef struct ckks_rng ckks_rng;
+enum { CKKS_DIST_BOUNDED_UNIFORM = 0, CKKS_DIST_GAUSSIAN = 1 };
+/* ChaCha20Rng::seed_from_u64 / ChaCha20Rng::from_seed (32 bytes). */
+int32_t ckks_rng_create(uint64_t seed, ckks_rng** out);
+int32_t ckks_rng_create_from_seed(const uint8_t* seed32, ckks_rng** out);
+int32_t ckks_rng_destroy(ckks_rng* rng);
+/* RngCore::next_u32 / next_u64 (two words, low first); fill: n next words. */
+int32_t ckks_rng_next_u32(ckks_rng* rng, uint32_t* out);
+int32_t ckks_rng_next_u64(ckks_rng* rng, uint64_t* out);
+int32_t ckks_rng_fill_u32(ckks_rng* rng, uint32_t* out, uint64_t n);
+/* keystream words consumed so far */
+int32_t ckks_rng_word_position(const ckks_rng* rng, uint64_t* out);
+/* SecretKey::generate_with_rng (rlwe/secret_key.rs:25-40): gen_range(0u8..3)
+ * per coefficient (0, 1, -1), redrawn while all are zero. */
+int32_t ckks_rng_ternary_secret(ckks_rng* rng, uint32_t n, int8_t* out);
+/* sample_error_coefficients (rlwe/error.rs:33-57): kind BOUNDED_UNIFORM
+ * (param = integer bound, gen_range(-bound..=bound)) or GAUSSIAN (param =
+ * sigma, the 16-sigma table of :64-113). */
+int32_t ckks_rng_error(ckks_rng* rng, uint32_t n, int32_t kind, double param, int64_t* out);
+/* sample_uniform_residues (rlwe/uniform.rs:12-30): rejection below 2^64 mod q. */
+int32_t ckks_rng_uniform_residues(ckks_rng* rng, uint32_t n, uint64_t modulus, uint64_t* out);
+/* PreparedHybridRnsGaloisKey::generate_with_distribution_ntt_rng
+ * (ckks/hybrid_rns_galois_key.rs:61-170): per digit one error polynomial,
+ * then one uniform a per QP limb, entry = (NTT(target + e) - NTT(a) NTT(s),
+ * NTT(a)). */
+int32_t ckks_hybrid_key_generate_rng(ckks_ctx* ctx, uint32_t q_limbs, uint32_t base_log, uint64_t exponent,
+                                     const int8_t* secret_host, int32_t dist_kind, double dist_param, ckks_rng* rng,
+                                     ckks_ksk** out);
+/* BoundedRnsMultiplicationKey::generate_with_distribution_ntt_rng
+ * (grafting/bounded_key_switch.rs:28-106): entry j encrypts B^j s^2 over Q. */
+int32_t ckks_relin_key_generate_rng(ckks_ctx* ctx, uint32_t q_limbs, uint32_t base_log, const int8_t* secret_host,
+                                    int32_t dist_kind, double dist_param, ckks_rng* rng, ckks_ksk** out);
+/* encrypt_rns_raw_with_distribution_ntt_rng (grafting/rns_key_switch.rs:245-387):
+ * message [q_limbs][N] (coefficients) -> ciphertext [2][q_limbs][N] (b, a),
+ * b = m + e - a s. Host buffers, synchronous. */
+int32_t ckks_encrypt_rng_host(ckks_ctx* ctx, uint32_t q_limbs, const uint64_t* message_host,
+                              const int8_t* secret_host, int32_t dist_kind, double dist_param, ckks_rng* rng,
+                              uint64_t* ct_host);
+
 /* ---------------------------------------------------------- rotations ----
  * Key-switched Galois automorphism of n_ct ciphertexts [n_ct][2][q_limbs][N]
  * (coefficient domain) with one key; the output stays at the same level.

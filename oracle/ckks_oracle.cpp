@@ -1348,4 +1348,279 @@ void oracle_decode(uint32_t n, const uint64_t* q, uint32_t L, const uint64_t* po
     coeffs_to_slots(n, co.data(), slots);
 }
 
+
+// --------------------------------------------------- seeded ChaCha20 stream
+// rand_chacha 0.3.1 ChaCha20Rng as the reference consumes it: ChaCha20Core
+// refills a BlockRng of 64 words (four 16-word blocks, counters c .. c+3);
+// next_u32 / next_u64 follow rand_core 0.6.4 BlockRng (next_u64 joins two
+// words, low first, also across a refill). seed_from_u64 is rand_core's PCG32
+// fill of the 32-byte seed. gen_range is rand 0.8's UniformInt
+// sample_single_inclusive (u8 through u32 with a modulus zone, i64 with the
+// leading-zeros zone). Call sites: rlwe/secret_key.rs:25-40,
+// rlwe/error.rs:33-156, rlwe/uniform.rs:12-30.
+struct OracleChaCha {
+    uint32_t key[8];
+    uint64_t counter = 0;   // next block
+    uint32_t results[64];
+    uint32_t index = 64;
+
+    static uint32_t rotl(uint32_t v, int c) { return (v << c) | (v >> (32 - c)); }
+    void refill() {
+        for (int b = 0; b < 4; ++b) {
+            const uint64_t ctr = counter + (uint64_t)b;
+            uint32_t st[16] = {0x61707865u, 0x3320646eu, 0x79622d32u, 0x6b206574u};
+            for (int i = 0; i < 8; ++i) st[4 + i] = key[i];
+            st[12] = (uint32_t)ctr;
+            st[13] = (uint32_t)(ctr >> 32);
+            st[14] = 0;
+            st[15] = 0;
+            uint32_t w[16];
+            for (int i = 0; i < 16; ++i) w[i] = st[i];
+            auto qr = [&](int a, int b2, int c, int d) {
+                w[a] += w[b2]; w[d] = rotl(w[d] ^ w[a], 16);
+                w[c] += w[d]; w[b2] = rotl(w[b2] ^ w[c], 12);
+                w[a] += w[b2]; w[d] = rotl(w[d] ^ w[a], 8);
+                w[c] += w[d]; w[b2] = rotl(w[b2] ^ w[c], 7);
+            };
+            for (int r = 0; r < 20; r += 2) {
+                qr(0, 4, 8, 12); qr(1, 5, 9, 13); qr(2, 6, 10, 14); qr(3, 7, 11, 15);
+                qr(0, 5, 10, 15); qr(1, 6, 11, 12); qr(2, 7, 8, 13); qr(3, 4, 9, 14);
+            }
+            for (int i = 0; i < 16; ++i) results[16 * b + i] = w[i] + st[i];
+        }
+        counter += 4;
+    }
+    void seed_u64(uint64_t state) {
+        uint8_t seed[32];
+        for (int k = 0; k < 8; ++k) {  // pcg32: advance, then XSH-RR output
+            state = state * 6364136223846793005ull + 11634580027462260723ull;
+            const uint32_t xs = (uint32_t)(((state >> 18) ^ state) >> 27);
+            const uint32_t rot = (uint32_t)(state >> 59);
+            const uint32_t x = rot ? (xs >> rot) | (xs << (32 - rot)) : xs;
+            for (int i = 0; i < 4; ++i) seed[4 * k + i] = (uint8_t)(x >> (8 * i));
+        }
+        seed_bytes(seed);
+    }
+    void seed_bytes(const uint8_t* seed) {
+        for (int i = 0; i < 8; ++i)
+            key[i] = (uint32_t)seed[4 * i] | ((uint32_t)seed[4 * i + 1] << 8) | ((uint32_t)seed[4 * i + 2] << 16) |
+                     ((uint32_t)seed[4 * i + 3] << 24);
+        counter = 0;
+        index = 64;
+    }
+    uint32_t next_u32() {
+        if (index >= 64) {
+            refill();
+            index = 0;
+        }
+        return results[index++];
+    }
+    uint64_t next_u64() {
+        if (index < 63) {
+            const uint64_t v = (uint64_t)results[index] | ((uint64_t)results[index + 1] << 32);
+            index += 2;
+            return v;
+        }
+        if (index >= 64) {
+            refill();
+            index = 2;
+            return (uint64_t)results[0] | ((uint64_t)results[1] << 32);
+        }
+        const uint64_t lo = results[63];
+        refill();
+        index = 1;
+        return lo | ((uint64_t)results[0] << 32);
+    }
+    uint8_t gen_u8_below3() {  // gen_range(0u8..3): UniformInt<u8> via u32
+        const uint32_t range = 3, umax = 0xFFFFFFFFu;
+        const uint32_t zone = umax - (umax - range + 1) % range;
+        for (;;) {
+            const uint64_t prod = (uint64_t)next_u32() * range;
+            if ((uint32_t)prod <= zone) return (uint8_t)(prod >> 32);
+        }
+    }
+    int64_t gen_i64_inclusive(int64_t lo, int64_t hi) {
+        const uint64_t range = (uint64_t)(hi - lo) + 1;
+        if (range == 0) return (int64_t)next_u64();
+        int lz = 0;
+        while (!((range << lz) >> 63)) ++lz;
+        const uint64_t zone = (range << lz) - 1;
+        for (;;) {
+            const u128 prod = (u128)next_u64() * range;
+            if ((uint64_t)prod <= zone) return lo + (int64_t)(uint64_t)(prod >> 64);
+        }
+    }
+};
+
+void chacha_error(OracleChaCha& r, uint32_t n, int kind, double param, int64_t* out) {
+    if (kind == 0) {  // BoundedUniform (error.rs:44-50)
+        const int64_t bound = (int64_t)param;
+        for (uint32_t i = 0; i < n; ++i) out[i] = bound == 0 ? 0 : r.gen_i64_inclusive(-bound, bound);
+        return;
+    }
+    // DiscreteGaussian table (error.rs:73-113), uniform_open_unit (:141-151)
+    const double sigma = param;
+    const int64_t tail = (int64_t)std::ceil(16.0 * sigma);
+    std::vector<std::pair<int64_t, double>> weights;
+    double total = 0.0;
+    for (int64_t x = -tail; x <= tail; ++x) {
+        const double xf = (double)x;
+        const double w = std::exp(-(xf * xf) / (2.0 * sigma * sigma));
+        weights.emplace_back(x, w);
+        total += w;
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint64_t v = r.next_u64() >> 11;
+        const double u = ((double)v + 0.5) * (1.0 / (double)(1ull << 53));
+        const double target = u * total;
+        double cumulative = 0.0;
+        int64_t pick = tail;
+        for (auto& xw : weights) {
+            cumulative += xw.second;
+            if (target < cumulative) {
+                pick = xw.first;
+                break;
+            }
+        }
+        out[i] = pick;
+    }
+}
+
+void chacha_uniform(OracleChaCha& r, uint32_t n, uint64_t q, uint64_t* out) {  // uniform.rs:12-30
+    const uint64_t threshold = (0 - q) % q;
+    uint32_t k = 0;
+    while (k < n) {
+        const uint64_t c = r.next_u64();
+        if (c >= threshold) out[k++] = c % q;
+    }
+}
+
+// Reference-order RLWE encryption into NTT-domain limbs (rns_key_switch.rs:818-850):
+// one logical error, then per limb a uniform a; b_ntt = NTT(t + e) - NTT(a) NTT(s).
+void chacha_encrypt_ntt(OracleChaCha& r, const u64* m, uint32_t L, uint32_t n, const std::vector<u64>& s_ntt,
+                        const u64* target, int kind, double param, u64* b_out, size_t b_stride, u64* a_out,
+                        size_t a_stride) {
+    std::vector<i64> e(n);
+    chacha_error(r, n, kind, param, e.data());
+    std::vector<u64> a(n), t(n);
+    for (uint32_t l = 0; l < L; ++l) {
+        chacha_uniform(r, n, m[l], a.data());
+        ntt_forward_poly(m[l], n, a.data());
+        for (uint32_t c = 0; c < n; ++c) t[c] = add_mod(target[(size_t)l * n + c], signed_mod(e[c], m[l]), m[l]);
+        ntt_forward_poly(m[l], n, t.data());
+        u64* bo = b_out + l * b_stride;
+        u64* ao = a_out + l * a_stride;
+        for (uint32_t c = 0; c < n; ++c) {
+            ao[c] = a[c];
+            bo[c] = sub_mod(t[c], mul_mod(a[c], s_ntt[(size_t)l * n + c], m[l]), m[l]);
+        }
+    }
+}
+
+void* oracle_chacha_new(uint64_t seed) {
+    auto* r = new OracleChaCha();
+    r->seed_u64(seed);
+    return r;
+}
+void* oracle_chacha_new_from_seed(const uint8_t* seed32) {
+    auto* r = new OracleChaCha();
+    r->seed_bytes(seed32);
+    return r;
+}
+void oracle_chacha_free(void* rng) { delete (OracleChaCha*)rng; }
+void oracle_chacha_words(void* rng, uint32_t* out, uint64_t n) {
+    for (uint64_t i = 0; i < n; ++i) out[i] = ((OracleChaCha*)rng)->next_u32();
+}
+uint64_t oracle_chacha_next_u64(void* rng) { return ((OracleChaCha*)rng)->next_u64(); }
+void oracle_chacha_ternary(void* rng, uint32_t n, int8_t* out) {  // secret_key.rs:25-40
+    auto& r = *(OracleChaCha*)rng;
+    for (;;) {
+        bool any = false;
+        for (uint32_t i = 0; i < n; ++i) {
+            const uint8_t v = r.gen_u8_below3();
+            out[i] = v == 0 ? 0 : (v == 1 ? 1 : -1);
+            any = any || v;
+        }
+        if (any) return;
+    }
+}
+void oracle_chacha_error(void* rng, uint32_t n, int kind, double param, int64_t* out) {
+    chacha_error(*(OracleChaCha*)rng, n, kind, param, out);
+}
+void oracle_chacha_uniform(void* rng, uint32_t n, uint64_t q, uint64_t* out) {
+    chacha_uniform(*(OracleChaCha*)rng, n, q, out);
+}
+
+void oracle_hybrid_key_generate_chacha(const uint64_t* q, uint32_t L, const uint64_t* p, uint32_t K, uint32_t n,
+                                       uint32_t base_log, const int8_t* secret, uint64_t exponent, int kind,
+                                       double param, void* rng, uint64_t* key) {
+    // hybrid_rns_galois_key.rs:61-170 with the stream of encrypt_rns_raw_prepared_with_cached_secret_ntt_rng
+    auto m = qp_moduli(q, L, p, K);
+    uint32_t LK = L + K, D = digit_count(q, L, base_log);
+    exponent %= 2ull * n;
+    auto s_ntt = secret_ntt(m.data(), LK, n, secret);
+    auto ts = secret_automorphism(secret, n, exponent);
+    std::vector<u64> pf(LK, 1), gf(LK, 1), target((size_t)LK * n);
+    for (uint32_t l = 0; l < LK; ++l)
+        for (uint32_t k = 0; k < K; ++k) pf[l] = mul_mod(pf[l], p[k] % m[l], m[l]);
+    for (uint32_t j = 0; j < D; ++j) {
+        for (uint32_t l = 0; l < LK; ++l) {
+            u64 mult = mul_mod(pf[l], gf[l], m[l]);
+            for (uint32_t c = 0; c < n; ++c) target[(size_t)l * n + c] = mul_mod(signed_mod(ts[c], m[l]), mult, m[l]);
+        }
+        u64* e0 = key + (size_t)j * LK * 2 * n;
+        chacha_encrypt_ntt(*(OracleChaCha*)rng, m.data(), LK, n, s_ntt, target.data(), kind, param, e0, 2 * n, e0 + n,
+                           2 * n);
+        for (uint32_t l = 0; l < LK; ++l) gf[l] = mul_mod(gf[l], (u64)(((u128)1 << base_log) % m[l]), m[l]);
+    }
+}
+
+void oracle_bounded_relin_key_generate_chacha(const uint64_t* q, uint32_t L, uint32_t n, uint32_t base_log,
+                                              const int8_t* secret, int kind, double param, void* rng,
+                                              uint64_t* key) {
+    // bounded_key_switch.rs:28-104: entry j = encrypt_rns_raw_with_distribution_ntt_rng(B^j s^2), coefficient domain
+    uint32_t D = digit_count(q, L, base_log);
+    auto s_ntt = secret_ntt(q, L, n, secret);
+    std::vector<u64> s2((size_t)L * n), target((size_t)L * n);
+    for (uint32_t l = 0; l < L; ++l) {
+        for (uint32_t c = 0; c < n; ++c) s2[(size_t)l * n + c] = mul_mod(s_ntt[(size_t)l * n + c], s_ntt[(size_t)l * n + c], q[l]);
+        ntt_inverse_poly(q[l], n, &s2[(size_t)l * n]);
+    }
+    for (uint32_t j = 0; j < D; ++j) {
+        for (uint32_t l = 0; l < L; ++l) {
+            u64 f = 1, bm = ((u128)1 << base_log) % q[l];
+            for (uint32_t t = 0; t < j; ++t) f = mul_mod(f, bm, q[l]);
+            for (uint32_t c = 0; c < n; ++c) target[(size_t)l * n + c] = mul_mod(s2[(size_t)l * n + c], f, q[l]);
+        }
+        u64* e0 = key + (size_t)j * 2 * L * n;
+        chacha_encrypt_ntt(*(OracleChaCha*)rng, q, L, n, s_ntt, target.data(), kind, param, e0, n, e0 + (size_t)L * n, n);
+        for (uint32_t l = 0; l < L; ++l) {
+            ntt_inverse_poly(q[l], n, e0 + (size_t)l * n);
+            ntt_inverse_poly(q[l], n, e0 + (size_t)(L + l) * n);
+        }
+    }
+}
+
+void oracle_encrypt_chacha(const uint64_t* q, uint32_t L, uint32_t n, const int8_t* secret, int kind, double param,
+                           void* rng, const uint64_t* message, uint64_t* ct) {
+    // rns_key_switch.rs:278-387: one logical error, then per limb a uniform a (coefficients),
+    // b = m + e - a s with a s the negacyclic product
+    auto& r = *(OracleChaCha*)rng;
+    std::vector<i64> e(n);
+    chacha_error(r, n, kind, param, e.data());
+    auto s_ntt = secret_ntt(q, L, n, secret);
+    std::vector<u64> a(n), as(n);
+    for (uint32_t l = 0; l < L; ++l) {
+        chacha_uniform(r, n, q[l], a.data());
+        std::copy(a.begin(), a.end(), ct + (size_t)(L + l) * n);
+        as = a;
+        ntt_forward_poly(q[l], n, as.data());
+        for (uint32_t c = 0; c < n; ++c) as[c] = mul_mod(as[c], s_ntt[(size_t)l * n + c], q[l]);
+        ntt_inverse_poly(q[l], n, as.data());
+        for (uint32_t c = 0; c < n; ++c)
+            ct[(size_t)l * n + c] =
+                sub_mod(add_mod(message[(size_t)l * n + c], signed_mod(e[c], q[l]), q[l]), as[c], q[l]);
+    }
+}
+
 }  // extern "C"

@@ -152,6 +152,29 @@ void oracle_encode(uint32_t degree, const double* slots, const uint64_t* moduli,
 void oracle_decode(uint32_t degree, const uint64_t* moduli, uint32_t limbs, const uint64_t* poly,
                    double scale, double* slots);
 
+/* Seeded ChaCha20 stream of the reference (rand_chacha 0.3.1 ChaCha20Rng,
+ * rand_core 0.6.4 seed_from_u64, rand 0.8 gen_range) and the samplers and
+ * key generation / encryption that consume it in the reference's order
+ * (rlwe/secret_key.rs:25-40, rlwe/error.rs:33-156, rlwe/uniform.rs:12-30,
+ * ckks/hybrid_rns_galois_key.rs:61-170, grafting/bounded_key_switch.rs:28-104,
+ * grafting/rns_key_switch.rs:278-387). error kind 0 bounded uniform, 1 Gaussian. */
+void* oracle_chacha_new(uint64_t seed);
+void* oracle_chacha_new_from_seed(const uint8_t* seed32);
+void oracle_chacha_free(void* rng);
+void oracle_chacha_words(void* rng, uint32_t* out, uint64_t n);
+uint64_t oracle_chacha_next_u64(void* rng);
+void oracle_chacha_ternary(void* rng, uint32_t n, int8_t* out);
+void oracle_chacha_error(void* rng, uint32_t n, int kind, double param, int64_t* out);
+void oracle_chacha_uniform(void* rng, uint32_t n, uint64_t q, uint64_t* out);
+void oracle_hybrid_key_generate_chacha(const uint64_t* q, uint32_t L, const uint64_t* p, uint32_t K, uint32_t degree,
+                                       uint32_t base_log, const int8_t* secret, uint64_t exponent, int kind,
+                                       double param, void* rng, uint64_t* key);
+void oracle_bounded_relin_key_generate_chacha(const uint64_t* q, uint32_t L, uint32_t degree, uint32_t base_log,
+                                              const int8_t* secret, int kind, double param, void* rng,
+                                              uint64_t* key);
+void oracle_encrypt_chacha(const uint64_t* q, uint32_t L, uint32_t degree, const int8_t* secret, int kind,
+                           double param, void* rng, const uint64_t* message, uint64_t* ct);
+
 #ifdef __cplusplus
 }
 #endif

@@ -67,6 +67,19 @@ _SIGS = {
     "oracle_bounded_relin_key_generate": (None, [u64p, U32, U32, U32, i8p, U64, F64, u64p]),
     "oracle_bounded_relinearize": (None, [u64p, U32, U32, U32, u64p, u64p, u64p]),
     "oracle_mul_plain": (None, [u64p, U32, U32, u64p, u64p, u64p]),
+    "oracle_chacha_new": (ctypes.c_void_p, [U64]),
+    "oracle_chacha_new_from_seed": (ctypes.c_void_p, [ctypes.c_char_p]),
+    "oracle_chacha_free": (None, [ctypes.c_void_p]),
+    "oracle_chacha_words": (None, [ctypes.c_void_p, u32p, U64]),
+    "oracle_chacha_next_u64": (U64, [ctypes.c_void_p]),
+    "oracle_chacha_ternary": (None, [ctypes.c_void_p, U32, i8p]),
+    "oracle_chacha_error": (None, [ctypes.c_void_p, U32, ctypes.c_int, F64, i64p]),
+    "oracle_chacha_uniform": (None, [ctypes.c_void_p, U32, U64, u64p]),
+    "oracle_hybrid_key_generate_chacha": (None, [u64p, U32, u64p, U32, U32, U32, i8p, U64, ctypes.c_int, F64,
+                                                 ctypes.c_void_p, u64p]),
+    "oracle_bounded_relin_key_generate_chacha": (None, [u64p, U32, U32, U32, i8p, ctypes.c_int, F64,
+                                                        ctypes.c_void_p, u64p]),
+    "oracle_encrypt_chacha": (None, [u64p, U32, U32, i8p, ctypes.c_int, F64, ctypes.c_void_p, u64p, u64p]),
     "oracle_slots_to_coefficients": (None, [U32, f64p, f64p]),
     "oracle_coefficients_to_slots": (None, [U32, f64p, f64p]),
     "oracle_encode": (None, [U32, f64p, u64p, U32, F64, u64p]),
@@ -319,3 +332,63 @@ class Oracle:
         c = arr(coeffs, np.float64); n = len(c); out = np.zeros((n // 2, 2), np.float64)
         self.L.oracle_coefficients_to_slots(n, P(c, f64p), P(out, f64p))
         return out[:, 0] + 1j * out[:, 1]
+
+
+class OracleChaCha:
+    """The oracle's restatement of the reference's ChaCha20Rng stream and samplers."""
+
+    def __init__(self, seed=None, seed32=None):
+        self.L = lib()
+        self.h = self.L.oracle_chacha_new_from_seed(bytes(seed32)) if seed32 is not None else \
+            self.L.oracle_chacha_new(int(seed) & (2**64 - 1))
+
+    def words(self, n):
+        out = np.zeros(n, np.uint32)
+        self.L.oracle_chacha_words(self.h, P(out, u32p), n)
+        return out
+
+    def next_u64(self):
+        return int(self.L.oracle_chacha_next_u64(self.h))
+
+    def ternary_secret(self, n):
+        out = np.zeros(n, np.int8)
+        self.L.oracle_chacha_ternary(self.h, n, P(out, i8p))
+        return out
+
+    def error(self, n, kind, param):
+        out = np.zeros(n, np.int64)
+        self.L.oracle_chacha_error(self.h, n, kind, float(param), P(out, i64p))
+        return out
+
+    def uniform_residues(self, n, q):
+        out = np.zeros(n, np.uint64)
+        self.L.oracle_chacha_uniform(self.h, n, int(q), P(out))
+        return out
+
+    def hybrid_key(self, q, p, secret, exponent, base_log, kind=1, param=3.2):
+        q = arr(q); p = arr(p); s = arr(secret, np.int8); n = len(s)
+        D = int(self.L.oracle_bounded_digit_count(P(q), len(q), base_log))
+        key = np.zeros((D, len(q) + len(p), 2, n), np.uint64)
+        self.L.oracle_hybrid_key_generate_chacha(P(q), len(q), P(p), len(p), n, base_log, P(s, i8p), int(exponent),
+                                                 kind, float(param), self.h, P(key))
+        return key
+
+    def relin_key(self, q, secret, base_log, kind=1, param=3.2):
+        q = arr(q); s = arr(secret, np.int8); n = len(s)
+        D = int(self.L.oracle_bounded_digit_count(P(q), len(q), base_log))
+        key = np.zeros((D, 2, len(q), n), np.uint64)
+        self.L.oracle_bounded_relin_key_generate_chacha(P(q), len(q), n, base_log, P(s, i8p), kind, float(param),
+                                                        self.h, P(key))
+        return key
+
+    def encrypt(self, q, secret, message, kind=1, param=3.2):
+        q = arr(q); s = arr(secret, np.int8); m = arr(message); n = len(s)
+        ct = np.zeros((2, len(q), n), np.uint64)
+        self.L.oracle_encrypt_chacha(P(q), len(q), n, P(s, i8p), kind, float(param), self.h, P(m), P(ct))
+        return ct
+
+    def __del__(self):
+        try:
+            self.L.oracle_chacha_free(self.h)
+        except Exception:
+            pass
