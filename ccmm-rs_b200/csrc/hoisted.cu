@@ -584,7 +584,10 @@ constexpr u32 kBStage = kTS * kBSlot;          // 17472
 constexpr u32 kOffY = kARing * kAStage;                    // A ring
 constexpr u32 kOffB = kOffY + kRing * kYStage;             // 16 KB of Y
 constexpr u32 kOffCnt = kOffB + kBStages * kBStage;        // correction counts [c][g], g < kCntKeys
-constexpr int kCntKeys = 256;
+#ifndef CKKS_TC_CNT_KEYS
+#define CKKS_TC_CNT_KEYS 256
+#endif
+constexpr int kCntKeys = CKKS_TC_CNT_KEYS;  // keys whose correction counts are staged in shared memory
 constexpr u32 kSmemBytes = kOffCnt + kCt * kCntKeys * 4;   // 197 KB (16 A slots, 2 B stages): one CTA per SM
 static_assert(kSmemBytes <= 227 * 1024, "shared memory per CTA");
 constexpr u32 kTmemCols = 512;
@@ -654,9 +657,12 @@ __device__ __forceinline__ bool group_any(int id, int n, bool v) {
     return r != 0;
 }
 
-// 8-byte asynchronous global -> shared copy; src_bytes 0 stores zeros
+// 8- and 16-byte asynchronous global -> shared copies; src_bytes 0 stores zeros
 __device__ __forceinline__ void cp8(u32 dst, const void* src, u32 src_bytes) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp16(u32 dst, const void* src, u32 src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
@@ -761,11 +767,11 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
         const int ptid = tid - kProdWarp0 * 32;
         const int grp = ptid / kGrp, gtid = ptid % kGrp, bar = kBarGrp0 + grp;
         // A: one bulk copy of the item's packed key block (thread 0 of the group);
-        // Y copies: slot pi, digit pjj of the ciphertexts gtid / 16 and
-        // gtid / 16 + 8 (Y word gtid and gtid + 128 of the stage).
-        static_assert(kGrp == 128 && kTS * kJc * 8 == kGrp, "producer work split");
-        const int pi = gtid & 3, pjj = (gtid >> 2) & 3;
-        const int yc = gtid >> 4;
+        // Y copies: 16 bytes (slots 2 ph, 2 ph + 1) of digit pjj of ciphertext
+        // yc = gtid / 8 (Y words 2 gtid, 2 gtid + 1 of the stage, [c][jj][i]).
+        static_assert(kGrp == 128 && kTS * kJc * kCt == 2 * kGrp, "producer work split");
+        const int ph = gtid & 1, pjj = (gtid >> 1) & 3;
+        const int yc = gtid >> 3;
         const u32 a_bytes = (u32)rg * 1024u;
         int last_issued = -1;  // last item whose block this thread copied (thread 0 of a group)
         // A block of item t into A slot t % kARing (thread 0 of the group)
@@ -790,15 +796,13 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                 // digit j < D: the digit transform; j == D: NTT(b) on the Q limbs
                 const int j = it.ch * kJc + pjj;
                 const bool jok = j < D, bok = j == D && l < Lq;
-                const u64* ysrc = jok ? Yhat + ((((size_t)j * LK + l) << log_n) + s0 + pi)
-                                      : bok ? Bhat + (((size_t)l << log_n) + s0 + pi) : Yhat;
+                const u64* ysrc = jok ? Yhat + ((((size_t)j * LK + l) << log_n) + s0 + 2 * ph)
+                                      : bok ? Bhat + (((size_t)l << log_n) + s0 + 2 * ph) : Yhat;
                 const size_t ystep = jok ? y_stride : b_stride;
                 const u32 y_st = sbase + kOffY + (u32)(t & (kRing - 1)) * kYStage;
-#pragma unroll
-                for (int h = 0; h < 2; ++h)
-                    if (yc + 8 * h < n_ct)
-                        cp8(y_st + (u32)(gtid + kGrp * h) * 8, ysrc + (jok || bok ? (yc + 8 * h) * ystep : 0),
-                            jok || bok ? 8u : 0u);
+                // 16-byte aligned: s0 is a multiple of 4 slots and the workspaces are 256-byte aligned
+                if (yc < n_ct)
+                    cp16(y_st + (u32)gtid * 16, ysrc + (jok || bok ? yc * ystep : 0), jok || bok ? 16u : 0u);
             }
             cp_commit();
         };

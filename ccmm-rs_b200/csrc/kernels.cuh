@@ -31,6 +31,13 @@ int32_t bounded_decompose_launch(ckks_ctx* ctx, const u64* poly, u32 n_polys, u3
 int32_t digits_automorphism_launch(ckks_ctx* ctx, const i64* in, i64* out, u32 n_polys, u32 D, u32 base_log, u64 k,
                                    cudaStream_t st);
 // Forward NTT of signed digits lifted to every limb of `lm` ([D][limbs][N] out).
+// Bounded relinearization key sum from signed digits [n_ct][D][N] with the
+// digit transforms' second pass fused into the key MAC (FP64 networks: every
+// limb's prime below 2^50, transform halves of up to 2^8 points).
+// mid: workspace [n_ct][D][L][N]; key [D][2][L][N]; base, acc [n_ct][2][L][N].
+bool ntt_relin_fused_supported(const ckks_ctx* ctx, u32 L);
+int32_t ntt_relin_fused_launch(ckks_ctx* ctx, const i64* digits, u64* mid, const u64* key, const u64* base, u64* acc,
+                               u32 n_ct, u32 L, u32 D, cudaStream_t st);
 int32_t ntt_forward_digits_launch(ckks_ctx* ctx, const i64* digits, u64* out, u32 D, LimbMap lm, u32 limbs,
                                   cudaStream_t st);
 

@@ -92,7 +92,10 @@ int32_t multiply_relin_rescale_launch(ckks_ctx* ctx, const ckks_ksk* key, const 
 // Bounded relinearization key sum: c2 [n][L][N] coefficient domain; acc01
 // [n][2][L][N] holds the NTT-domain c0, c1 on entry and the NTT-domain
 // relinearized (b, a) on return.
-int32_t relin_core_launch(ckks_ctx* ctx, const ckks_ksk* key, const u64* c2, u64* acc01, u32 n, cudaStream_t st);
+// relin_fused: bounded keys over FP64-network limbs take the fused digit-transform
+// + key MAC kernel (false: separate transform and MAC launches, the same words).
+int32_t relin_core_launch(ckks_ctx* ctx, const ckks_ksk* key, const u64* c2, u64* acc01, u32 n, cudaStream_t st,
+                          bool relin_fused = true);
 int32_t mul_plain_launch(ckks_ctx* ctx, const u64* ct_in, const u64* plain_ntt, u64* out, u32 n_ct, u32 L,
                          bool plain_per_ct, cudaStream_t st);
 

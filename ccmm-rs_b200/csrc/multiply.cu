@@ -141,7 +141,8 @@ size_t relin_words_per_ct(const ckks_ctx* ctx, const ckks_ksk* key) {
 
 // c2: [n][L][N] coefficient domain; acc01: [n][2][L][N] NTT-domain c0, c1 on
 // entry, the NTT-domain relinearized (b, a) on return.
-int32_t relin_core_launch(ckks_ctx* ctx, const ckks_ksk* key, const u64* c2, u64* acc01, u32 n, cudaStream_t st) {
+int32_t relin_core_launch(ckks_ctx* ctx, const ckks_ksk* key, const u64* c2, u64* acc01, u32 n, cudaStream_t st,
+                          bool relin_fused) {
     const u32 L = key->q_limbs, D = key->D, N = ctx->n;
     Workspace<i64> dg;
     Workspace<u64> Y;
@@ -156,6 +157,8 @@ int32_t relin_core_launch(ckks_ctx* ctx, const ckks_ksk* key, const u64* c2, u64
     } else {
         if ((rc = dg.alloc((size_t)n * D * N, st))) return rc;
         if ((rc = bounded_decompose_launch(ctx, c2, n, L, key->base_log, dg.p, nullptr, st))) return rc;
+        if (relin_fused && ntt_relin_fused_supported(ctx, L))  // digit transforms stay on chip
+            return ntt_relin_fused_launch(ctx, dg.p, Y.p, key->d_entries, acc01, acc01, n, L, D, st);
         if ((rc = ntt_forward_digits_launch(ctx, dg.p, Y.p, n * D, LimbMap::range(0, L), L, st))) return rc;
     }
     dim3 g((N + kT - 1) / kT, L, (n + kRelinGroup - 1) / kRelinGroup);

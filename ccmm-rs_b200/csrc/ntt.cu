@@ -514,6 +514,97 @@ k_inv2(const u64* src, u64* dst, const NttTab* __restrict__ tabs,
     }
 }
 
+// Forward pass 2 of relinearization digit transforms fused with the key sum
+// (grafting/bounded_key_switch.rs:139-223): for ciphertext c (grid x, so
+// consecutive CTAs share the key tile in L2), a tile of C units and limb l,
+// every digit j's pass-1 output is finished in registers (FP64 network) and
+// multiplied by the key's b and a words at the same NTT positions. The exact
+// products (nttf::mulmod, Wp = fl(W fl(1/q)): |W/q - Wp| <= 2^-52, so for a
+// centred |v| < 2^49 the quotient is off by under 0.9 and |r| < 0.9 q) are
+// summed in doubles, centred every 8 digits (|sum| < 0.5 q + 8 * 0.9 q < 2^53),
+// and base (c0, c1 in the NTT domain) is added once: the same canonical
+// residues as k_fwd2 followed by k_relin_mac, with the digit transforms never
+// written to HBM.
+//   mid  [n_ct][D][L][N]  pass-1 outputs of the digits (k_fwd1<_, true>)
+//   key  [D][2][L][N]     NTT-domain relinearization key
+//   base, acc [n_ct][2][L][N] (may alias)
+template <int LOG_M>
+__global__ void __launch_bounds__(kMaxThreads, LOG_M <= 5 ? 3 : 2)
+k_fwd2_relin(const u64* __restrict__ mid, const u64* __restrict__ key, const u64* base, u64* acc,
+             const NttTab* __restrict__ tabs, int L, int D, int log_a, int log_c) {
+    using S = Split<LOG_M>;
+    extern __shared__ u64 sm[];
+    const int C = 1 << log_c, tid = threadIdx.x;
+    const size_t ct = blockIdx.x;
+    const int b0 = blockIdx.y << log_c;
+    const int limb = blockIdx.z;
+    const int log_n = LOG_M + log_a;
+    const NttTab& T = tabs[limb];
+    const double2* tab = stage_table_f64(sm + (S::M << log_c), T.fB, S::M);
+    const double qd = T.qd, qinv = T.qinv;
+    double* smd = reinterpret_cast<double*>(sm);
+    auto twf = [&](int s, u32 blk) { return tab[(1u << s) + blk]; };
+    const int c = tid & (C - 1);
+    const bool act_b = tid < (C << S::LR1);
+    const int g = tid >> log_c;
+    double sb[S::R2], sa[S::R2];
+#pragma unroll
+    for (int e = 0; e < S::R2; ++e) sb[e] = sa[e] = 0.0;
+    __syncthreads();
+    for (int j = 0; j < D; ++j) {
+        const size_t in_j = ((ct * D + j) * L + limb) << log_n;
+        if (tid < (C << S::LR2)) {
+            const int i0 = tid >> log_c;
+            double x[S::R1];
+#pragma unroll
+            for (int e = 0; e < S::R1; ++e)
+                x[e] = __longlong_as_double((long long)mid[in_j + ((size_t)(i0 + S::R2 * e) << log_a) + b0 + c]);
+            nttf::ct_stages<S::LR1>(x, 0, 0, twf, qd);
+#pragma unroll
+            for (int e = 0; e < S::R1; ++e) smd[((i0 + S::R2 * e) << log_c) + c] = nttf::center(x[e], qd, qinv);
+        }
+        __syncthreads();
+        if (act_b) {
+            double y[S::R2];
+#pragma unroll
+            for (int e = 0; e < S::R2; ++e) y[e] = smd[((S::R2 * g + e) << log_c) + c];
+            nttf::ct_stages<S::LR2>(y, S::LR1, g, twf, qd);
+            const u64* kb = key + ((((size_t)j * 2) * L + limb) << log_n) + b0 + c;
+            const u64* ka = kb + ((size_t)L << log_n);
+#pragma unroll
+            for (int e = 0; e < S::R2; ++e) {
+                const size_t pos = (size_t)brev(S::R2 * g + e, LOG_M) << log_a;
+                const double v = nttf::center(y[e], qd, qinv);
+                const double wb = nttf::from_u52(__ldg(kb + pos)), wa = nttf::from_u52(__ldg(ka + pos));
+                sb[e] = __dadd_rn(sb[e], nttf::mulmod(v, wb, __dmul_rn(wb, qinv), qd));
+                sa[e] = __dadd_rn(sa[e], nttf::mulmod(v, wa, __dmul_rn(wa, qinv), qd));
+            }
+            if ((j & 7) == 7) {
+#pragma unroll
+                for (int e = 0; e < S::R2; ++e) {
+                    sb[e] = nttf::center(sb[e], qd, qinv);
+                    sa[e] = nttf::center(sa[e], qd, qinv);
+                }
+            }
+        }
+        __syncthreads();  // smd is rewritten by the next digit
+    }
+    if (act_b) {
+        const size_t ob0 = ((ct * 2 * L + limb) << log_n) + b0 + c, oa0 = ob0 + ((size_t)L << log_n);
+#pragma unroll
+        for (int e = 0; e < S::R2; ++e) {
+            const size_t pos = (size_t)brev(S::R2 * g + e, LOG_M) << log_a;
+            double vb = sb[e], va = sa[e];
+            if (base) {
+                vb = __dadd_rn(vb, nttf::from_u52(base[ob0 + pos]));
+                va = __dadd_rn(va, nttf::from_u52(base[oa0 + pos]));
+            }
+            acc[ob0 + pos] = nttf::to_canonical(vb, qd, qinv);
+            acc[oa0 + pos] = nttf::to_canonical(va, qd, qinv);
+        }
+    }
+}
+
 // columns per CTA: min(16, available, 256 / RMAX), or the tuned choice `pref`
 // when it is within those limits
 template <int LOG_M>
@@ -627,6 +718,48 @@ int32_t ntt_forward_digits_launch(ckks_ctx* ctx, const i64* digits, u64* out, u3
     const int la = ctx->log_n1, lb = ctx->log_n2;
     if (int32_t rc = pass(1, la, digits, out, ctx->d_tabs, lm, limbs, D, lb, st, InvBase{}, ctx->ntt_log_c[1])) return rc;
     if (int32_t rc = pass(2, lb, out, out, ctx->d_tabs, lm, limbs, D, la, st, InvBase{}, ctx->ntt_log_c[2])) return rc;
+    CKKS_CUDA_TRY(cudaGetLastError());
+    return CKKS_OK;
+}
+
+bool ntt_relin_fused_supported(const ckks_ctx* ctx, u32 L) {
+    if (ctx->log_n2 < 2 || ctx->log_n2 > 8) return false;
+    for (u32 l = 0; l < L; ++l)
+        if (!ctx->h_tabs[l].f64) return false;
+    return true;
+}
+
+// Bounded relinearization key sum of n_ct ciphertexts from their signed digits
+// [n_ct][D][N]: digit lift + forward pass 1 into mid, then k_fwd2_relin.
+int32_t ntt_relin_fused_launch(ckks_ctx* ctx, const i64* digits, u64* mid, const u64* key, const u64* base, u64* acc,
+                               u32 n_ct, u32 L, u32 D, cudaStream_t st) {
+    if (n_ct == 0) return CKKS_OK;
+    const int la = ctx->log_n1, lb = ctx->log_n2;
+    const LimbMap lm = LimbMap::range(0, L);
+    if (int32_t rc = pass(1, la, digits, mid, ctx->d_tabs, lm, L, n_ct * D, lb, st, InvBase{}, ctx->ntt_log_c[1]))
+        return rc;
+    if (n_ct > 0x7FFFFFFFu || L > 65535) {
+        ckks_set_error("relinearization: batch outside the launch limits");
+        return CKKS_ERR_BAD_ARG;
+    }
+#define CKKS_RELIN_FUSED(LM)                                                                                  \
+    do {                                                                                                      \
+        const int lc = pick_log_c<LM>(la, ctx->ntt_log_c[2]);                                                 \
+        const size_t smem = (sizeof(u64) << (LM + lc)) + 2 * sizeof(u64) * (1u << LM);                        \
+        dim3 grid(n_ct, 1u << (la - lc), L);                                                                  \
+        k_fwd2_relin<LM><<<grid, Split<LM>::RMAX << lc, smem, st>>>(mid, key, base, acc, ctx->d_tabs, (int)L, \
+                                                                    (int)D, la, lc);                         \
+    } while (0)
+    switch (lb) {
+        case 2: CKKS_RELIN_FUSED(2); break;
+        case 3: CKKS_RELIN_FUSED(3); break;
+        case 4: CKKS_RELIN_FUSED(4); break;
+        case 5: CKKS_RELIN_FUSED(5); break;
+        case 6: CKKS_RELIN_FUSED(6); break;
+        case 7: CKKS_RELIN_FUSED(7); break;
+        default: CKKS_RELIN_FUSED(8); break;
+    }
+#undef CKKS_RELIN_FUSED
     CKKS_CUDA_TRY(cudaGetLastError());
     return CKKS_OK;
 }

@@ -75,6 +75,25 @@ def test_relinearize_bit_exact(oracle, cuda, small, base_log):
             assert np.array_equal(got[c], oracle.relinearize(q, quad[c], key_ref, base_log)), (count, c)
 
 
+def test_relinearize_ccmm_shape_bit_exact(oracle, cuda):
+    # N=2^15, 14 x 50-bit limbs, base 2^20 (36 digits): the CCMM configuration's
+    # relinearization, whose digit transforms are finished inside the key MAC
+    log_n, L, base_log = 15, 14, 20
+    n = 1 << log_n
+    q = [int(x) for x in oracle.primes_below_bits(50, n, L)]
+    ctx = cb.Context(log_n, q)
+    rng = np.random.default_rng(77)
+    s = rng.integers(-1, 2, n).astype(np.int8)
+    key = cb.KeySwitchKey.relin_generate(ctx, L, base_log, s, seed=5)
+    key_coef = oracle.ntt_inverse(q, key.download().reshape(-1, L, n)).reshape(-1, 2, L, n)
+    count = 3
+    quad = np.stack([np.stack([np.stack([rng.integers(0, m, n, dtype=np.uint64) for m in q]) for _ in range(3)])
+                     for _ in range(count)])
+    got = host(cb.relinearize(ctx, key, dev(quad)))
+    for c in (0, count - 1):
+        assert np.array_equal(got[c], oracle.relinearize(q, quad[c], key_coef, base_log)), c
+
+
 def test_multiply_relin_rescale_bit_exact_and_decodes(oracle, cuda, small):
     n, q, p, ctx = small
     rng = np.random.default_rng(7)
