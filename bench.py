@@ -36,6 +36,10 @@ ciphertexts per image at N=2^16 (24 x 50-bit Q, 3 x 60-bit P), with the
 radix-4 diagonal-rotation schedule: 4 row and 4 column stages, each
 sum(diagonal * rotation) + rescale. One step = 8 images. Metric: images/s.
 
+Workload "park": the Park Mod-PP-MM (ccmm/park.rs:1634-1647) of two 4096 x 4096
+u64 residue matrices mod 0x7ffff6001 (the largest size and the modulus of the
+reference's characterization binary). One step = one product. Metric: products/s.
+
 Workload "multiply": the plain CKKS chain at N=2^12 (q = 60 + 40 + 40 bits,
 P = 60 bits, the reference's prime search): HMult -> bounded relinearization
 (base 2^20) -> rescale -> key-switched rotation by one slot, for 64
@@ -1197,12 +1201,103 @@ def launch_replicas(args):
     os.execv(sys.executable, cmd)
 
 
+PARK_N = 4096
+PARK_Q = 0x7ffff6001  # research_profile_4096's first modulus, the reference characterization's
+
+
+def bench_park_gpu(args, world, rank, local):
+    """Park Mod-PP-MM (ccmm/park.rs:1634-1647) at n = 4096 (the reference's
+    characterization sizes run 256 .. 4096, src/bin/park_mod_pp_mm_characterization.rs):
+    square u64 matrices of residues, exact (lhs x rhs) mod q per step."""
+    import torch
+    import ckks_b200 as cb
+    dev = torch.device("cuda", local)
+    n, q = PARK_N, PARK_Q
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(77 + rank)
+    A = torch.empty((n, n), dtype=torch.int64, device=dev).random_(0, q, generator=gen)
+    B = torch.empty((n, n), dtype=torch.int64, device=dev).random_(0, q, generator=gen)
+    C = torch.empty((n, n), dtype=torch.int64, device=dev)
+    st = torch.cuda.current_stream()
+
+    def step():
+        cb.park_mod_pp_mm(A, B, q, out=C)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(st)
+    for _ in range(args.steps):
+        step()
+    t1.record(st)
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = t0.elapsed_time(t1)
+    clk = clocks.stop()
+    ms_max = max_over_ranks(world, ms)
+    value = args.steps * world / (ms_max / 1000.0)
+    # parity of sampled outputs against the oracle (outside the timed region)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import Oracle
+    o = Oracle()
+    a, b, c = cb.to_numpy_u64(A), cb.to_numpy_u64(B), cb.to_numpy_u64(C)
+    rows = [0, 1777, n - 1]
+    mism = sum(int(np.count_nonzero(o.park_mod_pp_mm(a[r:r + 1], b, q) != c[r:r + 1])) for r in rows)
+    # end to end through the host-buffer call
+    t = time.perf_counter()
+    cb.park_mod_pp_mm(a, b, q)
+    e2e_s = time.perf_counter() - t
+    peak, kind = peaks()
+    # the dominant (only) kernel is integer-multiply bound: n^3 exact 64 x 64 -> 128-bit
+    # products; memory traffic (3 n^2 words) is negligible, so the roofline is the product rate
+    prods = float(n) ** 3
+    return {"metric": "Park Mod-PP-MM/s (n=4096 square, modulus 0x7ffff6001, bit-exact)", "value": value,
+            "unit": "products/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded uniform residues)",
+            "config": {"workload": "Park Mod-PP-MM, 4096 x 4096 by 4096 x 4096, u64 residues mod 0x7ffff6001",
+                       "n": n, "modulus": q, "l2": "operands 134 MB each, above L2"},
+            "roofline": {"bound": "integer multiply", "achieved": prods / (ms_max / args.steps / 1000.0) / 1e9,
+                         "unit": "G exact modular MAC/s", "peak": None, "frac": None, "traffic": None,
+                         "kernel": "k_park_mm (192-bit exact dot products)"},
+            "e2e": {"value": 1.0 / e2e_s, "unit": "products/s", "h2d_bytes_per_step": 2 * n * n * 8,
+                    "d2h_bytes_per_step": n * n * 8, "path": "ckks_park_mod_pp_mm_host"},
+            "parity": {"words_compared": len(rows) * n, "mismatches": mism,
+                       "what": "three full output rows against the oracle's Reference backend"},
+            "gpu_launches": args.steps, "clocks": clk}
+
+
+def park_cpu_sample(threads):
+    """The oracle's Reference backend (u128 accumulator reduced every term) on an
+    n = 512 product, one row block per thread; scaled to n = 4096 by n^3."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import Oracle
+    import concurrent.futures as cf
+    o = Oracle()
+    m = 512
+    rng = np.random.default_rng(3)
+    a = rng.integers(0, PARK_Q, (m, m), dtype=np.uint64)
+    b = rng.integers(0, PARK_Q, (m, m), dtype=np.uint64)
+    blocks = np.array_split(np.arange(m), threads)
+    t = time.perf_counter()
+    with cf.ThreadPoolExecutor(threads) as ex:
+        list(ex.map(lambda r: o.park_mod_pp_mm(np.ascontiguousarray(a[r]), b, PARK_Q), blocks))
+    dt = time.perf_counter() - t
+    scale = (m / PARK_N) ** 3
+    return scale / dt, "one 512 x 512 product over %d threads in %.2f s, scaled by (512/4096)^3" % (threads, dt)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="rotation", choices=["rotation", "ntt", "multiply", "ccmm", "fft2"])
+    ap.add_argument("--workload", default="rotation", choices=["rotation", "ntt", "multiply", "ccmm", "fft2", "park"])
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     # rotation workload sizes (defaults: the headline configuration; smaller
     # values only for profiling captures that must stay within a few GB)
@@ -1237,6 +1332,19 @@ def main():
             threads = os.cpu_count() or 1
             v, sample = fft2_cpu_sample(threads)
             line["cpu_baseline"] = {"value": v, "unit": "images/s", "cores": threads, "kind": "port",
+                                    "sample": sample}
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    if args.workload == "park":
+        line = bench_park_gpu(args, world, rank, local)
+        if rank == 0 and world == 1:
+            threads = os.cpu_count() or 1
+            v, sample = park_cpu_sample(threads)
+            line["cpu_baseline"] = {"value": v, "unit": "products/s", "cores": threads, "kind": "port",
                                     "sample": sample}
         if rank == 0:
             print(json.dumps(line), flush=True)

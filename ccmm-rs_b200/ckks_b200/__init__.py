@@ -85,6 +85,8 @@ _SIGS = {
     "ckks_diag_stage": (I32, [VP, ctypes.POINTER(VP), U32, I32, VP, VP, VP, U32, U32, I32, VP]),
     "ckks_ccmm_structured": (I32, [VP, VP, VP, VP, VP, U32, U32, U32, VP]),
     "ckks_fft_stage_multi": (I32, [VP, ctypes.POINTER(VP), U32, u32p, U32, VP, VP, U32, VP, U32, U32, VP]),
+    "ckks_park_mod_pp_mm": (I32, [VP, VP, VP, U32, U32, U32, U64, VP]),
+    "ckks_park_mod_pp_mm_host": (I32, [u64p, u64p, u64p, U32, U32, U32, U64]),
     "ckks_rng_create": (I32, [U64, ctypes.POINTER(VP)]),
     "ckks_rng_create_from_seed": (I32, [ctypes.c_char_p, ctypes.POINTER(VP)]),
     "ckks_rng_destroy": (I32, [VP]),
@@ -443,6 +445,28 @@ def encrypt_rng(ctx, q_limbs, message, secret, rng, kind=ChaCha20Rng.GAUSSIAN, p
     out = np.zeros((2, q_limbs, ctx.n), np.uint64)
     check(lib().ckks_encrypt_rng_host(ctx.handle, q_limbs, m.ctypes.data_as(u64p), s.ctypes.data_as(i8p), kind,
                                       float(param), rng.handle, out.ctypes.data_as(u64p)))
+    return out
+
+
+def park_mod_pp_mm(lhs, rhs, modulus, out=None, stream=None):
+    """park_mod_pp_mm (ccmm/park.rs:1634-1647): (lhs x rhs) mod modulus.
+
+    lhs, rhs: row-major u64 matrices as torch CUDA int64 tensors (device path)
+    or numpy uint64 arrays (host path, synchronous)."""
+    if isinstance(lhs, np.ndarray):
+        a = np.ascontiguousarray(lhs, np.uint64); b = np.ascontiguousarray(rhs, np.uint64)
+        if a.ndim != 2 or b.ndim != 2 or a.shape[1] != b.shape[0]:
+            raise ValueError("park_mod_pp_mm: shapes do not chain")
+        c = np.zeros((a.shape[0], b.shape[1]), np.uint64)
+        check(lib().ckks_park_mod_pp_mm_host(a.ctypes.data_as(u64p), b.ctypes.data_as(u64p), c.ctypes.data_as(u64p),
+                                             a.shape[0], a.shape[1], b.shape[1], int(modulus)))
+        return c
+    import torch
+    if lhs.dim() != 2 or rhs.dim() != 2 or lhs.shape[1] != rhs.shape[0]:
+        raise ValueError("park_mod_pp_mm: shapes do not chain")
+    out = torch.empty((lhs.shape[0], rhs.shape[1]), dtype=torch.int64, device=lhs.device) if out is None else out
+    check(lib().ckks_park_mod_pp_mm(_dptr(lhs), _dptr(rhs), _dptr(out), lhs.shape[0], lhs.shape[1], rhs.shape[1],
+                                    int(modulus), _stream(stream)))
     return out
 
 

@@ -174,6 +174,13 @@ struct GaloisOut {
 };
 int32_t ntt_inverse_base_launch(ckks_ctx* ctx, const u64* in, u64* out, u32 n_polys, LimbMap lm, u32 limb_count,
                                 const InvBase& ib, cudaStream_t st, const GaloisOut& go = GaloisOut{});
+// Inverse NTT of key-switch accumulators [polys][q_limbs + K][N] with sigma
+// folded (go), fused with the FP64 ModDown into out [polys][q_limbs][N]
+// (ntt.cu). Supported when K <= 3, every Q prime is below 2^50 and the
+// transform halves have at most 2^8 points.
+bool ntt_inverse_moddown_supported(const ckks_ctx* ctx, u32 q_limbs);
+int32_t ntt_inverse_moddown_launch(ckks_ctx* ctx, const u64* in, u64* mid, double* words, u64* zp, u64* out,
+                                   u32 polys, u32 q_limbs, const GaloisOut& go, cudaStream_t st);
 // Times every admissible columns-per-CTA choice of the five NTT passes on a
 // scratch batch (limbs x polys) and keeps the fastest in ctx (ntt.cu).
 int32_t ntt_autotune(ckks_ctx* ctx, u32 limbs, u32 polys, cudaStream_t st);

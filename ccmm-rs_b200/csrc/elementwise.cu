@@ -5,6 +5,7 @@
 #include "context.cuh"
 #include "kernels.cuh"
 #include "ntt_core.cuh"
+#include "moddown_f64.cuh"
 
 namespace {
 
@@ -208,64 +209,12 @@ __global__ void __launch_bounds__(kT) k_mod_down_f64(const u64* __restrict__ in,
     u64 v[KT];
 #pragma unroll
     for (int i = 0; i < KT; ++i) v[i] = __ldg(x + ((size_t)(q_limbs + i) << log_n));
-#pragma unroll
-    for (int i = 0; i < KT; ++i) {  // mixed-radix digits (Garner), as k_mod_down
-        const u64 p = md.p[i];
-        u64 acc = 0;
-#pragma unroll
-        for (int j = 0; j < i; ++j) acc = add_mod(acc, mul_shoup(v[j], md.pp[i][j], md.pp_q[i][j], p), p);
-        v[i] = mul_shoup(sub_mod(v[i], acc, p), md.pinv[i], md.pinv_q[i], p);
-    }
-    bool neg = false, decided = false;  // value > floor(P/2) -> negative
-#pragma unroll
-    for (int i = KT - 1; i >= 0; --i) {
-        if (!decided && v[i] != md.half[i]) {
-            neg = v[i] > md.half[i];
-            decided = true;
-        }
-    }
-    // y = v0 + p0 (v1 + p1 v2) in three words
-    typedef unsigned __int128 u128;
-    u64 y0, y1 = 0, y2 = 0;
-    if (KT == 1) {
-        y0 = v[0];
-    } else if (KT == 2) {
-        const u128 a = (u128)v[1] * md.p[0] + v[0];
-        y0 = (u64)a;
-        y1 = (u64)(a >> 64);
-    } else {
-        const u128 tt = (u128)v[KT - 1] * md.p[1] + v[1];
-        const u128 a = (u128)(u64)tt * md.p[0] + v[0];
-        const u128 b = (u128)(u64)(tt >> 64) * md.p[0] + (u64)(a >> 64);
-        y0 = (u64)a;
-        y1 = (u64)b;
-        y2 = (u64)(b >> 64);
-    }
-    if (neg) {  // |y - P| = P - y
-        const u64 d0 = md.P3[0] - y0, b0 = md.P3[0] < y0;
-        const u64 t1 = md.P3[1] - y1, b1 = md.P3[1] < y1;
-        const u64 d1 = t1 - b0, b1b = t1 < b0;
-        const u64 d2 = md.P3[2] - y2 - (b1 | b1b);
-        y0 = d0;
-        y1 = d1;
-        y2 = d2;
-    }
-    const u64 m47 = (1ull << 47) - 1;
-    const double w0 = nttf::from_u52(y0 & m47), w1 = nttf::from_u52(((y0 >> 47) | (y1 << 17)) & m47),
-                 w2 = nttf::from_u52(((y1 >> 30) | (y2 << 34)) & m47), w3 = nttf::from_u52((y2 >> 13) & m47);
+    double w[4];
+    bool neg;
+    mdf::crt_words<KT>(v, md, w, neg);
     u64* o = out + dst + t;
-    for (int i = 0; i < q_limbs; ++i) {
-        const double* ci = fcs + i * 12;
-        const double q = ci[0], qinv = ci[1];
-        const double xd = nttf::from_u52(__ldg(x + ((size_t)i << log_n)));
-        const double r = nttf::mulmod(xd, ci[2], ci[3], q);
-        const double sm = __dadd_rn(__dadd_rn(nttf::mulmod(w0, ci[4], ci[5], q), nttf::mulmod(w1, ci[6], ci[7], q)),
-                                    __dadd_rn(nttf::mulmod(w2, ci[8], ci[9], q), nttf::mulmod(w3, ci[10], ci[11], q)));
-        double rr = nttf::center(neg ? __dadd_rn(r, sm) : __dsub_rn(r, sm), q, qinv);
-        if (flip) rr = -rr;
-        rr = rr < 0.0 ? __dadd_rn(rr, q) : rr;
-        o[(size_t)i << log_n] = (u64)__double_as_longlong(__dadd_rn(rr, nttf::kTwo52)) & 0xFFFFFFFFFFFFFull;
-    }
+    for (int i = 0; i < q_limbs; ++i)
+        o[(size_t)i << log_n] = mdf::limb(nttf::from_u52(__ldg(x + ((size_t)i << log_n))), w, neg, fcs + i * 12, flip);
 }
 
 }  // namespace

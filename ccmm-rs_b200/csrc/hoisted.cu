@@ -553,12 +553,21 @@ constexpr int kJc = 4;            // digits per chunk (K = 32 bytes)
 #ifndef CKKS_TC_PROD_WARPS
 #define CKKS_TC_PROD_WARPS 8
 #endif
+// Two CTAs per SM (CKKS_TC_TWO_CTAS): twice the warps to hide the latency
+// chains of each role, at half the rings, 72 registers a thread and one TMEM
+// accumulator buffer (256 columns) per CTA: the other CTA's MMAs overlap an
+// epilogue instead of the CTA's own second buffer.
+#ifndef CKKS_TC_TWO_CTAS
+#define CKKS_TC_TWO_CTAS 0
+#endif
+constexpr int kCtasPerSm = CKKS_TC_TWO_CTAS ? 2 : 1;
+constexpr int kAccBufs = CKKS_TC_TWO_CTAS ? 1 : 2;  // TMEM accumulator buffers (256 columns each)
 constexpr int kEpiWarps = CKKS_TC_EPI_WARPS;
 constexpr int kBStages = CKKS_TC_BSTAGES;      // B operand stages
-constexpr int kRing = 8;                       // Y prefetch ring depth
+constexpr int kRing = CKKS_TC_TWO_CTAS ? 4 : 8;  // Y prefetch ring depth
 constexpr int kAhead = kRing - kBStages;       // items whose Y is fetched ahead
 #ifndef CKKS_TC_ARING
-#define CKKS_TC_ARING 16
+#define CKKS_TC_ARING (CKKS_TC_TWO_CTAS ? 8 : 16)
 #endif
 constexpr int kARing = CKKS_TC_ARING;          // A (packed key block) ring depth
 constexpr int kAAhead = kARing - 2 * kBStages;  // items whose A block is fetched ahead
@@ -585,16 +594,19 @@ constexpr u32 kOffY = kARing * kAStage;                    // A ring
 constexpr u32 kOffB = kOffY + kRing * kYStage;             // 16 KB of Y
 constexpr u32 kOffCnt = kOffB + kBStages * kBStage;        // correction counts [c][g], g < kCntKeys
 #ifndef CKKS_TC_CNT_KEYS
-#define CKKS_TC_CNT_KEYS 256
+#define CKKS_TC_CNT_KEYS (CKKS_TC_TWO_CTAS ? 64 : 256)
 #endif
 constexpr int kCntKeys = CKKS_TC_CNT_KEYS;  // keys whose correction counts are staged in shared memory
 constexpr u32 kSmemBytes = kOffCnt + kCt * kCntKeys * 4;   // 197 KB (16 A slots, 2 B stages): one CTA per SM
-static_assert(kSmemBytes <= 227 * 1024, "shared memory per CTA");
-constexpr u32 kTmemCols = 512;
+static_assert(kSmemBytes * kCtasPerSm + kCtasPerSm * 2048 <= 228 * 1024, "shared memory per SM");
+constexpr u32 kTmemCols = 256 * kAccBufs;
 // Bounded waits: a waiting thread sleeps in mbarrier.try_wait (woken when the
 // phase completes, at the latest after kSuspendNs) so spinning warps do not
 // take issue slots from the working ones; it gives up after kWaitCycles.
-constexpr u32 kSuspendNs = 20000;
+#ifndef CKKS_TC_SUSPEND_NS
+#define CKKS_TC_SUSPEND_NS 20000
+#endif
+constexpr u32 kSuspendNs = CKKS_TC_SUSPEND_NS;
 constexpr long long kWaitCycles = 1ll << 31;   // about a second
 
 __device__ __forceinline__ u32 smem_u32(const void* p) { return (u32)__cvta_generic_to_shared(p); }
@@ -657,10 +669,7 @@ __device__ __forceinline__ bool group_any(int id, int n, bool v) {
     return r != 0;
 }
 
-// 8- and 16-byte asynchronous global -> shared copies; src_bytes 0 stores zeros
-__device__ __forceinline__ void cp8(u32 dst, const void* src, u32 src_bytes) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
-}
+// 16-byte asynchronous global -> shared copy; src_bytes 0 stores zeros
 __device__ __forceinline__ void cp16(u32 dst, const void* src, u32 src_bytes) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
 }
@@ -704,7 +713,7 @@ static_assert(kCt == (int)kGroupMax, "group size of the packed sets");
 // Same arguments and results as k_mac_tiled for bounded keys (up to 16
 // ciphertexts per call, any number of keys, D < 4096, N >= 4); the A operand
 // comes from the packed set of the keys (rg row groups per block).
-__global__ void __launch_bounds__(tc::kThreads, 1)
+__global__ void __launch_bounds__(tc::kThreads, tc::kCtasPerSm)
     k_mac_tc(const u64* __restrict__ Yhat, size_t y_stride, const u64* __restrict__ Bhat, size_t b_stride, int Lq,
              const u64* __restrict__ packed, int rg, const u64* const* __restrict__ keys,
              const u64* __restrict__ exps_inv, u64* __restrict__ acc, const NttTab* __restrict__ tabs, LimbMap lm,
@@ -717,7 +726,8 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     // ready / empty: B stages (producer group -> MMA, MMA -> producer group);
     // full / free: TMEM accumulator halves (MMA -> epilogue, epilogue -> MMA);
     // afull: A ring slots (bulk copy -> MMA)
-    __shared__ __align__(8) uint64_t s_ready[kBStages], s_empty[kBStages], s_full[2], s_free[2], s_afull[kARing];
+    __shared__ __align__(8) uint64_t s_ready[kBStages], s_empty[kBStages], s_full[kAccBufs], s_free[kAccBufs],
+        s_afull[kARing];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const u32 n = 1u << log_n;
     const int n_tiles_s = (int)(n / kTS), lts = log_n - 2;  // tiles per limb (a power of two)
@@ -735,7 +745,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_ready[i])), "r"(1));
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_empty[i])), "r"(1));
         }
-        for (int i = 0; i < 2; ++i) {
+        for (int i = 0; i < kAccBufs; ++i) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_full[i])), "r"(1));
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_free[i])), "r"(1));
         }
@@ -923,7 +933,8 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                 }
                 if (it.ch == 0) {
                     ++unit;
-                    if ((unit >= 2 && !wait_parity(smem_u32(&s_free[unit & 1]), (u32)(((unit >> 1) - 1) & 1))) ||
+                    if ((unit >= kAccBufs &&
+                         !wait_parity(smem_u32(&s_free[unit % kAccBufs]), (u32)(((unit / kAccBufs) - 1) & 1))) ||
                         s_abort) {
                         atomicExch(err, 3);
                         s_abort = 1;
@@ -933,14 +944,14 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                 }
                 const u32 a0 = sbase + (u32)(t & (kARing - 1)) * kAStage, b0 = sbase + kOffB + (u32)bst * kBStage;
                 // accumulator of slot i: columns 256 buf + 128 (i / 2), TMEM lanes 16 (i % 2) + ..
-                const u32 dbase = tmem + (u32)(256 * (unit & 1));
+                const u32 dbase = tmem + (u32)(256 * (unit % kAccBufs));
 #pragma unroll
                 for (int i = 0; i < kTS; ++i)
                     mma_i8(dbase + ((u32)(16 * (i & 1)) << 16) + (u32)(i >> 1) * 128u,
                            sdesc(a0 + i * kASlot, kLboA, kSboA), sdesc(b0 + i * kBSlot, kLboB, kSboB),
                            it.ch > 0 ? 1u : 0u);
                 commit(smem_u32(&s_empty[bst]));
-                if (it.ch == n_chunks - 1) commit(smem_u32(&s_full[unit & 1]));
+                if (it.ch == n_chunks - 1) commit(smem_u32(&s_full[unit % kAccBufs]));
                 last_t = t;
             }
             // drain: the last commit covers every MMA issued
@@ -965,7 +976,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
             const u32 s0 = (u32)(tile & (n_tiles_s - 1)) * kTS;
             const int g0 = kc * kKeys;
             const int gn = n_keys - g0 < kKeys ? n_keys - g0 : kKeys;
-            const bool bad = !wait_parity(smem_u32(&s_full[u & 1]), (u32)((u >> 1) & 1));
+            const bool bad = !wait_parity(smem_u32(&s_full[u % kAccBufs]), (u32)((u / kAccBufs) & 1));
             if (group_any(kBarEpi, kEpi, bad || s_abort)) {  // one decision for all epilogue threads
                 if (tid == 0) {
                     atomicExch(err, 4);
@@ -987,7 +998,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                 r_limb = l;
             }
             // lane L of warp qd: row m = 16 qd + (L % 16); slot 2 pp + (L / 16) of slot pair pp
-            const u32 taddr = tmem + ((u32)(32 * qd) << 16) + (u32)(256 * (u & 1));
+            const u32 taddr = tmem + ((u32)(32 * qd) << 16) + (u32)(256 * (u % kAccBufs));
             const int m = 16 * qd + (lane & 15);
             const int gl = m >> 1, comp = m & 1, g = g0 + gl;
             const bool row_ok = gl < gn;
@@ -1002,67 +1013,97 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
             // output word (c, s) at acc_row + c * c_stride + s
             u64* acc_row = acc + (((((size_t)g * 2 + comp) * LK + l) << log_n) + s0);
             const size_t c_stride = ((size_t)n_keys * 2 * LK) << log_n;
-            for (int pp = pp0; pp < pp1; ++pp) {
+            // the 4 ciphertexts cb .. cb + 3 of slot 2 pp + (lane / 16) of this row, reduced
+            auto slot_values = [&](int pp, int cb, u64 (&v)[4]) {
                 const int i = 2 * pp + (lane >> 4);
                 const u32 s = s0 + i;
+                u32 r[32];
+                __syncwarp();
+                tmem_ld32(taddr + (u32)(pp * 128 + 8 * cb), r);
+                // sum_a 2^(8a) P_a with P_a < 2^25 as L + 2^32 H (L, H < 2^49.01) for the
+                // 4 ciphertexts at once: independent chains, no branches
+                if (wide_q) {
+#pragma unroll
+                    for (int cc = 0; cc < 4; ++cc) {
+                        const u32* P = r + 8 * cc;
+                        const u64 L = (u64)P[0] + ((u64)P[1] << 8) + ((u64)P[2] << 16) + ((u64)P[3] << 24);
+                        const u64 H = (u64)P[4] + ((u64)P[5] << 8) + ((u64)P[6] << 16) + ((u64)P[7] << 24);
+                        // L < q: 2^32 H mod q lazily in [0, 2q), plus L, below 3q
+                        u64 x = mul_shoup_lazy(H, r32, r32q, q) + L;
+                        x = x >= 2 * q ? x - 2 * q : x;
+                        v[cc] = x >= q ? x - q : x;
+                    }
+                } else {
+#pragma unroll
+                    for (int cc = 0; cc < 4; ++cc) {
+                        const u32* P = r + 8 * cc;
+                        const u64 L = (u64)P[0] + ((u64)P[1] << 8) + ((u64)P[2] << 16) + ((u64)P[3] << 24);
+                        const u64 H = (u64)P[4] + ((u64)P[5] << 8) + ((u64)P[6] << 16) + ((u64)P[7] << 24);
+                        const u64 lo = L + (H << 32), hi = (H >> 32) + (lo < L);  // exact 128-bit sum
+                        v[cc] = add_mod(reduce_2q(mul_shoup_lazy(lo, 1, one_q, q), q), mul_shoup(hi, r64, r64q, q), q);
+                    }
+                }
+                if ((corr >> cb) & 15) {  // rare: sparse carry corrections of the hoisted digits
+                    const u64 ps = psi[lm(l)];
+                    const u32 k = galois_src(s, exps_inv[g], log_n);
+                    const u64* key = keys[g];
+                    for (int cc = 0; cc < 4; ++cc) {
+                        const int c = cb + cc;
+                        if (!((corr >> c) & 1)) continue;
+                        const u32 cnt = cnt_staged ? s_cnt[c * n_keys + g] : exc_count[(size_t)c * n_keys + g];
+                        const Exc* list = exc + ((size_t)c * n_keys + g) * cap;
+                        for (u32 e = 0; e < cnt; ++e) {
+                            const Exc xe = list[e];
+                            u64 wv = pow_mod_dev(ps, ((2ull * k + 1) * xe.t) & (2ull * n - 1), bm);
+                            u64 dm = xe.delta < 0 ? (u64)(-xe.delta) % q : (u64)xe.delta % q;
+                            if (xe.delta < 0 && dm) dm = q - dm;
+                            const u64 tv = mul_barrett(wv, dm, bm);
+                            const size_t kofs = (((size_t)xe.j * LK + l) * 2 + comp) << log_n;
+                            v[cc] = add_mod(v[cc], mul_barrett(tv, key[kofs + s], bm), q);
+                        }
+                    }
+                }
+            };
+            if (kEpiWarps == 4) {
+                // Each (row, ciphertext) output is 4 consecutive slots, one 32-byte sector.
+                // Lane L holds slots L / 16 and 2 + L / 16 of its row after both column
+                // blocks; one exchange with lane L ^ 16 gives lane L < 16 slots 0, 1 and
+                // lane L + 16 slots 2, 3, so every store instruction writes whole sectors
+                // (16 bytes a lane) instead of half sectors completed by a later instruction.
+                const bool lo_half = lane < 16;
                 for (int cb = 0; cb < kCt; cb += 4) {
-                    u32 r[32];
-                    __syncwarp();
-                    tmem_ld32(taddr + (u32)(pp * 128 + 8 * cb), r);
-                    // sum_a 2^(8a) P_a with P_a < 2^25 as L + 2^32 H (L, H < 2^49.01) for the
-                    // 4 ciphertexts at once: independent chains, no branches
-                    u64 v[4];
-                    if (wide_q) {
+                    u64 va[4], vb[4];
+                    slot_values(0, cb, va);
+                    slot_values(1, cb, vb);
 #pragma unroll
-                        for (int cc = 0; cc < 4; ++cc) {
-                            const u32* P = r + 8 * cc;
-                            const u64 L = (u64)P[0] + ((u64)P[1] << 8) + ((u64)P[2] << 16) + ((u64)P[3] << 24);
-                            const u64 H = (u64)P[4] + ((u64)P[5] << 8) + ((u64)P[6] << 16) + ((u64)P[7] << 24);
-                            // L < q: 2^32 H mod q lazily in [0, 2q), plus L, below 3q
-                            u64 x = mul_shoup_lazy(H, r32, r32q, q) + L;
-                            x = x >= 2 * q ? x - 2 * q : x;
-                            v[cc] = x >= q ? x - q : x;
-                        }
-                    } else {
-#pragma unroll
-                        for (int cc = 0; cc < 4; ++cc) {
-                            const u32* P = r + 8 * cc;
-                            const u64 L = (u64)P[0] + ((u64)P[1] << 8) + ((u64)P[2] << 16) + ((u64)P[3] << 24);
-                            const u64 H = (u64)P[4] + ((u64)P[5] << 8) + ((u64)P[6] << 16) + ((u64)P[7] << 24);
-                            const u64 lo = L + (H << 32), hi = (H >> 32) + (lo < L);  // exact 128-bit sum
-                            v[cc] = add_mod(reduce_2q(mul_shoup_lazy(lo, 1, one_q, q), q), mul_shoup(hi, r64, r64q, q), q);
+                    for (int cc = 0; cc < 4; ++cc) {
+                        const u64 send = lo_half ? vb[cc] : va[cc];
+                        const u64 got = ((u64)__shfl_xor_sync(0xffffffffu, (u32)(send >> 32), 16) << 32) |
+                                        (u64)__shfl_xor_sync(0xffffffffu, (u32)send, 16);
+                        const u64 x0 = lo_half ? va[cc] : got, x1 = lo_half ? got : vb[cc];
+                        if (row_ok && cb + cc < n_ct) {
+                            u64* dst = acc_row + (size_t)(cb + cc) * c_stride + (lo_half ? 0 : 2);
+                            asm volatile("st.global.v2.u64 [%0], {%1, %2};" ::"l"(dst), "l"(x0), "l"(x1) : "memory");
                         }
                     }
-                    if ((corr >> cb) & 15) {  // rare: sparse carry corrections of the hoisted digits
-                        const u64 ps = psi[lm(l)];
-                        const u32 k = galois_src(s, exps_inv[g], log_n);
-                        const u64* key = keys[g];
-                        for (int cc = 0; cc < 4; ++cc) {
-                            const int c = cb + cc;
-                            if (!((corr >> c) & 1)) continue;
-                            const u32 cnt = cnt_staged ? s_cnt[c * n_keys + g] : exc_count[(size_t)c * n_keys + g];
-                            const Exc* list = exc + ((size_t)c * n_keys + g) * cap;
-                            for (u32 e = 0; e < cnt; ++e) {
-                                const Exc xe = list[e];
-                                u64 wv = pow_mod_dev(ps, ((2ull * k + 1) * xe.t) & (2ull * n - 1), bm);
-                                u64 dm = xe.delta < 0 ? (u64)(-xe.delta) % q : (u64)xe.delta % q;
-                                if (xe.delta < 0 && dm) dm = q - dm;
-                                const u64 tv = mul_barrett(wv, dm, bm);
-                                const size_t kofs = (((size_t)xe.j * LK + l) * 2 + comp) << log_n;
-                                v[cc] = add_mod(v[cc], mul_barrett(tv, key[kofs + s], bm), q);
-                            }
-                        }
-                    }
-                    if (row_ok) {
+                }
+            } else {
+                for (int pp = pp0; pp < pp1; ++pp) {
+                    const int i = 2 * pp + (lane >> 4);
+                    for (int cb = 0; cb < kCt; cb += 4) {
+                        u64 v[4];
+                        slot_values(pp, cb, v);
+                        if (row_ok) {
 #pragma unroll
-                        for (int cc = 0; cc < 4; ++cc)
-                            if (cb + cc < n_ct) acc_row[(size_t)(cb + cc) * c_stride + i] = v[cc];
+                            for (int cc = 0; cc < 4; ++cc)
+                                if (cb + cc < n_ct) acc_row[(size_t)(cb + cc) * c_stride + i] = v[cc];
+                        }
                     }
                 }
             }
             fence_before();
             named_sync(kBarEpi, kEpi);
-            if (tid == 0) arrive(smem_u32(&s_free[u & 1]));
+            if (tid == 0) arrive(smem_u32(&s_free[u % kAccBufs]));
         }
     }
     // teardown: every role has left its loop (on abort, after a bounded wait)
@@ -1108,6 +1149,12 @@ struct StatusReadback {
 #define CKKS_FOLD_SIGMA 0
 #endif
 constexpr bool kFoldSigma = CKKS_FOLD_SIGMA != 0;
+// Inverse transform's second pass fused with ModDown on the tensor-core path
+// (ntt_inverse_moddown_launch): the Q limbs' inverse-transform output stays on chip.
+#ifndef CKKS_FUSE_MODDOWN
+#define CKKS_FUSE_MODDOWN 1
+#endif
+constexpr bool kFuseModDown = CKKS_FUSE_MODDOWN != 0;
 
 // Hoisted hybrid rotations of n_ct ciphertexts by n_keys Galois keys (bounded
 // or RNS-block gadget), out [n_ct][n_keys][2][Lq][N]. Ciphertexts are
@@ -1157,6 +1204,24 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
         Y.release(), Bh.release(), acc.release(), Z.release(), karr.release(), dig.release(), flags.release();
         cnt.release(), exc.release();
         G = G > 4 ? G - 4 : G / 2;
+    }
+    // the tensor-core path fuses the inverse transform's second pass with ModDown
+    // (FP64 networks and ModDown); its P-CRT words
+    // (and zp, the K auxiliary limbs of pass 2) need G * n_keys * 2 * N * (4 + K)
+    // words, which the accumulators' buffer holds once pass 1 has read it
+    const bool fuse_md = use_tc && kFuseModDown && ntt_inverse_moddown_supported(ctx, Lq);
+    Workspace<u64> wsp;
+    double* words = nullptr;
+    u64* zp = nullptr;
+    if (fuse_md) {
+        const size_t per = (size_t)G * n_keys * 2 * n;
+        u64* base = acc.p;
+        if (LK < 4 + ctx->K) {
+            if ((rc = wsp.alloc(per * (4 + ctx->K), st))) return rc;
+            base = wsp.p;
+        }
+        words = reinterpret_cast<double*>(base);
+        zp = base + per * 4;
     }
     // key pointers, exponents and psi per modulus
     std::vector<u64> hk(3 * (size_t)n_keys + ctx->moduli.size());
@@ -1227,7 +1292,10 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
             const int n_tiles = (int)(LK * (n / tc::kTS));
             CKKS_CUDA_TRY(cudaFuncSetAttribute(k_mac_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                (int)tc::kSmemBytes));
-            k_mac_tc<<<n_tiles < n_sm ? n_tiles : n_sm, tc::kThreads, tc::kSmemBytes, st>>>(
+            if (tc::kCtasPerSm > 1)  // the whole carveout as shared memory, so two CTAs fit an SM
+                CKKS_CUDA_TRY(cudaFuncSetAttribute(k_mac_tc, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+            const int n_cta = n_sm * tc::kCtasPerSm;
+            k_mac_tc<<<n_tiles < n_cta ? n_tiles : n_cta, tc::kThreads, tc::kSmemBytes, st>>>(
                 Y.p, y_stride, Bh.p, b_stride, (int)Lq, pset->d, (int)pset->rg, d_keys, d_exps_inv, acc.p,
                 ctx->d_tabs, lqp, (int)gn,
                 (int)n_keys, (int)LK, (int)D, (int)ctx->log_n, exc.p, cnt.p, cap, d_psi, terr.p);
@@ -1284,14 +1352,30 @@ int32_t rotate_hoisted_ntt(ckks_ctx* ctx, const ckks_ksk* const* keys, u32 n_key
             go.exps_inv = d_exps_inv;
             go.n_keys = n_keys;
         }
-        if ((rc = ntt_inverse_base_launch(ctx, acc.p, Z.p, gn * n_keys * 2, lqp, LK, ib, st, go))) return rc;
-        pt.end();
-        pt.begin(5);
-        // ModDown of every (ciphertext, key) pair (and sigma_g unless folded above), into the output
-        if ((rc = mod_down_sigma_multi(ctx, Z.p, ct_out + (size_t)c0 * n_keys * ct_words, gn * n_keys * 2, Lq,
-                                       go.exps ? nullptr : d_exps_inv, n_keys, st)))
-            return rc;
-        pt.end();
+        if (fuse_md) {
+            // sigma folded into pass 1; pass 2 of the auxiliary limbs leaves the P-CRT
+            // words (in the accumulators' buffer, which pass 1 has consumed) and pass 2
+            // of each Q limb writes its ModDown output directly
+            GaloisOut gf;
+            gf.exps = d_exps;
+            gf.exps_inv = d_exps_inv;
+            gf.n_keys = n_keys;
+            if ((rc = ntt_inverse_moddown_launch(ctx, acc.p, Z.p, words, zp, ct_out + (size_t)c0 * n_keys * ct_words,
+                                                 gn * n_keys * 2, Lq, gf, st)))
+                return rc;
+            pt.end();
+            pt.begin(5);
+            pt.end();
+        } else {
+            if ((rc = ntt_inverse_base_launch(ctx, acc.p, Z.p, gn * n_keys * 2, lqp, LK, ib, st, go))) return rc;
+            pt.end();
+            pt.begin(5);
+            // ModDown of every (ciphertext, key) pair (and sigma_g unless folded above), into the output
+            if ((rc = mod_down_sigma_multi(ctx, Z.p, ct_out + (size_t)c0 * n_keys * ct_words, gn * n_keys * 2, Lq,
+                                           go.exps ? nullptr : d_exps_inv, n_keys, st)))
+                return rc;
+            pt.end();
+        }
         // pairs whose correction lists overflowed are recomputed exactly
         int h_err = 0;
         if (rb.ok()) {

@@ -23,6 +23,7 @@
 #include <cstdio>
 
 #include "ntt_core.cuh"
+#include "moddown_f64.cuh"
 
 namespace {
 
@@ -514,6 +515,194 @@ k_inv2(const u64* src, u64* dst, const NttTab* __restrict__ tabs,
     }
 }
 
+// ----------------------------------------------------------------------------
+// Inverse pass 2 fused with ModDown (hoisted rotations; ring/auxiliary_modulus.rs:89-171).
+// Pass 1 ran with sigma_k folded in (GaloisOut), so every column tile of pass 2
+// holds the same output coefficients in every limb. k_inv2_pcrt finishes the
+// K auxiliary limbs of a tile and writes, per coefficient, the four 47-bit
+// words of the centred P-CRT value with its sign folded in (mdf::crt_words:
+// the ModDown products are odd in the words, so negating them negates each
+// product exactly); k_inv2_moddown finishes one Q limb of a tile and applies
+// mdf::limb with those words, writing the ModDown output. The inverse
+// transform's Q-limb output never reaches HBM, and the same canonical residues
+// as k_inv2 followed by k_mod_down_f64 come out.
+
+// Pass 2 of one limb of a column tile, sigma folded (k_inv2 with go.exps):
+// thread (i0, c) ends with v[e] = output row i0 + R2 e, column c0 + c.
+template <int LOG_M>
+__device__ __forceinline__ void inv2_tile_folded(const u64* __restrict__ src, const NttTab& T, u64* sm, int log_b,
+                                                 int log_c, int c0, u32 poly, const GaloisOut& go, bool act,
+                                                 u64 (&v)[Split<LOG_M>::R1]) {
+    using S = Split<LOG_M>;
+    const int C = 1 << log_c, tid = threadIdx.x;
+    const int c = tid & (C - 1);
+    const u64 q = T.q;
+    const bool f64 = T.f64;
+    u64* st = sm + (S::M << log_c);
+    if (f64) stage_table_f64(st, T.fA_inv, S::M);
+    else stage_table(st, T.psiA_inv, T.psiA_inv_q, S::M);
+    const double2* tabf = reinterpret_cast<const double2*>(st);
+    const double qd = T.qd, qinv = T.qinv;
+    double* smd = reinterpret_cast<double*>(sm);
+    auto tw = [&](int s, u32 blk, u64& W, u64& Wq) {
+        u32 idx = (S::M >> (s + 1)) + blk;
+        W = st[idx];
+        Wq = st[S::M + idx];
+    };
+    auto twf = [&](int s, u32 blk) { return tabf[(S::M >> (s + 1)) + blk]; };
+    __syncthreads();
+    if (tid < (C << S::LR1)) {
+        const int g = tid >> log_c;
+        if (f64) {
+            double x[S::R2];
+#pragma unroll
+            for (int e = 0; e < S::R2; ++e)
+                x[e] = nttf::center(
+                    __longlong_as_double((long long)src[c0 + c + ((size_t)brev(S::R2 * g + e, LOG_M) << log_b)]), qd,
+                    qinv);
+            nttf::gs_stages<S::LR2>(x, 0, g, twf, qd);
+#pragma unroll
+            for (int e = 0; e < S::R2; ++e) smd[((S::R2 * g + e) << log_c) + c] = nttf::center(x[e], qd, qinv);
+        } else {
+            u64 x[S::R2];
+#pragma unroll
+            for (int e = 0; e < S::R2; ++e) x[e] = src[c0 + c + ((size_t)brev(S::R2 * g + e, LOG_M) << log_b)];
+            if (q < nttc::kLazyGsBound) nttc::gs_stages<S::LR2, true>(x, 0, g, tw, q);
+            else nttc::gs_stages<S::LR2, false>(x, 0, g, tw, q);
+#pragma unroll
+            for (int e = 0; e < S::R2; ++e) sm[((S::R2 * g + e) << log_c) + c] = x[e];
+        }
+    }
+    __syncthreads();
+    const int i0 = tid >> log_c;
+    if (act) {
+        if (f64) {
+            double y[S::R1];
+#pragma unroll
+            for (int e = 0; e < S::R1; ++e) y[e] = smd[((i0 + S::R2 * e) << log_c) + c];
+            nttf::gs_stages<S::LR1>(y, S::LR2, 0, twf, qd);
+#pragma unroll
+            for (int e = 0; e < S::R1; ++e) v[e] = nttf::to_canonical(y[e], qd, qinv);
+        } else {
+#pragma unroll
+            for (int e = 0; e < S::R1; ++e) v[e] = sm[((i0 + S::R2 * e) << log_c) + c];
+            if (q < nttc::kLazyGsBound) {
+                nttc::gs_stages<S::LR1, true>(v, S::LR2, 0, tw, q);
+                const u64 one_q = (~0ull) / q;
+#pragma unroll
+                for (int e = 0; e < S::R1; ++e) v[e] = reduce_2q(mul_shoup_lazy(v[e], 1, one_q, q), q);
+            } else {
+                nttc::gs_stages<S::LR1, false>(v, S::LR2, 0, tw, q);
+#pragma unroll
+                for (int e = 0; e < S::R1; ++e) v[e] = reduce_2q(v[e], q);
+            }
+        }
+    }
+    {  // every element to its image row (as k_inv2)
+        const u32 gk = (poly >> 1) % go.n_keys;
+        const u64 k = go.exps[gk], kinv = go.exps_inv[gk];
+        const u32 bmask = (1u << log_b) - 1, amask2 = (2u << LOG_M) - 1;
+        const u32 jl = (u32)(((u64)(c0 + c) * (kinv & bmask)) & bmask);
+        const u32 m = (u32)((((u64)jl * k) & ((2ull << (LOG_M + log_b)) - 1)) >> log_b);
+        const u32 k2a = (u32)(k & amask2);
+        __syncthreads();
+        if (act) {
+#pragma unroll
+            for (int e = 0; e < S::R1; ++e) {
+                const u32 r = (m + (u32)(i0 + S::R2 * e) * k2a) & amask2;
+                const bool neg = r >= (u32)S::M;
+                sm[((r & (S::M - 1)) << log_c) + c] = neg ? neg_mod(v[e], q) : v[e];
+            }
+        }
+        __syncthreads();
+        if (act) {
+#pragma unroll
+            for (int e = 0; e < S::R1; ++e) v[e] = sm[((i0 + S::R2 * e) << log_c) + c];
+        }
+    }
+}
+
+// One auxiliary limb (grid y: k, local limb q_limbs + k of the [polys][LK][N]
+// pass-1 output, table L_ctx + k) of a column tile, sigma folded, into
+// zp [polys][K][N] (canonical).
+template <int LOG_M>
+__global__ void __launch_bounds__(kMaxThreads, min_ctas<LOG_M>(3))
+k_inv2_p(const u64* __restrict__ src, u64* __restrict__ zp, const NttTab* __restrict__ tabs, int q_limbs,
+         int L_ctx, int LK, int K, int log_b, int log_c, GaloisOut go) {
+    using S = Split<LOG_M>;
+    extern __shared__ u64 sm[];
+    const int C = 1 << log_c, tid = threadIdx.x;
+    const int c0 = blockIdx.x << log_c;
+    const int k = blockIdx.y;
+    const u32 poly = blockIdx.z;
+    const int log_n = LOG_M + log_b;
+    const bool act = tid < (C << S::LR2);
+    const int c = tid & (C - 1), i0 = tid >> log_c;
+    u64 v[S::R1];
+    inv2_tile_folded<LOG_M>(src + (((size_t)poly * LK + q_limbs + k) << log_n), tabs[L_ctx + k], sm, log_b, log_c,
+                            c0, poly, go, act, v);
+    if (act) {
+        u64* o = zp + (((size_t)poly * K + k) << log_n);
+#pragma unroll
+        for (int e = 0; e < S::R1; ++e) o[c0 + c + ((size_t)(i0 + S::R2 * e) << log_b)] = v[e];
+    }
+}
+
+// Per coefficient of zp [polys][KT][N]: the four 47-bit words of the centred
+// P-CRT value, sign folded in, as words [polys][N][4] (doubles).
+template <int KT>
+__global__ void __launch_bounds__(256) k_pwords(const u64* __restrict__ zp, double* __restrict__ words,
+                                                ModDownConst md, int log_n) {
+    const u32 n = 1u << log_n;
+    const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const size_t poly = blockIdx.y;
+    u64 v[KT];
+#pragma unroll
+    for (int k = 0; k < KT; ++k) v[k] = __ldg(zp + ((poly * KT + k) << log_n) + t);
+    double w[4];
+    bool neg;
+    mdf::crt_words<KT>(v, md, w, neg);
+    double2* o = reinterpret_cast<double2*>(words + (((poly << log_n) + t) << 2));
+    o[0] = neg ? make_double2(-w[0], -w[1]) : make_double2(w[0], w[1]);
+    o[1] = neg ? make_double2(-w[2], -w[3]) : make_double2(w[2], w[3]);
+}
+
+// One Q limb (grid x, fastest: the tile's words are reused from L2 by every
+// limb) of a column tile: pass 2, then ModDown into dst [polys][q_limbs][N].
+template <int LOG_M>
+__global__ void __launch_bounds__(kMaxThreads, min_ctas<LOG_M>(3))
+k_inv2_moddown(const u64* __restrict__ src, u64* __restrict__ dst, const double* __restrict__ words,
+               const NttTab* __restrict__ tabs, const double* __restrict__ f64c, int q_limbs, int LK, int log_b,
+               int log_c, GaloisOut go) {
+    using S = Split<LOG_M>;
+    extern __shared__ u64 sm[];
+    const int C = 1 << log_c, tid = threadIdx.x;
+    const int limb = blockIdx.x;
+    const int c0 = blockIdx.y << log_c;
+    const u32 poly = blockIdx.z;
+    const int log_n = LOG_M + log_b;
+    const bool act = tid < (C << S::LR2);
+    const int c = tid & (C - 1), i0 = tid >> log_c;
+    u64 v[S::R1];
+    inv2_tile_folded<LOG_M>(src + (((size_t)poly * LK + limb) << log_n), tabs[limb], sm, log_b, log_c, c0, poly, go,
+                            act, v);
+    if (act) {
+        double ci[12];
+#pragma unroll
+        for (int k = 0; k < 12; ++k) ci[k] = __ldg(f64c + limb * 12 + k);
+        u64* o = dst + (((size_t)poly * q_limbs + limb) << log_n);
+#pragma unroll
+        for (int e = 0; e < S::R1; ++e) {
+            const size_t pos = c0 + c + ((size_t)(i0 + S::R2 * e) << log_b);
+            const double2* wp = reinterpret_cast<const double2*>(words + ((((size_t)poly << log_n) + pos) << 2));
+            const double2 wa = __ldg(wp), wb = __ldg(wp + 1);
+            const double w[4] = {wa.x, wa.y, wb.x, wb.y};
+            o[pos] = mdf::limb(nttf::from_u52(v[e]), w, false, ci, false);
+        }
+    }
+}
+
 // Forward pass 2 of relinearization digit transforms fused with the key sum
 // (grafting/bounded_key_switch.rs:139-223): for ciphertext c (grid x, so
 // consecutive CTAs share the key tile in L2), a tile of C units and limb l,
@@ -760,6 +949,60 @@ int32_t ntt_relin_fused_launch(ckks_ctx* ctx, const i64* digits, u64* mid, const
         default: CKKS_RELIN_FUSED(8); break;
     }
 #undef CKKS_RELIN_FUSED
+    CKKS_CUDA_TRY(cudaGetLastError());
+    return CKKS_OK;
+}
+
+bool ntt_inverse_moddown_supported(const ckks_ctx* ctx, u32 q_limbs) {
+    if (ctx->K < 1 || ctx->K > 3 || ctx->log_n1 > 8 || ctx->log_n2 < 1) return false;
+    for (u32 l = 0; l < q_limbs; ++l)
+        if (!ctx->h_tabs[l].f64 || ctx->moduli[l] >= (1ull << 50)) return false;
+    for (u32 k = 0; k < ctx->K; ++k)
+        if (ctx->moduli[ctx->L + k] >= (1ull << 62)) return false;
+    return true;
+}
+
+// Inverse NTT of key-switch accumulators [polys][LK][N] (LK = q_limbs + K) with
+// sigma folded, and ModDown into out [polys][q_limbs][N]. mid: workspace for
+// pass 1 ([polys][LK][N]); words: workspace of polys * N * 4 doubles and zp of
+// polys * K * N words (both may lie in `in`, which pass 1 has consumed).
+int32_t ntt_inverse_moddown_launch(ckks_ctx* ctx, const u64* in, u64* mid, double* words, u64* zp, u64* out,
+                                   u32 polys, u32 q_limbs, const GaloisOut& go, cudaStream_t st) {
+    if (polys == 0) return CKKS_OK;
+    if (!go.exps || !go.exps_inv || polys > 65535) {
+        ckks_set_error("inverse NTT + ModDown: needs a Galois exponent table and at most 65535 polynomials");
+        return CKKS_ERR_BAD_ARG;
+    }
+    const int la = ctx->log_n1, lb = ctx->log_n2;
+    const u32 LK = q_limbs + ctx->K;
+    const LimbMap lm = LimbMap::qp(ctx, q_limbs);
+    if (int32_t rc = pass(3, lb, in, mid, ctx->d_tabs, lm, LK, polys, la, st, InvBase{}, ctx->ntt_log_c[3], go))
+        return rc;
+#define CKKS_INV_MD(LM)                                                                                            \
+    do {                                                                                                           \
+        const int lc = pick_log_c<LM>(lb, ctx->ntt_log_c[4]);                                                      \
+        const int threads = Split<LM>::RMAX << lc;                                                                 \
+        const size_t smem = (sizeof(u64) << (LM + lc)) + 2 * sizeof(u64) * (1u << LM);                            \
+        k_inv2_p<LM><<<dim3(1u << (lb - lc), ctx->K, polys), threads, smem, st>>>(                                  \
+            mid, zp, ctx->d_tabs, (int)q_limbs, (int)ctx->L, (int)LK, (int)ctx->K, lb, lc, go);                    \
+        const dim3 gw((ctx->n + 255) / 256, polys);                                                                \
+        if (ctx->K == 1) k_pwords<1><<<gw, 256, 0, st>>>(zp, words, ctx->mod_down, (int)ctx->log_n);              \
+        else if (ctx->K == 2) k_pwords<2><<<gw, 256, 0, st>>>(zp, words, ctx->mod_down, (int)ctx->log_n);         \
+        else k_pwords<3><<<gw, 256, 0, st>>>(zp, words, ctx->mod_down, (int)ctx->log_n);                          \
+        k_inv2_moddown<LM><<<dim3(q_limbs, 1u << (lb - lc), polys), threads, smem, st>>>(                          \
+            mid, out, words, ctx->d_tabs, ctx->mod_down.f64c, (int)q_limbs, (int)LK, lb, lc, go);                  \
+    } while (0)
+    switch (la) {
+        case 1: CKKS_INV_MD(1); break;
+        case 2: CKKS_INV_MD(2); break;
+        case 3: CKKS_INV_MD(3); break;
+        case 4: CKKS_INV_MD(4); break;
+        case 5: CKKS_INV_MD(5); break;
+        case 6: CKKS_INV_MD(6); break;
+        case 7: CKKS_INV_MD(7); break;
+        default: CKKS_INV_MD(8); break;
+    }
+#undef CKKS_INV_MD
     CKKS_CUDA_TRY(cudaGetLastError());
     return CKKS_OK;
 }

@@ -260,6 +260,19 @@ int32_t ckks_ksk_info(const ckks_ksk* key, uint32_t* digits, uint64_t* words);
 int32_t ckks_ksk_download(const ckks_ksk* key, uint64_t* entries_host);
 int32_t ckks_ksk_destroy(ckks_ksk* key);
 
+/* --------------------------------------------------- Park Mod-PP-MM -----
+ * park_mod_pp_mm (ccmm/park.rs:1634-1647, backends :1405-1620): the modular
+ * plaintext matrix product out = (lhs x rhs) mod modulus of row-major u64
+ * matrices (lhs rows x inner, rhs inner x cols), for any modulus > 1 and any
+ * u64 entries: the canonical residue of each exact integer dot product (the
+ * reference's Reference backend; the others agree on canonical inputs).
+ * Device pointers on the current device, stream-ordered; _host: host buffers,
+ * synchronous. Empty operands or a modulus below 2 return CKKS_ERR_BAD_ARG. */
+int32_t ckks_park_mod_pp_mm(const uint64_t* lhs, const uint64_t* rhs, uint64_t* out, uint32_t rows, uint32_t inner,
+                            uint32_t cols, uint64_t modulus, void* stream);
+int32_t ckks_park_mod_pp_mm_host(const uint64_t* lhs, const uint64_t* rhs, uint64_t* out, uint32_t rows,
+                                 uint32_t inner, uint32_t cols, uint64_t modulus);
+
 /* --------------------------------------------- seeded sampling stream -----
  * The reference draws every secret, error and uniform mask from
  * rand_chacha 0.3.1's ChaCha20Rng (ChaCha20, 64-bit block counter, stream 0)

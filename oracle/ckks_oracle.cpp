@@ -1623,4 +1623,21 @@ void oracle_encrypt_chacha(const uint64_t* q, uint32_t L, uint32_t n, const int8
     }
 }
 
+
+// ccmm/park.rs:1405-1434 (park_matrix_mul_reference): per output, accumulate
+// lhs[row][k] * rhs[k][col] in u128 and reduce mod q after every term.
+void oracle_park_mod_pp_mm(const uint64_t* lhs, const uint64_t* rhs, uint32_t rows, uint32_t inner, uint32_t cols,
+                           uint64_t q, uint64_t* out) {
+    const u128 Q = q;
+    for (uint32_t r = 0; r < rows; ++r)
+        for (uint32_t c = 0; c < cols; ++c) {
+            u128 acc = 0;
+            for (uint32_t k = 0; k < inner; ++k) {
+                acc += (u128)lhs[(size_t)r * inner + k] * rhs[(size_t)k * cols + c];
+                acc %= Q;
+            }
+            out[(size_t)r * cols + c] = (uint64_t)acc;
+        }
+}
+
 }  // extern "C"

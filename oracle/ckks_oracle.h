@@ -175,6 +175,10 @@ void oracle_bounded_relin_key_generate_chacha(const uint64_t* q, uint32_t L, uin
 void oracle_encrypt_chacha(const uint64_t* q, uint32_t L, uint32_t degree, const int8_t* secret, int kind,
                            double param, void* rng, const uint64_t* message, uint64_t* ct);
 
+/* ccmm/park.rs:1405-1434 Mod-PP-MM, Reference backend (row-major). */
+void oracle_park_mod_pp_mm(const uint64_t* lhs, const uint64_t* rhs, uint32_t rows, uint32_t inner, uint32_t cols,
+                           uint64_t q, uint64_t* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -80,6 +80,7 @@ _SIGS = {
     "oracle_bounded_relin_key_generate_chacha": (None, [u64p, U32, U32, U32, i8p, ctypes.c_int, F64,
                                                         ctypes.c_void_p, u64p]),
     "oracle_encrypt_chacha": (None, [u64p, U32, U32, i8p, ctypes.c_int, F64, ctypes.c_void_p, u64p, u64p]),
+    "oracle_park_mod_pp_mm": (None, [u64p, u64p, U32, U32, U32, U64, u64p]),
     "oracle_slots_to_coefficients": (None, [U32, f64p, f64p]),
     "oracle_coefficients_to_slots": (None, [U32, f64p, f64p]),
     "oracle_encode": (None, [U32, f64p, u64p, U32, F64, u64p]),
@@ -301,6 +302,12 @@ class Oracle:
         moduli = arr(moduli); quad = arr(quad); key = arr(key); L = len(moduli); n = quad.shape[-1]
         out = np.zeros((2, L, n), np.uint64)
         self.L.oracle_bounded_relinearize(P(moduli), L, n, base_log, P(quad), P(key), P(out))
+        return out
+
+    def park_mod_pp_mm(self, lhs, rhs, q):
+        lhs = arr(lhs); rhs = arr(rhs)
+        out = np.zeros((lhs.shape[0], rhs.shape[1]), np.uint64)
+        self.L.oracle_park_mod_pp_mm(P(lhs), P(rhs), lhs.shape[0], lhs.shape[1], rhs.shape[1], int(q), P(out))
         return out
 
     def mul_plain(self, moduli, ct, plain):
