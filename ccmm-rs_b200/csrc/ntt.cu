@@ -911,6 +911,13 @@ int32_t ntt_forward_digits_launch(ckks_ctx* ctx, const i64* digits, u64* out, u3
     return CKKS_OK;
 }
 
+// Units per CTA of the fused relinearization pass (log2); -1 follows the
+// forward pass 2's tuned choice.
+#ifndef CKKS_RELIN_LOG_C
+#define CKKS_RELIN_LOG_C -1
+#endif
+constexpr int kRelinLogC = CKKS_RELIN_LOG_C;
+
 bool ntt_relin_fused_supported(const ckks_ctx* ctx, u32 L) {
     if (ctx->log_n2 < 2 || ctx->log_n2 > 8) return false;
     for (u32 l = 0; l < L; ++l)
@@ -933,7 +940,7 @@ int32_t ntt_relin_fused_launch(ckks_ctx* ctx, const i64* digits, u64* mid, const
     }
 #define CKKS_RELIN_FUSED(LM)                                                                                  \
     do {                                                                                                      \
-        const int lc = pick_log_c<LM>(la, ctx->ntt_log_c[2]);                                                 \
+        const int lc = pick_log_c<LM>(la, kRelinLogC >= 0 ? kRelinLogC : ctx->ntt_log_c[2]);                  \
         const size_t smem = (sizeof(u64) << (LM + lc)) + 2 * sizeof(u64) * (1u << LM);                        \
         dim3 grid(n_ct, 1u << (la - lc), L);                                                                  \
         k_fwd2_relin<LM><<<grid, Split<LM>::RMAX << lc, smem, st>>>(mid, key, base, acc, ctx->d_tabs, (int)L, \
