@@ -544,11 +544,11 @@ def bench_rot_gpu(args, world, rank, local):
     mac_bytes = (groups * len(keys) * key_bytes + ROT_NCT * D * LK * n * 8 + ROT_NCT * ROT_L * n * 8
                  + rots * 2 * LK * n * 8)
     peak, kind = peaks()
-    # DRAM traffic per launch: an ncu capture of k_mac_tc on the same limbs,
-    # digits, keys and ciphertexts at N=2^11 read 1.430 GB and wrote 0.447 GB for
-    # 1.804 GB of algorithmic bytes; every term scales with N, so the full launch
-    # moves the same multiple of its algorithmic bytes
-    mac_traffic = mac_bytes * (1.430 + 0.447) / 1.804
+    # DRAM traffic per launch: a one-pass ncu capture (dram__bytes_read.sum +
+    # dram__bytes_write.sum) of the full-size launch at this shape read 49.954 GB
+    # and wrote 14.480 GB against 57.730 GB of algorithmic bytes (the packed key set
+    # is 5 % larger than the keys); other shapes scale by the same ratio
+    mac_traffic = mac_bytes * (49.954 + 14.480) / 57.730
     mac_ms = phases["key-switch MAC"]
     achieved = mac_bytes / (mac_ms / 1000.0) / 1e9
     ct_bytes = 2 * ROT_L * n * 8
@@ -625,7 +625,7 @@ def bench_rot_gpu(args, world, rank, local):
         "dtype": "u64", "data": "synthetic (seeded uniform ciphertexts, GPU-generated keys)",
         "config": dict(rot_config(), autotune=tuning.strip().splitlines()),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": mac_traffic, "traffic_source": "ncu capture at N=2^11 scaled by N",
+                     "traffic": mac_traffic, "traffic_source": "one-pass ncu capture of the full-size launch",
                      "peak_kind": kind,
                      "kernel": "k_mac_tc (INT8 tcgen05 key-switch MAC, %d digits, keys %.3f GB each, read once "
                                "per %d ct)" % (D, key_bytes / 1e9, min(group, ROT_NCT)),
