@@ -540,7 +540,14 @@ namespace tc {
 constexpr int kTS = 4;            // slots per tile
 constexpr int kCt = 16;           // ciphertexts per group (N = 8 kCt = 128)
 constexpr int kKeys = 32;         // keys per pass (M = 2 kKeys = 64)
-constexpr int kJc = 4;            // digits per chunk (K = 32 bytes)
+// Digits per item (CKKS_TC_DIGITS): 4 (one K = 32 MMA per slot) or 8 (two, with
+// half as many items, so the per-item waits and copy issue cover twice the work).
+#ifndef CKKS_TC_DIGITS
+#define CKKS_TC_DIGITS 4
+#endif
+constexpr int kJc = CKKS_TC_DIGITS;  // digits per item
+constexpr int kSub = kJc / 4;        // MMAs (K = 32 bytes, 4 digits) per slot and item
+static_assert(kJc == 4 || kJc == 8, "digits per item");
 // Tuning (measured on B200, see the design notes): epilogue warps (4 or 8; the
 // other 12 - kEpiWarps warps produce, in groups of 4 that take alternate items)
 // and B stages (2 or 4; the prefetch distance is kRing - kBStages items).
@@ -564,10 +571,10 @@ constexpr int kCtasPerSm = CKKS_TC_TWO_CTAS ? 2 : 1;
 constexpr int kAccBufs = CKKS_TC_TWO_CTAS ? 1 : 2;  // TMEM accumulator buffers (256 columns each)
 constexpr int kEpiWarps = CKKS_TC_EPI_WARPS;
 constexpr int kBStages = CKKS_TC_BSTAGES;      // B operand stages
-constexpr int kRing = CKKS_TC_TWO_CTAS ? 4 : 8;  // Y prefetch ring depth
+constexpr int kRing = (CKKS_TC_TWO_CTAS || kJc == 8) ? 4 : 8;  // Y prefetch ring depth
 constexpr int kAhead = kRing - kBStages;       // items whose Y is fetched ahead
 #ifndef CKKS_TC_ARING
-#define CKKS_TC_ARING (CKKS_TC_TWO_CTAS ? 8 : 16)
+#define CKKS_TC_ARING ((CKKS_TC_TWO_CTAS || CKKS_TC_DIGITS == 8) ? 8 : 16)
 #endif
 constexpr int kARing = CKKS_TC_ARING;          // A (packed key block) ring depth
 constexpr int kAAhead = kARing - 2 * kBStages;  // items whose A block is fetched ahead
@@ -586,15 +593,15 @@ static_assert((kARing & (kARing - 1)) == 0 && kAAhead >= kAhead, "A ring");
 // multiples of 128 B) so the producers' shared-memory stores spread over the banks.
 constexpr u32 kSboA = 1024, kLboA = 128, kASlot = 256;
 constexpr u32 kSboB = 128, kLboB = 1088;       // B: ciphertext pairs, digits
-constexpr u32 kBSlot = 4368;                   // 4 digits x 8 weights x 128 B (+padding)
-constexpr u32 kAStage = 8192;                  // 8 row groups
+constexpr u32 kBSlot = kJc * kLboB + 16;       // digits x 8 weights x 128 B (+padding)
+constexpr u32 kAStage = 8192 * kSub;           // 8 row groups per 4-digit block
 constexpr u32 kYStage = kCt * kJc * kTS * 8;   // 2048: Y words [c][jj][i]
 constexpr u32 kBStage = kTS * kBSlot;          // 17472
 constexpr u32 kOffY = kARing * kAStage;                    // A ring
 constexpr u32 kOffB = kOffY + kRing * kYStage;             // 16 KB of Y
 constexpr u32 kOffCnt = kOffB + kBStages * kBStage;        // correction counts [c][g], g < kCntKeys
 #ifndef CKKS_TC_CNT_KEYS
-#define CKKS_TC_CNT_KEYS (CKKS_TC_TWO_CTAS ? 64 : 256)
+#define CKKS_TC_CNT_KEYS ((CKKS_TC_TWO_CTAS || CKKS_TC_DIGITS == 8) ? 64 : 256)
 #endif
 constexpr int kCntKeys = CKKS_TC_CNT_KEYS;  // keys whose correction counts are staged in shared memory
 constexpr u32 kSmemBytes = kOffCnt + kCt * kCntKeys * 4;   // 197 KB (16 A slots, 2 B stages): one CTA per SM
@@ -779,16 +786,19 @@ __global__ void __launch_bounds__(tc::kThreads, tc::kCtasPerSm)
         // A: one bulk copy of the item's packed key block (thread 0 of the group);
         // Y copies: 16 bytes (slots 2 ph, 2 ph + 1) of digit pjj of ciphertext
         // yc = gtid / 8 (Y words 2 gtid, 2 gtid + 1 of the stage, [c][jj][i]).
-        static_assert(kGrp == 128 && kTS * kJc * kCt == 2 * kGrp, "producer work split");
-        const int ph = gtid & 1, pjj = (gtid >> 1) & 3;
+        static_assert(kGrp == 128 && kTS * kJc * kCt == 2 * kSub * kGrp, "producer work split");
+        // kJc 4: 16 bytes (slots 2 ph, 2 ph + 1) of digit pjj; kJc 8: all 4 slots of digit pjj
+        const int ph = kJc == 4 ? (gtid & 1) : 0, pjj = kJc == 4 ? ((gtid >> 1) & 3) : (gtid & 7);
         const int yc = gtid >> 3;
-        const u32 a_bytes = (u32)rg * 1024u;
+        const int n4 = (D + 1 + 3) / 4;  // 4-digit blocks of the packed set per tile and key chunk
         int last_issued = -1;  // last item whose block this thread copied (thread 0 of a group)
         // A block of item t into A slot t % kARing (thread 0 of the group)
         auto prefetch_a = [&](int t, const Item& it) {
             if (t < n_items && gtid == 0) {
                 const int tile = (int)blockIdx.x + it.tl * (int)gridDim.x;
-                const u64* src = packed + ((((size_t)tile * n_kc + it.kc) * n_chunks + it.ch) * (size_t)rg << 7);
+                const int b4 = it.ch * kSub;  // first 4-digit block of the item (consecutive in the set)
+                const u32 a_bytes = (u32)((n4 - b4) < kSub ? (n4 - b4) : kSub) * (u32)rg * 1024u;
+                const u64* src = packed + ((((size_t)tile * n_kc + it.kc) * n4 + b4) * (size_t)rg << 7);
                 const u32 bar = smem_u32(&s_afull[t & (kARing - 1)]);
                 asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}\n"
                              ::"r"(bar), "r"(a_bytes) : "memory");
@@ -810,9 +820,14 @@ __global__ void __launch_bounds__(tc::kThreads, tc::kCtasPerSm)
                                       : bok ? Bhat + (((size_t)l << log_n) + s0 + 2 * ph) : Yhat;
                 const size_t ystep = jok ? y_stride : b_stride;
                 const u32 y_st = sbase + kOffY + (u32)(t & (kRing - 1)) * kYStage;
-                // 16-byte aligned: s0 is a multiple of 4 slots and the workspaces are 256-byte aligned
-                if (yc < n_ct)
-                    cp16(y_st + (u32)gtid * 16, ysrc + (jok || bok ? yc * ystep : 0), jok || bok ? 16u : 0u);
+                // 16-byte aligned: s0 is a multiple of 4 slots and the workspaces are 256-byte aligned;
+                // stage layout [c][jj][i]
+                if (yc < n_ct) {
+#pragma unroll
+                    for (int h = 0; h < kSub; ++h)
+                        cp16(y_st + (u32)(((yc * kJc + pjj) * kTS + 2 * ph + 2 * h) * 8),
+                             ysrc + (jok || bok ? yc * ystep + 2 * h : 0), jok || bok ? 16u : 0u);
+                }
             }
             cp_commit();
         };
@@ -874,13 +889,18 @@ __global__ void __launch_bounds__(tc::kThreads, tc::kCtasPerSm)
                 uint8_t* d0 = smem + kOffB + bst * kBStage + i * kBSlot + jj * kLboB + (c >> 1) * kSboB + (c & 1) * 8;
                 uint8_t* d1 = d0 + 4 * kSboB;  // ciphertext c + 8
                 const bool ok0 = c < n_ct, ok1 = c + 8 < n_ct;
-                u64 w0 = ys[(c * kJc + jj) * kTS + i], w1 = ys[((c + 8) * kJc + jj) * kTS + i];
+#pragma unroll
+                for (int h = 0; h < kSub; ++h) {  // digits jj and (kJc 8) jj + 4
+                const int jh = jj + 4 * h;
+                uint8_t* d0h = d0 + h * 4 * kLboB;
+                uint8_t* d1h = d1 + h * 4 * kLboB;
+                u64 w0 = ys[(c * kJc + jh) * kTS + i], w1 = ys[((c + 8) * kJc + jh) * kTS + i];
                 if (near_pow2) {
                     // q in (2^e - 2^(e-9), 2^e), e <= 55: w < 2^(e+1) stays below 2^(e+1)
 #pragma unroll
                     for (int b = 0; b < 8; ++b) {
-                        if (ok0) *(u64*)(d0 + b * 16) = w0;
-                        if (ok1) *(u64*)(d1 + b * 16) = w1;
+                        if (ok0) *(u64*)(d0h + b * 16) = w0;
+                        if (ok1) *(u64*)(d1h + b * 16) = w1;
                         const u64 x0 = w0 << 8, x1 = w1 << 8;
                         w0 = x0 - (x0 >> q_bits) * q;
                         w1 = x1 - (x1 >> q_bits) * q;
@@ -888,11 +908,12 @@ __global__ void __launch_bounds__(tc::kThreads, tc::kCtasPerSm)
                 } else {
 #pragma unroll
                     for (int b = 0; b < 8; ++b) {
-                        if (ok0) *(u64*)(d0 + b * 16) = w0;
-                        if (ok1) *(u64*)(d1 + b * 16) = w1;
+                        if (ok0) *(u64*)(d0h + b * 16) = w0;
+                        if (ok1) *(u64*)(d1h + b * 16) = w1;
                         w0 = mul_shoup_lazy(w0, f256, f256q, q);
                         w1 = mul_shoup_lazy(w1, f256, f256q, q);
                     }
+                }
                 }
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -920,6 +941,7 @@ __global__ void __launch_bounds__(tc::kThreads, tc::kCtasPerSm)
         if (lane == 0) {
             Item it{0, 0, 0};
             int unit = -1, last_t = -1;
+            const u32 a_block = (u32)rg * 1024u;  // one 4-digit block of the packed set
             // Every mbarrier wait costs the issuing thread a few hundred cycles even when the
             // phase is complete, and the MMAs of one item issue back to back: per item this
             // thread waits on `ready` only (the producers have already seen the key block
@@ -947,9 +969,12 @@ __global__ void __launch_bounds__(tc::kThreads, tc::kCtasPerSm)
                 const u32 dbase = tmem + (u32)(256 * (unit % kAccBufs));
 #pragma unroll
                 for (int i = 0; i < kTS; ++i)
-                    mma_i8(dbase + ((u32)(16 * (i & 1)) << 16) + (u32)(i >> 1) * 128u,
-                           sdesc(a0 + i * kASlot, kLboA, kSboA), sdesc(b0 + i * kBSlot, kLboB, kSboB),
-                           it.ch > 0 ? 1u : 0u);
+#pragma unroll
+                    for (int h = 0; h < kSub; ++h)  // 4-digit block h of the item: A block h, B digits 4 h ..
+                        mma_i8(dbase + ((u32)(16 * (i & 1)) << 16) + (u32)(i >> 1) * 128u,
+                               sdesc(a0 + (u32)h * a_block + i * kASlot, kLboA, kSboA),
+                               sdesc(b0 + i * kBSlot + (u32)h * 4 * kLboB, kLboB, kSboB),
+                               (it.ch > 0 || h > 0) ? 1u : 0u);
                 commit(smem_u32(&s_empty[bst]));
                 if (it.ch == n_chunks - 1) commit(smem_u32(&s_full[unit % kAccBufs]));
                 last_t = t;
