@@ -39,17 +39,23 @@ constexpr int kThreads = 32 * (kMmaWarp + 1);
 constexpr int kProd = 32 * kProdWarps, kEpi = 32 * kEpiWarps;
 constexpr int kBarProd = 1, kBarEpi = 2;  // named barriers
 constexpr int kCB = 16;                   // columns per block (N = 2 x 16 x 8 = 256)
-constexpr int kKT = 8;                    // inner indices per item (two MMAs of K = 32 bytes)
-constexpr int kRing = 8, kBStages = 2, kAhead = kRing - kBStages;
-constexpr u32 kRingSlot = 2048;           // raw entries of one item: 128 producers x 2 x 8 bytes
+#ifndef CKKS_CCMM_TC_KT
+#define CKKS_CCMM_TC_KT 8
+#endif
+constexpr int kKT = CKKS_CCMM_TC_KT;      // inner indices per item (kKT / 4 MMAs of K = 32 bytes)
+constexpr int kSubK = kKT / 4;
+static_assert(kKT == 4 || kKT == 8 || kKT == 16, "inner indices per item");
+constexpr int kRing = kKT == 16 ? 4 : 8, kBStages = 2, kAhead = kRing - kBStages;
+constexpr u32 kRingSlot = 1024 * kSubK;   // raw entries of one item: 128 producers x kSubK x 8 bytes
 // A: 128 rows x 512 K bytes; core matrices 8 rows x 16 B, K chunks 128 B apart, row groups 4 KB
 constexpr u32 kLboA = 128, kSboA = 4096, kABytes = 65536;
-// B stage: 8 K groups (inner index) x 16 N chunks; strides chosen so the
+// B stage: kKT K groups (inner index) x 16 N chunks; strides chosen so the
 // producers' 8-byte stores take two wavefronts per warp (no bank conflicts)
 constexpr u32 kSboB = 144, kLboB = 2304, kBBytes = kKT * kLboB;
 constexpr u32 kOffA = 0, kOffRing = 2 * kABytes, kOffB = kOffRing + kRing * kRingSlot,
               kOffX = kOffB + kBStages * kBBytes;
-constexpr u32 kSmemBytes = kOffX + 64 * kCB * 8;  // 188 KB: one CTA per SM
+constexpr u32 kSmemBytes = kOffX + 64 * kCB * 8;  // 188 KB at kKT 8: one CTA per SM
+static_assert(kSmemBytes <= 227 * 1024, "shared memory per CTA");
 constexpr u32 kTmemCols = 512;
 constexpr u32 kIdesc = idesc_i8(128, 256, true);
 
@@ -142,7 +148,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 const long long gs = slot_of(p.j);
                 const int c = kCB * p.cb + c_loc;
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
+                for (int h = 0; h < kSubK; ++h) {
                     const int tt = kKT * p.t + t_loc + 4 * h;
                     const bool ok = tt < kd && c < nc;
                     const u64* src = Bt + (size_t)gs * 2 * b_ent + (size_t)comp * b_ent + tt + (size_t)(c_begin + c) * kd;
@@ -210,28 +216,31 @@ __global__ void __launch_bounds__(kThreads, 1)
                 near_pow2 = q_bits <= 55 && ((1ull << q_bits) - q) < (1ull << (q_bits - 9));
                 f_limb = l;
             }
-            {   // the 8 weights of this thread's two entries: K rows (t_loc + 4 h, b), N bytes 128 comp + 8 c_loc
+            {   // the 8 weights of this thread's entries: K rows (t_loc + 4 h, b), N bytes 128 comp + 8 c_loc
                 const uint8_t* ring = smem + kOffRing + (it & (kRing - 1)) * kRingSlot;
-                u64 w0 = *(const u64*)(ring + gtid * 8), w1 = *(const u64*)(ring + (kProd + gtid) * 8);
                 uint8_t* d0 = smem + kOffB + bst * kBBytes + t_loc * kLboB + (comp * 8 + (c_loc >> 1)) * kSboB +
                               (c_loc & 1) * 8;
-                uint8_t* d1 = d0 + 4 * kLboB;
+                u64 w[kSubK];
+#pragma unroll
+                for (int h = 0; h < kSubK; ++h) w[h] = *(const u64*)(ring + (h * kProd + gtid) * 8);
                 if (near_pow2) {  // q in (2^e - 2^(e-9), 2^e), e <= 55: w < 2^(e+1) stays below 2^(e+1)
 #pragma unroll
                     for (int b = 0; b < 8; ++b) {
-                        *(u64*)(d0 + b * 16) = w0;
-                        *(u64*)(d1 + b * 16) = w1;
-                        const u64 x0 = w0 << 8, x1 = w1 << 8;
-                        w0 = x0 - (x0 >> q_bits) * q;
-                        w1 = x1 - (x1 >> q_bits) * q;
+#pragma unroll
+                        for (int h = 0; h < kSubK; ++h) {
+                            *(u64*)(d0 + h * 4 * kLboB + b * 16) = w[h];
+                            const u64 x = w[h] << 8;
+                            w[h] = x - (x >> q_bits) * q;
+                        }
                     }
                 } else {
 #pragma unroll
                     for (int b = 0; b < 8; ++b) {
-                        *(u64*)(d0 + b * 16) = w0;
-                        *(u64*)(d1 + b * 16) = w1;
-                        w0 = mul_shoup_lazy(w0, f256, f256q, q);
-                        w1 = mul_shoup_lazy(w1, f256, f256q, q);
+#pragma unroll
+                        for (int h = 0; h < kSubK; ++h) {
+                            *(u64*)(d0 + h * 4 * kLboB + b * 16) = w[h];
+                            w[h] = mul_shoup_lazy(w[h], f256, f256q, q);
+                        }
                     }
                 }
             }
@@ -260,11 +269,11 @@ __global__ void __launch_bounds__(kThreads, 1)
                     }
                     fence_after();
                 }
-                // two MMAs of 4 inner indices each: A K chunks (2 inner indices of 16 bytes)
-                // 4 (2 t + h) .., B K groups 4 h ..
+                // kSubK MMAs of 4 inner indices each: A K chunks (2 inner indices of 16 bytes)
+                // 2 (kSubK t + h) .., B K groups 4 h ..
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const uint64_t a = sdesc(sbase + kOffA + (u32)(j & 1) * kABytes + (u32)(2 * t + h) * 2 * kLboA,
+                for (int h = 0; h < kSubK; ++h) {
+                    const uint64_t a = sdesc(sbase + kOffA + (u32)(j & 1) * kABytes + (u32)(kSubK * t + h) * 2 * kLboA,
                                              kLboA, kSboA);
                     const uint64_t b = sdesc(sbase + kOffB + (u32)bst * kBBytes + (u32)h * 4 * kLboB, kLboB, kSboB);
                     mma_i8(tmem + (u32)(u & 1) * 256u, a, b, kIdesc, (t > 0 || h > 0) ? 1u : 0u);
