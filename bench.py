@@ -69,6 +69,7 @@ sys.path.insert(0, os.path.join(ROOT, "ccmm-rs_b200"))
 
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
+FALLBACK_BF16_TFLOPS = 1590.0
 
 
 def peaks():
@@ -78,6 +79,15 @@ def peaks():
         return float(p["hbm_gbs"]), "measured"
     except Exception:
         return FALLBACK_HBM_GBS, "fallback"
+
+
+def bf16_peak():
+    """Dense bf16 TF/s of this pool's B200s (burst figure) and where it came from."""
+    try:
+        with open(PEAKS_PATH) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured"
+    except Exception:
+        return FALLBACK_BF16_TFLOPS, "fallback"
 
 
 # ------------------------------------------------------------ clocks sampler
@@ -1220,12 +1230,17 @@ def bench_park_gpu(args, world, rank, local):
     C = torch.empty((n, n), dtype=torch.int64, device=dev)
     st = torch.cuda.current_stream()
 
-    def step():
-        cb.park_mod_pp_mm(A, B, q, out=C)
+    gemm_ms = []
+
+    def step(backend="tensor_cores"):
+        cb.park_mod_pp_mm(A, B, q, out=C, backend=backend)
+        if backend == "tensor_cores":
+            gemm_ms.append(cb.park_last_timing()[1])
 
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
+    gemm_ms.clear()
     clocks = Clocks(local)
     clocks.start()
     barrier(world)
@@ -1241,6 +1256,19 @@ def bench_park_gpu(args, world, rank, local):
     clk = clocks.stop()
     ms_max = max_over_ranks(world, ms)
     value = args.steps * world / (ms_max / 1000.0)
+    gemm = sum(gemm_ms) / len(gemm_ms)
+    # the plain GPU form: the same product with 192-bit sums on the CUDA cores
+    C2 = torch.empty_like(C)
+    cb.park_mod_pp_mm(A, B, q, out=C2, backend="cuda_cores")
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    cb.park_mod_pp_mm(A, B, q, out=C2, backend="cuda_cores")
+    e1.record(st)
+    torch.cuda.synchronize()
+    cuda_core_ms = e0.elapsed_time(e1)
+    backends_equal = bool(torch.equal(C, C2))
+    del C2
     # parity of sampled outputs against the oracle (outside the timed region)
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from oracle_lib import Oracle
@@ -1252,24 +1280,33 @@ def bench_park_gpu(args, world, rank, local):
     t = time.perf_counter()
     cb.park_mod_pp_mm(a, b, q)
     e2e_s = time.perf_counter() - t
-    peak, kind = peaks()
-    # the dominant (only) kernel is integer-multiply bound: n^3 exact 64 x 64 -> 128-bit
-    # products; memory traffic (3 n^2 words) is negligible, so the roofline is the product rate
-    prods = float(n) ** 3
+    # the dominant kernel k_park_tc runs nb^2 n^3 unsigned 8-bit multiply-adds (nb = 5 bytes
+    # per residue of the 35-bit modulus) on the tensor cores; INT8 dense is twice the bf16
+    # dense rate on B200, so the peak is twice the measured bf16 burst figure
+    nb = ((q - 1).bit_length() + 7) // 8
+    ops = 2.0 * nb * nb * float(n) ** 3
+    bf16, bf16_kind = bf16_peak()
+    i8_peak = 2.0 * bf16 if bf16 else None
+    achieved = ops / (gemm / 1000.0) / 1e12
     return {"metric": "Park Mod-PP-MM/s (n=4096 square, modulus 0x7ffff6001, bit-exact)", "value": value,
             "unit": "products/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded uniform residues)",
             "config": {"workload": "Park Mod-PP-MM, 4096 x 4096 by 4096 x 4096, u64 residues mod 0x7ffff6001",
                        "n": n, "modulus": q, "l2": "operands 134 MB each, above L2"},
-            "roofline": {"bound": "integer multiply", "achieved": prods / (ms_max / args.steps / 1000.0) / 1e9,
-                         "unit": "G exact modular MAC/s", "peak": None, "frac": None, "traffic": None,
-                         "kernel": "k_park_mm (192-bit exact dot products)"},
+            "roofline": {"bound": "tensor", "achieved": achieved, "unit": "TOP/s (INT8)", "peak": i8_peak,
+                         "frac": achieved / i8_peak if i8_peak else None, "traffic": None,
+                         "kernel": "k_park_tc (INT8 tcgen05 products of byte planes, %d x %d planes)" % (nb, nb),
+                         "kernel_ms": gemm, "rest_of_step_ms": (ms_max / args.steps) - gemm,
+                         "peak_source": "2 x bf16 dense (%s %s)" % (bf16_kind, bf16),
+                         "ops_per_launch": ops},
+            "plain_gpu": {"backend": "cuda_cores (k_park_mm, 192-bit exact sums)", "ms": cuda_core_ms,
+                          "value": 1000.0 / cuda_core_ms, "unit": "products/s", "words_equal": backends_equal},
             "e2e": {"value": 1.0 / e2e_s, "unit": "products/s", "h2d_bytes_per_step": 2 * n * n * 8,
                     "d2h_bytes_per_step": n * n * 8, "path": "ckks_park_mod_pp_mm_host"},
             "parity": {"words_compared": len(rows) * n, "mismatches": mism,
                        "what": "three full output rows against the oracle's Reference backend"},
-            "gpu_launches": args.steps, "clocks": clk}
+            "gpu_launches": 3 * args.steps, "clocks": clk}
 
 
 def park_cpu_sample(threads):

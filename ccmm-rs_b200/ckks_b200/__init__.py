@@ -87,6 +87,8 @@ _SIGS = {
     "ckks_fft_stage_multi": (I32, [VP, ctypes.POINTER(VP), U32, u32p, U32, VP, VP, U32, VP, U32, U32, VP]),
     "ckks_park_mod_pp_mm": (I32, [VP, VP, VP, U32, U32, U32, U64, VP]),
     "ckks_park_mod_pp_mm_host": (I32, [u64p, u64p, u64p, U32, U32, U32, U64]),
+    "ckks_park_mod_pp_mm_with_backend": (I32, [VP, VP, VP, U32, U32, U32, U64, I32, VP]),
+    "ckks_park_last_timing": (I32, [ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
     "ckks_rng_create": (I32, [U64, ctypes.POINTER(VP)]),
     "ckks_rng_create_from_seed": (I32, [ctypes.c_char_p, ctypes.POINTER(VP)]),
     "ckks_rng_destroy": (I32, [VP]),
@@ -448,11 +450,19 @@ def encrypt_rng(ctx, q_limbs, message, secret, rng, kind=ChaCha20Rng.GAUSSIAN, p
     return out
 
 
-def park_mod_pp_mm(lhs, rhs, modulus, out=None, stream=None):
+PARK_BACKENDS = {"auto": 0, "tensor_cores": 1, "cuda_cores": 2}
+
+
+def park_mod_pp_mm(lhs, rhs, modulus, out=None, stream=None, backend="auto"):
     """park_mod_pp_mm (ccmm/park.rs:1634-1647): (lhs x rhs) mod modulus.
 
     lhs, rhs: row-major u64 matrices as torch CUDA int64 tensors (device path)
-    or numpy uint64 arrays (host path, synchronous)."""
+    or numpy uint64 arrays (host path, synchronous, backend "auto").
+    backend (device path): "auto" / "tensor_cores" (INT8 tcgen05 products of
+    byte planes) / "cuda_cores" (192-bit exact sums); all give the same words,
+    like the reference's ParkModPpMmBackend variants."""
+    if backend not in PARK_BACKENDS:
+        raise ValueError("park_mod_pp_mm: backend is one of %s" % sorted(PARK_BACKENDS))
     if isinstance(lhs, np.ndarray):
         a = np.ascontiguousarray(lhs, np.uint64); b = np.ascontiguousarray(rhs, np.uint64)
         if a.ndim != 2 or b.ndim != 2 or a.shape[1] != b.shape[0]:
@@ -464,10 +474,20 @@ def park_mod_pp_mm(lhs, rhs, modulus, out=None, stream=None):
     import torch
     if lhs.dim() != 2 or rhs.dim() != 2 or lhs.shape[1] != rhs.shape[0]:
         raise ValueError("park_mod_pp_mm: shapes do not chain")
+    if not (lhs.is_contiguous() and rhs.is_contiguous()):
+        raise ValueError("park_mod_pp_mm: operands must be contiguous")
     out = torch.empty((lhs.shape[0], rhs.shape[1]), dtype=torch.int64, device=lhs.device) if out is None else out
-    check(lib().ckks_park_mod_pp_mm(_dptr(lhs), _dptr(rhs), _dptr(out), lhs.shape[0], lhs.shape[1], rhs.shape[1],
-                                    int(modulus), _stream(stream)))
+    check(lib().ckks_park_mod_pp_mm_with_backend(_dptr(lhs), _dptr(rhs), _dptr(out), lhs.shape[0], lhs.shape[1],
+                                                 rhs.shape[1], int(modulus), PARK_BACKENDS[backend],
+                                                 _stream(stream)))
     return out
+
+
+def park_last_timing():
+    """(pack ms, GEMM ms) of this thread's last tensor-core Park call (CUDA events)."""
+    p, g = ctypes.c_float(), ctypes.c_float()
+    check(lib().ckks_park_last_timing(ctypes.byref(p), ctypes.byref(g)))
+    return p.value, g.value
 
 
 class KeySwitchKey:

@@ -57,18 +57,24 @@ __device__ __forceinline__ void mbar_init(u32 bar, u32 count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
 }
 
-// true once the phase with the given parity has completed (bounded)
+__device__ __forceinline__ bool try_parity(u32 bar, u32 parity) {
+    u32 done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity), "r"(kSuspendNs)
+        : "memory");
+    return done != 0;
+}
+
+// true once the phase with the given parity has completed (bounded; the clock
+// is read only when the first try finds the phase open)
 __device__ __forceinline__ bool wait_parity(u32 bar, u32 parity) {
+    if (try_parity(bar, parity)) return true;
     const long long t0 = clock64();
     do {
-        u32 done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(done)
-            : "r"(bar), "r"(parity), "r"(kSuspendNs)
-            : "memory");
-        if (done) return true;
+        if (try_parity(bar, parity)) return true;
     } while (clock64() - t0 < kWaitCycles);
     return false;
 }
@@ -95,6 +101,29 @@ __device__ __forceinline__ void cp8(u32 dst, const void* src, u32 src_bytes) {
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// Untiled bulk copy global -> shared that completes `bytes` of the transaction
+// count of mbarrier `bar` (16-byte aligned addresses, size a multiple of 16).
+// The barrier's expected count is raised first by expect_tx (one arrival).
+__device__ __forceinline__ void expect_tx(u32 bar, u32 bytes) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}\n" ::"r"(bar),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(u32 dst, const void* src, u32 bytes, u32 bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+// 32 TMEM lanes x 8 columns (with the wait, as below)
+__device__ __forceinline__ void tmem_ld8(u32 taddr, u32 (&r)[8]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+        : "r"(taddr));
+}
 
 // 32 TMEM lanes x 32 columns: lane L of the warp gets columns 0 .. 31 of lane L.
 // The wait is part of the same statement, so no use of r is scheduled before it.

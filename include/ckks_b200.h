@@ -266,10 +266,25 @@ int32_t ckks_ksk_destroy(ckks_ksk* key);
  * matrices (lhs rows x inner, rhs inner x cols), for any modulus > 1 and any
  * u64 entries: the canonical residue of each exact integer dot product (the
  * reference's Reference backend; the others agree on canonical inputs).
- * Device pointers on the current device, stream-ordered; _host: host buffers,
+ * Device pointers on the current device (see the backends below); _host: host buffers,
  * synchronous. Empty operands or a modulus below 2 return CKKS_ERR_BAD_ARG. */
 int32_t ckks_park_mod_pp_mm(const uint64_t* lhs, const uint64_t* rhs, uint64_t* out, uint32_t rows, uint32_t inner,
                             uint32_t cols, uint64_t modulus, void* stream);
+/* park_matrix_mul_with_backend (ccmm/park.rs:1643-1655) for the device
+ * backends: AUTO takes the tensor cores (unsigned 8-bit products of the
+ * residues' bytes against byte-split weights 2^(8i) rhs mod q, summed exactly
+ * in 32 bits; the call waits for its status word, so it returns with the
+ * stream drained) and otherwise the CUDA cores (exact 192-bit sums, stream-
+ * ordered). Both return the same words. A backend that cannot run returns
+ * CKKS_ERR_BAD_ARG; a tensor-core pipeline wait that timed out returns
+ * CKKS_ERR_TIMEOUT. */
+enum { CKKS_PARK_AUTO = 0, CKKS_PARK_TENSOR_CORES = 1, CKKS_PARK_CUDA_CORES = 2 };
+int32_t ckks_park_mod_pp_mm_with_backend(const uint64_t* lhs, const uint64_t* rhs, uint64_t* out, uint32_t rows,
+                                         uint32_t inner, uint32_t cols, uint64_t modulus, int32_t backend,
+                                         void* stream);
+/* CUDA-event times (ms) of the byte packing and of the GEMM launches of this
+ * thread's last tensor-core Park call; CKKS_ERR_BAD_ARG before the first. */
+int32_t ckks_park_last_timing(float* pack_ms, float* gemm_ms);
 int32_t ckks_park_mod_pp_mm_host(const uint64_t* lhs, const uint64_t* rhs, uint64_t* out, uint32_t rows,
                                  uint32_t inner, uint32_t cols, uint64_t modulus);
 
