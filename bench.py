@@ -1222,7 +1222,7 @@ def bench_park_gpu(args, world, rank, local):
     import torch
     import ckks_b200 as cb
     dev = torch.device("cuda", local)
-    n, q = PARK_N, PARK_Q
+    n, q = args.park_n, PARK_Q
     gen = torch.Generator(device=dev)
     gen.manual_seed(77 + rank)
     A = torch.empty((n, n), dtype=torch.int64, device=dev).random_(0, q, generator=gen)
@@ -1274,12 +1274,28 @@ def bench_park_gpu(args, world, rank, local):
     from oracle_lib import Oracle
     o = Oracle()
     a, b, c = cb.to_numpy_u64(A), cb.to_numpy_u64(B), cb.to_numpy_u64(C)
-    rows = [0, 1777, n - 1]
+    rows = [0, (7 * n) // 16, n - 1]
     mism = sum(int(np.count_nonzero(o.park_mod_pp_mm(a[r:r + 1], b, q) != c[r:r + 1])) for r in rows)
-    # end to end through the host-buffer call
-    t = time.perf_counter()
-    cb.park_mod_pp_mm(a, b, q)
-    e2e_s = time.perf_counter() - t
+    # end to end: each step copies both operands from pinned host memory, runs the
+    # product through the public call and reads the result back (CUDA events)
+    Ah, Bh = A.cpu().pin_memory(), B.cpu().pin_memory()
+    Ch = torch.empty_like(Ah).pin_memory()
+
+    def e2e_step():
+        A.copy_(Ah, non_blocking=True)
+        B.copy_(Bh, non_blocking=True)
+        cb.park_mod_pp_mm(A, B, q, out=C)
+        Ch.copy_(C, non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    e0.record(st)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(st)
+    torch.cuda.synchronize()
+    e2e_s = e0.elapsed_time(e1) / 1000.0 / args.steps
+    e2e_equal = bool(torch.equal(Ch, C.cpu()))
     # the dominant kernel k_park_tc runs nb^2 n^3 unsigned 8-bit multiply-adds (nb = 5 bytes
     # per residue of the 35-bit modulus) on the tensor cores; INT8 dense is twice the bf16
     # dense rate on B200, so the peak is twice the measured bf16 burst figure
@@ -1288,12 +1304,13 @@ def bench_park_gpu(args, world, rank, local):
     bf16, bf16_kind = bf16_peak()
     i8_peak = 2.0 * bf16 if bf16 else None
     achieved = ops / (gemm / 1000.0) / 1e12
-    return {"metric": "Park Mod-PP-MM/s (n=4096 square, modulus 0x7ffff6001, bit-exact)", "value": value,
+    return {"metric": "Park Mod-PP-MM/s (n=%d square, modulus 0x7ffff6001, bit-exact)" % n, "value": value,
             "unit": "products/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded uniform residues)",
-            "config": {"workload": "Park Mod-PP-MM, 4096 x 4096 by 4096 x 4096, u64 residues mod 0x7ffff6001",
-                       "n": n, "modulus": q, "l2": "operands 134 MB each, above L2"},
+            "config": {"workload": "Park Mod-PP-MM, %d x %d by %d x %d, u64 residues mod 0x7ffff6001" % (n, n, n, n),
+                       "n": n, "modulus": q, "l2": "operands %d MB each%s" % (
+                           n * n * 8 // 10**6, ", above L2" if n * n * 8 > 126 * 10**6 else "")},
             "roofline": {"bound": "tensor", "achieved": achieved, "unit": "TOP/s (INT8)", "peak": i8_peak,
                          "frac": achieved / i8_peak if i8_peak else None, "traffic": None,
                          "kernel": "k_park_tc (INT8 tcgen05 products of byte planes, %d x %d planes)" % (nb, nb),
@@ -1303,13 +1320,14 @@ def bench_park_gpu(args, world, rank, local):
             "plain_gpu": {"backend": "cuda_cores (k_park_mm, 192-bit exact sums)", "ms": cuda_core_ms,
                           "value": 1000.0 / cuda_core_ms, "unit": "products/s", "words_equal": backends_equal},
             "e2e": {"value": 1.0 / e2e_s, "unit": "products/s", "h2d_bytes_per_step": 2 * n * n * 8,
-                    "d2h_bytes_per_step": n * n * 8, "path": "ckks_park_mod_pp_mm_host"},
+                    "d2h_bytes_per_step": n * n * 8, "result_equal": e2e_equal,
+                    "path": "pinned host operands -> park_mod_pp_mm (tensor cores) -> pinned host result"},
             "parity": {"words_compared": len(rows) * n, "mismatches": mism,
                        "what": "three full output rows against the oracle's Reference backend"},
             "gpu_launches": 3 * args.steps, "clocks": clk}
 
 
-def park_cpu_sample(threads):
+def park_cpu_sample(threads, n=PARK_N):
     """The oracle's Reference backend (u128 accumulator reduced every term) on an
     n = 512 product, one row block per thread; scaled to n = 4096 by n^3."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
@@ -1325,8 +1343,8 @@ def park_cpu_sample(threads):
     with cf.ThreadPoolExecutor(threads) as ex:
         list(ex.map(lambda r: o.park_mod_pp_mm(np.ascontiguousarray(a[r]), b, PARK_Q), blocks))
     dt = time.perf_counter() - t
-    scale = (m / PARK_N) ** 3
-    return scale / dt, "one 512 x 512 product over %d threads in %.2f s, scaled by (512/4096)^3" % (threads, dt)
+    scale = (m / n) ** 3
+    return scale / dt, "one 512 x 512 product over %d threads in %.2f s, scaled by (512/%d)^3" % (threads, dt, n)
 
 
 def main():
@@ -1343,6 +1361,8 @@ def main():
     ap.add_argument("--rot-keys", type=int, default=32)
     ap.add_argument("--rot-base-log", type=int, default=32)
     ap.add_argument("--rot-log-n", type=int, default=16)
+    # Park product size (default: the characterization's largest, n = 4096)
+    ap.add_argument("--park-n", type=int, default=PARK_N)
     ap.add_argument("--no-ccmm", action="store_true",
                     help="rotation workload: leave out the 64x64 CCMM measured beside it")
     args = ap.parse_args()
@@ -1380,7 +1400,7 @@ def main():
         line = bench_park_gpu(args, world, rank, local)
         if rank == 0 and world == 1:
             threads = os.cpu_count() or 1
-            v, sample = park_cpu_sample(threads)
+            v, sample = park_cpu_sample(threads, args.park_n)
             line["cpu_baseline"] = {"value": v, "unit": "products/s", "cores": threads, "kind": "port",
                                     "sample": sample}
         if rank == 0:
