@@ -114,7 +114,12 @@ using namespace tcg;
 
 constexpr int kEpiWarps = 4, kProdWarp = 4, kMmaWarp = 5, kThreads = 32 * 6;
 constexpr int kEpi = 32 * kEpiWarps, kBarEpi = 1;
-constexpr int kSteps = 4, kStages = 4;  // inner steps of 32 bytes per stage (one wait per 4 MMAs)
+#ifndef CKKS_PARK_STEPS
+#define CKKS_PARK_STEPS 4
+#endif
+// inner steps of 32 bytes per stage (one barrier wait per kSteps MMAs), stages in 192 KB
+constexpr int kSteps = CKKS_PARK_STEPS, kStages = 16 / kSteps;
+static_assert(kSteps == 1 || kSteps == 2 || kSteps == 4 || kSteps == 8, "inner steps per stage");
 constexpr u32 kATile = 128 * 32;        // A step: 128 rows x 32 bytes
 constexpr u32 kOffB = kSteps * kATile;  // B steps after the stage's A steps (up to 256 rows x 32 bytes each)
 constexpr u32 kStageBytes = kOffB + kSteps * 256 * 32;
@@ -128,6 +133,13 @@ constexpr int cols_per_tile(int nb) {
 }
 // inner 32-blocks per launch: every P_j stays below 2^31
 constexpr int blocks_per_launch(int nb) { return (int)(0x7FFFFFFFull / (65025ull * (u64)nb) / 32); }
+
+// tile order: row tiles vary fastest (CTAs that run together share column tiles of B'')
+#ifndef CKKS_PARK_COLS_FIRST
+#define CKKS_PARK_COLS_FIRST 0
+#endif
+__device__ __forceinline__ int tile_row(int t, int n_mt, int n_nt) { return CKKS_PARK_COLS_FIRST ? t / n_nt : t % n_mt; }
+__device__ __forceinline__ int tile_col(int t, int n_mt, int n_nt) { return CKKS_PARK_COLS_FIRST ? t % n_nt : t / n_mt; }
 
 __device__ __forceinline__ u32 core_off(int row, int half) { return (u32)((row >> 3) * 256 + half * 128 + (row & 7) * 16); }
 
@@ -242,7 +254,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             bool bad = false;
             for (int lt = 0; lt < my_tiles && !bad; ++lt) {
                 const int t = (int)blockIdx.x + lt * (int)gridDim.x;
-                const int mt = t % n_mt, nt = t / n_mt;
+                const int mt = tile_row(t, n_mt, n_nt), nt = tile_col(t, n_mt, n_nt);
                 const uint8_t* a = Ap + ((size_t)mt * n_kb + kb0) * NB * kATile;
                 const uint8_t* b = Bp + ((size_t)nt * n_kb + kb0) * NB * kBStep;
                 for (int s = 0; s < steps; s += kSteps, ++g) {
@@ -309,7 +321,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int lt = 0; lt < my_tiles; ++lt) {
             const int buf = lt & 1;
             const int t = (int)blockIdx.x + lt * (int)gridDim.x;
-            const int mt = t % n_mt, nt = t / n_mt;
+            const int mt = tile_row(t, n_mt, n_nt), nt = tile_col(t, n_mt, n_nt);
             const bool bad = !wait_parity(smem_u32(&s_tfull[buf]), (u32)((lt >> 1) & 1));
             if (group_any(kBarEpi, kEpi, bad || s_abort)) {
                 if (tid == 0) {
