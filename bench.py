@@ -1,6 +1,6 @@
 """Throughput benchmark of the B200 RNS-CKKS hot path.
 
-python bench.py [--gpus N] [--steps K] [--warmup W] [--workload rotation|ntt|multiply|ccmm|fft2] [--impl reference]
+python bench.py [--gpus N] [--steps K] [--warmup W] [--workload rotation|ntt|multiply|ccmm|fft2|park] [--park-n n] [--impl reference]
 
 Workload "rotation" (default): hoisted key-switched Galois rotations at
 N=2^16 over 24 Q limbs of 50-bit primes and 3 auxiliary 60-bit primes (the
@@ -18,6 +18,9 @@ rotations per second. The line also carries, measured in the same run:
               (the "ccmm" workload below; 3 timed after 3 warm-up products)
               with its own roofline, e2e, parity and CPU baseline
               (--no-ccmm leaves it out);
+  park        Park Mod-PP-MM at n = 4096 (the "park" workload below; 5 timed
+              after 3 warm-up products) with its own roofline, e2e, parity,
+              CUDA-core form and CPU baseline (--no-park leaves it out);
   plain_gpu   the plain GPU forms of the same rotations.
 
 Workload "ntt": batched forward + inverse negacyclic NTT at N=2^16 over 32
@@ -1022,6 +1025,23 @@ def ccmm_object(args, world, rank, local):
     return {k: line[k] for k in keep if k in line}
 
 
+def park_object(args, world, rank, local):
+    """Park Mod-PP-MM at n = 4096 measured beside the headline rotations (same
+    run): 5 timed products after 3 warm-up ones, with its own roofline, e2e,
+    parity, the CUDA-core form and, at N=1, the CPU baseline."""
+    import copy
+    a = copy.copy(args)
+    a.steps, a.warmup = 5, 3
+    line = bench_park_gpu(a, world, rank, local)
+    if rank == 0 and world == 1:
+        threads = os.cpu_count() or 1
+        v, sample = park_cpu_sample(threads, a.park_n)
+        line["cpu_baseline"] = {"value": v, "unit": "products/s", "cores": threads, "kind": "port", "sample": sample}
+    keep = ["metric", "value", "unit", "steps", "warmup", "ms_per_step", "higher_is_better", "config", "roofline",
+            "plain_gpu", "e2e", "gpu_launches", "clocks", "parity", "cpu_baseline"]
+    return {k: line[k] for k in keep if k in line}
+
+
 def ccmm_cpu_sample(threads):
     """Times the oracle's restatement of one output entry of the reference
     CCMM (64 tensors summed, bounded relinearization, rescale) per thread at
@@ -1365,6 +1385,8 @@ def main():
     ap.add_argument("--park-n", type=int, default=PARK_N)
     ap.add_argument("--no-ccmm", action="store_true",
                     help="rotation workload: leave out the 64x64 CCMM measured beside it")
+    ap.add_argument("--no-park", action="store_true",
+                    help="rotation workload: leave out the Park Mod-PP-MM measured beside it")
     args = ap.parse_args()
     if args.gpus < 1:
         ap.error("--gpus must be at least 1")
@@ -1447,6 +1469,13 @@ def main():
             torch.cuda.synchronize()
             torch.cuda.empty_cache()
             line["ccmm"] = ccmm_object(args, world, rank, local)
+        if not args.no_park:
+            import gc
+            import torch
+            gc.collect()
+            torch.cuda.synchronize()
+            torch.cuda.empty_cache()
+            line["park"] = park_object(args, world, rank, local)
         if rank == 0:
             print(json.dumps(line), flush=True)
         if world > 1:
