@@ -45,7 +45,11 @@ constexpr int kCB = 16;                   // columns per block (N = 2 x 16 x 8 =
 constexpr int kKT = CKKS_CCMM_TC_KT;      // inner indices per item (kKT / 4 MMAs of K = 32 bytes)
 constexpr int kSubK = kKT / 4;
 static_assert(kKT == 4 || kKT == 8 || kKT == 16, "inner indices per item");
-constexpr int kRing = kKT == 16 ? 4 : 8, kBStages = 2, kAhead = kRing - kBStages;
+#ifndef CKKS_CCMM_TC_BSTAGES
+#define CKKS_CCMM_TC_BSTAGES 2
+#endif
+constexpr int kRing = kKT == 16 ? 4 : 8, kBStages = CKKS_CCMM_TC_BSTAGES, kAhead = kRing - kBStages;
+static_assert((kBStages & (kBStages - 1)) == 0 && kAhead >= 2, "B stages: a power of two below the raw ring");
 constexpr u32 kRingSlot = 1024 * kSubK;   // raw entries of one item: 128 producers x kSubK x 8 bytes
 // A: 128 rows x 512 K bytes; core matrices 8 rows x 16 B, K chunks 128 B apart, row groups 4 KB
 constexpr u32 kLboA = 128, kSboA = 4096, kABytes = 65536;
