@@ -128,6 +128,19 @@ class Fft2Plan:
         self.stages.append(("cross", lvl, [key], pt, tl))
         self.out_level = lvl - 1
         self.keys_bytes = None
+        self._cross = {}  # images -> (terms, diagonals) of the cross stage over every image at once
+
+    def _cross_batch(self, n_img):
+        """The cross stage's terms and diagonals for n_img images in one call:
+        image i's terms act on ciphertexts 2 i, 2 i + 1 with the same diagonals,
+        so one hoisted rotation group covers every image (one key-switch MAC
+        instead of one per image; the same words)."""
+        import torch
+        if n_img not in self._cross:
+            _, _, _, pt, tl = self.stages[-1]
+            terms = [(a + 2 * i, b + 2 * i, key) for i in range(n_img) for (a, b, key) in tl]
+            self._cross[n_img] = (terms, torch.cat([pt] * n_img) if n_img > 1 else pt)
+        return self._cross[n_img]
 
     def apply(self, cts, stream=None):
         """cts [n_images][2][2][level][N] -> [n_images][2][2][out_level][N]."""
@@ -138,9 +151,6 @@ class Fft2Plan:
             if st[0] == "single":
                 cur = fft_stage(self.ctx, st[2], st[3], cur, identity=True, stream=stream)
             else:
-                outs = []
-                for i in range(n_img):
-                    outs.append(fft_stage_multi(self.ctx, st[2], st[4], st[3], cur[2 * i:2 * i + 2], 2,
-                                                stream=stream))
-                cur = torch.cat(outs)
+                terms, diags = self._cross_batch(n_img)
+                cur = fft_stage_multi(self.ctx, st[2], terms, diags, cur, 2 * n_img, stream=stream)
         return cur.reshape((n_img, 2) + tuple(cur.shape[1:]))

@@ -188,3 +188,24 @@ def test_fft2_image_decodes_to_dft2(oracle, cuda):
     want = np.fft.fft2(img)
     err = np.linalg.norm(spec - want) / np.linalg.norm(want)
     assert err < 1e-6, err
+
+
+def test_fft2_several_images_in_one_call_match_one_by_one(oracle, cuda):
+    """Three images through one apply (the cross stage rotates all six
+    ciphertexts in one hoisted group) give the same words as three
+    single-image applies."""
+    import torch
+    from ckks_b200 import fft2
+    log_n, n, S = 12, 1 << 12, 64
+    q = [int(x) for x in oracle.primes_below_bits(50, n, 8)]
+    p = [int(x) for x in oracle.primes_below_bits(60, n, 2)]
+    ctx = cb.Context(log_n, q, p)
+    rng = np.random.default_rng(16)
+    s = rng.integers(-1, 2, n).astype(np.int8)
+    plan = fft2.Fft2Plan(ctx, S, len(q), s, base_log=20)
+    cts = np.stack([np.stack([np.stack([rng.integers(0, m, (2, n), dtype=np.uint64) for m in q], axis=1)
+                              for _ in range(2)]) for _ in range(3)])
+    together = host(plan.apply(dev(cts)))
+    torch.cuda.synchronize()
+    for i in range(3):
+        assert np.array_equal(together[i], host(plan.apply(dev(cts[i:i + 1]))[0])), i
