@@ -277,7 +277,11 @@ int32_t ckks_park_mod_pp_mm(const uint64_t* lhs, const uint64_t* rhs, uint64_t* 
  * stream drained) and otherwise the CUDA cores (exact 192-bit sums, stream-
  * ordered). Both return the same words. A backend that cannot run returns
  * CKKS_ERR_BAD_ARG; a tensor-core pipeline wait that timed out returns
- * CKKS_ERR_TIMEOUT. */
+ * CKKS_ERR_TIMEOUT. The tensor cores take stream-ordered workspace for the
+ * packed operands, about nb * rows * inner + nb^2 * inner * cols bytes (nb =
+ * bytes of modulus - 1, rows, inner and cols rounded up to their tiles); when
+ * it does not fit the call returns CKKS_ERR_OOM and leaves the choice of the
+ * CUDA-core backend to the caller. */
 enum { CKKS_PARK_AUTO = 0, CKKS_PARK_TENSOR_CORES = 1, CKKS_PARK_CUDA_CORES = 2 };
 int32_t ckks_park_mod_pp_mm_with_backend(const uint64_t* lhs, const uint64_t* rhs, uint64_t* out, uint32_t rows,
                                          uint32_t inner, uint32_t cols, uint64_t modulus, int32_t backend,
