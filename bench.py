@@ -396,6 +396,23 @@ def reference_arm(args, world, rank):
         }
     if args.workload == "rotation":
         return reference_rotation(args, world)
+    if args.workload == "park":
+        threads = os.cpu_count() or 1
+        vals, sample = [], None
+        for i in range(args.warmup + args.steps):
+            v, sample = park_cpu_sample(threads, args.park_n)
+            if i >= args.warmup:
+                vals.append(v)
+        value = float(np.median(vals))
+        return {
+            "metric": park_metric(args.park_n), "value": value, "unit": "products/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded uniform residues)",
+            "config": park_config(args.park_n), "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "products/s", "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "products/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
     threads = os.cpu_count() or 1
     per_step = []
     sample = None
@@ -461,6 +478,13 @@ def reference_rotation(args, world):
         ccmm = {"metric": "64x64 structured CCMM/s (N=2^15, 14 limbs, both operands encrypted, bit-exact)",
                 "value": cv, "unit": "CCMM/s", "higher_is_better": True, "config": ccmm_config(),
                 "cpu_baseline": {"value": cv, "unit": "CCMM/s", "cores": threads, "kind": "port", "sample": csample}}
+    park = None
+    if not args.no_park:
+        pv, psample = park_cpu_sample(threads, args.park_n)
+        park = {"metric": park_metric(args.park_n), "value": pv, "unit": "products/s", "higher_is_better": True,
+                "config": park_config(args.park_n),
+                "cpu_baseline": {"value": pv, "unit": "products/s", "cores": threads, "kind": "port",
+                                 "sample": psample}}
     return {
         "metric": "key-switched rotations/s (N=2^16, 24 limbs, hoisted, bit-exact)", "value": value,
         "unit": "rotations/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -476,6 +500,7 @@ def reference_rotation(args, world):
         "cpu_1thread": {"value": v_1t, "unit": "rotations/s", "cores": 1, "sample": sample_1t},
         "e2e": {"value": value, "unit": "rotations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "ccmm": ccmm,
+        "park": park,
     }
 
 
@@ -1324,13 +1349,11 @@ def bench_park_gpu(args, world, rank, local):
     bf16, bf16_kind = bf16_peak()
     i8_peak = 2.0 * bf16 if bf16 else None
     achieved = ops / (gemm / 1000.0) / 1e12
-    return {"metric": "Park Mod-PP-MM/s (n=%d square, modulus 0x7ffff6001, bit-exact)" % n, "value": value,
+    return {"metric": park_metric(n), "value": value,
             "unit": "products/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded uniform residues)",
-            "config": {"workload": "Park Mod-PP-MM, %d x %d by %d x %d, u64 residues mod 0x7ffff6001" % (n, n, n, n),
-                       "n": n, "modulus": q, "l2": "operands %d MB each%s" % (
-                           n * n * 8 // 10**6, ", above L2" if n * n * 8 > 126 * 10**6 else "")},
+            "config": park_config(n),
             "roofline": {"bound": "tensor", "achieved": achieved, "unit": "TOP/s (INT8)", "peak": i8_peak,
                          "frac": achieved / i8_peak if i8_peak else None, "traffic": None,
                          "kernel": "k_park_tc (INT8 tcgen05 products of byte planes, %d x %d planes)" % (nb, nb),
@@ -1345,6 +1368,16 @@ def bench_park_gpu(args, world, rank, local):
             "parity": {"words_compared": len(rows) * n, "mismatches": mism,
                        "what": "three full output rows against the oracle's Reference backend"},
             "gpu_launches": 3 * args.steps, "clocks": clk}
+
+
+def park_metric(n):
+    return "Park Mod-PP-MM/s (n=%d square, modulus 0x7ffff6001, bit-exact)" % n
+
+
+def park_config(n):
+    return {"workload": "Park Mod-PP-MM, %d x %d by %d x %d, u64 residues mod 0x7ffff6001" % (n, n, n, n),
+            "n": n, "modulus": PARK_Q, "l2": "operands %d MB each%s" % (
+                n * n * 8 // 10**6, ", above L2" if n * n * 8 > 126 * 10**6 else "")}
 
 
 def park_cpu_sample(threads, n=PARK_N):
