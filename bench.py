@@ -1355,7 +1355,11 @@ def bench_park_gpu(args, world, rank, local):
             "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded uniform residues)",
             "config": park_config(n),
             "roofline": {"bound": "tensor", "achieved": achieved, "unit": "TOP/s (INT8)", "peak": i8_peak,
-                         "frac": achieved / i8_peak if i8_peak else None, "traffic": None,
+                         "frac": achieved / i8_peak if i8_peak else None,
+                         # DRAM bytes of one launch at n = 2048 (read 127.0 MB, write 23.4 MB: the
+                         # packed operands once and the product), scaled by n^2 like those arrays
+                         "traffic": (127.0e6 + 23.4e6) * (n / 2048.0) ** 2,
+                         "traffic_source": "ncu capture of the n=2048 launch, scaled by (n/2048)^2",
                          "kernel": "k_park_tc (INT8 tcgen05 products of byte planes, %d x %d planes)" % (nb, nb),
                          "kernel_ms": gemm, "rest_of_step_ms": (ms_max / args.steps) - gemm,
                          "peak_source": "2 x bf16 dense (%s %s)" % (bf16_kind, bf16),
